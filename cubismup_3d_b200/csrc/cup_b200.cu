@@ -1,0 +1,1403 @@
+// C-ABI implementation of the B200-native periodic fractional-step solver.
+// Host orchestration: handle, device buffers, tensor maps, kernel launches
+// and the operator pipeline of Simulation::timestep (source/Simulation.cpp:593-623).
+
+#include "../../include/cup_b200.h"
+
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "common.cuh"
+#include "dht.cuh"
+#include "ops.cuh"
+#include "stencil.cuh"
+
+using namespace cup;
+
+namespace {
+
+// Device-resident step state: the CFL dt chain, reductions and counters.
+struct DevState {
+  double dt, lambda, umax, ke;
+  double corr, rhs_sums[3];
+  double force[3], torque[3];
+  double com[3], mass;
+  double time;
+  double res2, b2;
+  int step, n_solves, converged, pad_;
+};
+
+enum PartialRegion { P_GRAD = 0, P_PEN, P_RHSOB, P_CHI, P_MAX, P_RES, P_DIAG, P_COUNT };
+constexpr int kPartialCap = 16384;  // doubles per region
+
+constexpr int kBoxThreads = 256;
+constexpr int kBoxBlocksMax = 296;
+
+// ---------------------------------------------------------------------------
+// small device kernels
+
+template <typename T>
+__global__ void k_convert_from_f64(T* dst, const double* src, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (T)src[i];
+}
+template <typename T>
+__global__ void k_convert_to_f64(double* dst, const T* src, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+
+// findMaxU (source/operators/ProcessHelpers.h:74-99): per-CTA partial maxima.
+template <typename T>
+__global__ void k_max_u(const T* u, const T* v, const T* w, size_t n, double ux, double uy, double uz,
+                        double* partials) {
+  __shared__ double scratch[32];
+  double m[1] = {0.0};
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double a = fabs((double)u[i] + ux), b = fabs((double)v[i] + uy), c = fabs((double)w[i] + uz);
+    m[0] = fmax(m[0], fmax(fmax(a, b), c));
+  }
+  block_reduce<1, true>(m, scratch);
+  if (threadIdx.x == 0) partials[blockIdx.x] = m[0];
+}
+
+__global__ void k_finalize_max(const double* partials, int np, DevState* st) {
+  __shared__ double scratch[32];
+  double m[1] = {0.0};
+  for (int i = threadIdx.x; i < np; i += blockDim.x) m[0] = fmax(m[0], partials[i]);
+  block_reduce<1, true>(m, scratch);
+  if (threadIdx.x == 0) st->umax = m[0];
+}
+
+// Simulation::calcMaxTimestep (source/Simulation.cpp:403-424) on the device.
+__global__ void k_calc_dt(DevState* st, double h, double nu, double CFL, int rampup, double DLM) {
+  const double hMin = h;
+  const double dtDif = hMin * hMin / nu;
+  const double dtAdv = hMin / (st->umax + 1e-8);
+  double dt = CFL * fmin(dtDif, dtAdv);
+  if (st->step < rampup) {
+    const double x = (st->step + 1.0) / rampup;
+    const double rampCFL = exp(log(1e-3) * (1 - x) + log(CFL) * x);
+    dt = rampCFL * fmin(dtDif, dtAdv);
+  }
+  st->dt = dt;
+  if (DLM > 0) st->lambda = DLM / dt;
+}
+
+__global__ void k_set_dt(DevState* st, double dt, double DLM) {
+  st->dt = dt;
+  if (DLM > 0) st->lambda = DLM / dt;
+}
+
+// End of step: umax (grid part outside the obstacle box, box part after
+// penalization), kinetic energy, force/torque; advances step and time.
+__global__ void k_finalize_step(const double* pgrad, int ngrad, const double* ppen, int npen, DevState* st,
+                                double h3, int advance) {
+  __shared__ double scratch[8 * 32];
+  double mx[1] = {0.0};
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int i = threadIdx.x; i < ngrad; i += blockDim.x) {
+    mx[0] = fmax(mx[0], pgrad[2 * i]);
+    s[6] += pgrad[2 * i + 1];
+  }
+  for (int i = threadIdx.x; i < npen; i += blockDim.x) {
+    for (int k = 0; k < 6; ++k) s[k] += ppen[8 * i + k];
+    mx[0] = fmax(mx[0], ppen[8 * i + 6]);
+  }
+  block_reduce<7, false>(s, scratch);
+  block_reduce<1, true>(mx, scratch + 7 * 32);
+  if (threadIdx.x == 0) {
+    st->umax = mx[0];
+    st->ke = s[6] * h3;
+    if (npen > 0) {
+      for (int k = 0; k < 3; ++k) {
+        st->force[k] = s[k];
+        st->torque[k] = s[3 + k];
+      }
+    }
+    if (advance) {
+      st->step += 1;
+      st->time += st->dt;
+    }
+  }
+}
+
+// Penalization-only finalize (operator-by-operator path).
+__global__ void k_finalize_pen(const double* ppen, int npen, DevState* st) {
+  __shared__ double scratch[6 * 32];
+  double s[6] = {0, 0, 0, 0, 0, 0};
+  for (int i = threadIdx.x; i < npen; i += blockDim.x)
+    for (int k = 0; k < 6; ++k) s[k] += ppen[8 * i + k];
+  block_reduce<6, false>(s, scratch);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) {
+      st->force[k] = s[k];
+      st->torque[k] = s[3 + k];
+    }
+}
+
+// PressureRHS correction factor (source/operators/PressureRHS.cpp:328-334).
+__global__ void k_finalize_rhs_obstacle(const double* p, int np, DevState* st) {
+  __shared__ double scratch[3 * 32];
+  double s[3] = {0, 0, 0};
+  for (int i = threadIdx.x; i < np; i += blockDim.x)
+    for (int k = 0; k < 3; ++k) s[k] += p[3 * i + k];
+  block_reduce<3, false>(s, scratch);
+  if (threadIdx.x == 0) {
+    const double EPS = 2.220446049250313080847e-16;
+    const double sumRHS = s[0], posRHS = s[1], negRHS = s[2];
+    const double corrDenom = sumRHS > 0 ? posRHS : negRHS;
+    st->corr = sumRHS / fmax(corrDenom, EPS);
+    st->rhs_sums[0] = sumRHS;
+    st->rhs_sums[1] = posRHS;
+    st->rhs_sums[2] = negRHS;
+  }
+}
+
+// Grid centre of mass (source/operators/ObstaclesCreate.cpp:230-256) -> SphereParams.
+__global__ void k_finalize_com(const double* p, int np, DevState* st, SphereParams* sp) {
+  __shared__ double scratch[4 * 32];
+  double s[4] = {0, 0, 0, 0};
+  for (int i = threadIdx.x; i < np; i += blockDim.x)
+    for (int k = 0; k < 4; ++k) s[k] += p[4 * i + k];
+  block_reduce<4, false>(s, scratch);
+  if (threadIdx.x == 0) {
+    st->mass = s[0];
+    for (int k = 0; k < 3; ++k) {
+      st->com[k] = s[1 + k] / s[0];
+      sp->centerOfMass[k] = st->com[k];
+    }
+  }
+}
+
+// Diagnostics: kinetic energy and central-divergence norms (FP64).
+template <typename T>
+__global__ void k_diag(const T* u, const T* v, const T* w, int nx, int ny, int nz, double inv2h, double* partials) {
+  __shared__ double scratch[3 * 32];
+  double s[2] = {0, 0};
+  double m[1] = {0};
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+    const double uu = u[i], vv = v[i], ww = w[i];
+    s[0] += 0.5 * (uu * uu + vv * vv + ww * ww);
+    const double div =
+        inv2h * ((double)u[gidx(wrapi(x + 1, nx), y, z, nx, ny)] - (double)u[gidx(wrapi(x - 1, nx), y, z, nx, ny)] +
+                 (double)v[gidx(x, wrapi(y + 1, ny), z, nx, ny)] - (double)v[gidx(x, wrapi(y - 1, ny), z, nx, ny)] +
+                 (double)w[gidx(x, y, wrapi(z + 1, nz), nx, ny)] - (double)w[gidx(x, y, wrapi(z - 1, nz), nx, ny)]);
+    s[1] += div * div;
+    m[0] = fmax(m[0], fabs(div));
+  }
+  block_reduce<2, false>(s, scratch);
+  block_reduce<1, true>(m, scratch + 2 * 32);
+  if (threadIdx.x == 0) {
+    partials[3 * blockIdx.x + 0] = s[0];
+    partials[3 * blockIdx.x + 1] = s[1];
+    partials[3 * blockIdx.x + 2] = m[0];
+  }
+}
+
+// Periodic shift through the plane-streaming path (TestBoundaries restatement).
+struct OpShift {
+  double* out;
+  int dx, dy, dz;
+  int nx, ny;
+  template <class C>
+  __device__ __forceinline__ void cell(const C& c, int x, int y, int gy, int gz, double*) const {
+    out[gidx(x, gy, gz, nx, ny)] = c.v(0, x, y, -dx, -dy, -dz);
+  }
+  __device__ void finish(double*, double*) const {}
+};
+
+// ---------------------------------------------------------------------------
+// host helpers
+
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::mutex g_encode_mu;
+
+bool get_encode() {
+  std::lock_guard<std::mutex> lk(g_encode_mu);
+  if (g_encode) return true;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn)
+    return false;
+  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  return true;
+}
+
+template <typename T>
+CUtensorMapDataType tma_dtype();
+template <>
+CUtensorMapDataType tma_dtype<double>() {
+  return CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+}
+template <>
+CUtensorMapDataType tma_dtype<float>() {
+  return CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+}
+
+int ilog2(int n) {
+  int l = 0;
+  while ((1 << l) < n) ++l;
+  return l;
+}
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+template <int M>
+void build_table_M(std::vector<double2>& t64, std::vector<float2>& t32) {
+  using Pl = FFTPlan<M>;
+  const int L = Pl::table_len();
+  t64.assign(L, double2{0, 0});
+  t32.assign(L, float2{0, 0});
+  const long double PI = 3.141592653589793238462643383279502884L;
+  auto put = [&](int i, long double ang) {
+    t64[i] = double2{(double)cosl(ang), (double)sinl(ang)};
+    t32[i] = float2{(float)cosl(ang), (float)sinl(ang)};
+  };
+  for (int s = 1; s < Pl::nstages; ++s) {
+    const int R = Pl::radix(s), Ns = Pl::ns(s), off = Pl::tw_off(s);
+    for (int r = 0; r < R; ++r)
+      for (int j = 0; j < Ns; ++j) put(off + r * Ns + j, -2.0L * PI * r * j / ((long double)Ns * R));
+  }
+  for (int k = 0; k <= M / 2; ++k) put(Pl::post_off() + k, -2.0L * PI * k / (2.0L * M));
+}
+
+void build_table(int N, std::vector<double2>& t64, std::vector<float2>& t32) {
+  switch (N / 2) {
+    case 8: build_table_M<8>(t64, t32); break;
+    case 16: build_table_M<16>(t64, t32); break;
+    case 32: build_table_M<32>(t64, t32); break;
+    case 64: build_table_M<64>(t64, t32); break;
+    case 128: build_table_M<128>(t64, t32); break;
+    case 256: build_table_M<256>(t64, t32); break;
+    default: break;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct cup_handle {
+  cup_config cfg;
+  int nx = 0, ny = 0, nz = 0;
+  size_t n = 0;
+  double h = 0;
+  int dev = 0, num_sms = 148;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+  bool fp32 = false;
+  // fields (T = double or float by precision)
+  void *u = nullptr, *v = nullptr, *w = nullptr;
+  void *tu = nullptr, *tv = nullptr, *tw = nullptr;
+  void *u1 = nullptr, *v1 = nullptr, *w1 = nullptr;
+  void* chi = nullptr;
+  double* p = nullptr;    // pressure (FP64)
+  double* rhs = nullptr;  // pressure RHS (FP64); FP64 mode: also the FFT work array
+  float* work32 = nullptr;  // FP32_DC FFT work array
+  double* partials = nullptr;
+  DevState* dstate = nullptr;
+  int* derr = nullptr;
+  // FFT tables (per axis) and spectral cos tables
+  double2* tw64[3] = {nullptr, nullptr, nullptr};
+  float2* tw32[3] = {nullptr, nullptr, nullptr};
+  double *cosx = nullptr, *cosy = nullptr, *cosz = nullptr;
+  double norm_factor = 0;
+  // obstacle
+  bool has_sphere = false;
+  cup_sphere sphere{};
+  SphereParams* sp_dev = nullptr;
+  Box box{};
+  // host mirrors
+  int step = 0;
+  double time = 0, dt = 0, lambda = 0;
+  double uinf[3] = {0, 0, 0};
+  bool umax_fresh = false;
+  int n_grad_partials = 0, n_pen_partials = 0;
+  DevState* hstate = nullptr;  // pinned host copy
+  // per-step solve stats
+  int last_n_solves = 0;
+  // launch accounting and optional per-kernel CUDA-event profiling
+  long long launches = 0;
+  bool prof_on = false;
+  struct Pending {
+    const char* name;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> ev_pool;
+  std::map<std::string, std::pair<long long, double>> prof;  // name -> (count, ms)
+};
+
+namespace {
+
+int fail(cup_handle* H, int code, const char* fmt, ...) {
+  if (H) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    H->err = buf;
+  }
+  return code;
+}
+
+#define CK(call)                                                                                      \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess) return fail(H, CUP_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define CKL()                                                                                          \
+  do {                                                                                                 \
+    cudaError_t e_ = cudaGetLastError();                                                               \
+    if (e_ != cudaSuccess) return fail(H, CUP_ERR_CUDA, "kernel launch failed: %s", cudaGetErrorString(e_)); \
+  } while (0)
+
+double* partial(cup_handle* H, int region) { return H->partials + (size_t)region * kPartialCap; }
+
+cudaEvent_t ev_get(cup_handle* H) {
+  if (!H->ev_pool.empty()) {
+    cudaEvent_t e = H->ev_pool.back();
+    H->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Resolves recorded event pairs into the per-kernel totals (synchronises).
+void prof_flush(cup_handle* H) {
+  if (H->pending.empty()) return;
+  cudaStreamSynchronize(H->stream);
+  for (auto& p : H->pending) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, p.a, p.b);
+    auto& e = H->prof[p.name];
+    e.first += 1;
+    e.second += ms;
+    H->ev_pool.push_back(p.a);
+    H->ev_pool.push_back(p.b);
+  }
+  H->pending.clear();
+}
+
+// Counts one kernel launch and, when profiling is on, brackets it with events.
+template <class F>
+int launch_named(cup_handle* H, const char* name, F&& f) {
+  H->launches += 1;
+  cudaEvent_t a = nullptr;
+  if (H->prof_on) {
+    a = ev_get(H);
+    cudaEventRecord(a, H->stream);
+  }
+  const int rc = f();
+  if (H->prof_on) {
+    cudaEvent_t b = ev_get(H);
+    cudaEventRecord(b, H->stream);
+    H->pending.push_back({name, a, b});
+    if (H->pending.size() > 4096) prof_flush(H);
+  }
+  return rc;
+}
+
+int make_map(cup_handle* H, CUtensorMap* m, const void* base, CUtensorMapDataType dt, size_t elem, int bx, int by,
+             int bz) {
+  if (!get_encode()) return fail(H, CUP_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
+  cuuint64_t dims[3] = {(cuuint64_t)H->nx, (cuuint64_t)H->ny, (cuuint64_t)H->nz};
+  cuuint64_t strides[2] = {(cuuint64_t)H->nx * elem, (cuuint64_t)H->nx * H->ny * elem};
+  cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = g_encode(m, dt, 3, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(H, CUP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return CUP_OK;
+}
+
+template <class K>
+int prepare_kernel(cup_handle* H, K kern, size_t smem, int threads, int* blocks_per_sm) {
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, kern, threads, smem));
+  if (*blocks_per_sm < 1) return fail(H, CUP_ERR_ARG, "kernel does not fit on an SM (smem %zu)", smem);
+  return CUP_OK;
+}
+
+// Launches k_stencil_stream over `fields` (device arrays of T). Returns the
+// grid size through *grid_out (the number of per-CTA partials written).
+template <typename T, int NF, int G, int TY, int NS, class Op>
+int launch_stream(cup_handle* H, const char* name, const void* const* fields, const Op& op, int* grid_out = nullptr) {
+  FieldMaps<NF> maps;
+  for (int f = 0; f < NF; ++f) {
+    int rc = make_map(H, &maps.main[f], fields[f], tma_dtype<T>(), sizeof(T), H->nx, TY, 1);
+    if (rc) return rc;
+    rc = make_map(H, &maps.halo[f], fields[f], tma_dtype<T>(), sizeof(T), H->nx, G, 1);
+    if (rc) return rc;
+  }
+  const int zc = std::min(16, H->nz);
+  StreamGeom g{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
+  const size_t smem = stream_smem_bytes<T, NF, G, TY, NS>(H->nx) + 128;
+  auto kern = k_stencil_stream<T, NF, G, TY, NS, Op>;
+  int bpsm = 0;
+  int rc = prepare_kernel(H, kern, smem, 256, &bpsm);
+  if (rc) return rc;
+  const int grid = std::min(g.n_items, bpsm * H->num_sms);
+  if (grid > kPartialCap / 8) return fail(H, CUP_ERR_ARG, "too many CTAs for the partial buffers");
+  rc = launch_named(H, name, [&]() -> int {
+    kern<<<grid, 256, smem, H->stream>>>(maps, g, op, H->derr);
+    CKL();
+    return CUP_OK;
+  });
+  if (rc) return rc;
+  if (grid_out) *grid_out = grid;
+  return CUP_OK;
+}
+
+template <typename R>
+const typename Cplx<R>::T* table(cup_handle* H, int axis);
+template <>
+const double2* table<double>(cup_handle* H, int axis) {
+  return H->tw64[axis];
+}
+template <>
+const float2* table<float>(cup_handle* H, int axis) {
+  return H->tw32[axis];
+}
+
+template <int M, typename R>
+int launch_rows_M(cup_handle* H, const R* in, R* out) {
+  constexpr int N = 2 * M, TPL = M / 8;
+  constexpr bool PAD = FFTPlan<M>::nstages > 1;
+  const int lpc = 256 / TPL;
+  const int nrows = H->ny * H->nz;
+  const size_t smem = (size_t)lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
+                      FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + 16 + 128;
+  auto kern = k_dht_rows<M, R>;
+  int bpsm = 0;
+  int rc = prepare_kernel(H, kern, smem, lpc * TPL, &bpsm);
+  if (rc) return rc;
+  const int grid = (nrows + lpc - 1) / lpc;
+  return launch_named(H, "dht_x", [&]() -> int {
+    kern<<<grid, lpc * TPL, smem, H->stream>>>(in, out, nrows, lpc, table<R>(H, 0), H->derr);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+template <typename R>
+int launch_rows(cup_handle* H, const R* in, R* out) {
+  switch (H->nx / 2) {
+    case 8: return launch_rows_M<8, R>(H, in, out);
+    case 16: return launch_rows_M<16, R>(H, in, out);
+    case 32: return launch_rows_M<32, R>(H, in, out);
+    case 64: return launch_rows_M<64, R>(H, in, out);
+    case 128: return launch_rows_M<128, R>(H, in, out);
+    case 256: return launch_rows_M<256, R>(H, in, out);
+  }
+  return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
+}
+
+template <int M, typename R, int AXIS, bool DIVIDE>
+int launch_cols_M(cup_handle* H, R* buf) {
+  constexpr int N = 2 * M, TPL = M / 8;
+  const int W = std::min(256 / TPL, H->nx);
+  CUtensorMap map;
+  int rc = make_map(H, &map, buf, tma_dtype<R>(), sizeof(R), W, AXIS == 1 ? N : 1, AXIS == 2 ? N : 1);
+  if (rc) return rc;
+  const size_t smem = (size_t)N * W * sizeof(R) + FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + 16 + 128;
+  auto kern = k_dht_cols<M, R, AXIS, DIVIDE>;
+  int bpsm = 0;
+  rc = prepare_kernel(H, kern, smem, W * TPL, &bpsm);
+  if (rc) return rc;
+  const int ntx = H->nx / W;
+  const int grid = ntx * (AXIS == 1 ? H->nz : H->ny);
+  SpectralParams sp{H->cosx, H->cosy, H->cosz, H->norm_factor, H->nx, H->ny, H->nz};
+  return launch_named(H, AXIS == 1 ? "dht_y" : "dht_z_solve", [&]() -> int {
+    kern<<<grid, W * TPL, smem, H->stream>>>(map, map, W, ntx, table<R>(H, AXIS), sp, H->derr);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+template <typename R, int AXIS, bool DIVIDE>
+int launch_cols(cup_handle* H, R* buf) {
+  const int N = AXIS == 1 ? H->ny : H->nz;
+  switch (N / 2) {
+    case 8: return launch_cols_M<8, R, AXIS, DIVIDE>(H, buf);
+    case 16: return launch_cols_M<16, R, AXIS, DIVIDE>(H, buf);
+    case 32: return launch_cols_M<32, R, AXIS, DIVIDE>(H, buf);
+    case 64: return launch_cols_M<64, R, AXIS, DIVIDE>(H, buf);
+    case 128: return launch_cols_M<128, R, AXIS, DIVIDE>(H, buf);
+    case 256: return launch_cols_M<256, R, AXIS, DIVIDE>(H, buf);
+  }
+  return fail(H, CUP_ERR_ARG, "unsupported line length %d", N);
+}
+
+// p = H(f . H(work)) over the three axes, in place on `work`; the last x
+// pass writes to `out` (may equal work).
+template <typename R>
+int fft_poisson(cup_handle* H, R* work, R* out) {
+  int rc;
+  if ((rc = launch_rows<R>(H, work, work))) return rc;
+  if ((rc = launch_cols<R, 1, false>(H, work))) return rc;
+  if ((rc = launch_cols<R, 2, true>(H, work))) return rc;
+  if ((rc = launch_cols<R, 1, false>(H, work))) return rc;
+  if ((rc = launch_rows<R>(H, work, out))) return rc;
+  return CUP_OK;
+}
+
+int box_grid(const Box& b) {
+  const long long n = (long long)b.n[0] * b.n[1] * b.n[2];
+  return (int)std::max<long long>(1, std::min<long long>(kBoxBlocksMax, (n + kBoxThreads - 1) / kBoxThreads));
+}
+
+int check_dev_error(cup_handle* H) {
+  int e = 0;
+  CK(cudaMemcpy(&e, H->derr, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e & kDevErrMbarTimeout) return fail(H, CUP_ERR_TIMEOUT, "device wait timed out (mbarrier)");
+  if (e & kDevErrBulkTimeout) return fail(H, CUP_ERR_TIMEOUT, "device wait timed out (bulk store)");
+  return CUP_OK;
+}
+
+int read_state(cup_handle* H) {
+  CK(cudaMemcpyAsync(H->hstate, H->dstate, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+// ---- typed pipeline pieces -------------------------------------------------
+template <typename T>
+int do_advect_diffuse(cup_handle* H, DtArg dt) {
+  int rc;
+  T* u = (T*)H->u;
+  T* v = (T*)H->v;
+  T* w = (T*)H->w;
+  T* tu = (T*)H->tu;
+  T* tv = (T*)H->tv;
+  T* tw = (T*)H->tw;
+  const void* uvw[3] = {u, v, w};
+  if (H->cfg.scheme == CUP_SCHEME_REF) {
+    OpAdvectDiffuseRef<T> op{tu, tv, tw, dt, H->h, H->cfg.nu, {H->uinf[0], H->uinf[1], H->uinf[2]}, H->nx, H->ny};
+    if (H->fp32) rc = launch_stream<T, 3, 1, 8, 4>(H, "advect_diffuse_ref", uvw, op);
+    else rc = launch_stream<T, 3, 1, 4, 4>(H, "advect_diffuse_ref", uvw, op);
+  } else {
+    T* u1 = (T*)H->u1;
+    T* v1 = (T*)H->v1;
+    T* w1 = (T*)H->w1;
+    OpUpwind3Stage<T, false> s1{nullptr, nullptr, nullptr, u1, v1, w1, dt, H->h, H->cfg.nu,
+                                {H->uinf[0], H->uinf[1], H->uinf[2]}, H->nx, H->ny};
+    OpUpwind3Stage<T, true> s2{u, v, w, tu, tv, tw, dt, H->h, H->cfg.nu, {H->uinf[0], H->uinf[1], H->uinf[2]},
+                               H->nx, H->ny};
+    const void* uvw1[3] = {u1, v1, w1};
+    if (H->fp32) {
+      if ((rc = launch_stream<T, 3, 2, 4, 6>(H, "upwind3_stage1", uvw, s1))) return rc;
+      rc = launch_stream<T, 3, 2, 4, 6>(H, "upwind3_stage2", uvw1, s2);
+    } else {
+      if ((rc = launch_stream<T, 3, 2, 2, 6>(H, "upwind3_stage1", uvw, s1))) return rc;
+      rc = launch_stream<T, 3, 2, 2, 6>(H, "upwind3_stage2", uvw1, s2);
+    }
+  }
+  if (rc) return rc;
+  // UpdateAndCorrectInflow's tmp -> u copy (AdvectionDiffusion.cpp:315-328) is a pointer swap.
+  std::swap(H->u, H->tu);
+  std::swap(H->v, H->tv);
+  std::swap(H->w, H->tw);
+  return CUP_OK;
+}
+
+template <typename T>
+int do_pressure_rhs(cup_handle* H, DtArg dt) {
+  int rc;
+  const void* uvw[3] = {H->u, H->v, H->w};
+  OpPressureRHS<T> op{H->rhs, dt, H->h, H->nx, H->ny};
+  if (H->fp32) rc = launch_stream<T, 3, 1, 8, 4>(H, "pressure_rhs", uvw, op);
+  else rc = launch_stream<T, 3, 1, 4, 4>(H, "pressure_rhs", uvw, op);
+  if (rc) return rc;
+  if (H->has_sphere) {
+    const int gb = box_grid(H->box);
+    {
+      int rc_ = launch_named(H, "rhs_obstacle", [&]() -> int {
+        k_rhs_obstacle<T><<<gb, kBoxThreads, 0, H->stream>>>(H->rhs, (const T*)H->chi, H->box, H->nx, H->ny, H->nz,
+                                                         partial(H, P_RHSOB));
+        CKL();
+        return CUP_OK;
+      });
+      if (rc_) return rc_;
+    }
+    {
+      int rc_ = launch_named(H, "finalize_rhs_obstacle", [&]() -> int {
+        k_finalize_rhs_obstacle<<<1, 256, 0, H->stream>>>(partial(H, P_RHSOB), gb, H->dstate);
+        CKL();
+        return CUP_OK;
+      });
+      if (rc_) return rc_;
+    }
+    {
+      int rc_ = launch_named(H, "rhs_obstacle_correct", [&]() -> int {
+        k_rhs_obstacle_correct<T><<<gb, kBoxThreads, 0, H->stream>>>(H->rhs, (const T*)H->chi, H->box, H->nx, H->ny,
+                                                                 H->nz, &H->dstate->corr);
+        CKL();
+        return CUP_OK;
+      });
+      if (rc_) return rc_;
+    }
+  }
+  return CUP_OK;
+}
+
+int do_poisson(cup_handle* H) {
+  if (!H->fp32) return fft_poisson<double>(H, H->rhs, H->p);
+  return fail(H, CUP_ERR_ARG, "FP32 defect-correction solve not available in this build");
+}
+
+template <typename T>
+int do_grad(cup_handle* H, DtArg dt) {
+  const void* pf[1] = {H->p};
+  OpGradP<T> op{(const T*)H->u, (const T*)H->v, (const T*)H->w, (T*)H->u, (T*)H->v, (T*)H->w, partial(H, P_GRAD),
+                dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, H->box, H->has_sphere ? 1 : 0, H->nx, H->ny, H->nz};
+  // p is FP64 in both forms: the stream runs over an FP64 field.
+  return launch_stream<double, 1, 1, 4, 4>(H, "grad_p", pf, op, &H->n_grad_partials);
+}
+
+template <typename T>
+int do_penalize(cup_handle* H, DtArg dt, const double* lambda_dev) {
+  if (!H->has_sphere) {
+    H->n_pen_partials = 0;
+    return CUP_OK;
+  }
+  const int gb = box_grid(H->box);
+  {
+    int rc_ = launch_named(H, "penalize", [&]() -> int {
+      k_penalize<T><<<gb, kBoxThreads, 0, H->stream>>>((T*)H->u, (T*)H->v, (T*)H->w, (const T*)H->chi, H->sp_dev, H->box,
+                                                   H->nx, H->ny, H->nz, H->h, dt, lambda_dev, H->lambda,
+                                                   H->cfg.bImplicitPenalization, H->uinf[0], H->uinf[1], H->uinf[2],
+                                                   partial(H, P_PEN));
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  H->n_pen_partials = gb;
+  return CUP_OK;
+}
+
+template <typename T>
+int do_max_u(cup_handle* H) {
+  const int grid = std::min<size_t>(H->num_sms * 4, (H->n + 255) / 256);
+  {
+    int rc_ = launch_named(H, "max_u", [&]() -> int {
+      k_max_u<T><<<grid, 256, 0, H->stream>>>((const T*)H->u, (const T*)H->v, (const T*)H->w, H->n, H->uinf[0], H->uinf[1],
+                                          H->uinf[2], partial(H, P_MAX));
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  {
+    int rc_ = launch_named(H, "finalize_max", [&]() -> int {
+      k_finalize_max<<<1, 256, 0, H->stream>>>(partial(H, P_MAX), grid, H->dstate);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  return CUP_OK;
+}
+
+// One full step of the hot-path pipeline (Simulation::timestep with the
+// periodic pipeline of Simulation::setupOperators, source/Simulation.cpp:307-401):
+// AdvectionDiffusion -> PressureRHS -> PressureProjection -> UpdateObstacles
+// (forced sphere: no-op) -> Penalization, with grad-P and the reductions fused.
+template <typename T>
+int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance) {
+  int rc;
+  if ((rc = do_advect_diffuse<T>(H, dt))) return rc;
+  if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
+  if ((rc = do_poisson(H))) return rc;
+  if ((rc = do_grad<T>(H, dt))) return rc;
+  if ((rc = do_penalize<T>(H, dt, lambda_dev))) return rc;
+  {
+    int rc_ = launch_named(H, "finalize_step", [&]() -> int {
+      k_finalize_step<<<1, 256, 0, H->stream>>>(partial(H, P_GRAD), H->n_grad_partials, partial(H, P_PEN),
+                                            H->n_pen_partials, H->dstate, H->h * H->h * H->h, advance);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  return CUP_OK;
+}
+
+template <typename T>
+int set_field(cup_handle* H, void* dst, const double* src, int where) {
+  if (!H->fp32) {
+    CK(cudaMemcpyAsync(dst, src, H->n * sizeof(double),
+                       where == CUP_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, H->stream));
+    return CUP_OK;
+  }
+  const double* s = src;
+  if (where == CUP_WHERE_HOST) {
+    CK(cudaMemcpyAsync(H->rhs, src, H->n * sizeof(double), cudaMemcpyHostToDevice, H->stream));
+    s = H->rhs;
+  }
+  {
+    int rc_ = launch_named(H, "convert_from_f64", [&]() -> int {
+      k_convert_from_f64<T><<<H->num_sms * 4, 256, 0, H->stream>>>((T*)dst, s, H->n);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  return CUP_OK;
+}
+
+template <typename T>
+int get_field(cup_handle* H, const void* src, double* dst, int where) {
+  if (!H->fp32) {
+    CK(cudaMemcpyAsync(dst, src, H->n * sizeof(double),
+                       where == CUP_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, H->stream));
+    return CUP_OK;
+  }
+  double* d = where == CUP_WHERE_HOST ? H->rhs : dst;
+  {
+    int rc_ = launch_named(H, "convert_to_f64", [&]() -> int {
+      k_convert_to_f64<T><<<H->num_sms * 4, 256, 0, H->stream>>>(d, (const T*)src, H->n);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  if (where == CUP_WHERE_HOST)
+    CK(cudaMemcpyAsync(dst, H->rhs, H->n * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+  return CUP_OK;
+}
+
+int valid_where(int where) { return where == CUP_WHERE_HOST || where == CUP_WHERE_DEVICE; }
+
+}  // namespace
+
+#define DISPATCH_T(H, fn, ...) ((H)->fp32 ? fn<float>(H, ##__VA_ARGS__) : fn<double>(H, ##__VA_ARGS__))
+
+#define REQUIRE_H(H)                        \
+  do {                                      \
+    if (!(H)) return CUP_ERR_ARG;           \
+    cudaError_t e0_ = cudaSetDevice((H)->dev); \
+    if (e0_ != cudaSuccess) return fail(H, CUP_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e0_)); \
+  } while (0)
+
+extern "C" {
+
+int cup_create(const cup_config* cfg, cup_handle** out) {
+  if (!cfg || !out) return CUP_ERR_ARG;
+  *out = nullptr;
+  cup_handle* H = new cup_handle();
+  H->cfg = *cfg;
+  H->nx = cfg->bpdx * 16;
+  H->ny = cfg->bpdy * 16;
+  H->nz = cfg->bpdz * 16;
+  const int N[3] = {H->nx, H->ny, H->nz};
+  auto reject = [&](int code) {
+    // keep the handle so that the caller can read the message, then free it
+    fprintf(stderr, "cup_create: %s\n", H->err.c_str());
+    delete H;
+    return code;
+  };
+  for (int d = 0; d < 3; ++d)
+    if (N[d] < 16 || N[d] > 256 || !is_pow2(N[d])) {
+      fail(H, CUP_ERR_ARG, "cells per dimension must be a power of two in [16, 256] (got %d)", N[d]);
+      return reject(CUP_ERR_ARG);
+    }
+  if (!(cfg->maxextent > 0)) {
+    fail(H, CUP_ERR_ARG, "maxextent must be > 0");
+    return reject(CUP_ERR_ARG);
+  }
+  if (cfg->precision != CUP_PREC_FP64 && cfg->precision != CUP_PREC_FP32_DC) {
+    fail(H, CUP_ERR_ARG, "unknown precision %d", cfg->precision);
+    return reject(CUP_ERR_ARG);
+  }
+  if (cfg->scheme != CUP_SCHEME_REF && cfg->scheme != CUP_SCHEME_UPWIND3_RK2) {
+    fail(H, CUP_ERR_ARG, "unknown scheme %d", cfg->scheme);
+    return reject(CUP_ERR_ARG);
+  }
+  if (cfg->nu < 0 || !(cfg->CFL > 0)) {
+    fail(H, CUP_ERR_ARG, "need nu >= 0 and CFL > 0");
+    return reject(CUP_ERR_ARG);
+  }
+  H->fp32 = cfg->precision == CUP_PREC_FP32_DC;
+  if (H->fp32 && H->nx < 32) {
+    fail(H, CUP_ERR_ARG, "FP32 storage needs nx >= 32 (128-byte TMA rows)");
+    return reject(CUP_ERR_ARG);
+  }
+  H->n = (size_t)H->nx * H->ny * H->nz;
+  const double maxbpd = std::max({(double)N[0], (double)N[1], (double)N[2]});
+  H->h = cfg->maxextent / maxbpd;
+  H->lambda = cfg->lambda;
+  for (int d = 0; d < 3; ++d) H->uinf[d] = cfg->uinf[d];
+  H->dev = cfg->device;
+  cudaError_t e = cudaSetDevice(H->dev);
+  if (e != cudaSuccess) {
+    fail(H, CUP_ERR_CUDA, "cudaSetDevice(%d): %s", H->dev, cudaGetErrorString(e));
+    return reject(CUP_ERR_CUDA);
+  }
+  int rc = [&]() -> int {
+    CK(cudaDeviceGetAttribute(&H->num_sms, cudaDevAttrMultiProcessorCount, H->dev));
+    CK(cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
+    H->own_stream = true;
+    const size_t es = H->fp32 ? sizeof(float) : sizeof(double);
+    for (void** f : {&H->u, &H->v, &H->w, &H->tu, &H->tv, &H->tw}) CK(cudaMalloc(f, H->n * es));
+    if (cfg->scheme == CUP_SCHEME_UPWIND3_RK2)
+      for (void** f : {&H->u1, &H->v1, &H->w1}) CK(cudaMalloc(f, H->n * es));
+    CK(cudaMalloc(&H->p, H->n * sizeof(double)));
+    CK(cudaMalloc(&H->rhs, H->n * sizeof(double)));
+    if (H->fp32) CK(cudaMalloc(&H->work32, H->n * sizeof(float)));
+    for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, (void*)H->p, (void*)H->rhs})
+      CK(cudaMemsetAsync(f, 0, H->n * (f == (void*)H->p || f == (void*)H->rhs ? sizeof(double) : es), H->stream));
+    CK(cudaMalloc(&H->partials, sizeof(double) * kPartialCap * P_COUNT));
+    CK(cudaMalloc(&H->dstate, sizeof(DevState)));
+    CK(cudaMemsetAsync(H->dstate, 0, sizeof(DevState), H->stream));
+    CK(cudaMalloc(&H->derr, sizeof(int)));
+    CK(cudaMemsetAsync(H->derr, 0, sizeof(int), H->stream));
+    CK(cudaMallocHost(&H->hstate, sizeof(DevState)));
+    // FFT tables per axis, spectral cosines exactly as PoissonSolverPeriodic::_solve
+    // computes them (source/poisson/PoissonSolverPeriodic.cpp:23-33).
+    for (int d = 0; d < 3; ++d) {
+      std::vector<double2> t64;
+      std::vector<float2> t32;
+      build_table(N[d], t64, t32);
+      CK(cudaMalloc(&H->tw64[d], t64.size() * sizeof(double2)));
+      CK(cudaMalloc(&H->tw32[d], t32.size() * sizeof(float2)));
+      CK(cudaMemcpy(H->tw64[d], t64.data(), t64.size() * sizeof(double2), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(H->tw32[d], t32.data(), t32.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    }
+    const size_t gsize[3] = {(size_t)N[0], (size_t)N[1], (size_t)N[2]};
+    const double h = H->h;
+    H->norm_factor = 4 / (gsize[0] * h * gsize[1] * gsize[2]);
+    double** cs[3] = {&H->cosx, &H->cosy, &H->cosz};
+    for (int d = 0; d < 3; ++d) {
+      const long nK = (long)gsize[d];
+      const double wFac = 4 * M_PI / nK;
+      std::vector<double> c(nK);
+      for (long i = 0; i < nK; ++i) c[i] = std::cos(wFac * i);
+      CK(cudaMalloc(cs[d], nK * sizeof(double)));
+      CK(cudaMemcpy(*cs[d], c.data(), nK * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    H->hstate->lambda = H->lambda;
+    CK(cudaMemcpyAsync(&H->dstate->lambda, &H->lambda, sizeof(double), cudaMemcpyHostToDevice, H->stream));
+    CK(cudaStreamSynchronize(H->stream));
+    if (!get_encode()) return fail(H, CUP_ERR_CUDA, "cuTensorMapEncodeTiled entry point unavailable");
+    return CUP_OK;
+  }();
+  if (rc) {
+    fprintf(stderr, "cup_create: %s\n", H->err.c_str());
+    cup_destroy(H);
+    return rc;
+  }
+  *out = H;
+  return CUP_OK;
+}
+
+int cup_destroy(cup_handle* H) {
+  if (!H) return CUP_OK;
+  cudaSetDevice(H->dev);
+  if (H->stream) cudaStreamSynchronize(H->stream);
+  for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->chi, (void*)H->p, (void*)H->rhs,
+                  (void*)H->work32, (void*)H->partials, (void*)H->dstate, (void*)H->derr, (void*)H->cosx,
+                  (void*)H->cosy, (void*)H->cosz, (void*)H->sp_dev})
+    if (f) cudaFree(f);
+  for (int d = 0; d < 3; ++d) {
+    if (H->tw64[d]) cudaFree(H->tw64[d]);
+    if (H->tw32[d]) cudaFree(H->tw32[d]);
+  }
+  prof_flush(H);
+  for (cudaEvent_t e : H->ev_pool) cudaEventDestroy(e);
+  if (H->hstate) cudaFreeHost(H->hstate);
+  if (H->own_stream && H->stream) cudaStreamDestroy(H->stream);
+  delete H;
+  return CUP_OK;
+}
+
+const char* cup_last_error(const cup_handle* H) { return H ? H->err.c_str() : "null handle"; }
+
+int cup_set_stream(cup_handle* H, void* stream) {
+  REQUIRE_H(H);
+  CK(cudaStreamSynchronize(H->stream));
+  if (stream) {
+    if (H->own_stream) CK(cudaStreamDestroy(H->stream));
+    H->own_stream = false;
+    H->stream = (cudaStream_t)stream;
+  } else if (!H->own_stream) {
+    CK(cudaStreamCreateWithFlags(&H->stream, cudaStreamNonBlocking));
+    H->own_stream = true;
+  }
+  return CUP_OK;
+}
+
+int cup_sync(cup_handle* H) {
+  REQUIRE_H(H);
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+int cup_get_dims(const cup_handle* H, int cells[3], double* hgrid) {
+  if (!H || !cells) return CUP_ERR_ARG;
+  cells[0] = H->nx;
+  cells[1] = H->ny;
+  cells[2] = H->nz;
+  if (hgrid) *hgrid = H->h;
+  return CUP_OK;
+}
+
+int cup_set_velocity(cup_handle* H, const double* u, const double* v, const double* w, int where) {
+  REQUIRE_H(H);
+  if (!u || !v || !w || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad velocity arguments");
+  int rc;
+  if ((rc = DISPATCH_T(H, set_field, H->u, u, where))) return rc;
+  if ((rc = DISPATCH_T(H, set_field, H->v, v, where))) return rc;
+  if ((rc = DISPATCH_T(H, set_field, H->w, w, where))) return rc;
+  H->umax_fresh = false;
+  if (where == CUP_WHERE_HOST) CK(cudaStreamSynchronize(H->stream));
+  return CUP_OK;
+}
+
+int cup_get_velocity(cup_handle* H, double* u, double* v, double* w, int where) {
+  REQUIRE_H(H);
+  if (!u || !v || !w || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad velocity arguments");
+  int rc;
+  for (auto pr : {std::make_pair(H->u, u), std::make_pair(H->v, v), std::make_pair(H->w, w)}) {
+    if ((rc = DISPATCH_T(H, get_field, pr.first, pr.second, where))) return rc;
+    if (where == CUP_WHERE_HOST) CK(cudaStreamSynchronize(H->stream));
+  }
+  return check_dev_error(H);
+}
+
+int cup_get_pressure(cup_handle* H, double* p, int where) {
+  REQUIRE_H(H);
+  if (!p || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad pressure arguments");
+  CK(cudaMemcpyAsync(p, H->p, H->n * sizeof(double),
+                     where == CUP_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+int cup_get_rhs(cup_handle* H, double* r, int where) {
+  REQUIRE_H(H);
+  if (!r || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad rhs arguments");
+  CK(cudaMemcpyAsync(r, H->rhs, H->n * sizeof(double),
+                     where == CUP_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+int cup_get_chi(cup_handle* H, double* chi, int where) {
+  REQUIRE_H(H);
+  if (!chi || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad chi arguments");
+  if (!H->chi) {
+    if (where == CUP_WHERE_HOST) std::fill(chi, chi + H->n, 0.0);
+    else CK(cudaMemsetAsync(chi, 0, H->n * sizeof(double), H->stream));
+  } else {
+    int rc = DISPATCH_T(H, get_field, H->chi, chi, where);
+    if (rc) return rc;
+  }
+  CK(cudaStreamSynchronize(H->stream));
+  return CUP_OK;
+}
+
+int cup_blocks_to_global(const double* blocks, double* global, int nx, int ny, int nz) {
+  if (!blocks || !global || nx % 16 || ny % 16 || nz % 16 || nx <= 0 || ny <= 0 || nz <= 0) return CUP_ERR_ARG;
+  const int bx = nx / 16, by = ny / 16;
+  size_t i = 0;
+  for (int bz = 0; bz < nz / 16; ++bz)
+    for (int byy = 0; byy < by; ++byy)
+      for (int bxx = 0; bxx < bx; ++bxx)
+        for (int iz = 0; iz < 16; ++iz)
+          for (int iy = 0; iy < 16; ++iy)
+            for (int ix = 0; ix < 16; ++ix)
+              global[((size_t)(bz * 16 + iz) * ny + (byy * 16 + iy)) * nx + (bxx * 16 + ix)] = blocks[i++];
+  return CUP_OK;
+}
+
+int cup_global_to_blocks(const double* global, double* blocks, int nx, int ny, int nz) {
+  if (!blocks || !global || nx % 16 || ny % 16 || nz % 16 || nx <= 0 || ny <= 0 || nz <= 0) return CUP_ERR_ARG;
+  const int bx = nx / 16, by = ny / 16;
+  size_t i = 0;
+  for (int bz = 0; bz < nz / 16; ++bz)
+    for (int byy = 0; byy < by; ++byy)
+      for (int bxx = 0; bxx < bx; ++bxx)
+        for (int iz = 0; iz < 16; ++iz)
+          for (int iy = 0; iy < 16; ++iy)
+            for (int ix = 0; ix < 16; ++ix)
+              blocks[i++] = global[((size_t)(bz * 16 + iz) * ny + (byy * 16 + iy)) * nx + (bxx * 16 + ix)];
+  return CUP_OK;
+}
+
+int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
+  REQUIRE_H(H);
+  if (!s || !(s->radius > 0)) return fail(H, CUP_ERR_ARG, "sphere radius must be > 0");
+  if (H->has_sphere) return fail(H, CUP_ERR_STATE, "only one obstacle is supported");
+  bool anyForced = false;
+  for (int d = 0; d < 3; ++d) anyForced = anyForced || s->bForcedInSimFrame[d];
+  for (int d = 0; d < 3; ++d)
+    if (!s->bForcedInSimFrame[d])
+      return fail(H, CUP_ERR_ARG, "free (unforced) obstacle dofs are not supported; force all three");
+  (void)anyForced;
+  H->has_sphere = true;
+  H->sphere = *s;
+  const size_t es = H->fp32 ? sizeof(float) : sizeof(double);
+  CK(cudaMalloc(&H->chi, H->n * es));
+  CK(cudaMemsetAsync(H->chi, 0, H->n * es, H->stream));
+  CK(cudaMalloc(&H->sp_dev, sizeof(SphereParams)));
+  // updateUinf (source/obstacles/ObstacleVector.h:60-76) for one obstacle
+  for (int d = 0; d < 3; ++d) H->uinf[d] = s->bFixFrameOfRef[d] ? -s->enforcedVelocity[d] : H->cfg.uinf[d];
+  SphereParams sp{};
+  sp.radius = s->radius;
+  for (int d = 0; d < 3; ++d) {
+    sp.position[d] = s->position[d];
+    sp.transVel[d] = s->bForcedInSimFrame[d] ? s->enforcedVelocity[d] : 0.0;
+    sp.angVel[d] = 0.0;  // rotation blocked when any dof is forced (Obstacle.cpp:131-137)
+  }
+  sp.lambda_factor = 1.0;
+  // Active box: every cell within radius + (2 + SURFDH) h + 1 cell of the centre
+  // (SphereObstacle::FillBlocks safety margin, Sphere.cpp:21-27, plus the
+  // surface-detection neighbour).
+  const int N[3] = {H->nx, H->ny, H->nz};
+  for (int d = 0; d < 3; ++d) {
+    const double r = s->radius + 3 * H->h;
+    int lo = (int)std::floor((s->position[d] - r) / H->h - 0.5) - 1;
+    int hi = (int)std::ceil((s->position[d] + r) / H->h - 0.5) + 1;
+    int cnt = hi - lo + 1;
+    if (cnt >= N[d]) {
+      lo = 0;
+      cnt = N[d];
+    }
+    lo = ((lo % N[d]) + N[d]) % N[d];
+    H->box.lo[d] = lo;
+    H->box.n[d] = cnt;
+  }
+  CK(cudaMemcpyAsync(H->sp_dev, &sp, sizeof(sp), cudaMemcpyHostToDevice, H->stream));
+  // CreateObstacles: chi and centre of mass (the position does not move for a
+  // forced sphere in a frame fixed to it: dt (transVel + uinf) = 0).
+  const int gb = box_grid(H->box);
+  {
+    int rc_ = launch_named(H, "sphere_chi", [&]() -> int {
+      if (H->fp32)
+        k_sphere_chi<float><<<gb, kBoxThreads, 0, H->stream>>>((float*)H->chi, H->sp_dev, H->box, H->nx, H->ny, H->nz,
+                                                                H->h, partial(H, P_CHI));
+      else
+        k_sphere_chi<double><<<gb, kBoxThreads, 0, H->stream>>>((double*)H->chi, H->sp_dev, H->box, H->nx, H->ny,
+                                                                 H->nz, H->h, partial(H, P_CHI));
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  {
+    int rc_ = launch_named(H, "finalize_com", [&]() -> int {
+      k_finalize_com<<<1, 256, 0, H->stream>>>(partial(H, P_CHI), gb, H->dstate, H->sp_dev);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  H->umax_fresh = false;
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+int cup_get_obstacle_state(cup_handle* H, double force[3], double torque[3], double com[3], double uinf[3]) {
+  REQUIRE_H(H);
+  int rc = read_state(H);
+  if (rc) return rc;
+  for (int d = 0; d < 3; ++d) {
+    if (force) force[d] = H->hstate->force[d];
+    if (torque) torque[d] = H->hstate->torque[d];
+    if (com) com[d] = H->hstate->com[d];
+    if (uinf) uinf[d] = H->uinf[d];
+  }
+  return CUP_OK;
+}
+
+int cup_max_velocity(cup_handle* H, double* umax) {
+  REQUIRE_H(H);
+  int rc = DISPATCH_T(H, do_max_u);
+  if (rc) return rc;
+  if ((rc = read_state(H))) return rc;
+  if (umax) *umax = H->hstate->umax;
+  H->umax_fresh = true;
+  return CUP_OK;
+}
+
+int cup_calc_max_timestep(cup_handle* H, double* dt) {
+  REQUIRE_H(H);
+  int rc;
+  if (!H->umax_fresh) {
+    if ((rc = DISPATCH_T(H, do_max_u))) return rc;
+    H->umax_fresh = true;
+  }
+  // the device keeps its own step counter in sync with the host mirror
+  CK(cudaMemcpyAsync(&H->dstate->step, &H->step, sizeof(int), cudaMemcpyHostToDevice, H->stream));
+  {
+    int rc_ = launch_named(H, "calc_dt", [&]() -> int {
+      k_calc_dt<<<1, 1, 0, H->stream>>>(H->dstate, H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  if ((rc = read_state(H))) return rc;
+  H->dt = H->hstate->dt;
+  if (H->cfg.DLM > 0) H->lambda = H->hstate->lambda;
+  if (dt) *dt = H->dt;
+  return CUP_OK;
+}
+
+int cup_advect_diffuse(cup_handle* H, double dt) {
+  REQUIRE_H(H);
+  H->umax_fresh = false;
+  return DISPATCH_T(H, do_advect_diffuse, DtArg{dt, nullptr});
+}
+
+int cup_pressure_rhs(cup_handle* H, double dt) {
+  REQUIRE_H(H);
+  return DISPATCH_T(H, do_pressure_rhs, DtArg{dt, nullptr});
+}
+
+int cup_poisson_solve(cup_handle* H, cup_solve_stats* stats) {
+  REQUIRE_H(H);
+  int rc = do_poisson(H);
+  if (rc) return rc;
+  if (stats) {
+    stats->n_solves = 1;
+    stats->rel_residual = 0;
+  }
+  return CUP_OK;
+}
+
+int cup_grad_correct(cup_handle* H, double dt) {
+  REQUIRE_H(H);
+  H->umax_fresh = false;
+  return DISPATCH_T(H, do_grad, DtArg{dt, nullptr});
+}
+
+int cup_pressure_projection(cup_handle* H, double dt, cup_solve_stats* stats) {
+  int rc = cup_poisson_solve(H, stats);
+  if (rc) return rc;
+  return cup_grad_correct(H, dt);
+}
+
+int cup_penalize(cup_handle* H, double dt, double force_torque[6]) {
+  REQUIRE_H(H);
+  H->umax_fresh = false;
+  if (!H->has_sphere) {
+    if (force_torque) std::fill(force_torque, force_torque + 6, 0.0);
+    return CUP_OK;
+  }
+  CK(cudaMemcpyAsync(&H->dstate->lambda, &H->lambda, sizeof(double), cudaMemcpyHostToDevice, H->stream));
+  int rc = DISPATCH_T(H, do_penalize, DtArg{dt, nullptr}, (const double*)nullptr);
+  if (rc) return rc;
+  {
+    int rc_ = launch_named(H, "finalize_pen", [&]() -> int {
+      k_finalize_pen<<<1, 256, 0, H->stream>>>(partial(H, P_PEN), H->n_pen_partials, H->dstate);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  if (force_torque) {
+    if ((rc = read_state(H))) return rc;
+    for (int d = 0; d < 3; ++d) {
+      force_torque[d] = H->hstate->force[d];
+      force_torque[3 + d] = H->hstate->torque[d];
+    }
+  }
+  return CUP_OK;
+}
+
+static int fill_stats(cup_handle* H, cup_step_stats* st) {
+  int rc = read_state(H);
+  if (rc) return rc;
+  const DevState& s = *H->hstate;
+  st->dt = s.dt;
+  st->time = H->time;
+  st->step = H->step;
+  st->umax = s.umax;
+  st->kinetic_energy = s.ke;
+  for (int d = 0; d < 3; ++d) {
+    st->force[d] = s.force[d];
+    st->torque[d] = s.torque[d];
+  }
+  st->n_solves = H->fp32 ? s.n_solves : 1;
+  st->rel_residual = H->fp32 && s.b2 > 0 ? std::sqrt(s.res2 / s.b2) : 0.0;
+  if (!std::isfinite(s.umax) || !std::isfinite(s.ke)) return fail(H, CUP_ERR_NONFINITE, "non-finite velocity");
+  return CUP_OK;
+}
+
+int cup_step(cup_handle* H, double dt, cup_step_stats* stats) {
+  REQUIRE_H(H);
+  if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
+  H->dt = dt;
+  if (H->cfg.DLM > 0) H->lambda = H->cfg.DLM / dt;
+  // device dt/lambda follow the host values for this step
+  {
+    int rc_ = launch_named(H, "set_dt", [&]() -> int {
+      k_set_dt<<<1, 1, 0, H->stream>>>(H->dstate, dt, H->cfg.DLM);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  if (H->cfg.DLM <= 0) CK(cudaMemcpyAsync(&H->dstate->lambda, &H->lambda, sizeof(double), cudaMemcpyHostToDevice, H->stream));
+  int rc = DISPATCH_T(H, do_step, DtArg{dt, nullptr}, (const double*)&H->dstate->lambda, 1);
+  if (rc) return rc;
+  H->step += 1;
+  H->time += dt;
+  H->umax_fresh = true;
+  if (stats) return fill_stats(H, stats);
+  return CUP_OK;
+}
+
+int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
+  REQUIRE_H(H);
+  if (nsteps < 0) return fail(H, CUP_ERR_ARG, "nsteps must be >= 0");
+  int rc;
+  if (!H->umax_fresh) {
+    if ((rc = DISPATCH_T(H, do_max_u))) return rc;
+    H->umax_fresh = true;
+  }
+  CK(cudaMemcpyAsync(&H->dstate->step, &H->step, sizeof(int), cudaMemcpyHostToDevice, H->stream));
+  CK(cudaMemcpyAsync(&H->dstate->time, &H->time, sizeof(double), cudaMemcpyHostToDevice, H->stream));
+  if (H->cfg.DLM <= 0) CK(cudaMemcpyAsync(&H->dstate->lambda, &H->lambda, sizeof(double), cudaMemcpyHostToDevice, H->stream));
+  for (int i = 0; i < nsteps; ++i) {
+    {
+      int rc_ = launch_named(H, "calc_dt", [&]() -> int {
+        k_calc_dt<<<1, 1, 0, H->stream>>>(H->dstate, H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM);
+        CKL();
+        return CUP_OK;
+      });
+      if (rc_) return rc_;
+    }
+    rc = DISPATCH_T(H, do_step, DtArg{0.0, &H->dstate->dt}, (const double*)&H->dstate->lambda, 1);
+    if (rc) return rc;
+  }
+  if ((rc = read_state(H))) return rc;
+  H->step = H->hstate->step;
+  H->time = H->hstate->time;
+  H->dt = H->hstate->dt;
+  if (H->cfg.DLM > 0) H->lambda = H->hstate->lambda;
+  if (stats) return fill_stats(H, stats);
+  return CUP_OK;
+}
+
+int cup_poisson_solve_field(cup_handle* H, const double* rhs, double* p, int where) {
+  REQUIRE_H(H);
+  if (!rhs || !p || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad poisson arguments");
+  const cudaMemcpyKind in = where == CUP_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind out = where == CUP_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(H->rhs, rhs, H->n * sizeof(double), in, H->stream));
+  int rc = do_poisson(H);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(p, H->p, H->n * sizeof(double), out, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+int cup_diagnostics(cup_handle* H, double out[3]) {
+  REQUIRE_H(H);
+  if (!out) return fail(H, CUP_ERR_ARG, "null output");
+  const int grid = std::min<size_t>(H->num_sms * 4, (H->n + 255) / 256);
+  double* part = partial(H, P_DIAG);
+  {
+    int rc_ = launch_named(H, "diag", [&]() -> int {
+      if (H->fp32)
+        k_diag<float><<<grid, 256, 0, H->stream>>>((const float*)H->u, (const float*)H->v, (const float*)H->w, H->nx,
+                                                    H->ny, H->nz, 0.5 / H->h, part);
+      else
+        k_diag<double><<<grid, 256, 0, H->stream>>>((const double*)H->u, (const double*)H->v, (const double*)H->w,
+                                                     H->nx, H->ny, H->nz, 0.5 / H->h, part);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  std::vector<double> hp(3 * grid);
+  CK(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  double ke = 0, d2 = 0, dm = 0;
+  for (int i = 0; i < grid; ++i) {
+    ke += hp[3 * i];
+    d2 += hp[3 * i + 1];
+    dm = std::max(dm, hp[3 * i + 2]);
+  }
+  const double h3 = H->h * H->h * H->h;
+  out[0] = ke * h3;
+  out[1] = std::sqrt(d2 * h3);
+  out[2] = dm;
+  return check_dev_error(H);
+}
+
+int cup_debug_shift(cup_handle* H, const double* f, double* out, int g, int dx, int dy, int dz, int where) {
+  REQUIRE_H(H);
+  if (!f || !out || !valid_where(where) || (g != 1 && g != 2) || std::abs(dx) > g || std::abs(dy) > g ||
+      std::abs(dz) > g)
+    return fail(H, CUP_ERR_ARG, "bad shift arguments");
+  // stage through the (FP64) rhs and p buffers
+  const cudaMemcpyKind in = where == CUP_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind outk = where == CUP_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  CK(cudaMemcpyAsync(H->rhs, f, H->n * sizeof(double), in, H->stream));
+  const void* fl[1] = {H->rhs};
+  OpShift op{H->p, dx, dy, dz, H->nx, H->ny};
+  int rc = g == 1 ? launch_stream<double, 1, 1, 4, 4>(H, "debug_shift", fl, op)
+                  : launch_stream<double, 1, 2, 4, 6>(H, "debug_shift", fl, op);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(out, H->p, H->n * sizeof(double), outk, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+int cup_profile_enable(cup_handle* H, int on) {
+  REQUIRE_H(H);
+  prof_flush(H);
+  H->prof_on = on != 0;
+  return CUP_OK;
+}
+
+int cup_profile_report(cup_handle* H, char* buf, size_t len, int reset) {
+  REQUIRE_H(H);
+  prof_flush(H);
+  std::string js = "{";
+  bool first = true;
+  for (const auto& kv : H->prof) {
+    char item[256];
+    snprintf(item, sizeof item, "%s\"%s\": {\"count\": %lld, \"ms\": %.6f}", first ? "" : ", ", kv.first.c_str(),
+             kv.second.first, kv.second.second);
+    js += item;
+    first = false;
+  }
+  js += "}";
+  if (reset) H->prof.clear();
+  if (!buf || len == 0) return fail(H, CUP_ERR_ARG, "null buffer");
+  if (js.size() + 1 > len) return fail(H, CUP_ERR_ARG, "buffer too small (%zu needed)", js.size() + 1);
+  memcpy(buf, js.c_str(), js.size() + 1);
+  return CUP_OK;
+}
+
+int cup_launch_count(const cup_handle* H, long long* n) {
+  if (!H || !n) return CUP_ERR_ARG;
+  *n = H->launches;
+  return CUP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,399 @@
+// Shared-memory FFT passes of the periodic Poisson solve
+// (the device replacement of PoissonSolverPeriodic's FFTW r2c / _solve / c2r,
+// source/poisson/PoissonSolverPeriodic.cpp:15-146).
+//
+// The solve is p = H(f . H(b)) with H the separable real Hartley transform
+// H[k] = Re X[k] - Im X[k] (X the unnormalised DFT) applied along x, y and z,
+// and f the reference's grid-consistent factor
+//   f = 4 / (Nx h Ny Nz) / (2 (cos(4 pi kx/Nx) + cos(4 pi ky/Ny) + cos(4 pi kz/Nz)) - 6)
+// with the 8 modes kx in {0, Nx/2}, ky in {0, Ny/2}, kz in {0, Nz/2} zeroed.
+// Because the wide Laplacian is a sum of symmetric circulants, the cos/sin
+// pair of each DFT mode is one eigenspace, so H diagonalises it exactly like
+// the DFT does; H is its own inverse up to 1/N. Everything stays real, every
+// pass is in place on an Nx*Ny*Nz array, and the data layout never changes.
+//
+// A length-N Hartley transform is one length-M = N/2 complex FFT of
+// z[m] = x[2m] + i x[2m+1] (Stockham autosort, radix 8/4/2 stages, Govindaraju
+// et al., SC'08) followed by the standard even/odd split to X[k], k <= M.
+#pragma once
+
+#include "common.cuh"
+
+namespace cup {
+
+template <typename R>
+struct Cplx;
+template <>
+struct Cplx<double> {
+  using T = double2;
+};
+template <>
+struct Cplx<float> {
+  using T = float2;
+};
+
+template <typename R2>
+__device__ __forceinline__ R2 cmul(R2 a, R2 b) {
+  R2 r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
+}
+template <typename R2>
+__device__ __forceinline__ R2 cadd(R2 a, R2 b) {
+  R2 r;
+  r.x = a.x + b.x;
+  r.y = a.y + b.y;
+  return r;
+}
+template <typename R2>
+__device__ __forceinline__ R2 csub(R2 a, R2 b) {
+  R2 r;
+  r.x = a.x - b.x;
+  r.y = a.y - b.y;
+  return r;
+}
+// -i * a
+template <typename R2>
+__device__ __forceinline__ R2 cmul_mi(R2 a) {
+  R2 r;
+  r.x = a.y;
+  r.y = -a.x;
+  return r;
+}
+
+// Forward (e^{-2 pi i/R}) R-point DFTs in registers.
+template <int R, typename R2>
+struct DFT;
+template <typename R2>
+struct DFT<2, R2> {
+  __device__ __forceinline__ static void run(R2* v) {
+    const R2 a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+template <typename R2>
+struct DFT<4, R2> {
+  __device__ __forceinline__ static void run(R2* v) {
+    const R2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    const R2 t2 = cadd(v[1], v[3]), t3 = cmul_mi(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+  }
+};
+template <typename R2>
+struct DFT<8, R2> {
+  __device__ __forceinline__ static void run(R2* v) {
+    using S = decltype(v[0].x);
+    const S c = (S)0.70710678118654752440084436210484904;  // sqrt(2)/2
+    R2 e[4] = {v[0], v[2], v[4], v[6]};
+    R2 o[4] = {v[1], v[3], v[5], v[7]};
+    DFT<4, R2>::run(e);
+    DFT<4, R2>::run(o);
+    // twiddles W8^k, k = 0..3: 1, c(1-i), -i, -c(1+i)
+    R2 w1, w3;
+    w1.x = c * (o[1].x + o[1].y);
+    w1.y = c * (o[1].y - o[1].x);
+    const R2 w2 = cmul_mi(o[2]);
+    w3.x = c * (o[3].y - o[3].x);
+    w3.y = -c * (o[3].x + o[3].y);
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], w1);
+    v[5] = csub(e[1], w1);
+    v[2] = cadd(e[2], w2);
+    v[6] = csub(e[2], w2);
+    v[3] = cadd(e[3], w3);
+    v[7] = csub(e[3], w3);
+  }
+};
+
+// Radix plan of an M-point complex FFT: radix-8 stages then one 2 or 4.
+template <int M>
+struct FFTPlan {
+  static constexpr int nstages = (M == 8) ? 1 : (M == 16 || M == 32 || M == 64) ? 2 : 3;
+  static constexpr int radix(int s) {
+    return s == 0 ? 8
+           : s == 1 ? (M == 16 ? 2 : M == 32 ? 4 : 8)
+                    : (M == 128 ? 2 : 4);
+  }
+  static constexpr int ns(int s) { return s == 0 ? 1 : s == 1 ? 8 : 64; }
+  // offset of stage s's twiddle table (R*Ns entries) in the per-length table
+  static constexpr int tw_off(int s) { return s <= 1 ? 0 : radix(1) * ns(1); }
+  static constexpr int tw_stage_total() {
+    return nstages == 1 ? 0 : nstages == 2 ? radix(1) * ns(1) : radix(1) * ns(1) + radix(2) * ns(2);
+  }
+  // post-processing table W_N^k, k = 0..M/2, follows the stage tables
+  static constexpr int post_off() { return tw_stage_total(); }
+  static constexpr int table_len() { return tw_stage_total() + M / 2 + 1; }
+};
+
+// ---- line accessors -------------------------------------------------------
+// Row lines: line l starts at base + l*pitch (reals), complex m at reals 2m, 2m+1.
+template <typename R>
+struct RowLines {
+  using R2 = typename Cplx<R>::T;
+  R* base;
+  int pitch;
+  __device__ __forceinline__ R2 ld(int l, int m) const { return *reinterpret_cast<const R2*>(base + l * pitch + 2 * m); }
+  __device__ __forceinline__ void st(int l, int m, R2 v) const { *reinterpret_cast<R2*>(base + l * pitch + 2 * m) = v; }
+  __device__ __forceinline__ R ldr(int l, int n) const { return base[l * pitch + n]; }
+  __device__ __forceinline__ void str(int l, int n, R v) const { base[l * pitch + n] = v; }
+};
+// Padded row lines (complex m stored at m + m/8) to keep the first Stockham
+// stage's stride-8 stores free of bank conflicts.
+template <typename R>
+struct RowLinesPad {
+  using R2 = typename Cplx<R>::T;
+  R* base;
+  int pitch;  // reals per line (>= 2*(M + M/8))
+  __device__ __forceinline__ R2 ld(int l, int m) const {
+    return *reinterpret_cast<const R2*>(base + l * pitch + 2 * (m + (m >> 3)));
+  }
+  __device__ __forceinline__ void st(int l, int m, R2 v) const {
+    *reinterpret_cast<R2*>(base + l * pitch + 2 * (m + (m >> 3))) = v;
+  }
+};
+// Column lines of a tile [n][W]: element n of line l at n*W + l.
+template <typename R>
+struct ColLines {
+  using R2 = typename Cplx<R>::T;
+  R* base;
+  int W;
+  __device__ __forceinline__ R2 ld(int l, int m) const {
+    R2 v;
+    v.x = base[(2 * m) * W + l];
+    v.y = base[(2 * m + 1) * W + l];
+    return v;
+  }
+  __device__ __forceinline__ void st(int l, int m, R2 v) const {
+    base[(2 * m) * W + l] = v.x;
+    base[(2 * m + 1) * W + l] = v.y;
+  }
+  __device__ __forceinline__ R ldr(int l, int n) const { return base[n * W + l]; }
+  __device__ __forceinline__ void str(int l, int n, R v) const { base[n * W + l] = v; }
+};
+
+// One Stockham stage: each of the M/8 threads of a line does 8/R radix-R
+// butterflies j = t + b*M/8, reading in[j + r*M/R], writing
+// out[(j/Ns)*Ns*R + j%Ns + r*Ns]. All threads of the CTA take part
+// (every line in parallel), so the barriers are block-wide.
+template <int M, int R, int NS, bool INPLACE, typename R2, class In, class Out>
+__device__ __forceinline__ void fft_stage(const In& in, const Out& out, const R2* tw, int l, int t, bool active) {
+  constexpr int NB = 8 / R;
+  constexpr int TPL = M / 8;
+  R2 v[8];
+  if (active) {
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const int j = t + b * TPL;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b * R + r] = in.ld(l, j + r * (M / R));
+      if (NS > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[b * R + r] = cmul(v[b * R + r], tw[r * NS + (j % NS)]);
+      }
+    }
+  }
+  if (INPLACE) __syncthreads();
+  if (active) {
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const int j = t + b * TPL;
+      DFT<R, R2>::run(&v[b * R]);
+      const int idxD = (j / NS) * NS * R + (j % NS);
+#pragma unroll
+      for (int r = 0; r < R; ++r) out.st(l, idxD + r * NS, v[b * R + r]);
+    }
+  }
+  __syncthreads();
+}
+
+// Even/odd split of the packed M-point FFT Z into the Hartley transform H of
+// the length-2M real line, in place (task k handles Z[k], Z[M-k] and writes
+// H[k], H[N-k], H[M-k], H[M+k]).
+template <int M, typename R, typename R2, class Acc>
+__device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int t, bool active) {
+  constexpr int TPL = M / 8;
+  constexpr int NT = (M / 2 + 1 + TPL - 1) / TPL;
+  constexpr int N = 2 * M;
+  R2 A_[NT], B_[NT];
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      const int k = t + i * TPL;
+      if (k <= M / 2) {
+        A_[i] = a.ld(l, k);
+        B_[i] = a.ld(l, (M - k) & (M - 1));
+      }
+    }
+  }
+  __syncthreads();
+  if (active) {
+#pragma unroll
+    for (int i = 0; i < NT; ++i) {
+      const int k = t + i * TPL;
+      if (k > M / 2) continue;
+      const R2 A = A_[i], B = B_[i];
+      if (k == 0) {
+        a.str(l, 0, A.x + A.y);
+        a.str(l, M, A.x - A.y);
+      } else {
+        const R2 W = twp[k];
+        const R half = (R)0.5;
+        const R Er = (A.x + B.x) * half, Ei = (A.y - B.y) * half;
+        const R Or = (A.y + B.y) * half, Oi = (B.x - A.x) * half;
+        const R Xr = Er + (W.x * Or - W.y * Oi), Xi = Ei + (W.x * Oi + W.y * Or);
+        a.str(l, k, Xr - Xi);
+        a.str(l, N - k, Xr + Xi);
+        const R X2r = Er - W.x * Or + W.y * Oi, X2i = -Ei + W.x * Oi + W.y * Or;
+        a.str(l, M - k, X2r - X2i);
+        a.str(l, M + k, X2r + X2i);
+      }
+    }
+  }
+  __syncthreads();
+}
+
+// Full in-place Hartley transform of the lines of `a` (pad: scratch for the
+// first stage's output when USE_PAD). Thread `t` of line `l`, M/8 per line.
+template <int M, bool USE_PAD, typename R, class Acc, class P>
+__device__ __forceinline__ void dht_lines(const Acc& a, const P& pad, const typename Cplx<R>::T* tw, int l, int t,
+                                          bool active) {
+  using R2 = typename Cplx<R>::T;
+  using Pl = FFTPlan<M>;
+  if constexpr (Pl::nstages == 1) {
+    fft_stage<M, 8, 1, true, R2>(a, a, tw, l, t, active);
+  } else if constexpr (USE_PAD) {
+    fft_stage<M, 8, 1, false, R2>(a, pad, tw, l, t, active);
+    fft_stage<M, Pl::radix(1), 8, false, R2>(pad, a, tw + Pl::tw_off(1), l, t, active);
+    if constexpr (Pl::nstages == 3) fft_stage<M, Pl::radix(2), 64, true, R2>(a, a, tw + Pl::tw_off(2), l, t, active);
+  } else {
+    fft_stage<M, 8, 1, true, R2>(a, a, tw, l, t, active);
+    fft_stage<M, Pl::radix(1), 8, true, R2>(a, a, tw + Pl::tw_off(1), l, t, active);
+    if constexpr (Pl::nstages == 3) fft_stage<M, Pl::radix(2), 64, true, R2>(a, a, tw + Pl::tw_off(2), l, t, active);
+  }
+  dht_post<M, R, R2>(a, tw + Pl::post_off(), l, t, active);
+}
+
+template <typename R2>
+__device__ __forceinline__ void load_table(R2* dst, const R2* src, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// x pass: LPC consecutive rows of length N = 2M per CTA (rows are contiguous
+// in the [z][y][x] layout), loaded with one 1-D bulk copy, transformed, and
+// written back with one bulk store. in may equal out.
+template <int M, typename R>
+__global__ void __launch_bounds__(256) k_dht_rows(const R* in, R* out, int nrows, int lpc,
+                                                  const typename Cplx<R>::T* tw_g, int* err) {
+  using R2 = typename Cplx<R>::T;
+  constexpr int N = 2 * M, TPL = M / 8;
+  constexpr int TL = FFTPlan<M>::table_len();
+  constexpr bool PAD = FFTPlan<M>::nstages > 1;
+  constexpr int PPITCH = 2 * (M + M / 8);
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw = smem_align128(smem_dyn);
+  R* rows = reinterpret_cast<R*>(smem_raw);                        // lpc * N
+  R* padb = rows + (size_t)lpc * N;                                // lpc * PPITCH
+  R2* tw = reinterpret_cast<R2*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
+  const int row0 = blockIdx.x * lpc;
+  const int nr = min(lpc, nrows - row0);
+  if (nr <= 0) return;
+  const uint32_t bytes = (uint32_t)((size_t)nr * N * sizeof(R));
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+    mbar_arrive_expect_tx(bar, bytes);
+    bulk_load(rows, in + (size_t)row0 * N, bytes, bar);
+  }
+  load_table(tw, tw_g, TL);
+  const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
+  if (!ok) return;
+  const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
+  const bool active = l < nr;
+  RowLines<R> A{rows, N};
+  RowLinesPad<R> P{padb, PPITCH};
+  dht_lines<M, PAD, R>(A, P, tw, l, t, active);
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bulk_store(out + (size_t)row0 * N, rows, bytes);
+    bulk_commit();
+    bulk_wait_all();
+  }
+}
+
+// Spectral factor of PoissonSolverPeriodic::_solve (grid-consistent branch,
+// source/poisson/PoissonSolverPeriodic.cpp:23-61): cx/cy/cz hold
+// cos(4 pi k / N) evaluated on the host exactly as the reference does.
+struct SpectralParams {
+  const double* cx;
+  const double* cy;
+  const double* cz;
+  double norm_factor;
+  int nx, ny, nz;
+};
+
+__device__ __forceinline__ double spectral_factor(const SpectralParams& sp, int kx, int ky, int kz) {
+  const bool null_mode = (kx == 0 || kx == sp.nx / 2) && (ky == 0 || ky == sp.ny / 2) && (kz == 0 || kz == sp.nz / 2);
+  if (null_mode) return 0.0;
+  const double D = sp.cx[kx] + sp.cy[ky] + sp.cz[kz];
+  return sp.norm_factor / (2 * D - 6);
+}
+
+// y / z pass: a tile of W consecutive x columns by the whole line length,
+// moved with TMA tiled loads/stores. AXIS 1: box {W, Ny, 1} at (x0, 0, z);
+// AXIS 2: box {W, 1, Nz} at (x0, y, 0). With DIVIDE (z pass only) the tile is
+// transformed, multiplied by the spectral factor and transformed back.
+template <int M, typename R, int AXIS, bool DIVIDE>
+__global__ void __launch_bounds__(256) k_dht_cols(const __grid_constant__ CUtensorMap map_in,
+                                                  const __grid_constant__ CUtensorMap map_out, int W, int ntiles_x,
+                                                  const typename Cplx<R>::T* tw_g, SpectralParams sp, int* err) {
+  using R2 = typename Cplx<R>::T;
+  constexpr int N = 2 * M, TPL = M / 8;
+  constexpr int TL = FFTPlan<M>::table_len();
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw = smem_align128(smem_dyn);
+  R* tile = reinterpret_cast<R*>(smem_raw);  // [N][W]
+  R2* tw = reinterpret_cast<R2*>(tile + (size_t)N * W);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
+  const int x0 = (blockIdx.x % ntiles_x) * W;
+  const int other = blockIdx.x / ntiles_x;  // z for AXIS 1, y for AXIS 2
+  const int c1 = AXIS == 1 ? 0 : other, c2 = AXIS == 1 ? other : 0;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+    mbar_arrive_expect_tx(bar, (uint32_t)((size_t)N * W * sizeof(R)));
+    tma_load_3d(tile, &map_in, x0, c1, c2, bar);
+  }
+  load_table(tw, tw_g, TL);
+  const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
+  if (!ok) return;
+  const int l = threadIdx.x % W, t = threadIdx.x / W;
+  const bool active = t < TPL;
+  ColLines<R> A{tile, W};
+  dht_lines<M, false, R>(A, A, tw, l, t, active);
+  if constexpr (DIVIDE) {
+    for (int i = threadIdx.x; i < N * W; i += blockDim.x) {
+      const int n = i / W, w = i - n * W;
+      tile[i] = (R)((double)tile[i] * spectral_factor(sp, x0 + w, other, n));
+    }
+    __syncthreads();
+    dht_lines<M, false, R>(A, A, tw, l, t, active);
+  }
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    tma_store_3d(&map_out, x0, c1, c2, tile);
+    bulk_commit();
+    bulk_wait_all();
+  }
+}
+
+}  // namespace cup

@@ -1,0 +1,437 @@
+"""Python host side mirroring CubismUP_3D's pybind11 API for the periodic hot path.
+
+Reference interface (source/bindings/Simulation.cpp:59-94, source/bindings/Obstacles.cpp:79-129):
+``SimulationData(comm, CFL, cells, uinf)``, ``Simulation(SimulationData)`` with
+``run()`` and ``add_obstacle(Sphere(...))``; operators are the pipeline entries
+of ``Simulation::setupOperators`` (source/Simulation.cpp:307-401) driven by
+``operator()(double dt)`` with ``getName()``. Every call goes through the C ABI
+of ``libcup_b200.so`` (include/cup_b200.h); arguments the reference rejects
+with ``std::invalid_argument`` raise ``ValueError`` here as pybind11 would.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib as L
+
+PERIODIC = "periodic"
+BLOCK_SIZE = 16  # CUP_BLOCK_SIZE (source/Definitions.h:27-29)
+
+
+@dataclass
+class SimulationData:
+    """Hot-path subset of SimulationData (source/SimulationData.h:46-179).
+
+    Struct defaults follow the reference's struct (not its CLI defaults):
+    ``DLM = 1`` (lambda = 1/dt, SimulationData.h:98), ``rampup = 100``
+    (SimulationData.h:143). Only periodic boundaries are supported.
+    """
+
+    CFL: float = 0.1
+    cells: Tuple[int, int, int] = (64, 64, 64)
+    uinf: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    comm: object = None
+    nu: float = 0.0
+    lambda_: float = -1.0
+    DLM: float = 1.0
+    rampup: int = 100
+    nsteps: int = 0
+    endTime: float = 0.0
+    extent: float = 1.0  # maxextent: h = extent / max(cells)
+    bImplicitPenalization: bool = False
+    BCx_flag: str = PERIODIC
+    BCy_flag: str = PERIODIC
+    BCz_flag: str = PERIODIC
+    precision: str = "fp64"  # "fp64" | "fp32_dc"
+    scheme: str = "ref"      # "ref" | "upwind3_rk2"
+    dc_tol: float = 1e-10
+    dc_max_iter: int = 4
+    dc_min_iter: int = 1
+    device: int = 0
+    verbose: bool = False
+
+    def __post_init__(self):
+        self.setCells(*self.cells)
+
+    def setCells(self, nx: int, ny: int, nz: int):
+        """SimulationData::setCells (source/SimulationData.cpp:280-291)."""
+        if nx % BLOCK_SIZE or ny % BLOCK_SIZE or nz % BLOCK_SIZE:
+            raise ValueError("Number of cells must be multiple of block size * number of processes.")
+        self.cells = (int(nx), int(ny), int(nz))
+
+    @property
+    def bpd(self) -> Tuple[int, int, int]:
+        return tuple(c // BLOCK_SIZE for c in self.cells)
+
+    def to_config(self) -> L.CupConfig:
+        if (self.BCx_flag, self.BCy_flag, self.BCz_flag) != (PERIODIC,) * 3:
+            raise ValueError("only periodic boundaries are supported (bUseFourierBC)")
+        if self.lambda_ <= 0 and self.DLM <= 0:
+            raise ValueError("need lambda > 0 or DLM > 0 (SimulationData.cpp:203)")
+        cfg = L.CupConfig()
+        cfg.bpdx, cfg.bpdy, cfg.bpdz = self.bpd
+        cfg.maxextent = float(self.extent)
+        cfg.nu = float(self.nu)
+        cfg.CFL = float(self.CFL)
+        cfg.lambda_ = float(self.lambda_)
+        cfg.DLM = float(self.DLM)
+        cfg.uinf[:] = [float(x) for x in self.uinf]
+        cfg.rampup = int(self.rampup)
+        cfg.bImplicitPenalization = int(bool(self.bImplicitPenalization))
+        cfg.precision = {"fp64": L.CUP_PREC_FP64, "fp32_dc": L.CUP_PREC_FP32_DC}[self.precision]
+        cfg.scheme = {"ref": L.CUP_SCHEME_REF, "upwind3_rk2": L.CUP_SCHEME_UPWIND3_RK2}[self.scheme]
+        cfg.dc_tol = float(self.dc_tol)
+        cfg.dc_max_iter = int(self.dc_max_iter)
+        cfg.dc_min_iter = int(self.dc_min_iter)
+        cfg.device = int(self.device)
+        return cfg
+
+
+@dataclass
+class ObstacleArguments:
+    """ObstacleArguments (source/obstacles/Obstacle.h:60-75)."""
+
+    length: float = 0.0
+    position: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    quaternion: Tuple[float, float, float, float] = (1.0, 0.0, 0.0, 0.0)
+    enforcedVelocity: Tuple[float, float, float] = (0.0, 0.0, 0.0)
+    bForcedInSimFrame: Tuple[bool, bool, bool] = (False, False, False)
+    bFixFrameOfRef: Tuple[bool, bool, bool] = (False, False, False)
+    bFixToPlanar: bool = False
+    bComputeForces: bool = True
+
+
+class Sphere(ObstacleArguments):
+    """ObstacleAndSphereArguments constructor of the bindings
+    (source/bindings/Obstacles.cpp:57-82): ``Sphere(radius, umax, tmax,
+    accel_decel, bHemi, **kwargs)`` with ObstacleArguments as kwargs."""
+
+    def __init__(self, radius: float = -1.0, umax: float = 0.0, tmax: float = 1.0,
+                 accel_decel: bool = False, bHemi: bool = False, **kwargs):
+        length = float(kwargs.pop("length", 0.0))
+        if radius > 0 and length > 0 and radius != 0.5 * length:
+            raise ValueError("Cannot specify both `radius` and `length`.")
+        elif radius <= 0 and length <= 0:
+            raise ValueError("Expected a `radius` or `length`.")
+        elif radius > 0:
+            length = 2.0 * radius
+        else:
+            radius = 0.5 * length
+        super().__init__(length=length)
+        for k in ("position", "quaternion", "enforcedVelocity", "bForcedInSimFrame", "bFixFrameOfRef",
+                  "bFixToPlanar", "bComputeForces"):
+            if k in kwargs:
+                setattr(self, k, kwargs.pop(k))
+        if kwargs:
+            raise ValueError(f"unknown Sphere arguments: {sorted(kwargs)}")
+        if accel_decel or bHemi:
+            raise ValueError("accel_decel and hemisphere spheres are not supported")
+        self.radius = float(radius)
+        self.umax, self.tmax = umax, tmax
+        self.accel_decel, self.bHemi = accel_decel, bHemi
+
+    def to_struct(self) -> L.CupSphere:
+        s = L.CupSphere()
+        s.radius = self.radius
+        s.position[:] = [float(x) for x in self.position]
+        s.enforcedVelocity[:] = [float(x) for x in self.enforcedVelocity]
+        s.bForcedInSimFrame[:] = [int(bool(x)) for x in self.bForcedInSimFrame]
+        s.bFixFrameOfRef[:] = [int(bool(x)) for x in self.bFixFrameOfRef]
+        return s
+
+
+def _as_host_f64(a, shape) -> np.ndarray:
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    if arr.shape != shape:
+        raise ValueError(f"expected an array of shape {shape} (nz, ny, nx), got {arr.shape}")
+    return arr
+
+
+def _ptr(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _is_torch_cuda(a) -> bool:
+    return hasattr(a, "is_cuda") and a.is_cuda
+
+
+class Operator:
+    """Operator (source/operators/Operator.h:16-177): ``op(dt)``, ``getName()``."""
+
+    name = "Operator"
+
+    def __init__(self, sim: "Simulation"):
+        self.sim = sim
+
+    def getName(self) -> str:
+        return self.name
+
+    def __call__(self, dt: float):  # pragma: no cover - abstract
+        raise NotImplementedError
+
+
+class AdvectionDiffusion(Operator):
+    name = "AdvectionDiffusion"
+
+    def __call__(self, dt: float):
+        L.check(L.lib().cup_advect_diffuse(self.sim._h, float(dt)), self.sim._h, self.name)
+
+
+class PressureRHS(Operator):
+    name = "PressureRHS"
+
+    def __call__(self, dt: float):
+        L.check(L.lib().cup_pressure_rhs(self.sim._h, float(dt)), self.sim._h, self.name)
+
+
+class PressureProjection(Operator):
+    name = "PressureProjection"
+
+    def __call__(self, dt: float):
+        st = L.CupSolveStats()
+        L.check(L.lib().cup_pressure_projection(self.sim._h, float(dt), C.byref(st)), self.sim._h, self.name)
+        self.last_stats = st
+
+
+class Penalization(Operator):
+    name = "Penalization"
+
+    def __call__(self, dt: float):
+        ft = (C.c_double * 6)()
+        L.check(L.lib().cup_penalize(self.sim._h, float(dt), ft), self.sim._h, self.name)
+        self.force_torque = np.array(ft[:])
+
+
+class PoissonSolverPeriodic:
+    """PoissonSolverPeriodic (source/poisson/PoissonSolverPeriodic.cpp) bound
+    to a simulation's device buffers: ``solve()`` runs the FFT chain."""
+
+    def __init__(self, sim: "Simulation"):
+        self.sim = sim
+
+    def solve(self):
+        st = L.CupSolveStats()
+        L.check(L.lib().cup_poisson_solve(self.sim._h, C.byref(st)), self.sim._h, "PoissonSolverPeriodic")
+        return st
+
+    def solve_field(self, rhs) -> np.ndarray:
+        """Solves L_2h p = rhs / h^3 for an h^3-premultiplied rhs (nz, ny, nx)."""
+        r = _as_host_f64(rhs, self.sim.shape)
+        p = np.empty_like(r)
+        L.check(L.lib().cup_poisson_solve_field(self.sim._h, _ptr(r), _ptr(p), L.CUP_WHERE_HOST), self.sim._h)
+        return p
+
+
+@dataclass
+class StepStats:
+    dt: float
+    time: float
+    step: int
+    umax: float
+    kinetic_energy: float
+    force: np.ndarray
+    torque: np.ndarray
+    n_solves: int
+    rel_residual: float
+
+    @classmethod
+    def from_c(cls, s: L.CupStepStats) -> "StepStats":
+        return cls(s.dt, s.time, s.step, s.umax, s.kinetic_energy, np.array(s.force[:]), np.array(s.torque[:]),
+                   s.n_solves, s.rel_residual)
+
+
+class Simulation:
+    """Simulation (source/Simulation.cpp): owns one device handle."""
+
+    def __init__(self, sd: SimulationData):
+        self.sd = sd
+        cfg = sd.to_config()
+        h = C.c_void_p()
+        rc = L.lib().cup_create(C.byref(cfg), C.byref(h))
+        if rc != L.CUP_OK:
+            L.check(rc, None, "cup_create (see stderr for the reason)")
+        self._h = h
+        cells = (C.c_int * 3)()
+        hg = C.c_double()
+        L.lib().cup_get_dims(self._h, cells, C.byref(hg))
+        self.cells = tuple(cells[:])
+        self.h = hg.value
+        self.shape = (self.cells[2], self.cells[1], self.cells[0])
+        self.obstacles: List[Sphere] = []
+        self.pressureSolver = PoissonSolverPeriodic(self)
+        # pipeline of the periodic hot path (Simulation::setupOperators); the
+        # obstacle create/update operators are folded into add_obstacle and
+        # the forced-sphere no-op update.
+        self.pipeline: List[Operator] = [AdvectionDiffusion(self), PressureRHS(self), PressureProjection(self),
+                                         Penalization(self)]
+        self.step = 0
+        self.time = 0.0
+        self.dt = 0.0
+
+    # -- lifetime ------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().cup_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def sim(self) -> SimulationData:
+        return self.sd
+
+    def set_stream(self, stream_ptr: Optional[int]):
+        L.check(L.lib().cup_set_stream(self._h, C.c_void_p(stream_ptr or 0)), self._h, "set_stream")
+
+    def sync(self):
+        L.check(L.lib().cup_sync(self._h), self._h, "sync")
+
+    # -- obstacles -------------------------------------------------------------
+    def add_obstacle(self, obstacle):
+        if not isinstance(obstacle, Sphere):
+            raise ValueError(str(obstacle))
+        s = obstacle.to_struct()
+        L.check(L.lib().cup_add_sphere(self._h, C.byref(s)), self._h, "add_obstacle")
+        self.obstacles.append(obstacle)
+
+    def obstacle_state(self) -> dict:
+        f, t, c, u = (C.c_double * 3)(), (C.c_double * 3)(), (C.c_double * 3)(), (C.c_double * 3)()
+        L.check(L.lib().cup_get_obstacle_state(self._h, f, t, c, u), self._h, "obstacle_state")
+        return {"force": np.array(f[:]), "torque": np.array(t[:]), "com": np.array(c[:]), "uinf": np.array(u[:])}
+
+    # -- fields ----------------------------------------------------------------
+    def set_velocity(self, u, v, w):
+        if all(_is_torch_cuda(a) for a in (u, v, w)):
+            import torch
+            ts = [a.detach().to(torch.float64).contiguous() for a in (u, v, w)]
+            for t in ts:
+                if tuple(t.shape) != self.shape:
+                    raise ValueError(f"expected shape {self.shape}")
+            torch.cuda.current_stream().synchronize()
+            L.check(L.lib().cup_set_velocity(self._h, *[C.c_void_p(t.data_ptr()) for t in ts], L.CUP_WHERE_DEVICE),
+                    self._h, "set_velocity")
+            self.sync()
+            return
+        arrs = [_as_host_f64(a if not hasattr(a, "numpy") else a.detach().cpu().numpy(), self.shape) for a in (u, v, w)]
+        L.check(L.lib().cup_set_velocity(self._h, *[_ptr(a) for a in arrs], L.CUP_WHERE_HOST), self._h, "set_velocity")
+
+    def velocity(self) -> Tuple[np.ndarray, np.ndarray, np.ndarray]:
+        out = [np.empty(self.shape, dtype=np.float64) for _ in range(3)]
+        L.check(L.lib().cup_get_velocity(self._h, *[_ptr(a) for a in out], L.CUP_WHERE_HOST), self._h, "velocity")
+        return tuple(out)
+
+    def velocity_into(self, u, v, w):
+        """Copies the velocity into three FP64 CUDA torch tensors (device to device)."""
+        L.check(L.lib().cup_get_velocity(self._h, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
+                                         C.c_void_p(w.data_ptr()), L.CUP_WHERE_DEVICE), self._h, "velocity_into")
+
+    def _get1(self, fn, what) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        L.check(fn(self._h, _ptr(out), L.CUP_WHERE_HOST), self._h, what)
+        return out
+
+    def pressure(self) -> np.ndarray:
+        return self._get1(L.lib().cup_get_pressure, "pressure")
+
+    def chi(self) -> np.ndarray:
+        return self._get1(L.lib().cup_get_chi, "chi")
+
+    def rhs(self) -> np.ndarray:
+        return self._get1(L.lib().cup_get_rhs, "rhs")
+
+    # -- driver ------------------------------------------------------------------
+    def max_velocity(self) -> float:
+        m = C.c_double()
+        L.check(L.lib().cup_max_velocity(self._h, C.byref(m)), self._h, "max_velocity")
+        return m.value
+
+    def calcMaxTimestep(self) -> float:
+        dt = C.c_double()
+        L.check(L.lib().cup_calc_max_timestep(self._h, C.byref(dt)), self._h, "calcMaxTimestep")
+        self.dt = dt.value
+        return self.dt
+
+    def timestep(self, dt: float, stats: bool = True) -> Optional[StepStats]:
+        """Simulation::timestep (source/Simulation.cpp:593-623); returns True when finished."""
+        st = L.CupStepStats()
+        L.check(L.lib().cup_step(self._h, float(dt), C.byref(st) if stats else None), self._h, "timestep")
+        self.step += 1
+        self.time += dt
+        self.dt = dt
+        return StepStats.from_c(st) if stats else None
+
+    def run_steps(self, nsteps: int) -> StepStats:
+        """nsteps of calcMaxTimestep + timestep with dt chained on the device."""
+        st = L.CupStepStats()
+        L.check(L.lib().cup_run(self._h, int(nsteps), C.byref(st)), self._h, "run")
+        self.step, self.time, self.dt = st.step, st.time, st.dt
+        return StepStats.from_c(st)
+
+    def run(self) -> StepStats:
+        """Simulation::run (source/Simulation.cpp:582-591): until nsteps or endTime."""
+        if self.sd.nsteps <= 0 and self.sd.endTime <= 0:
+            raise ValueError("set nsteps or endTime before run()")
+        last = None
+        if self.sd.endTime <= 0:
+            return self.run_steps(self.sd.nsteps - self.step)
+        while True:
+            dt = self.calcMaxTimestep()
+            last = self.timestep(dt)
+            if (self.sd.endTime > 0 and self.time > self.sd.endTime) or (
+                    self.sd.nsteps != 0 and self.step >= self.sd.nsteps):
+                return last
+
+    def diagnostics(self) -> dict:
+        out = (C.c_double * 3)()
+        L.check(L.lib().cup_diagnostics(self._h, out), self._h, "diagnostics")
+        return {"ke": out[0], "div_l2": out[1], "div_max": out[2]}
+
+    def profile(self, on: bool = True):
+        L.check(L.lib().cup_profile_enable(self._h, int(on)), self._h, "profile")
+
+    def profile_report(self, reset: bool = True) -> dict:
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        L.check(L.lib().cup_profile_report(self._h, buf, len(buf), int(reset)), self._h, "profile_report")
+        return json.loads(buf.value.decode())
+
+    def launch_count(self) -> int:
+        n = C.c_longlong()
+        L.check(L.lib().cup_launch_count(self._h, C.byref(n)), self._h, "launch_count")
+        return n.value
+
+    def debug_shift(self, f, g: int, dx: int, dy: int, dz: int) -> np.ndarray:
+        a = _as_host_f64(f, self.shape)
+        out = np.empty_like(a)
+        L.check(L.lib().cup_debug_shift(self._h, _ptr(a), _ptr(out), g, dx, dy, dz, L.CUP_WHERE_HOST), self._h,
+                "debug_shift")
+        return out
+
+
+def blocks_to_global(blocks: np.ndarray, nx: int, ny: int, nz: int) -> np.ndarray:
+    b = np.ascontiguousarray(blocks, dtype=np.float64).ravel()
+    out = np.empty((nz, ny, nx), dtype=np.float64)
+    L.check(L.lib().cup_blocks_to_global(_ptr(b), _ptr(out), nx, ny, nz), None, "blocks_to_global")
+    return out
+
+
+def global_to_blocks(g: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(g, dtype=np.float64)
+    nz, ny, nx = a.shape
+    out = np.empty(a.size, dtype=np.float64)
+    L.check(L.lib().cup_global_to_blocks(_ptr(a), _ptr(out), nx, ny, nz), None, "global_to_blocks")
+    return out

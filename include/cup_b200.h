@@ -1,0 +1,183 @@
+/*
+ * cup_b200.h — C ABI of the B200-native fractional-step solver for a uniform
+ * periodic grid of 16^3-cell blocks (CubismUP_3D's hot path).
+ *
+ * The library owns all device memory of a simulation handle. Host pointers
+ * passed in are borrowed for the duration of the call; device pointers
+ * (CUP_WHERE_DEVICE) must stay valid until the call's work on the handle's
+ * stream has finished. Calls on one handle are stream-ordered and not
+ * re-entrant; different handles are independent. Every call returns a status
+ * code; cup_last_error() gives a message for the last failing call on a handle.
+ *
+ * Field layout everywhere: a dense array of nz*ny*nx values, x fastest, i.e.
+ * f[(z*ny + y)*nx + x] for the cell whose centre is ((x+.5)h, (y+.5)h, (z+.5)h).
+ * (The reference stores the same cells block-wise as FluidBlock data[z][y][x],
+ * source/Definitions.h:102-167; cup_blocks_to_global / cup_global_to_blocks
+ * convert between the two.)
+ */
+#ifndef CUP_B200_H
+#define CUP_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference aborts instead (source/SimulationData.cpp:180-226,
+ * source/poisson/PoissonSolverPeriodic.cpp:94-103, source/operators/Operator.h:40-46). */
+enum {
+  CUP_OK = 0,
+  CUP_ERR_ARG = 1,           /* invalid argument or unsupported configuration */
+  CUP_ERR_CUDA = 2,          /* a CUDA runtime call failed */
+  CUP_ERR_NONFINITE = 3,     /* NaN/Inf detected in a reduction */
+  CUP_ERR_NOT_CONVERGED = 4, /* defect correction hit max iterations */
+  CUP_ERR_STATE = 5,         /* call not valid in the handle's current state */
+  CUP_ERR_TIMEOUT = 6        /* a device-side wait ran past its time limit */
+};
+
+/* Storage / arithmetic form of a handle. */
+enum {
+  CUP_PREC_FP64 = 0,    /* FP64 storage and arithmetic throughout */
+  CUP_PREC_FP32_DC = 1  /* FP32 storage/advection, FP32 FFT inside FP64 defect correction */
+};
+
+/* Advection scheme. */
+enum {
+  CUP_SCHEME_REF = 0,         /* central 2nd order + explicit Euler: KernelAdvectDiffuse,
+                                 source/operators/AdvectionDiffusion.cpp:111-144 */
+  CUP_SCHEME_UPWIND3_RK2 = 1  /* 3rd-order upwind-biased advection + central diffusion, Heun RK2 */
+};
+
+enum { CUP_WHERE_HOST = 0, CUP_WHERE_DEVICE = 1 };
+
+/* Mirrors the hot-path subset of SimulationData (source/SimulationData.h:46-179).
+ * Only uniform periodic grids: BC*_flag = periodic, bUseFourierBC = true. */
+typedef struct cup_config {
+  int bpdx, bpdy, bpdz;   /* blocks per dimension (cells = 16*bpd); each a power of two, 16..256 cells */
+  double maxextent;       /* longest side; h = maxextent / max(cells)  (SimulationData.cpp:184-198) */
+  double nu;              /* kinematic viscosity */
+  double CFL;             /* Courant number (SimulationData.cpp:89) */
+  double lambda;          /* penalization coefficient (SimulationData.cpp:87) */
+  double DLM;             /* if > 0, lambda = DLM/dt each step (Simulation.cpp:418-419) */
+  double uinf[3];         /* frame velocity (SimulationData.cpp:90-92) */
+  int rampup;             /* CFL ramp-up steps (SimulationData.cpp:108) */
+  int bImplicitPenalization; /* SimulationData.cpp:73 */
+  int precision;          /* CUP_PREC_* */
+  int scheme;             /* CUP_SCHEME_* */
+  double dc_tol;          /* FP32_DC: relative FP64 residual tolerance (default 1e-10 if <= 0) */
+  int dc_max_iter;        /* FP32_DC: max correction solves per step (default 4 if <= 0) */
+  int dc_min_iter;        /* FP32_DC: solves always done per step (default 1 if <= 0) */
+  int device;             /* CUDA device ordinal */
+} cup_config;
+
+/* One sphere obstacle (source/obstacles/Sphere.cpp, ObstacleArguments in
+ * source/obstacles/Obstacle.h:60-75). Any forced dof blocks rotation
+ * (source/obstacles/Obstacle.cpp:131-137); free dofs are not supported. */
+typedef struct cup_sphere {
+  double radius;
+  double position[3];
+  double enforcedVelocity[3];
+  int bForcedInSimFrame[3];
+  int bFixFrameOfRef[3];
+} cup_sphere;
+
+typedef struct cup_solve_stats {
+  int n_solves;            /* Poisson solves done (FP32_DC: correction solves) */
+  double rel_residual;     /* final FP64 relative residual |b - L p| / |b| (FP32_DC), 0 for FP64 */
+} cup_solve_stats;
+
+typedef struct cup_step_stats {
+  double dt, time;
+  int step;
+  double umax;             /* max |u + uinf| after the step (next calcMaxTimestep input) */
+  double kinetic_energy;   /* sum h^3 |u|^2 / 2 after the step */
+  double force[3], torque[3]; /* penalization force / torque on the sphere */
+  int n_solves;
+  double rel_residual;
+} cup_step_stats;
+
+/* ---- lifetime (SimulationData ctor / Simulation ctor, source/Simulation.cpp:53-64) ---- */
+int cup_create(const cup_config* cfg, struct cup_handle** out);
+int cup_destroy(struct cup_handle* h);
+const char* cup_last_error(const struct cup_handle* h);
+/* Runs all subsequent work of the handle on this stream (cudaStream_t; NULL = the handle's own). */
+int cup_set_stream(struct cup_handle* h, void* stream);
+int cup_sync(struct cup_handle* h);
+int cup_get_dims(const struct cup_handle* h, int cells[3], double* hgrid);
+
+/* ---- fields ---- */
+/* where = CUP_WHERE_HOST or CUP_WHERE_DEVICE; arrays are FP64 (double). */
+int cup_set_velocity(struct cup_handle* h, const double* u, const double* v, const double* w, int where);
+int cup_get_velocity(struct cup_handle* h, double* u, double* v, double* w, int where);
+int cup_get_pressure(struct cup_handle* h, double* p, int where);
+int cup_get_chi(struct cup_handle* h, double* chi, int where);
+/* Pressure-RHS buffer (h^3 div u* / dt after PressureRHS), FP64 */
+int cup_get_rhs(struct cup_handle* h, double* rhs, int where);
+
+/* Block-structured <-> global layout (Cubism FluidBlock data[z][y][x] per block,
+ * blocks ordered x fastest): n = nx*ny*nz values. */
+int cup_blocks_to_global(const double* blocks, double* global, int nx, int ny, int nz);
+int cup_global_to_blocks(const double* global, double* blocks, int nx, int ny, int nz);
+
+/* ---- obstacles ---- */
+/* ObstacleVector::addObstacle (source/obstacles/ObstacleVector.h) for one sphere;
+ * then CreateObstacles (source/operators/ObstaclesCreate.cpp:444-540) and
+ * updateUinf (source/obstacles/ObstacleVector.h:60-76). At most one sphere. */
+int cup_add_sphere(struct cup_handle* h, const cup_sphere* s);
+/* Force / torque from the last Penalization (Penalization.cpp:101-123), centre of mass. */
+int cup_get_obstacle_state(struct cup_handle* h, double force[3], double torque[3], double com[3],
+                           double uinf[3]);
+
+/* ---- operators (source/operators/*.cpp; names as Operator::getName()) ---- */
+/* findMaxU (source/operators/ProcessHelpers.h:74-99) */
+int cup_max_velocity(struct cup_handle* h, double* umax);
+/* Simulation::calcMaxTimestep (source/Simulation.cpp:403-424) */
+int cup_calc_max_timestep(struct cup_handle* h, double* dt);
+/* AdvectionDiffusion::operator() (source/operators/AdvectionDiffusion.cpp:402-428) */
+int cup_advect_diffuse(struct cup_handle* h, double dt);
+/* PressureRHS::operator() (source/operators/PressureRHS.cpp:273-346) */
+int cup_pressure_rhs(struct cup_handle* h, double dt);
+/* PoissonSolverPeriodic::solve (source/poisson/PoissonSolverPeriodic.cpp:129-146) + _fftw2cub */
+int cup_poisson_solve(struct cup_handle* h, cup_solve_stats* stats);
+/* KernelGradP (source/operators/PressureProjection.cpp:38-50) */
+int cup_grad_correct(struct cup_handle* h, double dt);
+/* PressureProjection::operator() (source/operators/PressureProjection.cpp:107-129) */
+int cup_pressure_projection(struct cup_handle* h, double dt, cup_solve_stats* stats);
+/* Penalization::operator() (source/operators/Penalization.cpp:129-156) */
+int cup_penalize(struct cup_handle* h, double dt, double force_torque[6]);
+/* Simulation::timestep (source/Simulation.cpp:593-623): the hot-path pipeline with
+ * fused kernels. stats may be NULL (then no host synchronisation happens). */
+int cup_step(struct cup_handle* h, double dt, cup_step_stats* stats);
+/* Simulation::run (source/Simulation.cpp:582-591) for nsteps: calcMaxTimestep + timestep,
+ * with dt computed on the device (no host round trip per step). */
+int cup_run(struct cup_handle* h, int nsteps, cup_step_stats* stats);
+
+/* Stand-alone Poisson solve: p = (wide-Laplacian)^+ rhs / h^3 on the handle's grid
+ * (PoissonSolverPeriodic on an h^3-premultiplied RHS); rhs, p FP64. */
+int cup_poisson_solve_field(struct cup_handle* h, const double* rhs, double* p, int where);
+
+/* FP64 diagnostics of the current velocity: out[0] kinetic energy sum h^3|u|^2/2,
+ * out[1] L2 norm (sum h^3 div^2)^(1/2) of the central divergence, out[2] max |div|
+ * (ComputeDissipation.cpp:47-116 pattern, PoissonSolver.cpp:35-52 pattern). */
+int cup_diagnostics(struct cup_handle* h, double out[3]);
+
+/* Test hook for the halo staging (restates tests/cubismup3d/TestBoundaries.cpp):
+ * out(x) = f(x - d) through the same periodic plane-streaming TMA path the
+ * stencil kernels use, halo g in {1, 2}. f, out: device or host FP64 arrays. */
+int cup_debug_shift(struct cup_handle* h, const double* f, double* out, int g, int dx, int dy, int dz, int where);
+
+/* ---- profiling (the reference's Profiler regions, SimulationData.cpp:293-305,
+ * as CUDA-event ranges per kernel) ---- */
+/* Turns per-kernel CUDA-event timing on or off (off by default; no host sync while on). */
+int cup_profile_enable(struct cup_handle* h, int on);
+/* Writes {"kernel": {"count": n, "ms": total}, ...} as JSON into buf; reset != 0 clears the totals. */
+int cup_profile_report(struct cup_handle* h, char* buf, size_t len, int reset);
+/* Number of kernels this handle has launched so far. */
+int cup_launch_count(const struct cup_handle* h, long long* n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUP_B200_H */

@@ -1,0 +1,877 @@
+// ORACLE — test infrastructure only.
+//
+// A CPU FP64 restatement of CubismUP_3D's fractional-step time step on a
+// uniform periodic grid of 16^3-cell blocks. It is the checker for the CUDA
+// product path and the timed CPU baseline; the product never links or calls
+// it. Only tests/, __graft_entry__.smoke() and bench.py's CPU legs use it.
+//
+// Parity status:
+//   * periodic halo semantics (Cubism BlockLab, which is not in the reference
+//     snapshot) are pinned by a restatement of tests/cubismup3d/TestBoundaries.cpp
+//     (see orc_lab_shift and tests/test_oracle.py);
+//   * the FFT Poisson solve follows FFTW 3.3.7's published unnormalised DFT
+//     definition (third-party, absent here); it is pinned against numpy's
+//     pocketfft in tests/test_oracle.py and tests/golden/;
+//   * no outputs of the reference itself exist: it cannot be built in this
+//     image (MPI, FFTW-MPI, HDF5, GSL and the Cubism sources are absent).
+//
+// Every kernel cites the reference file:line it restates. Expression order
+// follows the reference so that rounding matches where the algorithm does.
+// Build: oracle/Makefile (g++ -O3 -march=x86-64-v3 -fopenmp, no -ffast-math,
+// -ffp-contract=off so results do not depend on FMA contraction).
+
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <string>
+#include <vector>
+#include <omp.h>
+
+namespace {
+
+constexpr int BS = 16;                 // CUP_BLOCK_SIZE (source/Definitions.h:27-29)
+typedef double Real;                   // source/Base.h:38-42
+constexpr Real EPS = std::numeric_limits<Real>::epsilon();
+constexpr int SURFDH = 1;              // source/ObstacleBlock.h:16
+
+struct Dims {
+  int nx, ny, nz;
+  size_t n() const { return (size_t)nx * ny * nz; }
+  size_t idx(int x, int y, int z) const { return ((size_t)z * ny + y) * nx + x; }
+  int bpd(int d) const { return (d == 0 ? nx : d == 1 ? ny : nz) / BS; }
+  int nblocks() const { return bpd(0) * bpd(1) * bpd(2); }
+};
+
+inline int wrap(int i, int n) { i %= n; return i < 0 ? i + n : i; }
+
+// One block of one scalar field plus a g-wide periodic halo, including edges
+// and corners (the "tensorial" fill). Replaces Cubism's BlockLab for periodic
+// boundaries: ghosts come from the neighbouring blocks with periodic wrap
+// (source/operators/Operator.h:112-170, source/Definitions.h:260-378).
+struct Lab {
+  int g = 1, W = BS + 2;
+  std::vector<Real> d;
+  void load(const Real* f, const Dims& D, int bx, int by, int bz, int g_) {
+    g = g_; W = BS + 2 * g;
+    d.resize((size_t)W * W * W);
+    const int x0 = bx * BS - g, y0 = by * BS - g, z0 = bz * BS - g;
+    for (int k = 0; k < W; ++k) {
+      const int z = wrap(z0 + k, D.nz);
+      for (int j = 0; j < W; ++j) {
+        const int y = wrap(y0 + j, D.ny);
+        const Real* row = f + D.idx(0, y, z);
+        Real* out = &d[((size_t)k * W + j) * W];
+        for (int i = 0; i < W; ++i) out[i] = row[wrap(x0 + i, D.nx)];
+      }
+    }
+  }
+  Real operator()(int ix, int iy, int iz) const {
+    return d[((size_t)(iz + g) * W + (iy + g)) * W + (ix + g)];
+  }
+};
+
+template <typename F>
+void for_each_block(const Dims& D, F&& f) {
+  const int nb = D.nblocks();
+  #pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; ++b) {
+    const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
+    f(bx, by, bz);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Complex radix-2 FFT on a contiguous line (unnormalised, FFTW sign
+// convention: forward e^{-2 pi i k n/N}, backward e^{+2 pi i k n/N}).
+// Twiddles are computed in long double on the host.
+struct FFTPlan {
+  int n = 0, logn = 0;
+  std::vector<std::complex<Real>> tw;  // e^{-2 pi i k/n}, k < n/2
+  std::vector<int> rev;
+  void init(int n_) {
+    n = n_; logn = 0;
+    while ((1 << logn) < n) ++logn;
+    tw.resize(n / 2 > 0 ? n / 2 : 1);
+    for (int k = 0; k < n / 2; ++k) {
+      const long double a = -2.0L * 3.141592653589793238462643383279502884L * k / n;
+      tw[k] = std::complex<Real>((Real)std::cos(a), (Real)std::sin(a));
+    }
+    rev.resize(n);
+    for (int i = 0; i < n; ++i) {
+      int r = 0;
+      for (int b = 0; b < logn; ++b) if (i & (1 << b)) r |= 1 << (logn - 1 - b);
+      rev[i] = r;
+    }
+  }
+  void exec(std::complex<Real>* a, int sign) const {
+    for (int i = 0; i < n; ++i) if (i < rev[i]) std::swap(a[i], a[rev[i]]);
+    for (int len = 2; len <= n; len <<= 1) {
+      const int half = len / 2, step = n / len;
+      for (int i = 0; i < n; i += len)
+        for (int j = 0; j < half; ++j) {
+          std::complex<Real> w = tw[j * step];
+          if (sign > 0) w = std::conj(w);
+          const std::complex<Real> t = w * a[i + j + half];
+          a[i + j + half] = a[i + j] - t;
+          a[i + j] = a[i + j] + t;
+        }
+    }
+  }
+};
+
+bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+// FFTW-layout buffer of the periodic Poisson solver:
+// data[x*stridex + y*stridey + z], stridez = 1, stridey = 2*nz_hat,
+// stridex = Ny*2*nz_hat (source/poisson/PoissonSolverPeriodic.cpp:108-116).
+struct PoissonBuffer {
+  Dims D;
+  int nz_hat;
+  size_t stridex, stridey, stridez;
+  std::vector<Real> data;
+  FFTPlan px, py, pz;
+  void init(const Dims& D_) {
+    D = D_;
+    nz_hat = D.nz / 2 + 1;
+    stridez = 1; stridey = 2 * (size_t)nz_hat; stridex = (size_t)D.ny * 2 * nz_hat;
+    data.assign((size_t)D.nx * stridex, 0.0);
+    px.init(D.nx); py.init(D.ny); pz.init(D.nz);
+  }
+  size_t dest(int x, int y, int z) const { return stridex * x + stridey * y + stridez * z; }
+  std::complex<Real>* cdata() { return reinterpret_cast<std::complex<Real>*>(data.data()); }
+  size_t cidx(int kx, int ky, int kz) const { return ((size_t)kx * D.ny + ky) * nz_hat + kz; }
+
+  // 3-D real-to-complex transform in place (FFTW r2c semantics; spectral
+  // layout here is [kx][ky][kz] — FFTW_MPI_TRANSPOSED_OUT's [ky][kx][kz]
+  // differs only in storage order, and _solve below indexes it accordingly).
+  void r2c() {
+    std::complex<Real>* c = cdata();
+    #pragma omp parallel
+    {
+      std::vector<std::complex<Real>> line(std::max({D.nx, D.ny, D.nz}));
+      #pragma omp for schedule(static) collapse(2)
+      for (int x = 0; x < D.nx; ++x)
+        for (int y = 0; y < D.ny; ++y) {
+          Real* r = &data[dest(x, y, 0)];
+          for (int z = 0; z < D.nz; ++z) line[z] = std::complex<Real>(r[z], 0.0);
+          pz.exec(line.data(), -1);
+          std::complex<Real>* o = c + cidx(x, y, 0);
+          for (int k = 0; k < nz_hat; ++k) o[k] = line[k];
+        }
+      #pragma omp for schedule(static) collapse(2)
+      for (int x = 0; x < D.nx; ++x)
+        for (int k = 0; k < nz_hat; ++k) {
+          for (int y = 0; y < D.ny; ++y) line[y] = c[cidx(x, y, k)];
+          py.exec(line.data(), -1);
+          for (int y = 0; y < D.ny; ++y) c[cidx(x, y, k)] = line[y];
+        }
+      #pragma omp for schedule(static) collapse(2)
+      for (int y = 0; y < D.ny; ++y)
+        for (int k = 0; k < nz_hat; ++k) {
+          for (int x = 0; x < D.nx; ++x) line[x] = c[cidx(x, y, k)];
+          px.exec(line.data(), -1);
+          for (int x = 0; x < D.nx; ++x) c[cidx(x, y, k)] = line[x];
+        }
+    }
+  }
+  // 3-D complex-to-real transform in place (FFTW c2r semantics, unnormalised).
+  void c2r() {
+    std::complex<Real>* c = cdata();
+    #pragma omp parallel
+    {
+      std::vector<std::complex<Real>> line(std::max({D.nx, D.ny, D.nz}));
+      #pragma omp for schedule(static) collapse(2)
+      for (int y = 0; y < D.ny; ++y)
+        for (int k = 0; k < nz_hat; ++k) {
+          for (int x = 0; x < D.nx; ++x) line[x] = c[cidx(x, y, k)];
+          px.exec(line.data(), +1);
+          for (int x = 0; x < D.nx; ++x) c[cidx(x, y, k)] = line[x];
+        }
+      #pragma omp for schedule(static) collapse(2)
+      for (int x = 0; x < D.nx; ++x)
+        for (int k = 0; k < nz_hat; ++k) {
+          for (int y = 0; y < D.ny; ++y) line[y] = c[cidx(x, y, k)];
+          py.exec(line.data(), +1);
+          for (int y = 0; y < D.ny; ++y) c[cidx(x, y, k)] = line[y];
+        }
+      #pragma omp for schedule(static) collapse(2)
+      for (int x = 0; x < D.nx; ++x)
+        for (int y = 0; y < D.ny; ++y) {
+          std::complex<Real>* h = c + cidx(x, y, 0);
+          for (int k = 0; k < nz_hat; ++k) line[k] = h[k];
+          for (int k = nz_hat; k < D.nz; ++k) line[k] = std::conj(h[D.nz - k]);
+          pz.exec(line.data(), +1);
+          Real* r = &data[dest(x, y, 0)];
+          for (int z = 0; z < D.nz; ++z) r[z] = line[z].real();
+        }
+    }
+  }
+};
+
+// PoissonSolverPeriodic::_solve, grid-consistent branch
+// (source/poisson/PoissonSolverPeriodic.cpp:15-61): spectral divide by the
+// eigenvalue of the wide (2h) Laplacian, then zero the 8 undefined modes.
+void poisson_solve(PoissonBuffer& B, Real h) {
+  B.r2c();
+  std::complex<Real>* in_out = B.cdata();
+  const size_t gsize[3] = {(size_t)B.D.nx, (size_t)B.D.ny, (size_t)B.D.nz};
+  const Real norm_factor = 4 / (gsize[0] * h * gsize[1] * gsize[2]);
+  const long nKx = (long)gsize[0], nKy = (long)gsize[1], nKz = (long)gsize[2];
+  const Real wFacX = 4 * M_PI / nKx, wFacY = 4 * M_PI / nKy, wFacZ = 4 * M_PI / nKz;
+  const long nz_hat = B.nz_hat;
+  #pragma omp parallel for schedule(static)
+  for (long j = 0; j < nKy; ++j)
+    for (long i = 0; i < nKx; ++i)
+      for (long k = 0; k < nz_hat; ++k) {
+        const size_t linidx = B.cidx((int)i, (int)j, (int)k);
+        const Real D = std::cos(wFacX * i) + std::cos(wFacY * j) + std::cos(wFacZ * k);
+        const Real solutionFactor = norm_factor / (2 * D - 6);
+        in_out[linidx] = std::complex<Real>(in_out[linidx].real() * solutionFactor,
+                                            in_out[linidx].imag() * solutionFactor);
+      }
+  const long lastI = nKx / 2, lastJ = nKy / 2, lastK = nKz / 2;
+  const long Is[2] = {0, lastI}, Js[2] = {0, lastJ}, Ks[2] = {0, lastK};
+  for (long a : Is) for (long b : Js) for (long c : Ks)
+    in_out[B.cidx((int)a, (int)b, (int)c)] = std::complex<Real>(0, 0);
+  B.c2r();
+}
+
+// ---------------------------------------------------------------------------
+// Simulation state (the subset of SimulationData on the hot path,
+// source/SimulationData.h:46-179) plus one optional sphere obstacle.
+struct Sphere {
+  Real radius = 0.1;
+  double position[3] = {0.5, 0.5, 0.5};
+  double transVel[3] = {0, 0, 0};
+  double angVel[3] = {0, 0, 0};
+  double centerOfMass[3] = {0, 0, 0};
+  bool bForcedInSimFrame[3] = {false, false, false};
+  bool bFixFrameOfRef[3] = {false, false, false};
+  double lambda_factor = 1.0;        // source/obstacles/Obstacle.h:106
+  double force[3] = {0, 0, 0}, torque[3] = {0, 0, 0};
+  std::vector<char> touched;         // obstacle block present (ObstacleBlock* != nullptr)
+  std::vector<Real> SDF, CHI;        // per cell, meaningful on touched blocks
+};
+
+}  // namespace
+
+extern "C" {
+
+typedef struct orc_config {
+  int nx, ny, nz;           // cells per dimension (multiples of 16, powers of two)
+  double maxextent;         // h = maxextent / max(nx, ny, nz)  (SimulationData.cpp:184-198)
+  double nu, CFL, lambda, DLM;
+  double uinf[3];
+  int rampup;
+  int implicit_penalization;
+  int scheme;               // 0: reference central2 + Euler, 1: upwind3 + RK2 (Heun)
+  int has_sphere;
+  double sphere_radius, sphere_position[3], sphere_velocity[3];
+  int sphere_forced[3], sphere_fix_frame[3];
+} orc_config;
+
+}  // extern "C"
+
+namespace {
+
+struct OState {
+  orc_config cfg;
+  Dims D;
+  Real h;
+  int step = 0;
+  double time = 0, dt = 0, lambda = 0, uMax_measured = 0;
+  double uinf[3];
+  std::vector<Real> u, v, w, p, chi, tmpU, tmpV, tmpW;
+  PoissonBuffer pois;
+  bool has_sphere = false;
+  Sphere sph;
+  double rhs_sums[3] = {0, 0, 0};
+  double corr = 0;
+};
+
+// findMaxU (source/operators/ProcessHelpers.h:74-99)
+double find_max_u(const OState& S) {
+  const Real uinf[3] = {S.uinf[0], S.uinf[1], S.uinf[2]};
+  Real maxU = 0;
+  const size_t n = S.D.n();
+  #pragma omp parallel for schedule(static) reduction(max : maxU)
+  for (size_t i = 0; i < n; ++i) {
+    const Real advu = std::fabs(S.u[i] + uinf[0]);
+    const Real advv = std::fabs(S.v[i] + uinf[1]);
+    const Real advw = std::fabs(S.w[i] + uinf[2]);
+    const Real maxUl = std::max({advu, advv, advw});
+    maxU = std::max(maxU, maxUl);
+  }
+  return maxU;
+}
+
+// KernelAdvectDiffuse (source/operators/AdvectionDiffusion.cpp:111-144):
+// central differences, explicit Euler; result into tmp.
+void advect_diffuse_ref(OState& S, double dt) {
+  const Dims D = S.D;
+  const Real h = S.h;
+  const Real mu = S.cfg.nu;
+  const Real uInf[3] = {S.uinf[0], S.uinf[1], S.uinf[2]};
+  for_each_block(D, [&](int bx, int by, int bz) {
+    Lab Lu, Lv, Lw;
+    Lu.load(S.u.data(), D, bx, by, bz, 1);
+    Lv.load(S.v.data(), D, bx, by, bz, 1);
+    Lw.load(S.w.data(), D, bx, by, bz, 1);
+    const Real facA = -dt / (2 * h);
+    const Real facD = (mu / h) * (dt / h);
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const Real Lu0 = Lu(ix, iy, iz), Lv0 = Lv(ix, iy, iz), Lw0 = Lw(ix, iy, iz);
+      const Real dudx = Lu(ix+1,iy,iz) - Lu(ix-1,iy,iz), dvdx = Lv(ix+1,iy,iz) - Lv(ix-1,iy,iz), dwdx = Lw(ix+1,iy,iz) - Lw(ix-1,iy,iz);
+      const Real dudy = Lu(ix,iy+1,iz) - Lu(ix,iy-1,iz), dvdy = Lv(ix,iy+1,iz) - Lv(ix,iy-1,iz), dwdy = Lw(ix,iy+1,iz) - Lw(ix,iy-1,iz);
+      const Real dudz = Lu(ix,iy,iz+1) - Lu(ix,iy,iz-1), dvdz = Lv(ix,iy,iz+1) - Lv(ix,iy,iz-1), dwdz = Lw(ix,iy,iz+1) - Lw(ix,iy,iz-1);
+      const Real uu = Lu0 + uInf[0], vv = Lv0 + uInf[1], ww = Lw0 + uInf[2];
+      const Real duD = Lu(ix,iy+1,iz) + Lu(ix,iy-1,iz) + Lu(ix+1,iy,iz) + Lu(ix-1,iy,iz) + Lu(ix,iy,iz-1) + Lu(ix,iy,iz+1) - Lu0 * 6;
+      const Real dvD = Lv(ix,iy+1,iz) + Lv(ix,iy-1,iz) + Lv(ix+1,iy,iz) + Lv(ix-1,iy,iz) + Lv(ix,iy,iz-1) + Lv(ix,iy,iz+1) - Lv0 * 6;
+      const Real dwD = Lw(ix,iy+1,iz) + Lw(ix,iy-1,iz) + Lw(ix+1,iy,iz) + Lw(ix-1,iy,iz) + Lw(ix,iy,iz-1) + Lw(ix,iy,iz+1) - Lw0 * 6;
+      const Real duA = uu * dudx + vv * dudy + ww * dudz;
+      const Real dvA = uu * dvdx + vv * dvdy + ww * dvdz;
+      const Real dwA = uu * dwdx + vv * dwdy + ww * dwdz;
+      const size_t o = D.idx(bx * BS + ix, by * BS + iy, bz * BS + iz);
+      S.tmpU[o] = Lu0 + facA * duA + facD * duD;
+      S.tmpV[o] = Lv0 + facA * dvA + facD * dvD;
+      S.tmpW[o] = Lw0 + facA * dwA + facD * dwD;
+    }
+  });
+}
+
+// Third-order upwind-biased first derivative times 6h, chosen by the sign of
+// the advecting velocity a: for a > 0 (2f_{+1} + 3f_0 - 6f_{-1} + f_{-2}),
+// otherwise (-f_{+2} + 6f_{+1} - 3f_0 - 2f_{-1}).
+inline Real up3(Real a, Real fm2, Real fm1, Real f0, Real fp1, Real fp2) {
+  return a > 0 ? (2 * fp1 + 3 * f0 - 6 * fm1 + fm2) : (-fp2 + 6 * fp1 - 3 * f0 - 2 * fm1);
+}
+
+// One explicit stage of upwind3 advection + central diffusion on the fields
+// (a,b,c); output[i] = base + facA*adv + facD*lap, where the stage form is
+//   stage 1: out = f + dt*A(f)
+//   stage 2: out = 0.5*(f0 + (f1 + dt*A(f1)))
+// This scheme is not in the reference snapshot (its KernelAdvectDiffuse is
+// central2 + Euler); it follows the same block/lab structure.
+void upwind3_stage(OState& S, double dt, const Real* a, const Real* b, const Real* c,
+                   const Real* base_u, const Real* base_v, const Real* base_w,
+                   Real* ou, Real* ov, Real* ow) {
+  const Dims D = S.D;
+  const Real h = S.h;
+  const Real mu = S.cfg.nu;
+  const Real uInf[3] = {S.uinf[0], S.uinf[1], S.uinf[2]};
+  const Real facA = -dt / (6 * h);
+  const Real facD = (mu / h) * (dt / h);
+  for_each_block(D, [&](int bx, int by, int bz) {
+    Lab L[3];
+    L[0].load(a, D, bx, by, bz, 2);
+    L[1].load(b, D, bx, by, bz, 2);
+    L[2].load(c, D, bx, by, bz, 2);
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const Real uu = L[0](ix, iy, iz) + uInf[0];
+      const Real vv = L[1](ix, iy, iz) + uInf[1];
+      const Real ww = L[2](ix, iy, iz) + uInf[2];
+      const size_t o = D.idx(bx * BS + ix, by * BS + iy, bz * BS + iz);
+      Real* outs[3] = {ou, ov, ow};
+      const Real* bases[3] = {base_u, base_v, base_w};
+      for (int q = 0; q < 3; ++q) {
+        const Lab& F = L[q];
+        const Real f0 = F(ix, iy, iz);
+        const Real dx = up3(uu, F(ix-2,iy,iz), F(ix-1,iy,iz), f0, F(ix+1,iy,iz), F(ix+2,iy,iz));
+        const Real dy = up3(vv, F(ix,iy-2,iz), F(ix,iy-1,iz), f0, F(ix,iy+1,iz), F(ix,iy+2,iz));
+        const Real dz = up3(ww, F(ix,iy,iz-2), F(ix,iy,iz-1), f0, F(ix,iy,iz+1), F(ix,iy,iz+2));
+        const Real lap = F(ix,iy+1,iz) + F(ix,iy-1,iz) + F(ix+1,iy,iz) + F(ix-1,iy,iz) + F(ix,iy,iz-1) + F(ix,iy,iz+1) - f0 * 6;
+        const Real adv = uu * dx + vv * dy + ww * dz;
+        const Real t = f0 + facA * adv + facD * lap;
+        outs[q][o] = bases[q] ? 0.5 * (bases[q][o] + t) : t;
+      }
+    }
+  });
+}
+
+void advect_diffuse_upwind3_rk2(OState& S, double dt) {
+  const size_t n = S.D.n();
+  std::vector<Real> u1(n), v1(n), w1(n);
+  upwind3_stage(S, dt, S.u.data(), S.v.data(), S.w.data(), nullptr, nullptr, nullptr,
+                u1.data(), v1.data(), w1.data());
+  upwind3_stage(S, dt, u1.data(), v1.data(), w1.data(), S.u.data(), S.v.data(), S.w.data(),
+                S.tmpU.data(), S.tmpV.data(), S.tmpW.data());
+}
+
+// AdvectionDiffusion::operator() (source/operators/AdvectionDiffusion.cpp:402-428):
+// kernel into tmp, then UpdateAndCorrectInflow_nonUniform copies tmp -> u
+// (:315-397); its inflow correction is inactive on periodic boundaries.
+void op_advection_diffusion(OState& S, double dt) {
+  if (S.cfg.scheme == 1) advect_diffuse_upwind3_rk2(S, dt);
+  else advect_diffuse_ref(S, dt);
+  std::copy(S.tmpU.begin(), S.tmpU.end(), S.u.begin());
+  std::copy(S.tmpV.begin(), S.tmpV.end(), S.v.begin());
+  std::copy(S.tmpW.begin(), S.tmpW.end(), S.w.begin());
+}
+
+// Signed distance of a sphere (source/obstacles/Sphere.cpp:44-48), positive inside.
+inline Real sphere_sdf(const Sphere& s, Real x, Real y, Real z) {
+  const Real dx = x - s.position[0], dy = y - s.position[1], dz = z - s.position[2];
+  return s.radius - std::sqrt(dx * dx + dy * dy + dz * dz);
+}
+
+// CreateObstacles for one sphere (source/operators/ObstaclesCreate.cpp:444-540):
+// reset chi=0, tmpU=-1; SDF fill on touching blocks (source/obstacles/Sphere.cpp:19-49,
+// source/obstacles/extra/ObstacleLibrary.h:45-62); characteristic function
+// (ObstaclesCreate.cpp:51-136); grid centre of mass (:230-256).
+void op_create_obstacles(OState& S) {
+  if (!S.has_sphere) return;
+  const Dims D = S.D;
+  const Real h = S.h;
+  Sphere& s = S.sph;
+  std::fill(S.chi.begin(), S.chi.end(), 0.0);
+  std::fill(S.tmpU.begin(), S.tmpU.end(), -1.0);
+  // updateUinf (source/obstacles/ObstacleVector.h:60-76) and Obstacle::update
+  // position advection (source/obstacles/Obstacle.cpp:314-321).
+  for (int d = 0; d < 3; ++d) S.uinf[d] = s.bFixFrameOfRef[d] ? -s.transVel[d] : 0.0;
+  for (int d = 0; d < 3; ++d) s.position[d] += S.dt * (s.transVel[d] + S.uinf[d]);
+  const Real safety = (2 + SURFDH) * h;
+  const Real box[3][2] = {
+    {(Real)s.position[0] - (s.radius + safety), (Real)s.position[0] + (s.radius + safety)},
+    {(Real)s.position[1] - (s.radius + safety), (Real)s.position[1] + (s.radius + safety)},
+    {(Real)s.position[2] - (s.radius + safety), (Real)s.position[2] + (s.radius + safety)}};
+  const int nb = D.nblocks();
+  s.touched.assign(nb, 0);
+  s.SDF.assign(D.n(), 0.0);
+  s.CHI.assign(D.n(), 0.0);
+  for (int b = 0; b < nb; ++b) {
+    const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
+    const int bi[3] = {bx, by, bz};
+    bool touch = true;
+    for (int d = 0; d < 3; ++d) {
+      const Real minp = (bi[d] * BS + 0.5) * h, maxp = (bi[d] * BS + BS - 1 + 0.5) * h;
+      const Real lo = std::max(minp, box[d][0]), hi = std::min(maxp, box[d][1]);
+      if (!(hi - lo > 0)) touch = false;
+    }
+    s.touched[b] = touch;
+    if (!touch) continue;
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const int gx = bx * BS + ix, gy = by * BS + iy, gz = bz * BS + iz;
+      const Real dist = sphere_sdf(s, (gx + 0.5) * h, (gy + 0.5) * h, (gz + 0.5) * h);
+      const size_t o = D.idx(gx, gy, gz);
+      s.SDF[o] = dist;
+      S.tmpU[o] = std::max(dist, S.tmpU[o]);
+    }
+  }
+  const Real inv2h = .5 / h, vol = h * h * h;
+  double com[4] = {0, 0, 0, 0};
+  for (int b = 0; b < nb; ++b) {
+    if (!s.touched[b]) continue;
+    const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
+    Lab L;
+    L.load(S.tmpU.data(), D, bx, by, bz, 1);
+    double m = 0, cx = 0, cy = 0, cz = 0;
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const int gx = bx * BS + ix, gy = by * BS + iy, gz = bz * BS + iz;
+      const size_t o = D.idx(gx, gy, gz);
+      const Real sdf = s.SDF[o];
+      Real chi;
+      if (sdf > +2 * h || sdf < -2 * h) {
+        chi = sdf > 0 ? 1 : 0;
+      } else {
+        const Real distPx = L(ix+1,iy,iz), distMx = L(ix-1,iy,iz);
+        const Real distPy = L(ix,iy+1,iz), distMy = L(ix,iy-1,iz);
+        const Real distPz = L(ix,iy,iz+1), distMz = L(ix,iy,iz-1);
+        const Real gradUX = inv2h * (distPx - distMx);
+        const Real gradUY = inv2h * (distPy - distMy);
+        const Real gradUZ = inv2h * (distPz - distMz);
+        const Real gradUSq = gradUX * gradUX + gradUY * gradUY + gradUZ * gradUZ + EPS;
+        const Real IplusX = distPx < 0 ? 0 : distPx, IminuX = distMx < 0 ? 0 : distMx;
+        const Real IplusY = distPy < 0 ? 0 : distPy, IminuY = distMy < 0 ? 0 : distMy;
+        const Real IplusZ = distPz < 0 ? 0 : distPz, IminuZ = distMz < 0 ? 0 : distMz;
+        const Real gradIX = inv2h * (IplusX - IminuX);
+        const Real gradIY = inv2h * (IplusY - IminuY);
+        const Real gradIZ = inv2h * (IplusZ - IminuZ);
+        const Real numH = gradIX * gradUX + gradIY * gradUY + gradIZ * gradUZ;
+        chi = numH / gradUSq;
+      }
+      s.CHI[o] = chi;
+      S.chi[o] = std::max(chi, S.chi[o]);
+      const Real p[3] = {(gx + 0.5) * h, (gy + 0.5) * h, (gz + 0.5) * h};
+      cx += chi * vol * p[0]; cy += chi * vol * p[1]; cz += chi * vol * p[2];
+      m += chi * vol;
+    }
+    com[0] += m; com[1] += cx; com[2] += cy; com[3] += cz;
+  }
+  s.centerOfMass[0] = com[1] / com[0];
+  s.centerOfMass[1] = com[2] / com[0];
+  s.centerOfMass[2] = com[3] / com[0];
+}
+
+// PressureRHS::operator() (source/operators/PressureRHS.cpp:273-346), uniform grid:
+// KernelPressureRHS (:51-76), obstacle visitor (:78-112), correction factors
+// (:331-334) and KernelFinalizePerimeters (:215-256).
+void op_pressure_rhs(OState& S, double dt) {
+  const Dims D = S.D;
+  const Real h = S.h;
+  PoissonBuffer& P = S.pois;
+  std::fill(P.data.begin(), P.data.end(), 0.0);   // reset() (PoissonSolver.cpp:132-135)
+  const Real fac = 0.5 * h * h / dt;
+  for_each_block(D, [&](int bx, int by, int bz) {
+    Lab Lu, Lv, Lw;
+    Lu.load(S.u.data(), D, bx, by, bz, 1);
+    Lv.load(S.v.data(), D, bx, by, bz, 1);
+    Lw.load(S.w.data(), D, bx, by, bz, 1);
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix)
+      P.data[P.dest(bx * BS + ix, by * BS + iy, bz * BS + iz)] =
+          fac * (Lu(ix+1,iy,iz) - Lu(ix-1,iy,iz) + Lv(ix,iy+1,iz) - Lv(ix,iy-1,iz) + Lw(ix,iy,iz+1) - Lw(ix,iy,iz-1));
+  });
+  S.rhs_sums[0] = S.rhs_sums[1] = S.rhs_sums[2] = 0;
+  S.corr = 0;
+  if (!S.has_sphere) return;
+  const Sphere& s = S.sph;
+  std::vector<char> touchSurf(D.n(), 0);
+  double sumRHS = 0, posRHS = 0, negRHS = 0;
+  const int nb = D.nblocks();
+  #pragma omp parallel for schedule(static) reduction(+ : sumRHS, posRHS, negRHS)
+  for (int b = 0; b < nb; ++b) {
+    if (!s.touched[b]) continue;
+    const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
+    Lab Lc;
+    Lc.load(S.chi.data(), D, bx, by, bz, 1);
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const int gx = bx * BS + ix, gy = by * BS + iy, gz = bz * BS + iz;
+      const size_t o = D.idx(gx, gy, gz);
+      if (Lc(ix, iy, iz) > s.CHI[o]) continue;
+      const size_t idx = P.dest(gx, gy, gz);
+      const Real dXx = Lc(ix+1,iy,iz) - Lc(ix-1,iy,iz);
+      const Real dXy = Lc(ix,iy+1,iz) - Lc(ix,iy-1,iz);
+      const Real dXz = Lc(ix,iy,iz+1) - Lc(ix,iy,iz-1);
+      const bool bSurface = dXx * dXx + dXy * dXy + dXz * dXz > 0;
+      if (bSurface) touchSurf[o] = 1;
+      const Real srcBulk = -s.CHI[o] * P.data[idx];
+      sumRHS += srcBulk;
+      P.data[idx] += srcBulk;
+      posRHS += bSurface * P.data[idx] * (P.data[idx] > 0);
+      negRHS -= bSurface * P.data[idx] * (P.data[idx] < 0);
+    }
+  }
+  const double corrDenom = sumRHS > 0 ? posRHS : negRHS;
+  const double corr = sumRHS / std::max(corrDenom, (double)EPS);
+  S.rhs_sums[0] = sumRHS; S.rhs_sums[1] = posRHS; S.rhs_sums[2] = negRHS;
+  S.corr = corr;
+  #pragma omp parallel for schedule(static)
+  for (int b = 0; b < nb; ++b) {
+    if (!s.touched[b]) continue;
+    const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const int gx = bx * BS + ix, gy = by * BS + iy, gz = bz * BS + iz;
+      if (!touchSurf[D.idx(gx, gy, gz)]) continue;
+      Real& r = P.data[P.dest(gx, gy, gz)];
+      if (r > 0 and corr > 0) r -= corr * r;
+      else if (r < 0 and corr < 0) r += corr * r;
+    }
+  }
+}
+
+// PressureProjection::operator() (source/operators/PressureProjection.cpp:107-129):
+// solve, _fftw2cub (source/poisson/PoissonSolver.cpp:116-130), KernelGradP (:38-50).
+void op_pressure_projection(OState& S, double dt) {
+  const Dims D = S.D;
+  const Real h = S.h;
+  poisson_solve(S.pois, h);
+  #pragma omp parallel for schedule(static)
+  for (int z = 0; z < D.nz; ++z)
+    for (int y = 0; y < D.ny; ++y)
+      for (int x = 0; x < D.nx; ++x) S.p[D.idx(x, y, z)] = S.pois.data[S.pois.dest(x, y, z)];
+  const Real fac = -0.5 * dt / h;
+  for_each_block(D, [&](int bx, int by, int bz) {
+    Lab Lp;
+    Lp.load(S.p.data(), D, bx, by, bz, 1);
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const size_t o = D.idx(bx * BS + ix, by * BS + iy, bz * BS + iz);
+      S.u[o] += fac * (Lp(ix+1,iy,iz) - Lp(ix-1,iy,iz));
+      S.v[o] += fac * (Lp(ix,iy+1,iz) - Lp(ix,iy-1,iz));
+      S.w[o] += fac * (Lp(ix,iy,iz+1) - Lp(ix,iy,iz-1));
+    }
+  });
+}
+
+// UpdateObstacles for a sphere with every translational dof forced: all rotation
+// blocked (source/obstacles/Obstacle.cpp:131-137), translational velocity kept
+// at the imposed value and angular velocity zero (:153-264). Free dofs are out
+// of scope for this oracle.
+void op_update_obstacles(OState&) {}
+
+// Penalization::operator() (source/operators/Penalization.cpp:129-156):
+// KernelPenalization<implicit> (:40-98) + KernelFinalizePenalizationForce (:101-123).
+void op_penalization(OState& S, double dt) {
+  if (!S.has_sphere) return;
+  const Dims D = S.D;
+  const Real h = S.h;
+  Sphere& s = S.sph;
+  const bool implicitPen = S.cfg.implicit_penalization != 0;
+  const double lambda = S.lambda, invdt = 1.0 / dt;
+  const std::array<double, 3> CM = {s.centerOfMass[0], s.centerOfMass[1], s.centerOfMass[2]};
+  const std::array<double, 3> vel = {s.transVel[0], s.transVel[1], s.transVel[2]};
+  const std::array<double, 3> omega = {s.angVel[0], s.angVel[1], s.angVel[2]};
+  const Real dv = std::pow(h, 3);
+  const double lambdaFac = s.lambda_factor * (implicitPen ? lambda : invdt);
+  double M[6] = {0, 0, 0, 0, 0, 0};
+  const int nb = D.nblocks();
+  #pragma omp parallel for schedule(static) reduction(+ : M[:6])
+  for (int b = 0; b < nb; ++b) {
+    if (!s.touched[b]) continue;
+    const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
+    double FX = 0, FY = 0, FZ = 0, TX = 0, TY = 0, TZ = 0;
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const int gx = bx * BS + ix, gy = by * BS + iy, gz = bz * BS + iz;
+      const size_t o = D.idx(gx, gy, gz);
+      if (S.chi[o] > s.CHI[o]) continue;
+      if (s.CHI[o] <= 0) continue;
+      double p[3] = {(gx + 0.5) * h, (gy + 0.5) * h, (gz + 0.5) * h};
+      p[0] -= CM[0]; p[1] -= CM[1]; p[2] -= CM[2];
+      const double X = s.CHI[o], U_TOT[3] = {
+          vel[0] + omega[1] * p[2] - omega[2] * p[1],
+          vel[1] + omega[2] * p[0] - omega[0] * p[2],
+          vel[2] + omega[0] * p[1] - omega[1] * p[0]};
+      const Real penalFac = implicitPen ? X * lambdaFac / (1 + lambdaFac * dt * X) : X * lambdaFac;
+      const Real FPX = penalFac * (U_TOT[0] - S.u[o]);
+      const Real FPY = penalFac * (U_TOT[1] - S.v[o]);
+      const Real FPZ = penalFac * (U_TOT[2] - S.w[o]);
+      S.u[o] = S.u[o] + dt * FPX;
+      S.v[o] = S.v[o] + dt * FPY;
+      S.w[o] = S.w[o] + dt * FPZ;
+      FX += dv * FPX; FY += dv * FPY; FZ += dv * FPZ;
+      TX += dv * (p[1] * FPZ - p[2] * FPY);
+      TY += dv * (p[2] * FPX - p[0] * FPZ);
+      TZ += dv * (p[0] * FPY - p[1] * FPX);
+    }
+    M[0] += FX; M[1] += FY; M[2] += FZ; M[3] += TX; M[4] += TY; M[5] += TZ;
+  }
+  for (int d = 0; d < 3; ++d) { s.force[d] = M[d]; s.torque[d] = M[3 + d]; }
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_num_threads(void) { return omp_get_max_threads(); }
+void orc_set_num_threads(int n) { if (n > 0) omp_set_num_threads(n); }
+
+void* orc_create(const orc_config* cfg) {
+  if (!cfg) return nullptr;
+  const int N[3] = {cfg->nx, cfg->ny, cfg->nz};
+  for (int d = 0; d < 3; ++d)
+    if (N[d] < BS || N[d] % BS || !is_pow2(N[d])) return nullptr;
+  OState* S = new OState();
+  S->cfg = *cfg;
+  S->D = Dims{cfg->nx, cfg->ny, cfg->nz};
+  const double maxbpd = std::max({(double)N[0], (double)N[1], (double)N[2]});
+  S->h = cfg->maxextent / maxbpd;
+  S->lambda = cfg->lambda;
+  for (int d = 0; d < 3; ++d) S->uinf[d] = cfg->uinf[d];
+  const size_t n = S->D.n();
+  for (auto* f : {&S->u, &S->v, &S->w, &S->p, &S->chi, &S->tmpU, &S->tmpV, &S->tmpW}) f->assign(n, 0.0);
+  S->pois.init(S->D);
+  if (cfg->has_sphere) {
+    S->has_sphere = true;
+    Sphere& s = S->sph;
+    s.radius = cfg->sphere_radius;
+    for (int d = 0; d < 3; ++d) {
+      s.position[d] = cfg->sphere_position[d];
+      s.bForcedInSimFrame[d] = cfg->sphere_forced[d] != 0;
+      s.bFixFrameOfRef[d] = cfg->sphere_fix_frame[d] != 0;
+      if (s.bForcedInSimFrame[d]) s.transVel[d] = cfg->sphere_velocity[d];
+    }
+    // Initial CreateObstacles call with dt = 0 (source/Simulation.cpp:399-400).
+    S->dt = 0;
+    op_create_obstacles(*S);
+  }
+  return S;
+}
+
+void orc_destroy(void* h) { delete static_cast<OState*>(h); }
+
+double orc_h(void* h) { return static_cast<OState*>(h)->h; }
+
+void orc_set_velocity(void* hdl, const double* u, const double* v, const double* w) {
+  OState* S = static_cast<OState*>(hdl);
+  const size_t n = S->D.n();
+  std::copy(u, u + n, S->u.begin());
+  std::copy(v, v + n, S->v.begin());
+  std::copy(w, w + n, S->w.begin());
+}
+
+// which: 0 u, 1 v, 2 w, 3 p, 4 chi, 5 tmpU, 6 tmpV, 7 tmpW, 8 rhs (buffer, unpadded view)
+void orc_get_field(void* hdl, int which, double* out) {
+  OState* S = static_cast<OState*>(hdl);
+  const Dims D = S->D;
+  const std::vector<Real>* f = nullptr;
+  switch (which) {
+    case 0: f = &S->u; break; case 1: f = &S->v; break; case 2: f = &S->w; break;
+    case 3: f = &S->p; break; case 4: f = &S->chi; break;
+    case 5: f = &S->tmpU; break; case 6: f = &S->tmpV; break; case 7: f = &S->tmpW; break;
+    case 8:
+      for (int z = 0; z < D.nz; ++z) for (int y = 0; y < D.ny; ++y) for (int x = 0; x < D.nx; ++x)
+        out[D.idx(x, y, z)] = S->pois.data[S->pois.dest(x, y, z)];
+      return;
+    default: return;
+  }
+  std::copy(f->begin(), f->end(), out);
+}
+
+// Simulation::calcMaxTimestep (source/Simulation.cpp:403-424).
+double orc_calc_max_timestep(void* hdl) {
+  OState* S = static_cast<OState*>(hdl);
+  const double hMin = S->h, CFL = S->cfg.CFL;
+  S->uMax_measured = find_max_u(*S);
+  const double dtDif = hMin * hMin / S->cfg.nu;
+  const double dtAdv = hMin / (S->uMax_measured + 1e-8);
+  S->dt = CFL * std::min(dtDif, dtAdv);
+  if (S->step < S->cfg.rampup) {
+    const double x = (S->step + 1.0) / S->cfg.rampup;
+    const double rampCFL = std::exp(std::log(1e-3) * (1 - x) + std::log(CFL) * x);
+    S->dt = rampCFL * std::min(dtDif, dtAdv);
+  }
+  if (S->cfg.DLM > 0) S->lambda = S->cfg.DLM / S->dt;
+  return S->dt;
+}
+
+double orc_max_u(void* hdl) { return find_max_u(*static_cast<OState*>(hdl)); }
+
+// Pipeline operators by reference name (source/Simulation.cpp:307-401).
+int orc_operator(void* hdl, const char* name, double dt) {
+  OState* S = static_cast<OState*>(hdl);
+  S->dt = dt;
+  const std::string n(name);
+  if (n == "CreateObstacles") op_create_obstacles(*S);
+  else if (n == "AdvectionDiffusion") op_advection_diffusion(*S, dt);
+  else if (n == "PressureRHS") op_pressure_rhs(*S, dt);
+  else if (n == "PressureProjection") op_pressure_projection(*S, dt);
+  else if (n == "UpdateObstacles") op_update_obstacles(*S);
+  else if (n == "Penalization") op_penalization(*S, dt);
+  else return 1;
+  return 0;
+}
+
+// Simulation::timestep (source/Simulation.cpp:593-623) over the hot-path pipeline.
+void orc_timestep(void* hdl, double dt) {
+  OState* S = static_cast<OState*>(hdl);
+  S->dt = dt;
+  if (S->has_sphere) op_create_obstacles(*S);
+  op_advection_diffusion(*S, dt);
+  op_pressure_rhs(*S, dt);
+  op_pressure_projection(*S, dt);
+  op_update_obstacles(*S);
+  op_penalization(*S, dt);
+  S->step++;
+  S->time += dt;
+}
+
+// Runs nsteps of calcMaxTimestep + timestep; writes the dt sequence if dts != NULL.
+// If fixed_dts != NULL, replays that dt sequence instead of calcMaxTimestep.
+void orc_run(void* hdl, int nsteps, const double* fixed_dts, double* dts) {
+  OState* S = static_cast<OState*>(hdl);
+  for (int i = 0; i < nsteps; ++i) {
+    double dt;
+    if (fixed_dts) {
+      orc_calc_max_timestep(hdl);
+      dt = fixed_dts[i];
+      S->dt = dt;
+      if (S->cfg.DLM > 0) S->lambda = S->cfg.DLM / dt;
+    } else {
+      dt = orc_calc_max_timestep(hdl);
+    }
+    if (dts) dts[i] = dt;
+    orc_timestep(hdl, dt);
+  }
+}
+
+// stats: [0..2] force, [3..5] torque, [6] time, [7] step, [8..10] uinf,
+// [11] dt, [12] lambda, [13..15] centre of mass, [16..18] rhs sums, [19] corr, [20] uMax
+void orc_get_stats(void* hdl, double* out) {
+  OState* S = static_cast<OState*>(hdl);
+  for (int d = 0; d < 3; ++d) { out[d] = S->sph.force[d]; out[3 + d] = S->sph.torque[d]; }
+  out[6] = S->time; out[7] = S->step;
+  for (int d = 0; d < 3; ++d) out[8 + d] = S->uinf[d];
+  out[11] = S->dt; out[12] = S->lambda;
+  for (int d = 0; d < 3; ++d) out[13 + d] = S->sph.centerOfMass[d];
+  for (int d = 0; d < 3; ++d) out[16 + d] = S->rhs_sums[d];
+  out[19] = S->corr; out[20] = S->uMax_measured;
+}
+
+// Stand-alone periodic Poisson solve of rhs (premultiplied by h^3, as the
+// reference's PressureRHS leaves it) -> p, through the FFTW-layout buffer.
+int orc_poisson_solve_field(int nx, int ny, int nz, double h, const double* rhs, double* p) {
+  const int N[3] = {nx, ny, nz};
+  for (int d = 0; d < 3; ++d) if (N[d] < 2 || !is_pow2(N[d])) return 1;
+  PoissonBuffer B;
+  Dims D{nx, ny, nz};
+  B.init(D);
+  for (int z = 0; z < nz; ++z) for (int y = 0; y < ny; ++y) for (int x = 0; x < nx; ++x)
+    B.data[B.dest(x, y, z)] = rhs[D.idx(x, y, z)];
+  poisson_solve(B, h);
+  for (int z = 0; z < nz; ++z) for (int y = 0; y < ny; ++y) for (int x = 0; x < nx; ++x)
+    p[D.idx(x, y, z)] = B.data[B.dest(x, y, z)];
+  return 0;
+}
+
+// Restatement of tests/cubismup3d/TestBoundaries.cpp:19-52: through a periodic
+// lab of halo g, out(cell) = lab(-dx,-dy,-dz) of f.
+int orc_lab_shift(const double* f, double* out, int nx, int ny, int nz, int g, int dx, int dy, int dz) {
+  Dims D{nx, ny, nz};
+  if (nx % BS || ny % BS || nz % BS) return 1;
+  if (std::abs(dx) > g || std::abs(dy) > g || std::abs(dz) > g) return 1;
+  for_each_block(D, [&](int bx, int by, int bz) {
+    Lab L;
+    L.load(f, D, bx, by, bz, g);
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix)
+      out[D.idx(bx * BS + ix, by * BS + iy, bz * BS + iz)] = L(ix - dx, iy - dy, iz - dz);
+  });
+  return 0;
+}
+
+// FP64 diagnostics: [0] kinetic energy sum h^3 |u|^2 / 2
+// (source/operators/ComputeDissipation.cpp:47-116 pattern), [1] L2 norm of the
+// central divergence (sum h^3 div^2)^(1/2), [2] max |div|.
+void orc_diagnostics(void* hdl, double* out) {
+  OState* S = static_cast<OState*>(hdl);
+  const Dims D = S->D;
+  const Real h = S->h, h3 = h * h * h, inv2h = 0.5 / h;
+  double ke = 0, d2 = 0, dmax = 0;
+  #pragma omp parallel for schedule(static) reduction(+ : ke, d2) reduction(max : dmax)
+  for (int z = 0; z < D.nz; ++z)
+    for (int y = 0; y < D.ny; ++y)
+      for (int x = 0; x < D.nx; ++x) {
+        const size_t o = D.idx(x, y, z);
+        ke += 0.5 * h3 * (S->u[o] * S->u[o] + S->v[o] * S->v[o] + S->w[o] * S->w[o]);
+        const double div = inv2h * (S->u[D.idx(wrap(x + 1, D.nx), y, z)] - S->u[D.idx(wrap(x - 1, D.nx), y, z)] +
+                                    S->v[D.idx(x, wrap(y + 1, D.ny), z)] - S->v[D.idx(x, wrap(y - 1, D.ny), z)] +
+                                    S->w[D.idx(x, y, wrap(z + 1, D.nz))] - S->w[D.idx(x, y, wrap(z - 1, D.nz))]);
+        d2 += h3 * div * div;
+        dmax = std::max(dmax, std::fabs(div));
+      }
+  out[0] = ke; out[1] = std::sqrt(d2); out[2] = dmax;
+}
+
+}  // extern "C"

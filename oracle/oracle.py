@@ -1,0 +1,198 @@
+"""ORACLE — test infrastructure only.
+
+ctypes binding of ``oracle/liboracle.so``, the CPU FP64 restatement of
+CubismUP_3D's periodic fractional-step time step (see ``cup_oracle.cpp`` for
+the reference file:line of every kernel and for the parity status). Only the
+tests, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU legs import this
+module; the product package never does.
+
+Fields are numpy float64 arrays of shape (nz, ny, nx), x fastest, the same
+global layout the CUDA library uses.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    """Compile liboracle.so with the committed Makefile (gcc + OpenMP)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+class OrcConfig(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+        ("maxextent", C.c_double),
+        ("nu", C.c_double), ("CFL", C.c_double), ("lambda_", C.c_double), ("DLM", C.c_double),
+        ("uinf", C.c_double * 3),
+        ("rampup", C.c_int),
+        ("implicit_penalization", C.c_int),
+        ("scheme", C.c_int),
+        ("has_sphere", C.c_int),
+        ("sphere_radius", C.c_double),
+        ("sphere_position", C.c_double * 3),
+        ("sphere_velocity", C.c_double * 3),
+        ("sphere_forced", C.c_int * 3),
+        ("sphere_fix_frame", C.c_int * 3),
+    ]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        L.orc_create.argtypes = [C.POINTER(OrcConfig)]
+        L.orc_create.restype = C.c_void_p
+        L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_h.argtypes = [C.c_void_p]
+        L.orc_h.restype = C.c_double
+        L.orc_set_velocity.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_get_field.argtypes = [C.c_void_p, C.c_int, dp]
+        L.orc_calc_max_timestep.argtypes = [C.c_void_p]
+        L.orc_calc_max_timestep.restype = C.c_double
+        L.orc_max_u.argtypes = [C.c_void_p]
+        L.orc_max_u.restype = C.c_double
+        L.orc_operator.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
+        L.orc_operator.restype = C.c_int
+        L.orc_timestep.argtypes = [C.c_void_p, C.c_double]
+        L.orc_run.argtypes = [C.c_void_p, C.c_int, dp, dp]
+        L.orc_get_stats.argtypes = [C.c_void_p, dp]
+        L.orc_poisson_solve_field.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, dp, dp]
+        L.orc_poisson_solve_field.restype = C.c_int
+        L.orc_lab_shift.argtypes = [dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.orc_lab_shift.restype = C.c_int
+        L.orc_diagnostics.argtypes = [C.c_void_p, dp]
+        L.orc_num_threads.restype = C.c_int
+        L.orc_set_num_threads.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+FIELDS = {"u": 0, "v": 1, "w": 2, "p": 3, "chi": 4, "tmpU": 5, "tmpV": 6, "tmpW": 7, "rhs": 8}
+
+
+class OracleSim:
+    """One oracle simulation (the hot-path subset of SimulationData + pipeline)."""
+
+    def __init__(self, nx, ny, nz, maxextent, nu, CFL=0.1, lambda_=1e6, DLM=0.0,
+                 uinf=(0.0, 0.0, 0.0), rampup=0, implicit_penalization=True, scheme="ref",
+                 sphere=None):
+        cfg = OrcConfig()
+        cfg.nx, cfg.ny, cfg.nz = nx, ny, nz
+        cfg.maxextent = maxextent
+        cfg.nu, cfg.CFL, cfg.lambda_, cfg.DLM = nu, CFL, lambda_, DLM
+        cfg.uinf[:] = list(uinf)
+        cfg.rampup = rampup
+        cfg.implicit_penalization = int(bool(implicit_penalization))
+        cfg.scheme = {"ref": 0, "upwind3_rk2": 1}[scheme]
+        if sphere is not None:
+            cfg.has_sphere = 1
+            cfg.sphere_radius = sphere["radius"]
+            cfg.sphere_position[:] = list(sphere["position"])
+            cfg.sphere_velocity[:] = list(sphere.get("velocity", (0, 0, 0)))
+            cfg.sphere_forced[:] = [int(x) for x in sphere.get("forced", (1, 1, 1))]
+            cfg.sphere_fix_frame[:] = [int(x) for x in sphere.get("fix_frame", (0, 0, 0))]
+        self.shape = (nz, ny, nx)
+        self._h = lib().orc_create(C.byref(cfg))
+        if not self._h:
+            raise ValueError("oracle: invalid configuration")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    @property
+    def h(self) -> float:
+        return lib().orc_h(self._h)
+
+    def set_velocity(self, u, v, w):
+        u, v, w = (np.ascontiguousarray(a, dtype=np.float64) for a in (u, v, w))
+        lib().orc_set_velocity(self._h, _p(u), _p(v), _p(w))
+
+    def get(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        lib().orc_get_field(self._h, FIELDS[name], _p(out))
+        return out
+
+    def velocity(self):
+        return self.get("u"), self.get("v"), self.get("w")
+
+    def calc_max_timestep(self) -> float:
+        return lib().orc_calc_max_timestep(self._h)
+
+    def max_u(self) -> float:
+        return lib().orc_max_u(self._h)
+
+    def operator(self, name: str, dt: float):
+        if lib().orc_operator(self._h, name.encode(), dt) != 0:
+            raise ValueError(f"oracle: unknown operator {name}")
+
+    def timestep(self, dt: float):
+        lib().orc_timestep(self._h, dt)
+
+    def run(self, nsteps: int, fixed_dts=None) -> np.ndarray:
+        dts = np.zeros(nsteps, dtype=np.float64)
+        fx = None
+        if fixed_dts is not None:
+            fx = np.ascontiguousarray(fixed_dts, dtype=np.float64)
+        lib().orc_run(self._h, nsteps, _p(fx) if fx is not None else None, _p(dts))
+        return dts
+
+    def stats(self) -> dict:
+        out = np.zeros(21, dtype=np.float64)
+        lib().orc_get_stats(self._h, _p(out))
+        return {
+            "force": out[0:3].copy(), "torque": out[3:6].copy(), "time": out[6], "step": int(out[7]),
+            "uinf": out[8:11].copy(), "dt": out[11], "lambda": out[12], "com": out[13:16].copy(),
+            "rhs_sums": out[16:19].copy(), "corr": out[19], "umax": out[20],
+        }
+
+    def diagnostics(self) -> dict:
+        out = np.zeros(3, dtype=np.float64)
+        lib().orc_diagnostics(self._h, _p(out))
+        return {"ke": out[0], "div_l2": out[1], "div_max": out[2]}
+
+
+def poisson_solve(rhs: np.ndarray, h: float) -> np.ndarray:
+    """PoissonSolverPeriodic on an h^3-premultiplied RHS (shape (nz,ny,nx))."""
+    rhs = np.ascontiguousarray(rhs, dtype=np.float64)
+    nz, ny, nx = rhs.shape
+    p = np.empty_like(rhs)
+    if lib().orc_poisson_solve_field(nx, ny, nz, h, _p(rhs), _p(p)) != 0:
+        raise ValueError("oracle: sizes must be powers of two")
+    return p
+
+
+def lab_shift(f: np.ndarray, g: int, dx: int, dy: int, dz: int) -> np.ndarray:
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    nz, ny, nx = f.shape
+    out = np.empty_like(f)
+    if lib().orc_lab_shift(_p(f), _p(out), nx, ny, nz, g, dx, dy, dz) != 0:
+        raise ValueError("oracle: bad lab shift arguments")
+    return out
+
+
+def set_num_threads(n: int):
+    lib().orc_set_num_threads(n)
+
+
+def num_threads() -> int:
+    return lib().orc_num_threads()

@@ -1,0 +1,240 @@
+"""GPU parity tests: the sm_100a path through the C ABI against the FP64 oracle.
+
+Tolerances: FP64 plain form 1e-10 relative L2 per field per step (the stated
+bar); single operators are held to 1e-12 (the FFT is a different but exact
+algorithm, so only rounding differs).
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1e-10
+
+
+def make_sim(cells, extent, **kw):
+    import cubismup_3d_b200 as cup
+    sd = cup.SimulationData(CFL=kw.pop("CFL", 0.5), cells=cells, uinf=kw.pop("uinf", (0.0, 0.0, 0.0)))
+    sd.extent = extent
+    for k, v in kw.items():
+        setattr(sd, k, v)
+    return cup.Simulation(sd)
+
+
+def element_value(x, y, z):
+    return x + 1000 * y + 1000000 * z
+
+
+@pytest.mark.parametrize("g,shift", [(1, (-1, 0, 0)), (1, (+1, 0, 0)), (2, (-1, +1, +2))])
+def test_halo_staging_test_boundaries(g, shift):
+    # tests/cubismup3d/TestBoundaries.cpp:55-75 through the TMA plane-streaming path.
+    nx, ny, nz = 128, 32, 32
+    sim = make_sim((nx, ny, nz), 1.0)
+    Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    f = element_value(X, Y, Z).astype(np.float64)
+    dx, dy, dz = shift
+    out = sim.debug_shift(f, g, dx, dy, dz)
+    assert np.array_equal(out, element_value((X - dx) % nx, (Y - dy) % ny, (Z - dz) % nz))
+
+
+@pytest.mark.parametrize("cells", [(16, 16, 16), (64, 32, 16), (32, 64, 128), (256, 16, 32)])
+def test_poisson_vs_oracle(oracle, cells):
+    nx, ny, nz = cells
+    sim = make_sim(cells, 1.7)
+    rhs = np.random.default_rng(11).standard_normal((nz, ny, nx))
+    p = sim.pressureSolver.solve_field(rhs)
+    po = oracle.poisson_solve(rhs, sim.h)
+    assert rel_l2(p, po) < 1e-12
+
+
+def test_poisson_single_mode_known_answer():
+    nx, ny, nz = 64, 32, 16
+    sim = make_sim((nx, ny, nz), 6.4)
+    h = sim.h
+    Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    a, b, c = 3, 5, 2
+    phase = 2 * np.pi * (a * X / nx + b * Y / ny + c * Z / nz)
+    lam = sum((2 * np.cos(4 * np.pi * k / n) - 2) / (4 * h * h) for k, n in ((a, nx), (b, ny), (c, nz)))
+    p = sim.pressureSolver.solve_field(h ** 3 * np.cos(phase))
+    assert rel_l2(p, np.cos(phase) / lam) < 1e-12
+
+
+def random_velocity(cells, seed, scale=1.0):
+    nx, ny, nz = cells
+    rng = np.random.default_rng(seed)
+    return tuple(scale * rng.standard_normal((nz, ny, nx)) for _ in range(3))
+
+
+@pytest.mark.parametrize("scheme", ["ref", "upwind3_rk2"])
+def test_operators_vs_oracle(oracle, scheme):
+    cells = (64, 32, 32)
+    nx, ny, nz = cells
+    uinf = (0.3, -0.2, 0.1)
+    sim = make_sim(cells, 2.0, nu=0.02, uinf=uinf, scheme=scheme, rampup=0, DLM=0.0, lambda_=1.0)
+    orc = oracle.OracleSim(nx, ny, nz, 2.0, nu=0.02, CFL=0.5, uinf=uinf, rampup=0, DLM=0.0, lambda_=1.0,
+                           scheme=scheme)
+    u, v, w = random_velocity(cells, 5)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    dt = 1e-3
+    for op in sim.pipeline[:1]:
+        op(dt)
+    orc.operator("AdvectionDiffusion", dt)
+    for a, b in zip(sim.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < 1e-13
+    sim.pipeline[1](dt)
+    orc.operator("PressureRHS", dt)
+    assert rel_l2(sim.rhs(), orc.get("rhs")) < 1e-13
+    sim.pipeline[2](dt)
+    orc.operator("PressureProjection", dt)
+    assert rel_l2(sim.pressure(), orc.get("p")) < 1e-12
+    for a, b in zip(sim.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < 1e-12
+
+
+def run_parity(sim, orc, nsteps, tol, fields=("u", "v", "w")):
+    worst = 0.0
+    for s in range(nsteps):
+        dt_o = orc.calc_max_timestep()
+        dt_g = sim.calcMaxTimestep()
+        assert dt_g == pytest.approx(dt_o, rel=1e-12)
+        sim.timestep(dt_o, stats=False)
+        orc.timestep(dt_o)
+        got = dict(zip(("u", "v", "w"), sim.velocity()))
+        got["p"] = sim.pressure()
+        for f in fields:
+            e = rel_l2(got[f], orc.get(f))
+            worst = max(worst, e)
+            assert e < tol, (s, f, e)
+    return worst
+
+
+def test_taylor_green_64_fp64_50_steps(oracle):
+    # C1: TG on [0, 2pi]^3 at 64^3, nu = 0.01, CFL = 0.5, 50 steps, no obstacle.
+    from cubismup_3d_b200 import initial_conditions as ic
+    n = 64
+    L = 2 * np.pi
+    sim = make_sim((n, n, n), L, nu=0.01, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0)
+    orc = oracle.OracleSim(n, n, n, L, nu=0.01, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0)
+    u, v, w = ic.taylor_green((n, n, n), L / n)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    run_parity(sim, orc, 50, TOL_STEP, fields=("u", "v", "w", "p"))
+
+
+def test_taylor_green_upwind3_rk2_fp64(oracle):
+    from cubismup_3d_b200 import initial_conditions as ic
+    n = 32
+    L = 2 * np.pi
+    sim = make_sim((n, n, n), L, nu=0.01, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0, scheme="upwind3_rk2")
+    orc = oracle.OracleSim(n, n, n, L, nu=0.01, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0, scheme="upwind3_rk2")
+    u, v, w = ic.perturbed_taylor_green((n, n, n), L / n, seed=1)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    run_parity(sim, orc, 20, TOL_STEP)
+
+
+def test_device_chained_run_matches_host_steps(oracle):
+    # cup_run chains calcMaxTimestep on the device; same trajectory as the oracle.
+    from cubismup_3d_b200 import initial_conditions as ic
+    n = 32
+    L = 2 * np.pi
+    sim = make_sim((n, n, n), L, nu=0.01, CFL=0.5, rampup=5, DLM=0.0, lambda_=1.0)
+    orc = oracle.OracleSim(n, n, n, L, nu=0.01, CFL=0.5, rampup=5, DLM=0.0, lambda_=1.0)
+    u, v, w = ic.taylor_green((n, n, n), L / n)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    st = sim.run_steps(12)
+    dts = orc.run(12)
+    assert st.step == 12
+    assert st.time == pytest.approx(float(np.sum(dts)), rel=1e-12)
+    for a, b in zip(sim.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < TOL_STEP
+    assert st.kinetic_energy == pytest.approx(orc.diagnostics()["ke"], rel=1e-12)
+
+
+SPHERE = dict(radius=0.25, position=(0.5, 0.5, 0.5), enforcedVelocity=(1.0, 0.0, 0.0),
+              bForcedInSimFrame=(True, True, True), bFixFrameOfRef=(True, True, True))
+
+
+def sphere_pair(oracle, cells, extent, nu, scheme="ref", lambda_=1e6):
+    import cubismup_3d_b200 as cup
+    nx, ny, nz = cells
+    sim = make_sim(cells, extent, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=lambda_,
+                   bImplicitPenalization=True, scheme=scheme)
+    sim.add_obstacle(cup.Sphere(**SPHERE))
+    orc = oracle.OracleSim(nx, ny, nz, extent, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=lambda_,
+                           implicit_penalization=True, scheme=scheme,
+                           sphere={"radius": SPHERE["radius"], "position": SPHERE["position"],
+                                   "velocity": SPHERE["enforcedVelocity"], "forced": (1, 1, 1),
+                                   "fix_frame": (1, 1, 1)})
+    return sim, orc
+
+
+def test_sphere_chi_vs_oracle(oracle):
+    sim, orc = sphere_pair(oracle, (64, 32, 32), 2.0, nu=1e-3)
+    assert np.max(np.abs(sim.chi() - orc.get("chi"))) < 1e-14
+    st = sim.obstacle_state()
+    ost = orc.stats()
+    assert np.allclose(st["com"], ost["com"], rtol=0, atol=1e-13)
+    assert np.allclose(st["uinf"], ost["uinf"])
+
+
+def test_sphere_steps_vs_oracle(oracle):
+    # C3 in miniature: forced sphere in a frame fixed to it, implicit penalization.
+    sim, orc = sphere_pair(oracle, (64, 32, 32), 2.0, nu=2 * 0.25 / 300)
+    z = np.zeros(orc.shape)
+    sim.set_velocity(z, z, z)
+    orc.set_velocity(z, z, z)
+    for s in range(5):
+        dt = orc.calc_max_timestep()
+        assert sim.calcMaxTimestep() == pytest.approx(dt, rel=1e-12)
+        st = sim.timestep(dt)
+        orc.timestep(dt)
+        for a, b in zip(sim.velocity(), orc.velocity()):
+            assert rel_l2(a, b) < TOL_STEP
+        of = orc.stats()["force"]
+        assert np.allclose(st.force, of, rtol=1e-10, atol=1e-12 * np.abs(of).max())
+
+
+def test_sphere_operator_by_operator_vs_oracle(oracle):
+    sim, orc = sphere_pair(oracle, (32, 32, 32), 1.0, nu=1e-3)
+    u, v, w = random_velocity((32, 32, 32), 9, 0.1)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    dt = 2e-3
+    names = [op.getName() for op in sim.pipeline]
+    assert names == ["AdvectionDiffusion", "PressureRHS", "PressureProjection", "Penalization"]
+    for op in sim.pipeline:
+        op(dt)
+        orc.operator(op.getName(), dt)
+        if op.getName() == "PressureRHS":
+            assert rel_l2(sim.rhs(), orc.get("rhs")) < 1e-13
+    for a, b in zip(sim.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < 1e-12
+    ft = sim.pipeline[-1].force_torque
+    assert np.allclose(ft[:3], orc.stats()["force"], rtol=1e-10, atol=1e-14)
+
+
+def test_calc_max_timestep_rampup_and_dlm(oracle):
+    n = 32
+    sim = make_sim((n, n, n), 1.0, nu=0.01, CFL=0.5, rampup=10, DLM=1.0, lambda_=1.0)
+    orc = oracle.OracleSim(n, n, n, 1.0, nu=0.01, CFL=0.5, rampup=10, DLM=1.0, lambda_=1.0)
+    u, v, w = random_velocity((n, n, n), 2)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    assert sim.max_velocity() == orc.max_u()
+    assert sim.calcMaxTimestep() == pytest.approx(orc.calc_max_timestep(), rel=1e-14)
+
+
+def test_invalid_configurations_are_rejected():
+    import cubismup_3d_b200 as cup
+    with pytest.raises(Exception):
+        make_sim((48, 32, 32), 1.0)  # not a power of two
+    sim = make_sim((32, 32, 32), 1.0)
+    with pytest.raises(ValueError):
+        sim.add_obstacle(cup.Sphere(radius=0.1, bForcedInSimFrame=(True, False, True)))
+    with pytest.raises(ValueError):
+        sim.timestep(-1.0)

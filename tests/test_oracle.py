@@ -1,0 +1,163 @@
+"""CPU tests of the oracle (the FP64 restatement used as the parity checker).
+
+Pins: the periodic lab semantics against the restated
+tests/cubismup3d/TestBoundaries.cpp, the FFT Poisson solve against numpy's
+pocketfft (FFTW 3.3.7's DFT definition) and the committed golden vectors,
+plus analytic known answers.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def element_value(x, y, z):
+    # tests/cubismup3d/TestBoundaries.cpp:13-16
+    return x + 1000 * y + 1000000 * z
+
+
+@pytest.mark.parametrize("g,shift", [(1, (-1, 0, 0)), (1, (+1, 0, 0)), (2, (-1, +1, +2))])
+def test_periodic_lab_test_boundaries(oracle, g, shift):
+    # tests/cubismup3d/TestBoundaries.cpp:55-75: 128x32x32 periodic grid.
+    nx, ny, nz = 128, 32, 32
+    Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    f = element_value(X, Y, Z).astype(np.float64)
+    dx, dy, dz = shift
+    out = oracle.lab_shift(f, g, dx, dy, dz)
+    expected = element_value((X - dx) % nx, (Y - dy) % ny, (Z - dz) % nz)
+    assert np.array_equal(out, expected)
+
+
+def numpy_poisson(rhs, h):
+    """Independent restatement of PoissonSolverPeriodic::solve with numpy's
+    pocketfft in FFTW's layout (x slowest, z r2c last)."""
+    nz, ny, nx = rhs.shape
+    B = np.fft.rfftn(rhs.transpose(2, 1, 0), axes=(0, 1, 2))
+    i = np.arange(nx)[:, None, None]
+    l = np.arange(ny)[None, :, None]
+    k = np.arange(nz // 2 + 1)[None, None, :]
+    D = np.cos(4 * np.pi / nx * i) + np.cos(4 * np.pi / ny * l) + np.cos(4 * np.pi / nz * k)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        fac = 4 / (nx * h * ny * nz) / (2 * D - 6)
+        B = B * fac
+    for a in (0, nx // 2):
+        for c in (0, ny // 2):
+            for d in (0, nz // 2):
+                B[a, c, d] = 0
+    return (np.fft.irfftn(B, s=(nx, ny, nz), axes=(0, 1, 2)) * (nx * ny * nz)).transpose(2, 1, 0)
+
+
+@pytest.mark.parametrize("shape", [(16, 16, 16), (32, 16, 64), (64, 32, 16)])
+def test_poisson_matches_pocketfft(oracle, shape):
+    rng = np.random.default_rng(7)
+    rhs = rng.standard_normal(shape)
+    h = 0.37
+    p = oracle.poisson_solve(rhs, h)
+    assert rel_l2(p, numpy_poisson(rhs, h)) < 1e-13
+
+
+def test_poisson_golden_vectors(oracle):
+    d = np.load(os.path.join(GOLDEN, "poisson_golden.npz"))
+    for key in ("a", "b"):
+        rhs, h, p = d[f"{key}_rhs"], float(d[f"{key}_h"]), d[f"{key}_p"]
+        assert rel_l2(oracle.poisson_solve(rhs, h), p) < 1e-13
+
+
+def wide_laplacian(p, h):
+    out = np.zeros_like(p)
+    for ax in range(3):
+        out += (np.roll(p, -2, ax) - 2 * p + np.roll(p, 2, ax)) / (4 * h * h)
+    return out
+
+
+def test_poisson_single_mode_known_answer(oracle):
+    # rhs = h^3 cos(2 pi (a x / nx + b y / ny + c z / nz)): p = rhs / (h^3 lambda),
+    # lambda = sum_d (2 cos(4 pi k_d / N_d) - 2) / (4 h^2).
+    nz, ny, nx = 16, 32, 64
+    h = 0.1
+    Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    a, b, c = 3, 5, 2
+    phase = 2 * np.pi * (a * X / nx + b * Y / ny + c * Z / nz)
+    rhs = h ** 3 * np.cos(phase)
+    lam = sum((2 * np.cos(4 * np.pi * k / n) - 2) / (4 * h * h) for k, n in ((a, nx), (b, ny), (c, nz)))
+    p = oracle.poisson_solve(rhs, h)
+    assert rel_l2(p, np.cos(phase) / lam) < 1e-13
+    assert rel_l2(wide_laplacian(p, h) * h ** 3, rhs) < 1e-12
+
+
+def test_projection_makes_divergence_free(oracle):
+    from cubismup_3d_b200 import initial_conditions as ic
+    n = 32
+    h = 2 * np.pi / n
+    sim = oracle.OracleSim(n, n, n, 2 * np.pi, nu=0.01, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0)
+    u, v, w = ic.random_solenoidal((n, n, n), 3, lambda k: np.exp(-k), rms=1.0)
+    u = u + 0.3 * np.sin(np.arange(n) * h)[None, None, :]  # add a divergent part
+    sim.set_velocity(u, v, w)
+    d0 = sim.diagnostics()["div_l2"]
+    dt = 0.01
+    sim.operator("AdvectionDiffusion", dt)
+    sim.operator("PressureRHS", dt)
+    sim.operator("PressureProjection", dt)
+    d1 = sim.diagnostics()
+    assert d0 > 1e-2
+    assert d1["div_l2"] < 1e-12 * max(1.0, d0)
+
+
+def test_taylor_green_viscous_decay(oracle):
+    # small dt, pure TG: KE decays like exp(-2 * 3 nu t) to leading order (the
+    # central-difference modified wavenumber makes it a little slower).
+    from cubismup_3d_b200 import initial_conditions as ic
+    n = 32
+    h = 2 * np.pi / n
+    nu = 0.05
+    sim = oracle.OracleSim(n, n, n, 2 * np.pi, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=1.0)
+    sim.set_velocity(*ic.taylor_green((n, n, n), h))
+    ke0 = sim.diagnostics()["ke"]
+    dts = sim.run(20)
+    ke1 = sim.diagnostics()["ke"]
+    t = float(np.sum(dts))
+    ratio = ke1 / ke0
+    assert np.exp(-6 * nu * t) < ratio < 1.0
+    assert abs(ratio - np.exp(-6 * nu * t)) < 0.02
+
+
+def test_calc_max_timestep_rampup(oracle):
+    n = 16
+    sim = oracle.OracleSim(n, n, n, 1.0, nu=0.01, CFL=0.5, rampup=10, DLM=1.0, lambda_=1.0)
+    u = np.full((n, n, n), 0.5)
+    sim.set_velocity(u, 0 * u, 0 * u)
+    dt = sim.calc_max_timestep()
+    h = 1.0 / n
+    base = min(h * h / 0.01, h / (0.5 + 1e-8))
+    x = 1.0 / 10
+    ramp = np.exp(np.log(1e-3) * (1 - x) + np.log(0.5) * x)
+    assert dt == pytest.approx(ramp * base, rel=1e-15)
+    assert sim.stats()["lambda"] == pytest.approx(1.0 / dt, rel=1e-15)
+
+
+def test_sphere_chi_and_penalization(oracle):
+    # sphere at rest in a fixed frame: chi in [0,1], CoM at the centre, and the
+    # implicit penalization pulls the velocity inside the body to U_s.
+    n = 32
+    sphere = {"radius": 0.2, "position": (0.5, 0.5, 0.5), "velocity": (1.0, 0, 0), "forced": (1, 1, 1),
+              "fix_frame": (1, 1, 1)}
+    sim = oracle.OracleSim(n, n, n, 1.0, nu=0.01, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6,
+                           implicit_penalization=True, sphere=sphere)
+    chi = sim.get("chi")
+    st = sim.stats()
+    assert chi.min() >= 0 and chi.max() <= 1 + 1e-12
+    assert np.allclose(st["com"], 0.5, atol=1e-12)
+    assert np.allclose(st["uinf"], (-1, 0, 0))
+    vol = chi.sum() / n ** 3
+    assert abs(vol - 4 / 3 * np.pi * 0.2 ** 3) / (4 / 3 * np.pi * 0.2 ** 3) < 0.02
+    dts = sim.run(2)
+    u = sim.get("u")
+    inside = chi >= 1.0
+    assert np.allclose(u[inside], 1.0, atol=1e-4)
+    assert st["force"].shape == (3,)
+    assert np.all(np.isfinite(sim.stats()["force"]))
+    assert dts[0] > 0
