@@ -34,11 +34,12 @@ struct DevState {
   double com[3], mass;
   double time;
   double res2, b2;
+  double cmean[8];  // parity-class means of p (the 8 null-mode components)
   int step, n_solves, converged, pad_;
 };
 
 enum PartialRegion { P_GRAD = 0, P_PEN, P_RHSOB, P_CHI, P_MAX, P_RES, P_DIAG, P_COUNT };
-constexpr int kPartialCap = 16384;  // doubles per region
+constexpr int kPartialCap = 32768;  // doubles per region (>= 16 per CTA)
 
 constexpr int kBoxThreads = 256;
 constexpr int kBoxBlocksMax = 296;
@@ -177,6 +178,49 @@ __global__ void k_finalize_com(const double* p, int np, DevState* st, SpherePara
       st->com[k] = s[1 + k] / s[0];
       sp->centerOfMass[k] = st->com[k];
     }
+  }
+}
+
+// Defect-correction bookkeeping after a residual pass (check k, before solve k):
+// FP64 norms with the null-mode components projected out (they are not
+// reachable by any pressure: the spectral factor is zero there), the
+// parity-class means of p, and the decision |r| <= tol |b| (from check
+// min_iter on; check max_iter is final).
+__global__ void k_finalize_residual(const double* p, int np, DevState* st, double tol, int k, int min_iter,
+                                    int max_iter, double inv_class_cells) {
+  __shared__ double scratch[18 * 32];
+  if (k > 0 && st->converged) return;
+  double s[18];
+  for (int j = 0; j < 18; ++j) s[j] = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x)
+    for (int j = 0; j < 18; ++j) s[j] += p[18 * i + j];
+  block_reduce<18, false>(s, scratch);
+  if (threadIdx.x == 0) {
+    double null2 = 0.0;
+    for (int j = 0; j < 8; ++j) null2 += s[10 + j] * s[10 + j] * inv_class_cells;
+    const double res2 = fmax(s[0] - null2, 0.0), b2 = fmax(s[1] - null2, 0.0);
+    st->res2 = res2;
+    st->b2 = b2;
+    for (int j = 0; j < 8; ++j) st->cmean[j] = s[2 + j] * inv_class_cells;
+    const bool met = b2 == 0.0 || sqrt(res2) <= tol * sqrt(b2);
+    st->n_solves = k;
+    st->converged = (k >= min_iter && met) ? 1 : 0;
+    if (k >= max_iter) st->converged = met ? 1 : 2;  // 2: not converged after max_iter solves
+  }
+}
+
+// p += delta (FP32 correction) minus the parity-class means of p measured by
+// the preceding residual pass, which removes the 8 null-mode components of
+// p (the mean-pressure fix) in FP64.
+__global__ void k_add_correction(double* p, const float* d, int nx, int ny, size_t n, const DevState* st,
+                                 const int* skip) {
+  if (skip && *skip) return;
+  double cm[8];
+  for (int j = 0; j < 8; ++j) cm[j] = st->cmean[j];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+    const int cls = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
+    p[i] = p[i] + (double)d[i] - cm[cls];
   }
 }
 
@@ -440,7 +484,8 @@ int prepare_kernel(cup_handle* H, K kern, size_t smem, int threads, int* blocks_
 // Launches k_stencil_stream over `fields` (device arrays of T). Returns the
 // grid size through *grid_out (the number of per-CTA partials written).
 template <typename T, int NF, int G, int TY, int NS, class Op>
-int launch_stream(cup_handle* H, const char* name, const void* const* fields, const Op& op, int* grid_out = nullptr) {
+int launch_stream(cup_handle* H, const char* name, const void* const* fields, const Op& op, int* grid_out = nullptr,
+                  const int* skip = nullptr) {
   FieldMaps<NF> maps;
   for (int f = 0; f < NF; ++f) {
     int rc = make_map(H, &maps.main[f], fields[f], tma_dtype<T>(), sizeof(T), H->nx, TY, 1);
@@ -456,9 +501,9 @@ int launch_stream(cup_handle* H, const char* name, const void* const* fields, co
   int rc = prepare_kernel(H, kern, smem, 256, &bpsm);
   if (rc) return rc;
   const int grid = std::min(g.n_items, bpsm * H->num_sms);
-  if (grid > kPartialCap / 8) return fail(H, CUP_ERR_ARG, "too many CTAs for the partial buffers");
+  if (grid > kPartialCap / 16) return fail(H, CUP_ERR_ARG, "too many CTAs for the partial buffers");
   rc = launch_named(H, name, [&]() -> int {
-    kern<<<grid, 256, smem, H->stream>>>(maps, g, op, H->derr);
+    kern<<<grid, 256, smem, H->stream>>>(maps, g, op, H->derr, skip);
     CKL();
     return CUP_OK;
   });
@@ -479,7 +524,7 @@ const float2* table<float>(cup_handle* H, int axis) {
 }
 
 template <int M, typename R>
-int launch_rows_M(cup_handle* H, const R* in, R* out) {
+int launch_rows_M(cup_handle* H, const R* in, R* out, const int* skip) {
   constexpr int N = 2 * M, TPL = M / 8;
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
   const int lpc = 256 / TPL;
@@ -492,27 +537,27 @@ int launch_rows_M(cup_handle* H, const R* in, R* out) {
   if (rc) return rc;
   const int grid = (nrows + lpc - 1) / lpc;
   return launch_named(H, "dht_x", [&]() -> int {
-    kern<<<grid, lpc * TPL, smem, H->stream>>>(in, out, nrows, lpc, table<R>(H, 0), H->derr);
+    kern<<<grid, lpc * TPL, smem, H->stream>>>(in, out, nrows, lpc, table<R>(H, 0), H->derr, skip);
     CKL();
     return CUP_OK;
   });
 }
 
 template <typename R>
-int launch_rows(cup_handle* H, const R* in, R* out) {
+int launch_rows(cup_handle* H, const R* in, R* out, const int* skip) {
   switch (H->nx / 2) {
-    case 8: return launch_rows_M<8, R>(H, in, out);
-    case 16: return launch_rows_M<16, R>(H, in, out);
-    case 32: return launch_rows_M<32, R>(H, in, out);
-    case 64: return launch_rows_M<64, R>(H, in, out);
-    case 128: return launch_rows_M<128, R>(H, in, out);
-    case 256: return launch_rows_M<256, R>(H, in, out);
+    case 8: return launch_rows_M<8, R>(H, in, out, skip);
+    case 16: return launch_rows_M<16, R>(H, in, out, skip);
+    case 32: return launch_rows_M<32, R>(H, in, out, skip);
+    case 64: return launch_rows_M<64, R>(H, in, out, skip);
+    case 128: return launch_rows_M<128, R>(H, in, out, skip);
+    case 256: return launch_rows_M<256, R>(H, in, out, skip);
   }
   return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
 }
 
 template <int M, typename R, int AXIS, bool DIVIDE>
-int launch_cols_M(cup_handle* H, R* buf) {
+int launch_cols_M(cup_handle* H, R* buf, const int* skip) {
   constexpr int N = 2 * M, TPL = M / 8;
   const int W = std::min(256 / TPL, H->nx);
   CUtensorMap map;
@@ -527,22 +572,22 @@ int launch_cols_M(cup_handle* H, R* buf) {
   const int grid = ntx * (AXIS == 1 ? H->nz : H->ny);
   SpectralParams sp{H->cosx, H->cosy, H->cosz, H->norm_factor, H->nx, H->ny, H->nz};
   return launch_named(H, AXIS == 1 ? "dht_y" : "dht_z_solve", [&]() -> int {
-    kern<<<grid, W * TPL, smem, H->stream>>>(map, map, W, ntx, table<R>(H, AXIS), sp, H->derr);
+    kern<<<grid, W * TPL, smem, H->stream>>>(map, map, W, ntx, table<R>(H, AXIS), sp, H->derr, skip);
     CKL();
     return CUP_OK;
   });
 }
 
 template <typename R, int AXIS, bool DIVIDE>
-int launch_cols(cup_handle* H, R* buf) {
+int launch_cols(cup_handle* H, R* buf, const int* skip) {
   const int N = AXIS == 1 ? H->ny : H->nz;
   switch (N / 2) {
-    case 8: return launch_cols_M<8, R, AXIS, DIVIDE>(H, buf);
-    case 16: return launch_cols_M<16, R, AXIS, DIVIDE>(H, buf);
-    case 32: return launch_cols_M<32, R, AXIS, DIVIDE>(H, buf);
-    case 64: return launch_cols_M<64, R, AXIS, DIVIDE>(H, buf);
-    case 128: return launch_cols_M<128, R, AXIS, DIVIDE>(H, buf);
-    case 256: return launch_cols_M<256, R, AXIS, DIVIDE>(H, buf);
+    case 8: return launch_cols_M<8, R, AXIS, DIVIDE>(H, buf, skip);
+    case 16: return launch_cols_M<16, R, AXIS, DIVIDE>(H, buf, skip);
+    case 32: return launch_cols_M<32, R, AXIS, DIVIDE>(H, buf, skip);
+    case 64: return launch_cols_M<64, R, AXIS, DIVIDE>(H, buf, skip);
+    case 128: return launch_cols_M<128, R, AXIS, DIVIDE>(H, buf, skip);
+    case 256: return launch_cols_M<256, R, AXIS, DIVIDE>(H, buf, skip);
   }
   return fail(H, CUP_ERR_ARG, "unsupported line length %d", N);
 }
@@ -550,13 +595,13 @@ int launch_cols(cup_handle* H, R* buf) {
 // p = H(f . H(work)) over the three axes, in place on `work`; the last x
 // pass writes to `out` (may equal work).
 template <typename R>
-int fft_poisson(cup_handle* H, R* work, R* out) {
+int fft_poisson(cup_handle* H, R* work, R* out, const int* skip = nullptr) {
   int rc;
-  if ((rc = launch_rows<R>(H, work, work))) return rc;
-  if ((rc = launch_cols<R, 1, false>(H, work))) return rc;
-  if ((rc = launch_cols<R, 2, true>(H, work))) return rc;
-  if ((rc = launch_cols<R, 1, false>(H, work))) return rc;
-  if ((rc = launch_rows<R>(H, work, out))) return rc;
+  if ((rc = launch_rows<R>(H, work, work, skip))) return rc;
+  if ((rc = launch_cols<R, 1, false>(H, work, skip))) return rc;
+  if ((rc = launch_cols<R, 2, true>(H, work, skip))) return rc;
+  if ((rc = launch_cols<R, 1, false>(H, work, skip))) return rc;
+  if ((rc = launch_rows<R>(H, work, out, skip))) return rc;
   return CUP_OK;
 }
 
@@ -659,9 +704,49 @@ int do_pressure_rhs(cup_handle* H, DtArg dt) {
   return CUP_OK;
 }
 
+// FP32 correction solve inside an FP64 defect-correction loop, warm-started
+// from the current p: check k computes r = b - h^3 L_2h p (FP64) and decides
+// convergence on the device; solve k transforms r in FP32 and adds the
+// correction to p in FP64. Kernels after convergence exit at entry.
+int do_poisson_dc(cup_handle* H) {
+  const double tol = H->cfg.dc_tol > 0 ? H->cfg.dc_tol : 1e-10;
+  const int max_iter = H->cfg.dc_max_iter > 0 ? H->cfg.dc_max_iter : 4;
+  const int min_iter = std::min(max_iter, H->cfg.dc_min_iter > 0 ? H->cfg.dc_min_iter : 1);
+  const int* conv = &H->dstate->converged;
+  const double inv_class = 8.0 / (double)H->n;
+  int rc;
+  for (int k = 0; k <= max_iter; ++k) {
+    const void* pf[1] = {H->p};
+    OpResidual op{H->rhs, H->work32, partial(H, P_RES), H->h / 4, H->nx, H->ny};
+    int grid = 0;
+    if ((rc = launch_stream<double, 1, 2, 4, 6>(H, "dc_residual", pf, op, &grid, k > 0 ? conv : nullptr))) return rc;
+    {
+      int rc_ = launch_named(H, "finalize_residual", [&]() -> int {
+        k_finalize_residual<<<1, 256, 0, H->stream>>>(partial(H, P_RES), grid, H->dstate, tol, k, min_iter, max_iter,
+                                                      inv_class);
+        CKL();
+        return CUP_OK;
+      });
+      if (rc_) return rc_;
+    }
+    if (k == max_iter) break;
+    if ((rc = fft_poisson<float>(H, H->work32, H->work32, conv))) return rc;
+    {
+      const int g = std::min<size_t>(H->num_sms * 8, (H->n + 255) / 256);
+      int rc_ = launch_named(H, "dc_update", [&]() -> int {
+        k_add_correction<<<g, 256, 0, H->stream>>>(H->p, H->work32, H->nx, H->ny, H->n, H->dstate, conv);
+        CKL();
+        return CUP_OK;
+      });
+      if (rc_) return rc_;
+    }
+  }
+  return CUP_OK;
+}
+
 int do_poisson(cup_handle* H) {
   if (!H->fp32) return fft_poisson<double>(H, H->rhs, H->p);
-  return fail(H, CUP_ERR_ARG, "FP32 defect-correction solve not available in this build");
+  return do_poisson_dc(H);
 }
 
 template <typename T>
@@ -1130,6 +1215,14 @@ int cup_get_obstacle_state(cup_handle* H, double force[3], double torque[3], dou
   return CUP_OK;
 }
 
+int cup_set_clock(cup_handle* H, int step, double time) {
+  REQUIRE_H(H);
+  if (step < 0) return fail(H, CUP_ERR_ARG, "step must be >= 0");
+  H->step = step;
+  H->time = time;
+  return CUP_OK;
+}
+
 int cup_max_velocity(cup_handle* H, double* umax) {
   REQUIRE_H(H);
   int rc = DISPATCH_T(H, do_max_u);
@@ -1182,6 +1275,14 @@ int cup_poisson_solve(cup_handle* H, cup_solve_stats* stats) {
   if (stats) {
     stats->n_solves = 1;
     stats->rel_residual = 0;
+    if (H->fp32) {
+      if ((rc = read_state(H))) return rc;
+      stats->n_solves = H->hstate->n_solves;
+      stats->rel_residual = H->hstate->b2 > 0 ? std::sqrt(H->hstate->res2 / H->hstate->b2) : 0.0;
+      if (H->hstate->converged == 2)
+        return fail(H, CUP_ERR_NOT_CONVERGED, "defect correction: relative residual %.3e after %d solves",
+                    stats->rel_residual, stats->n_solves);
+    }
   }
   return CUP_OK;
 }
@@ -1241,6 +1342,9 @@ static int fill_stats(cup_handle* H, cup_step_stats* st) {
   }
   st->n_solves = H->fp32 ? s.n_solves : 1;
   st->rel_residual = H->fp32 && s.b2 > 0 ? std::sqrt(s.res2 / s.b2) : 0.0;
+  if (H->fp32 && s.converged == 2)
+    return fail(H, CUP_ERR_NOT_CONVERGED, "defect correction: relative residual %.3e after %d solves",
+                st->rel_residual, s.n_solves);
   if (!std::isfinite(s.umax) || !std::isfinite(s.ke)) return fail(H, CUP_ERR_NONFINITE, "non-finite velocity");
   return CUP_OK;
 }
@@ -1307,6 +1411,7 @@ int cup_poisson_solve_field(cup_handle* H, const double* rhs, double* p, int whe
   const cudaMemcpyKind in = where == CUP_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   const cudaMemcpyKind out = where == CUP_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
   CK(cudaMemcpyAsync(H->rhs, rhs, H->n * sizeof(double), in, H->stream));
+  if (H->fp32) CK(cudaMemsetAsync(H->p, 0, H->n * sizeof(double), H->stream));
   int rc = do_poisson(H);
   if (rc) return rc;
   CK(cudaMemcpyAsync(p, H->p, H->n * sizeof(double), out, H->stream));

@@ -290,8 +290,9 @@ __device__ __forceinline__ void load_table(R2* dst, const R2* src, int n) {
 // written back with one bulk store. in may equal out.
 template <int M, typename R>
 __global__ void __launch_bounds__(256) k_dht_rows(const R* in, R* out, int nrows, int lpc,
-                                                  const typename Cplx<R>::T* tw_g, int* err) {
+                                                  const typename Cplx<R>::T* tw_g, int* err, const int* skip) {
   using R2 = typename Cplx<R>::T;
+  if (skip && *skip) return;
   constexpr int N = 2 * M, TPL = M / 8;
   constexpr int TL = FFTPlan<M>::table_len();
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
@@ -306,9 +307,13 @@ __global__ void __launch_bounds__(256) k_dht_rows(const R* in, R* out, int nrows
   const int nr = min(lpc, nrows - row0);
   if (nr <= 0) return;
   const uint32_t bytes = (uint32_t)((size_t)nr * N * sizeof(R));
+  // the barrier must be initialised before any thread waits on it
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
     mbar_arrive_expect_tx(bar, bytes);
     bulk_load(rows, in + (size_t)row0 * N, bytes, bar);
   }
@@ -354,8 +359,10 @@ __device__ __forceinline__ double spectral_factor(const SpectralParams& sp, int 
 template <int M, typename R, int AXIS, bool DIVIDE>
 __global__ void __launch_bounds__(256) k_dht_cols(const __grid_constant__ CUtensorMap map_in,
                                                   const __grid_constant__ CUtensorMap map_out, int W, int ntiles_x,
-                                                  const typename Cplx<R>::T* tw_g, SpectralParams sp, int* err) {
+                                                  const typename Cplx<R>::T* tw_g, SpectralParams sp, int* err,
+                                                  const int* skip) {
   using R2 = typename Cplx<R>::T;
+  if (skip && *skip) return;
   constexpr int N = 2 * M, TPL = M / 8;
   constexpr int TL = FFTPlan<M>::table_len();
   extern __shared__ __align__(128) unsigned char smem_dyn[];
@@ -366,9 +373,13 @@ __global__ void __launch_bounds__(256) k_dht_cols(const __grid_constant__ CUtens
   const int x0 = (blockIdx.x % ntiles_x) * W;
   const int other = blockIdx.x / ntiles_x;  // z for AXIS 1, y for AXIS 2
   const int c1 = AXIS == 1 ? 0 : other, c2 = AXIS == 1 ? other : 0;
+  // the barrier must be initialised before any thread waits on it
   if (threadIdx.x == 0) {
     mbar_init(bar, 1);
     mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
     mbar_arrive_expect_tx(bar, (uint32_t)((size_t)N * W * sizeof(R)));
     tma_load_3d(tile, &map_in, x0, c1, c2, bar);
   }

@@ -134,6 +134,50 @@ struct OpPressureRHS {
   __device__ void finish(double*, double*) const {}
 };
 
+// FP64 defect of the Poisson equation, r = b - h^3 L_2h p, with L_2h the
+// wide Laplacian sum_d (p(+2) - 2p + p(-2)) / (4h^2) that the spectral factor
+// inverts (source/poisson/PoissonSolverPeriodic.cpp:19-37); written as FP32
+// for the FP32 correction solve. Per-CTA FP64 partials: [0] sum r^2,
+// [1] sum b^2, [2..9] sums of p and [10..17] sums of r over the 8 parity
+// classes (x&1, y&1, z&1). The class sums give the components along the 8
+// null modes of L_2h (mean and checkerboards), which the solve cannot change:
+// they are removed from p (the mean-pressure fix) and left out of the
+// convergence test.
+struct OpResidual {
+  const double* b;
+  float* r;
+  double* partials;  // [gridDim.x][18]
+  double c;          // h / 4 = h^3 / (4 h^2)
+  int nx, ny;
+  template <class C>
+  __device__ __forceinline__ void cell(const C& q, int x, int y, int gy, int gz, double* acc) const {
+    const double p0 = q.v(0, x, y, 0, 0, 0);
+    const double lx = q.v(0, x, y, 2, 0, 0) - 2 * p0 + q.v(0, x, y, -2, 0, 0);
+    const double ly = q.v(0, x, y, 0, 2, 0) - 2 * p0 + q.v(0, x, y, 0, -2, 0);
+    const double lz = q.v(0, x, y, 0, 0, 2) - 2 * p0 + q.v(0, x, y, 0, 0, -2);
+    const size_t o = gidx(x, gy, gz, nx, ny);
+    const double bb = b[o];
+    const double res = bb - c * (lx + ly + lz);
+    r[o] = (float)res;
+    acc[0] += res * res;
+    acc[1] += bb * bb;
+    const int cls = (x & 1) | ((gy & 1) << 1) | ((gz & 1) << 2);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      acc[2 + k] += (k == cls) ? p0 : 0.0;
+      acc[10 + k] += (k == cls) ? res : 0.0;
+    }
+  }
+  __device__ void finish(double* acc, double* scratch) const {
+    double v[18];
+#pragma unroll
+    for (int k = 0; k < 18; ++k) v[k] = acc[k];
+    block_reduce<18, false>(v, scratch);
+    if (threadIdx.x == 0)
+      for (int k = 0; k < 18; ++k) partials[18 * blockIdx.x + k] = v[k];
+  }
+};
+
 // Active box of the obstacle: cells [lo, lo+n) per dimension (global indices,
 // wrapped periodically). Outside it chi == 0 and the obstacle terms vanish.
 struct Box {

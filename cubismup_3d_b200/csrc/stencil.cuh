@@ -16,7 +16,7 @@
 
 namespace cup {
 
-constexpr int kStreamAcc = 4;
+constexpr int kStreamAcc = 20;
 
 template <int NF>
 struct FieldMaps {
@@ -46,7 +46,7 @@ struct PlaneCtx {
 
 template <typename T, int NF, int G, int TY, int NS>
 constexpr size_t stream_smem_bytes(int nx) {
-  return (size_t)NS * NF * (TY + 2 * G) * nx * sizeof(T) + NS * sizeof(uint64_t) + 32 * 8 * sizeof(double);
+  return (size_t)NS * NF * (TY + 2 * G) * nx * sizeof(T) + NS * sizeof(uint64_t) + 32 * kStreamAcc * sizeof(double);
 }
 
 // Op must provide:
@@ -55,8 +55,9 @@ constexpr size_t stream_smem_bytes(int nx) {
 // acc[kStreamAcc] is a per-thread accumulator array, zero-initialised.
 template <typename T, int NF, int G, int TY, int NS, class Op>
 __global__ void __launch_bounds__(256) k_stencil_stream(const __grid_constant__ FieldMaps<NF> maps,
-                                                       const StreamGeom g, Op op, int* err) {
+                                                       const StreamGeom g, Op op, int* err, const int* skip) {
   static_assert(NS >= 2 * G + 1, "ring must hold the stencil planes");
+  if (skip && *skip) return;  // device-side early exit (converged defect correction)
   constexpr int ROWS = TY + 2 * G;
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
@@ -105,7 +106,9 @@ __global__ void __launch_bounds__(256) k_stencil_stream(const __grid_constant__ 
     for (; q_issued < min(L, NS); ++q_issued) issue(q_issued);
 
   const int cells = nx * TY;
-  double acc[kStreamAcc] = {0, 0, 0, 0};
+  double acc[kStreamAcc];
+#pragma unroll
+  for (int i = 0; i < kStreamAcc; ++i) acc[i] = 0.0;
   int a = 0;
   bool ok = true;
   for (int it = 0; it < my_items && ok; ++it) {

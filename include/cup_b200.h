@@ -130,6 +130,10 @@ int cup_get_obstacle_state(struct cup_handle* h, double force[3], double torque[
                            double uinf[3]);
 
 /* ---- operators (source/operators/*.cpp; names as Operator::getName()) ---- */
+/* Sets the simulation clock (sim.step, sim.time) that calcMaxTimestep's CFL
+ * ramp-up reads (source/Simulation.cpp:412-417) when the pipeline is driven
+ * operator by operator rather than through cup_step / cup_run. */
+int cup_set_clock(struct cup_handle* h, int step, double time);
 /* findMaxU (source/operators/ProcessHelpers.h:74-99) */
 int cup_max_velocity(struct cup_handle* h, double* umax);
 /* Simulation::calcMaxTimestep (source/Simulation.cpp:403-424) */

@@ -238,3 +238,111 @@ def test_invalid_configurations_are_rejected():
         sim.add_obstacle(cup.Sphere(radius=0.1, bForcedInSimFrame=(True, False, True)))
     with pytest.raises(ValueError):
         sim.timestep(-1.0)
+
+
+# ---- FP32 storage + FP32 FFT inside FP64 defect correction ----------------
+
+def test_fp32_dc_poisson_converges_to_oracle(oracle):
+    cells = (64, 32, 128)
+    nx, ny, nz = cells
+    sim = make_sim(cells, 3.0, precision="fp32_dc", dc_tol=1e-12, dc_max_iter=8, dc_min_iter=1)
+    rng = np.random.default_rng(3)
+    rhs = rng.standard_normal((nz, ny, nx))
+    # remove the null-mode content (b of the projection never has any)
+    Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    cls = (X & 1) | ((Y & 1) << 1) | ((Z & 1) << 2)
+    for c in range(8):
+        rhs[cls == c] -= rhs[cls == c].mean()
+    p = sim.pressureSolver.solve_field(rhs)
+    po = oracle.poisson_solve(rhs, sim.h)
+    assert rel_l2(p, po) < 1e-10
+
+
+def test_fp32_dc_taylor_green_error_vs_fp64_oracle(oracle):
+    from cubismup_3d_b200 import initial_conditions as ic
+    n = 64
+    L = 2 * np.pi
+    sim = make_sim((n, n, n), L, nu=0.01, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0, precision="fp32_dc",
+                   dc_tol=1e-10, dc_max_iter=4)
+    orc = oracle.OracleSim(n, n, n, L, nu=0.01, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0)
+    u, v, w = ic.perturbed_taylor_green((n, n, n), L / n, seed=4)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    worst = 0.0
+    for s in range(20):
+        dt = orc.calc_max_timestep()
+        st = sim.timestep(dt)
+        orc.timestep(dt)
+        assert 1 <= st.n_solves <= 4
+        assert st.rel_residual <= 1e-10
+        for a, b in zip(sim.velocity(), orc.velocity()):
+            worst = max(worst, rel_l2(a, b))
+    assert worst < 1e-6, worst
+
+
+def test_fp32_dc_not_converged_is_reported():
+    # tolerance below what an FP32 correction can reach in one solve
+    import cubismup_3d_b200 as cup
+    from cubismup_3d_b200 import _lib
+    from cubismup_3d_b200 import initial_conditions as ic
+    n = 32
+    sim = make_sim((n, n, n), 2 * np.pi, nu=0.01, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0, precision="fp32_dc",
+                   dc_tol=1e-30, dc_max_iter=1)
+    sim.set_velocity(*ic.taylor_green((n, n, n), 2 * np.pi / n))
+    with pytest.raises(_lib.CupError) as e:
+        sim.timestep(0.01)
+    assert e.value.code == _lib.CUP_ERR_NOT_CONVERGED
+
+
+def test_fp32_dc_sphere_runs_and_tracks_oracle(oracle):
+    import cubismup_3d_b200 as cup
+    cells = (64, 32, 32)
+    # the obstacle makes the RHS rough (surface-concentrated), so the FP32
+    # corrections contract the residual more slowly than for smooth flow
+    sim = make_sim(cells, 2.0, nu=1e-3, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6, bImplicitPenalization=True,
+                   precision="fp32_dc", dc_max_iter=8)
+    sim.add_obstacle(cup.Sphere(**SPHERE))
+    _, orc = sphere_pair(oracle, cells, 2.0, nu=1e-3)
+    z = np.zeros(orc.shape)
+    sim.set_velocity(z, z, z)
+    orc.set_velocity(z, z, z)
+    for s in range(5):
+        dt = orc.calc_max_timestep()
+        st = sim.timestep(dt)
+        orc.timestep(dt)
+    for a, b in zip(sim.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < 1e-5
+    of = orc.stats()["force"]
+    assert abs(st.force[0] - of[0]) < 1e-3 * abs(of[0])
+
+
+# ---- full-width cases: 256-long FFT lines in every direction and stream ---
+# CTAs that process several work items back to back (n_items > grid).
+
+def test_poisson_256_lines_vs_oracle(oracle):
+    cells = (64, 256, 256)
+    nx, ny, nz = cells
+    sim = make_sim(cells, 1.0)
+    rhs = np.random.default_rng(21).standard_normal((nz, ny, nx))
+    assert rel_l2(sim.pressureSolver.solve_field(rhs), oracle.poisson_solve(rhs, sim.h)) < 1e-12
+
+
+@pytest.mark.parametrize("scheme,precision", [("upwind3_rk2", "fp64"), ("ref", "fp64"),
+                                              ("upwind3_rk2", "fp32_dc")])
+def test_wide_grid_steps_vs_oracle(oracle, scheme, precision):
+    cells = (256, 256, 32)
+    nx, ny, nz = cells
+    sim = make_sim(cells, 2 * np.pi, nu=1e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0, scheme=scheme,
+                   precision=precision)
+    orc = oracle.OracleSim(nx, ny, nz, 2 * np.pi, nu=1e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0, scheme=scheme)
+    from cubismup_3d_b200 import initial_conditions as ic
+    u, v, w = ic.random_solenoidal(cells, 5, lambda k: k ** 4 * np.exp(-2 * (k / 4) ** 2), rms=1.0)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    tol = TOL_STEP if precision == "fp64" else 1e-6
+    for s in range(2):
+        dt = orc.calc_max_timestep()
+        sim.timestep(dt)
+        orc.timestep(dt)
+        for a, b in zip(sim.velocity(), orc.velocity()):
+            assert rel_l2(a, b) < tol
