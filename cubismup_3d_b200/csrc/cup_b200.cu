@@ -14,9 +14,11 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <utility>
 #include <vector>
 
+#include "advect.cuh"
 #include "common.cuh"
 #include "dht.cuh"
 #include "ops.cuh"
@@ -35,11 +37,13 @@ struct DevState {
   double time;
   double res2, b2;
   double cmean[8];  // parity-class means of p (the 8 null-mode components)
+  double rmean[8];  // parity-class means of the first residual (the RHS's null parts)
+  double res_hist[16];  // relative residual at each check of the last solve
   int step, n_solves, converged, pad_;
 };
 
 enum PartialRegion { P_GRAD = 0, P_PEN, P_RHSOB, P_CHI, P_MAX, P_RES, P_DIAG, P_COUNT };
-constexpr int kPartialCap = 32768;  // doubles per region (>= 16 per CTA)
+constexpr int kPartialCap = 98304;  // doubles per region (>= 20 per CTA of a 4096-CTA pass)
 
 constexpr int kBoxThreads = 256;
 constexpr int kBoxBlocksMax = 296;
@@ -196,31 +200,28 @@ __global__ void k_finalize_residual(const double* p, int np, DevState* st, doubl
     for (int j = 0; j < 18; ++j) s[j] += p[18 * i + j];
   block_reduce<18, false>(s, scratch);
   if (threadIdx.x == 0) {
-    double null2 = 0.0;
-    for (int j = 0; j < 8; ++j) null2 += s[10 + j] * s[10 + j] * inv_class_cells;
-    const double res2 = fmax(s[0] - null2, 0.0), b2 = fmax(s[1] - null2, 0.0);
+    double res2, b2;
+    if (k == 0) {
+      // the null parts of r are those of b (L_2h p has none); keep them for later checks
+      double null2 = 0.0;
+      for (int j = 0; j < 8; ++j) {
+        st->rmean[j] = s[10 + j] * inv_class_cells;
+        null2 += s[10 + j] * s[10 + j] * inv_class_cells;
+      }
+      b2 = fmax(s[1] - null2, 0.0);
+      res2 = fmax(s[0] - null2, 0.0);
+    } else {
+      b2 = st->b2;
+      res2 = s[0];  // accumulated with the null parts removed per cell
+    }
     st->res2 = res2;
     st->b2 = b2;
+    if (k < 16) st->res_hist[k] = b2 > 0 ? sqrt(res2 / b2) : 0.0;
     for (int j = 0; j < 8; ++j) st->cmean[j] = s[2 + j] * inv_class_cells;
     const bool met = b2 == 0.0 || sqrt(res2) <= tol * sqrt(b2);
     st->n_solves = k;
     st->converged = (k >= min_iter && met) ? 1 : 0;
     if (k >= max_iter) st->converged = met ? 1 : 2;  // 2: not converged after max_iter solves
-  }
-}
-
-// p += delta (FP32 correction) minus the parity-class means of p measured by
-// the preceding residual pass, which removes the 8 null-mode components of
-// p (the mean-pressure fix) in FP64.
-__global__ void k_add_correction(double* p, const float* d, int nx, int ny, size_t n, const DevState* st,
-                                 const int* skip) {
-  if (skip && *skip) return;
-  double cm[8];
-  for (int j = 0; j < 8; ++j) cm[j] = st->cmean[j];
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
-    const int cls = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
-    p[i] = p[i] + (double)d[i] - cm[cls];
   }
 }
 
@@ -523,37 +524,45 @@ const float2* table<float>(cup_handle* H, int axis) {
   return H->tw32[axis];
 }
 
-template <int M, typename R>
-int launch_rows_M(cup_handle* H, const R* in, R* out, const int* skip) {
+template <int M, typename R, class Prod, class Cons>
+int launch_rows_M(cup_handle* H, const char* name, const Prod& prod, const Cons& cons, const int* skip) {
   constexpr int N = 2 * M, TPL = M / 8;
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
   const int lpc = 256 / TPL;
   const int nrows = H->ny * H->nz;
   const size_t smem = (size_t)lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
-                      FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + 16 + 128;
-  auto kern = k_dht_rows<M, R>;
+                      FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + 16 + 32 * 20 * sizeof(double) + 128;
+  auto kern = k_dht_rows<M, R, Prod, Cons>;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, lpc * TPL, &bpsm);
   if (rc) return rc;
   const int grid = (nrows + lpc - 1) / lpc;
-  return launch_named(H, "dht_x", [&]() -> int {
-    kern<<<grid, lpc * TPL, smem, H->stream>>>(in, out, nrows, lpc, table<R>(H, 0), H->derr, skip);
+  if (grid > kPartialCap / 20) return fail(H, CUP_ERR_ARG, "too many row tiles for the partial buffers");
+  return launch_named(H, name, [&]() -> int {
+    kern<<<grid, lpc * TPL, smem, H->stream>>>(prod, cons, nrows, lpc, table<R>(H, 0), H->derr, skip);
     CKL();
     return CUP_OK;
   });
 }
 
-template <typename R>
-int launch_rows(cup_handle* H, const R* in, R* out, const int* skip) {
+template <typename R, class Prod, class Cons>
+int launch_rows(cup_handle* H, const char* name, const Prod& prod, const Cons& cons, const int* skip) {
   switch (H->nx / 2) {
-    case 8: return launch_rows_M<8, R>(H, in, out, skip);
-    case 16: return launch_rows_M<16, R>(H, in, out, skip);
-    case 32: return launch_rows_M<32, R>(H, in, out, skip);
-    case 64: return launch_rows_M<64, R>(H, in, out, skip);
-    case 128: return launch_rows_M<128, R>(H, in, out, skip);
-    case 256: return launch_rows_M<256, R>(H, in, out, skip);
+    case 8: return launch_rows_M<8, R>(H, name, prod, cons, skip);
+    case 16: return launch_rows_M<16, R>(H, name, prod, cons, skip);
+    case 32: return launch_rows_M<32, R>(H, name, prod, cons, skip);
+    case 64: return launch_rows_M<64, R>(H, name, prod, cons, skip);
+    case 128: return launch_rows_M<128, R>(H, name, prod, cons, skip);
+    case 256: return launch_rows_M<256, R>(H, name, prod, cons, skip);
   }
   return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
+}
+
+// number of CTAs of a rows pass (= partials written by a reducing producer)
+int rows_grid(const cup_handle* H) {
+  const int TPL = std::max(1, H->nx / 16);
+  const int lpc = 256 / TPL;
+  return (H->ny * H->nz + lpc - 1) / lpc;
 }
 
 template <int M, typename R, int AXIS, bool DIVIDE>
@@ -594,14 +603,24 @@ int launch_cols(cup_handle* H, R* buf, const int* skip) {
 
 // p = H(f . H(work)) over the three axes, in place on `work`; the last x
 // pass writes to `out` (may equal work).
+// The y, z (+ divide + inverse) and y passes, in place on `work`.
 template <typename R>
-int fft_poisson(cup_handle* H, R* work, R* out, const int* skip = nullptr) {
+int fft_middle(cup_handle* H, R* work, const int* skip) {
   int rc;
-  if ((rc = launch_rows<R>(H, work, work, skip))) return rc;
   if ((rc = launch_cols<R, 1, false>(H, work, skip))) return rc;
   if ((rc = launch_cols<R, 2, true>(H, work, skip))) return rc;
   if ((rc = launch_cols<R, 1, false>(H, work, skip))) return rc;
-  if ((rc = launch_rows<R>(H, work, out, skip))) return rc;
+  return CUP_OK;
+}
+
+// p = H(f . H(work)) over the three axes, in place on `work`; the last x
+// pass writes to `out` (may equal work).
+template <typename R>
+int fft_poisson(cup_handle* H, R* work, R* out, const int* skip = nullptr) {
+  int rc;
+  if ((rc = launch_rows<R>(H, "dht_x", RowsFromArray<R>{work}, RowsToArray<R>{work}, skip))) return rc;
+  if ((rc = fft_middle<R>(H, work, skip))) return rc;
+  if ((rc = launch_rows<R>(H, "dht_x", RowsFromArray<R>{work}, RowsToArray<R>{out}, skip))) return rc;
   return CUP_OK;
 }
 
@@ -625,35 +644,56 @@ int read_state(cup_handle* H) {
 }
 
 // ---- typed pipeline pieces -------------------------------------------------
+// Launches one k_advect_zq pass: fields `in` (stencil), `base` (stage-2
+// point-wise u^n, else unused), output `out`.
+template <typename T, int SCHEME, int TY, int NS, int CPT>
+int launch_advect(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out, DtArg dt) {
+  constexpr int G = AdvectTraits<SCHEME>::G;
+  const int cells = TY * H->nx;
+  if (cells % CPT || cells / CPT > 512 || H->ny % TY)
+    return fail(H, CUP_ERR_ARG, "advection tile does not fit the grid");
+  AdvectMaps maps;
+  for (int f = 0; f < 3; ++f) {
+    int rc = make_map(H, &maps.main[f], in[f], tma_dtype<T>(), sizeof(T), H->nx, TY, 1);
+    if (!rc) rc = make_map(H, &maps.halo[f], in[f], tma_dtype<T>(), sizeof(T), H->nx, G, 1);
+    if (!rc) rc = make_map(H, &maps.base[f], AdvectTraits<SCHEME>::BASE ? base[f] : in[f], tma_dtype<T>(), sizeof(T),
+                           H->nx, TY, 1);
+    if (rc) return rc;
+  }
+  const int zc = std::min(16, H->nz);
+  StreamGeom g{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
+  const size_t smem = advect_smem_bytes<T, SCHEME, TY, NS, CPT>(H->nx) + 128;
+  auto kern = k_advect_zq<T, SCHEME, TY, NS, CPT>;
+  const int threads = cells / CPT;
+  int bpsm = 0;
+  int rc = prepare_kernel(H, kern, smem, threads, &bpsm);
+  if (rc) return rc;
+  const int grid = std::min(g.n_items, bpsm * H->num_sms);
+  return launch_named(H, name, [&]() -> int {
+    kern<<<grid, threads, smem, H->stream>>>(maps, g, (T*)out[0], (T*)out[1], (T*)out[2], dt, H->h, H->cfg.nu,
+                                             H->uinf[0], H->uinf[1], H->uinf[2], H->derr);
+    CKL();
+    return CUP_OK;
+  });
+}
+
 template <typename T>
 int do_advect_diffuse(cup_handle* H, DtArg dt) {
+  constexpr bool F32 = std::is_same<T, float>::value;
   int rc;
-  T* u = (T*)H->u;
-  T* v = (T*)H->v;
-  T* w = (T*)H->w;
-  T* tu = (T*)H->tu;
-  T* tv = (T*)H->tv;
-  T* tw = (T*)H->tw;
-  const void* uvw[3] = {u, v, w};
+  void* uvw[3] = {H->u, H->v, H->w};
+  void* tmp[3] = {H->tu, H->tv, H->tw};
   if (H->cfg.scheme == CUP_SCHEME_REF) {
-    OpAdvectDiffuseRef<T> op{tu, tv, tw, dt, H->h, H->cfg.nu, {H->uinf[0], H->uinf[1], H->uinf[2]}, H->nx, H->ny};
-    if (H->fp32) rc = launch_stream<T, 3, 1, 8, 4>(H, "advect_diffuse_ref", uvw, op);
-    else rc = launch_stream<T, 3, 1, 4, 4>(H, "advect_diffuse_ref", uvw, op);
+    if constexpr (F32) rc = launch_advect<T, 0, 8, 5, 4>(H, "advect_diffuse_ref", uvw, uvw, tmp, dt);
+    else rc = launch_advect<T, 0, 4, 5, 2>(H, "advect_diffuse_ref", uvw, uvw, tmp, dt);
   } else {
-    T* u1 = (T*)H->u1;
-    T* v1 = (T*)H->v1;
-    T* w1 = (T*)H->w1;
-    OpUpwind3Stage<T, false> s1{nullptr, nullptr, nullptr, u1, v1, w1, dt, H->h, H->cfg.nu,
-                                {H->uinf[0], H->uinf[1], H->uinf[2]}, H->nx, H->ny};
-    OpUpwind3Stage<T, true> s2{u, v, w, tu, tv, tw, dt, H->h, H->cfg.nu, {H->uinf[0], H->uinf[1], H->uinf[2]},
-                               H->nx, H->ny};
-    const void* uvw1[3] = {u1, v1, w1};
-    if (H->fp32) {
-      if ((rc = launch_stream<T, 3, 2, 4, 6>(H, "upwind3_stage1", uvw, s1))) return rc;
-      rc = launch_stream<T, 3, 2, 4, 6>(H, "upwind3_stage2", uvw1, s2);
+    void* st1[3] = {H->u1, H->v1, H->w1};
+    if constexpr (F32) {
+      if ((rc = launch_advect<T, 1, 8, 5, 4>(H, "upwind3_stage1", uvw, uvw, st1, dt))) return rc;
+      rc = launch_advect<T, 2, 8, 3, 4>(H, "upwind3_stage2", st1, uvw, tmp, dt);
     } else {
-      if ((rc = launch_stream<T, 3, 2, 2, 6>(H, "upwind3_stage1", uvw, s1))) return rc;
-      rc = launch_stream<T, 3, 2, 2, 6>(H, "upwind3_stage2", uvw1, s2);
+      if ((rc = launch_advect<T, 1, 4, 4, 2>(H, "upwind3_stage1", uvw, uvw, st1, dt))) return rc;
+      rc = launch_advect<T, 2, 4, 3, 2>(H, "upwind3_stage2", st1, uvw, tmp, dt);
     }
   }
   if (rc) return rc;
@@ -705,8 +745,10 @@ int do_pressure_rhs(cup_handle* H, DtArg dt) {
 }
 
 // FP32 correction solve inside an FP64 defect-correction loop, warm-started
-// from the current p: check k computes r = b - h^3 L_2h p (FP64) and decides
-// convergence on the device; solve k transforms r in FP32 and adds the
+// from the current p, on the RHS array b. Check k: the FP64 residual
+// r = b - h^3 L_2h p (TMA plane stream over p with a 2-ring halo), its norms
+// and parity-class sums, FP32 r out; a one-block kernel decides convergence on
+// the device. Solve k: the five FFT passes in FP32, the last x pass adding the
 // correction to p in FP64. Kernels after convergence exit at entry.
 int do_poisson_dc(cup_handle* H) {
   const double tol = H->cfg.dc_tol > 0 ? H->cfg.dc_tol : 1e-10;
@@ -717,7 +759,7 @@ int do_poisson_dc(cup_handle* H) {
   int rc;
   for (int k = 0; k <= max_iter; ++k) {
     const void* pf[1] = {H->p};
-    OpResidual op{H->rhs, H->work32, partial(H, P_RES), H->h / 4, H->nx, H->ny};
+    OpResidual op{H->rhs, H->work32, partial(H, P_RES), k > 0 ? H->dstate->rmean : nullptr, H->h / 4, H->nx, H->ny};
     int grid = 0;
     if ((rc = launch_stream<double, 1, 2, 4, 6>(H, "dc_residual", pf, op, &grid, k > 0 ? conv : nullptr))) return rc;
     {
@@ -730,20 +772,27 @@ int do_poisson_dc(cup_handle* H) {
       if (rc_) return rc_;
     }
     if (k == max_iter) break;
-    if ((rc = fft_poisson<float>(H, H->work32, H->work32, conv))) return rc;
-    {
-      const int g = std::min<size_t>(H->num_sms * 8, (H->n + 255) / 256);
-      int rc_ = launch_named(H, "dc_update", [&]() -> int {
-        k_add_correction<<<g, 256, 0, H->stream>>>(H->p, H->work32, H->nx, H->ny, H->n, H->dstate, conv);
-        CKL();
-        return CUP_OK;
-      });
-      if (rc_) return rc_;
-    }
+    if ((rc = launch_rows<float>(H, "dht_x", RowsFromArray<float>{H->work32}, RowsToArray<float>{H->work32}, conv)))
+      return rc;
+    if ((rc = fft_middle<float>(H, H->work32, conv))) return rc;
+    if ((rc = launch_rows<float>(H, "dht_x_update_p", RowsFromArray<float>{H->work32},
+                                 RowsUpdateP{H->p, H->dstate->cmean, H->nx, H->ny}, conv)))
+      return rc;
   }
   return CUP_OK;
 }
 
+// FP64 solve with the RHS computed inside the first x pass (no RHS array).
+template <typename T>
+int do_poisson_fused_fp64(cup_handle* H, DtArg dt) {
+  int rc;
+  RowsRhs<T> prod{(const T*)H->u, (const T*)H->v, (const T*)H->w, dt, H->h, H->nx, H->ny, H->nz};
+  if ((rc = launch_rows<double>(H, "rhs_dht_x", prod, RowsToArray<double>{H->rhs}, nullptr))) return rc;
+  if ((rc = fft_middle<double>(H, H->rhs, nullptr))) return rc;
+  return launch_rows<double>(H, "dht_x", RowsFromArray<double>{H->rhs}, RowsToArray<double>{H->p}, nullptr);
+}
+
+// Poisson solve of the RHS array (operator-by-operator path, obstacles).
 int do_poisson(cup_handle* H) {
   if (!H->fp32) return fft_poisson<double>(H, H->rhs, H->p);
   return do_poisson_dc(H);
@@ -811,8 +860,16 @@ template <typename T>
 int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance) {
   int rc;
   if ((rc = do_advect_diffuse<T>(H, dt))) return rc;
-  if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
-  if ((rc = do_poisson(H))) return rc;
+  if (H->has_sphere) {
+    // the obstacle terms need global sums over the RHS first: unfused path
+    if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
+    if ((rc = do_poisson(H))) return rc;
+  } else if (H->fp32) {
+    if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
+    if ((rc = do_poisson_dc(H))) return rc;
+  } else {
+    if ((rc = do_poisson_fused_fp64<T>(H, dt))) return rc;
+  }
   if ((rc = do_grad<T>(H, dt))) return rc;
   if ((rc = do_penalize<T>(H, dt, lambda_dev))) return rc;
   {
@@ -1470,6 +1527,17 @@ int cup_debug_shift(cup_handle* H, const double* f, double* out, int g, int dx, 
   CK(cudaMemcpyAsync(out, H->p, H->n * sizeof(double), outk, H->stream));
   CK(cudaStreamSynchronize(H->stream));
   return check_dev_error(H);
+}
+
+int cup_dc_history(cup_handle* H, double* out, int n, int* n_checks) {
+  REQUIRE_H(H);
+  if (!out || n <= 0) return fail(H, CUP_ERR_ARG, "bad history buffer");
+  int rc = read_state(H);
+  if (rc) return rc;
+  const int m = H->fp32 ? std::min(std::min(n, 16), H->hstate->n_solves + 1) : 0;
+  for (int i = 0; i < m; ++i) out[i] = H->hstate->res_hist[i];
+  if (n_checks) *n_checks = m;
+  return CUP_OK;
 }
 
 int cup_profile_enable(cup_handle* H, int on) {

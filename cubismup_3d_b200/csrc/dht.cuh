@@ -286,10 +286,32 @@ __device__ __forceinline__ void load_table(R2* dst, const R2* src, int n) {
 
 // ---------------------------------------------------------------------------
 // x pass: LPC consecutive rows of length N = 2M per CTA (rows are contiguous
-// in the [z][y][x] layout), loaded with one 1-D bulk copy, transformed, and
-// written back with one bulk store. in may equal out.
-template <int M, typename R>
-__global__ void __launch_bounds__(256) k_dht_rows(const R* in, R* out, int nrows, int lpc,
+// in the [z][y][x] layout: row r is (y, z) = (r % ny, r / ny)). A producer
+// fills the rows in shared memory (a 1-D bulk copy, or rows computed from
+// other fields), the rows are transformed, and a consumer drains them (a bulk
+// store, or an update of another field).
+
+// Producer: rows copied from an array (one bulk copy).
+template <typename R>
+struct RowsFromArray {
+  static constexpr bool kBulk = true;
+  const R* in;
+  __device__ const R* src(int row0, int N) const { return in + (size_t)row0 * N; }
+  __device__ void fill(R*, int, int, int, double*) const {}
+  __device__ void finish(double*, double*) const {}
+};
+
+// Consumer: rows stored to an array (one bulk store).
+template <typename R>
+struct RowsToArray {
+  static constexpr bool kBulk = true;
+  R* out;
+  __device__ R* dst(int row0, int N) const { return out + (size_t)row0 * N; }
+  __device__ void drain(const R*, int, int, int) const {}
+};
+
+template <int M, typename R, class Prod, class Cons>
+__global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons cons, int nrows, int lpc,
                                                   const typename Cplx<R>::T* tw_g, int* err, const int* skip) {
   using R2 = typename Cplx<R>::T;
   if (skip && *skip) return;
@@ -303,35 +325,50 @@ __global__ void __launch_bounds__(256) k_dht_rows(const R* in, R* out, int nrows
   R* padb = rows + (size_t)lpc * N;                                // lpc * PPITCH
   R2* tw = reinterpret_cast<R2*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
+  double* scratch = reinterpret_cast<double*>(bar + 1);            // 32 * 20 doubles
   const int row0 = blockIdx.x * lpc;
   const int nr = min(lpc, nrows - row0);
   if (nr <= 0) return;
   const uint32_t bytes = (uint32_t)((size_t)nr * N * sizeof(R));
-  // the barrier must be initialised before any thread waits on it
-  if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    mbar_fence_init();
+  double acc[20];
+#pragma unroll
+  for (int i = 0; i < 20; ++i) acc[i] = 0.0;
+  if constexpr (Prod::kBulk) {
+    // the barrier must be initialised before any thread waits on it
+    if (threadIdx.x == 0) {
+      mbar_init(bar, 1);
+      mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      mbar_arrive_expect_tx(bar, bytes);
+      bulk_load(rows, prod.src(row0, N), bytes, bar);
+    }
+    load_table(tw, tw_g, TL);
+    const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
+    if (!ok) return;
+  } else {
+    load_table(tw, tw_g, TL);
+    prod.fill(rows, row0, nr, N, acc);
+    __syncthreads();
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    mbar_arrive_expect_tx(bar, bytes);
-    bulk_load(rows, in + (size_t)row0 * N, bytes, bar);
-  }
-  load_table(tw, tw_g, TL);
-  const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
-  if (!ok) return;
   const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
   const bool active = l < nr;
   RowLines<R> A{rows, N};
   RowLinesPad<R> P{padb, PPITCH};
   dht_lines<M, PAD, R>(A, P, tw, l, t, active);
-  fence_proxy_async_smem();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    bulk_store(out + (size_t)row0 * N, rows, bytes);
-    bulk_commit();
-    bulk_wait_all();
+  if constexpr (Cons::kBulk) {
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      bulk_store(cons.dst(row0, N), rows, bytes);
+      bulk_commit();
+      bulk_wait_all();
+    }
+  } else {
+    cons.drain(rows, row0, nr, N);
   }
+  if constexpr (!Prod::kBulk) prod.finish(acc, scratch);
 }
 
 // Spectral factor of PoissonSolverPeriodic::_solve (grid-consistent branch,

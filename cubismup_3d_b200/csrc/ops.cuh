@@ -12,6 +12,9 @@ __device__ __forceinline__ size_t gidx(int x, int y, int z, int nx, int ny) {
   return ((size_t)z * ny + y) * nx + x;
 }
 
+// periodic wrap of an index at most one period outside [0, n)
+__device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
 // Time step argument: host value, or a device scalar when chaining steps on
 // the GPU without a host round trip (the CFL dt is computed on the device).
 struct DtArg {
@@ -146,7 +149,8 @@ struct OpPressureRHS {
 struct OpResidual {
   const double* b;
   float* r;
-  double* partials;  // [gridDim.x][18]
+  double* partials;     // [gridDim.x][18]
+  const double* rmean;  // parity-class means of r from the first check (null parts), or nullptr
   double c;          // h / 4 = h^3 / (4 h^2)
   int nx, ny;
   template <class C>
@@ -158,10 +162,14 @@ struct OpResidual {
     const size_t o = gidx(x, gy, gz, nx, ny);
     const double bb = b[o];
     const double res = bb - c * (lx + ly + lz);
-    r[o] = (float)res;
-    acc[0] += res * res;
-    acc[1] += bb * bb;
     const int cls = (x & 1) | ((gy & 1) << 1) | ((gz & 1) << 2);
+    // Null parts removed per cell, before the FP32 cast (their FP32 rounding
+    // would otherwise feed the correction noise of their own size) and before
+    // squaring (subtracting norms afterwards cancels catastrophically).
+    const double rp = rmean ? res - rmean[cls] : res;
+    r[o] = (float)rp;
+    acc[0] += rp * rp;
+    acc[1] += bb * bb;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
       acc[2 + k] += (k == cls) ? p0 : 0.0;
@@ -175,6 +183,50 @@ struct OpResidual {
     block_reduce<18, false>(v, scratch);
     if (threadIdx.x == 0)
       for (int k = 0; k < 18; ++k) partials[18 * blockIdx.x + k] = v[k];
+  }
+};
+
+// ---- producers / consumers of the fused x pass (k_dht_rows) ---------------
+
+// Rows of the pressure RHS computed from u* (KernelPressureRHS,
+// source/operators/PressureRHS.cpp:51-76): fused into the first x pass so the
+// RHS never goes to HBM.
+template <typename T>
+struct RowsRhs {
+  static constexpr bool kBulk = false;
+  const T *u, *v, *w;
+  DtArg dt;
+  double h;
+  int nx, ny, nz;
+  __device__ void fill(double* rows, int row0, int nr, int N, double*) const {
+    const double fac = 0.5 * h * h / dt.get();
+    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) {
+      const int l = i / N, x = i - l * N;
+      const int r = row0 + l, y = r % ny, z = r / ny;
+      const double uE = u[gidx(wrapi(x + 1, nx), y, z, nx, ny)], uW = u[gidx(wrapi(x - 1, nx), y, z, nx, ny)];
+      const double vN = v[gidx(x, wrapi(y + 1, ny), z, nx, ny)], vS = v[gidx(x, wrapi(y - 1, ny), z, nx, ny)];
+      const double wB = w[gidx(x, y, wrapi(z + 1, nz), nx, ny)], wF = w[gidx(x, y, wrapi(z - 1, nz), nx, ny)];
+      rows[i] = fac * (uE - uW + vN - vS + wB - wF);
+    }
+  }
+  __device__ void finish(double*, double*) const {}
+};
+
+// Consumer of the last x pass of a correction solve: p += delta - (parity-class
+// means of p measured by the preceding residual pass), in FP64.
+struct RowsUpdateP {
+  static constexpr bool kBulk = false;
+  double* p;
+  const double* cmean;
+  int nx, ny;
+  __device__ void drain(const float* rows, int row0, int nr, int N) const {
+    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) {
+      const int l = i / N, x = i - l * N;
+      const int r = row0 + l, y = r % ny, z = r / ny;
+      const size_t o = (size_t)r * N + x;
+      const int cls = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
+      p[o] = p[o] + (double)rows[i] - cmean[cls];
+    }
   }
 };
 
@@ -256,7 +308,6 @@ __device__ __forceinline__ double sphere_sdf(const SphereParams& s, double x, do
   return s.radius - sqrt(dx * dx + dy * dy + dz * dz);
 }
 
-__device__ __forceinline__ int wrapi(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
 
 // KernelCharacteristicFunction (source/operators/ObstaclesCreate.cpp:51-136)
 // with the sphere SDF of source/obstacles/Sphere.cpp:44-48 evaluated

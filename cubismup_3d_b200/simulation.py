@@ -400,6 +400,13 @@ class Simulation:
         L.check(L.lib().cup_diagnostics(self._h, out), self._h, "diagnostics")
         return {"ke": out[0], "div_l2": out[1], "div_max": out[2]}
 
+    def dc_history(self) -> list:
+        """Relative residuals at each defect-correction check of the last solve."""
+        out = (C.c_double * 16)()
+        n = C.c_int()
+        L.check(L.lib().cup_dc_history(self._h, out, 16, C.byref(n)), self._h, "dc_history")
+        return list(out[:n.value])
+
     def profile(self, on: bool = True):
         L.check(L.lib().cup_profile_enable(self._h, int(on)), self._h, "profile")
 

@@ -171,6 +171,11 @@ int cup_diagnostics(struct cup_handle* h, double out[3]);
  * stencil kernels use, halo g in {1, 2}. f, out: device or host FP64 arrays. */
 int cup_debug_shift(struct cup_handle* h, const double* f, double* out, int g, int dx, int dy, int dz, int where);
 
+/* FP32_DC: relative residuals |r| / |b| (null-mode parts excluded) at each
+ * check of the last defect-correction solve, check 0 being the warm-started
+ * residual before the first FP32 correction; *n_checks = entries written. */
+int cup_dc_history(struct cup_handle* h, double* out, int n, int* n_checks);
+
 /* ---- profiling (the reference's Profiler regions, SimulationData.cpp:293-305,
  * as CUDA-event ranges per kernel) ---- */
 /* Turns per-kernel CUDA-event timing on or off (off by default; no host sync while on). */
