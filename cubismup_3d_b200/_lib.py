@@ -107,6 +107,8 @@ SIGNATURES = {
     "cup_poisson_solve_field": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_int]),
     "cup_diagnostics": (C.c_int, [_H, _dp]),
     "cup_debug_shift": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "cup_max_velocity_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, _dp, C.c_void_p,
+                                           C.c_void_p]),
     "cup_dc_history": (C.c_int, [_H, _dp, C.c_int, C.POINTER(C.c_int)]),
     "cup_profile_enable": (C.c_int, [_H, C.c_int]),
     "cup_profile_report": (C.c_int, [_H, C.c_char_p, C.c_size_t, C.c_int]),

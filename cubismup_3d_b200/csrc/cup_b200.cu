@@ -265,6 +265,39 @@ struct OpShift {
 };
 
 // ---------------------------------------------------------------------------
+// Allocation-free max |u + uinf| (cup_max_velocity_noalloc). Its per-CTA
+// partial maxima live in this fixed device array instead of handle-owned
+// memory: every GPU that loads the library holds the array until exit, and all
+// calls share it. Each CTA reduces one chunk of kNoAllocChunk cells, so one
+// call handles at most kNoAllocMaxCtas * kNoAllocChunk cells.
+constexpr int kNoAllocMaxCtas = 4096;
+constexpr long long kNoAllocChunk = 65536;
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxCtas];
+
+__global__ void k_noalloc_max_partial(const double* __restrict__ u, const double* __restrict__ v,
+                                      const double* __restrict__ w, long long n, double ux, double uy, double uz,
+                                      double* partials) {
+  __shared__ double scratch[32];
+  double m[1] = {0.0};
+  const long long lo = blockIdx.x * kNoAllocChunk;
+  const long long hi = lo + kNoAllocChunk < n ? lo + kNoAllocChunk : n;
+  for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    const double a = fabs(u[i] + ux), b = fabs(v[i] + uy), c = fabs(w[i] + uz);
+    m[0] = fmax(m[0], fmax(fmax(a, b), c));
+  }
+  block_reduce<1, true>(m, scratch);
+  if (threadIdx.x == 0) partials[blockIdx.x] = m[0];  // every used slot is written before it is read
+}
+
+__global__ void k_noalloc_max_final(const double* partials, int np, double* out) {
+  __shared__ double scratch[32];
+  double m[1] = {0.0};
+  for (int i = threadIdx.x; i < np; i += blockDim.x) m[0] = fmax(m[0], partials[i]);
+  block_reduce<1, true>(m, scratch);
+  if (threadIdx.x == 0) *out = m[0];
+}
+
+// ---------------------------------------------------------------------------
 // host helpers
 
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
@@ -1527,6 +1560,54 @@ int cup_debug_shift(cup_handle* H, const double* f, double* out, int g, int dx, 
   CK(cudaMemcpyAsync(out, H->p, H->n * sizeof(double), outk, H->stream));
   CK(cudaStreamSynchronize(H->stream));
   return check_dev_error(H);
+}
+
+// Device address of g_noalloc_partials per device, looked up once with that
+// device current (host code must not use the symbol itself as an address).
+static double* noalloc_partials_ptr(int dev, int* err_out) {
+  static std::mutex mu;
+  static double* ptrs[64] = {nullptr};
+  if (dev < 0 || dev >= 64) {
+    *err_out = CUP_ERR_ARG;
+    return nullptr;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (!ptrs[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (e != cudaSuccess || !p) {
+      fprintf(stderr, "cup_max_velocity_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
+      *err_out = CUP_ERR_CUDA;
+      return nullptr;
+    }
+    ptrs[dev] = static_cast<double*>(p);
+  }
+  return ptrs[dev];
+}
+
+int cup_max_velocity_noalloc(const double* u, const double* v, const double* w, long long n, const double uinf[3],
+                             double* umax_dev, void* stream) {
+  if (!u || !v || !w || !uinf || !umax_dev || n <= 0) return CUP_ERR_ARG;
+  const long long max_cells = (long long)kNoAllocMaxCtas * kNoAllocChunk;
+  if (n > max_cells) {
+    fprintf(stderr,
+            "cup_max_velocity_noalloc: %lld cells exceed the fixed scratch limit of %lld cells per call "
+            "(%d partials of %lld cells); split the field or use cup_max_velocity\n",
+            n, max_cells, kNoAllocMaxCtas, kNoAllocChunk);
+    return CUP_ERR_ARG;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return CUP_ERR_CUDA;
+  int rc = CUP_OK;
+  double* partials = noalloc_partials_ptr(dev, &rc);
+  if (!partials) return rc;
+  const int nblocks = (int)((n + kNoAllocChunk - 1) / kNoAllocChunk);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  k_noalloc_max_partial<<<nblocks, 256, 0, st>>>(u, v, w, n, uinf[0], uinf[1], uinf[2], partials);
+  if (cudaGetLastError() != cudaSuccess) return CUP_ERR_CUDA;
+  k_noalloc_max_final<<<1, 256, 0, st>>>(partials, nblocks, umax_dev);
+  if (cudaGetLastError() != cudaSuccess) return CUP_ERR_CUDA;
+  return CUP_OK;
 }
 
 int cup_dc_history(cup_handle* H, double* out, int n, int* n_checks) {

@@ -171,6 +171,25 @@ int cup_diagnostics(struct cup_handle* h, double out[3]);
  * stencil kernels use, halo g in {1, 2}. f, out: device or host FP64 arrays. */
 int cup_debug_shift(struct cup_handle* h, const double* f, double* out, int g, int dx, int dy, int dz, int where);
 
+/* Allocation-free findMaxU: max over n cells of max(|u+uinf0|, |v+uinf1|, |w+uinf2|)
+ * for caller-owned device arrays u, v, w (FP64), written to the device double
+ * *umax_dev on `stream` (a cudaStream_t; NULL = the legacy default stream); the
+ * call is asynchronous. It has no counterpart in the reference. It exists for
+ * callers that cannot call cudaMalloc: code whose device memory all comes from
+ * another allocator or a budget fixed up front (a framework's caching pool, a
+ * long-running service), and loops that must not allocate once running, since
+ * cudaMalloc can synchronise the device and can fail late. It allocates
+ * nothing: its per-block partial maxima live in a fixed 32 KiB array inside the
+ * library (4096 partials of 65536 cells), which every GPU that loads the library
+ * keeps until exit; n above 2^28 cells is rejected with CUP_ERR_ARG and a message
+ * on stderr. The first call on a device looks up that array's device address
+ * with the device current; make that first call before any stream capture. All
+ * calls share the array, so calls that overlap on the GPU (other streams, other
+ * host threads) race; every slot a call reads is written by the same call first,
+ * so nothing needs clearing between calls. */
+int cup_max_velocity_noalloc(const double* u, const double* v, const double* w, long long n,
+                             const double uinf[3], double* umax_dev, void* stream);
+
 /* FP32_DC: relative residuals |r| / |b| (null-mode parts excluded) at each
  * check of the last defect-correction solve, check 0 being the warm-started
  * residual before the first FP32 correction; *n_checks = entries written. */
