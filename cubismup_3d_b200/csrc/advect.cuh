@@ -122,8 +122,14 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
   const T facD = (T)((nu / h) * (dtv / h));
   const T uinf[3] = {(T)ux, (T)uy, (T)uz};
 
-  T qv[3][Q][CPT];   // centre values of the last 2G+1 planes
-  T part[3][G][CPT]; // x/y partials of the planes awaiting their z terms
+  // Register rings: qv holds the centre values of the last Q = 2G+1 planes
+  // (plane j in slot j % Q), part the x/y partials awaiting their z terms
+  // (the partial of load j in slot j % G). The plane loop is unrolled by
+  // U = lcm(Q, G) and every item's PL = ZC + 2G planes is a multiple of U, so
+  // all ring indices fold to constants: no register shuffling.
+  constexpr int U = (G == 1) ? 3 : 10;
+  T qv[3][Q][CPT];
+  T part[3][G][CPT];
 #pragma unroll
   for (int f = 0; f < 3; ++f)
 #pragma unroll
@@ -137,98 +143,105 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
 #pragma unroll
       for (int i = 0; i < CPT; ++i) part[f][d][i] = (T)0;
 
+  // One block barrier per plane (slot release). Each thread waits on the
+  // slot's mbarrier itself; a thread whose wait timed out stops waiting and
+  // computing but keeps taking the barrier, so the block never deadlocks and
+  // the error word tells the host.
   bool ok = true;
   int q = 0;
-  for (int it = 0; it < my_items && ok; ++it) {
+  for (int it = 0; it < my_items; ++it) {
     const int item = blockIdx.x + it * gridDim.x;
     const int ty = item % g.items_y, zi = item / g.items_y;
     const int y0 = ty * TY, z0 = zi * g.zc;
-    for (int j = 0; j < PL; ++j, ++q) {
-      const int s = q % NS;
-      ok = __syncthreads_and(mbar_wait(&full[s], (q / NS) & 1, err));
-      if (!ok) break;
-      const T* sl = slots + s * slot_elems;
-      // 1. push centre values
+    for (int j0 = 0; j0 < PL; j0 += U) {
 #pragma unroll
-      for (int f = 0; f < 3; ++f)
+      for (int jj = 0; jj < U; ++jj) {
+        const int j = j0 + jj;
+        const int s = q % NS;
+        if (ok) ok = mbar_wait(&full[s], (q / NS) & 1, err);
+        if (ok) {
+          const T* sl = slots + s * slot_elems;
+          const int QN = jj % Q;  // slot of the newest plane
+          // 1. centre values of plane j
 #pragma unroll
-        for (int i = 0; i < CPT; ++i) {
+          for (int f = 0; f < 3; ++f)
 #pragma unroll
-          for (int d = 0; d < Q - 1; ++d) qv[f][d][i] = qv[f][d + 1][i];
-          qv[f][Q - 1][i] = sl[f * field_elems + (G + cy[i]) * nx + cx[i]];
-        }
-      // 2. finish output plane k = j - 2G
-      if (j >= 2 * G) {
-        const int k = j - 2 * G;
+            for (int i = 0; i < CPT; ++i) qv[f][QN][i] = sl[f * field_elems + (G + cy[i]) * nx + cx[i]];
+          // 2. finish output plane k = j - 2G (queue slot of plane k + d - G: (jj - 2G + d) mod Q)
+          if (j >= 2 * G) {
+            const int k = j - 2 * G;
+            const int QC = (jj + 3 * Q - G) % Q;       // centre (load j - G)
+            const int QM1 = (jj + 3 * Q - G - 1) % Q;  // plane k - 1
+            const int QP1 = (jj + 3 * Q - G + 1) % Q;  // plane k + 1
+            const int QM2 = (jj + 3 * Q - G - 2) % Q;  // plane k - 2 (G = 2)
+            const int QP2 = (jj + 3 * Q - G + 2) % Q;  // plane k + 2 (G = 2)
+            const int PS = jj % G;                      // partial of load j - G
 #pragma unroll
-        for (int i = 0; i < CPT; ++i) {
-          const size_t o = gidx(cx[i], y0 + cy[i], z0 + k, nx, ny);
-          const T ww = qv[2][G][i] + uinf[2];
-          T outv[3];
+            for (int i = 0; i < CPT; ++i) {
+              const size_t o = gidx(cx[i], y0 + cy[i], z0 + k, nx, ny);
+              const T ww = qv[2][QC][i] + uinf[2];
+              T outv[3];
 #pragma unroll
-          for (int f = 0; f < 3; ++f) {
-            const T f0 = qv[f][G][i];
-            T dz;
-            if constexpr (SCHEME == 0) {
-              dz = qv[f][G + 1][i] - qv[f][G - 1][i];
-            } else {
-              dz = up3(ww, qv[f][G - 2][i], qv[f][G - 1][i], f0, qv[f][G + 1][i], qv[f][G + 2][i]);
-            }
-            const T lz = qv[f][G - 1][i] + qv[f][G + 1][i];
-            outv[f] = f0 + part[f][0][i] + facA * (ww * dz) + facD * (lz - f0 * 6);
-          }
-          if (BASE) {
-            const T* bs = sl + stencil_elems + cy[i] * nx + cx[i];
-            ou[o] = (T)0.5 * (bs[0] + outv[0]);
-            ov[o] = (T)0.5 * (bs[TY * nx] + outv[1]);
-            ow[o] = (T)0.5 * (bs[2 * TY * nx] + outv[2]);
-          } else {
-            ou[o] = outv[0];
-            ov[o] = outv[1];
-            ow[o] = outv[2];
-          }
-        }
-      }
-      // 3. x/y partial of plane j (output plane j - G)
-      if (j >= G) {
-#pragma unroll
-        for (int f = 0; f < 3; ++f)
-#pragma unroll
-          for (int d = 0; d < G - 1; ++d)
-#pragma unroll
-            for (int i = 0; i < CPT; ++i) part[f][d][i] = part[f][d + 1][i];
-        if (j < G + g.zc) {
-#pragma unroll
-          for (int i = 0; i < CPT; ++i) {
-            const T uu = qv[0][Q - 1][i] + uinf[0], vv = qv[1][Q - 1][i] + uinf[1];
-            const int x = cx[i], r = G + cy[i];
-#pragma unroll
-            for (int f = 0; f < 3; ++f) {
-              const T* F = sl + f * field_elems;
-              const T f0 = qv[f][Q - 1][i];
-              const T xm1 = F[r * nx + ((x - 1) & mask)], xp1 = F[r * nx + ((x + 1) & mask)];
-              const T ym1 = F[(r - 1) * nx + x], yp1 = F[(r + 1) * nx + x];
-              T dx, dy;
-              if constexpr (SCHEME == 0) {
-                dx = xp1 - xm1;
-                dy = yp1 - ym1;
-              } else {
-                const T xm2 = F[r * nx + ((x - 2) & mask)], xp2 = F[r * nx + ((x + 2) & mask)];
-                const T ym2 = F[(r - 2) * nx + x], yp2 = F[(r + 2) * nx + x];
-                dx = up3(uu, xm2, xm1, f0, xp1, xp2);
-                dy = up3(vv, ym2, ym1, f0, yp1, yp2);
+              for (int f = 0; f < 3; ++f) {
+                const T f0 = qv[f][QC][i];
+                T dz;
+                if constexpr (SCHEME == 0) {
+                  dz = qv[f][QP1][i] - qv[f][QM1][i];
+                } else {
+                  dz = up3(ww, qv[f][QM2][i], qv[f][QM1][i], f0, qv[f][QP1][i], qv[f][QP2][i]);
+                }
+                const T lz = qv[f][QM1][i] + qv[f][QP1][i];
+                outv[f] = f0 + part[f][PS][i] + facA * (ww * dz) + facD * (lz - f0 * 6);
               }
-              part[f][G - 1][i] = facA * (uu * dx + vv * dy) + facD * (yp1 + ym1 + xp1 + xm1);
+              if constexpr (BASE) {
+                const T* bs = sl + stencil_elems + cy[i] * nx + cx[i];
+                ou[o] = (T)0.5 * (bs[0] + outv[0]);
+                ov[o] = (T)0.5 * (bs[TY * nx] + outv[1]);
+                ow[o] = (T)0.5 * (bs[2 * TY * nx] + outv[2]);
+              } else {
+                ou[o] = outv[0];
+                ov[o] = outv[1];
+                ow[o] = outv[2];
+              }
+            }
+          }
+          // 3. x/y partial of plane j (output plane j - G), into slot j % G
+          if (j >= G && j < G + g.zc) {
+            const int PS = jj % G;
+#pragma unroll
+            for (int i = 0; i < CPT; ++i) {
+              const T uu = qv[0][QN][i] + uinf[0], vv = qv[1][QN][i] + uinf[1];
+              const int x = cx[i], r = G + cy[i];
+#pragma unroll
+              for (int f = 0; f < 3; ++f) {
+                const T* F = sl + f * field_elems;
+                const T f0 = qv[f][QN][i];
+                const T xm1 = F[r * nx + ((x - 1) & mask)], xp1 = F[r * nx + ((x + 1) & mask)];
+                const T ym1 = F[(r - 1) * nx + x], yp1 = F[(r + 1) * nx + x];
+                T dx, dy;
+                if constexpr (SCHEME == 0) {
+                  dx = xp1 - xm1;
+                  dy = yp1 - ym1;
+                } else {
+                  const T xm2 = F[r * nx + ((x - 2) & mask)], xp2 = F[r * nx + ((x + 2) & mask)];
+                  const T ym2 = F[(r - 2) * nx + x], yp2 = F[(r + 2) * nx + x];
+                  dx = up3(uu, xm2, xm1, f0, xp1, xp2);
+                  dy = up3(vv, ym2, ym1, f0, yp1, yp2);
+                }
+                part[f][PS][i] = facA * (uu * dx + vv * dy) + facD * (yp1 + ym1 + xp1 + xm1);
+              }
             }
           }
         }
+        __syncthreads();  // slot s fully consumed
+        if (tid == 0 && ok && q_issued < L && q_issued == q + NS) issue(q_issued++);
+        ++q;
       }
-      __syncthreads();  // slot s fully consumed
-      if (tid == 0 && q_issued < L && q_issued == q + NS) issue(q_issued++);
     }
   }
   if (!ok && tid == 0) {
-    for (int r = q; r < q_issued; ++r) mbar_wait(&full[r % NS], (r / NS) & 1, nullptr);
+    // bounded drain of this CTA's loads still in flight
+    for (int r = q - NS < 0 ? 0 : q - NS; r < q_issued; ++r) mbar_wait(&full[r % NS], (r / NS) & 1, nullptr);
   }
 }
 

@@ -669,6 +669,70 @@ void op_penalization(OState& S, double dt) {
   for (int d = 0; d < 3; ++d) { s.force[d] = M[d]; s.torque[d] = M[3 + d]; }
 }
 
+// ---------------------------------------------------------------------------
+// Tangent-linear model of the step (test infrastructure: the FP64 directional
+// derivative that GPU adjoints are checked against). The advecting-velocity
+// signs of the upwind stencil are frozen at the base state; the projection is
+// linear and applied to the tangent as is; penalization scales by (1 - dt pf).
+
+// Tangent of one explicit stage S(f) = f + facA sum_d a_d D_d(f) + facD Lap f
+// at base f = (a,b,c) along g = (ga,gb,gc); stage-2 form when base_g given:
+// out = 0.5 (base_g + S'(f) g).
+void stage_tangent(OState& S, double dt, const Real* a, const Real* b, const Real* c, const Real* ga,
+                   const Real* gb, const Real* gc, const Real* bg_u, const Real* bg_v, const Real* bg_w, Real* ou,
+                   Real* ov, Real* ow) {
+  const Dims D = S.D;
+  const Real h = S.h;
+  const Real mu = S.cfg.nu;
+  const bool up = S.cfg.scheme == 1;
+  const Real uInf[3] = {S.uinf[0], S.uinf[1], S.uinf[2]};
+  const Real facA = up ? -dt / (6 * h) : -dt / (2 * h);
+  const Real facD = (mu / h) * (dt / h);
+  const int g = up ? 2 : 1;
+  for_each_block(D, [&](int bx, int by, int bz) {
+    Lab F[3], T[3];
+    F[0].load(a, D, bx, by, bz, g); F[1].load(b, D, bx, by, bz, g); F[2].load(c, D, bx, by, bz, g);
+    T[0].load(ga, D, bx, by, bz, g); T[1].load(gb, D, bx, by, bz, g); T[2].load(gc, D, bx, by, bz, g);
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const Real adv[3] = {F[0](ix, iy, iz) + uInf[0], F[1](ix, iy, iz) + uInf[1], F[2](ix, iy, iz) + uInf[2]};
+      const Real dadv[3] = {T[0](ix, iy, iz), T[1](ix, iy, iz), T[2](ix, iy, iz)};
+      const size_t o = D.idx(bx * BS + ix, by * BS + iy, bz * BS + iz);
+      Real* outs[3] = {ou, ov, ow};
+      const Real* bgs[3] = {bg_u, bg_v, bg_w};
+      auto deriv = [&](const Lab& L, int d, Real av) -> Real {
+        const int ex = d == 0, ey = d == 1, ez = d == 2;
+        const Real fm2 = up ? L(ix - 2 * ex, iy - 2 * ey, iz - 2 * ez) : 0, fp2 = up ? L(ix + 2 * ex, iy + 2 * ey, iz + 2 * ez) : 0;
+        const Real fm1 = L(ix - ex, iy - ey, iz - ez), fp1 = L(ix + ex, iy + ey, iz + ez), f0 = L(ix, iy, iz);
+        return up ? up3(av, fm2, fm1, f0, fp1, fp2) : fp1 - fm1;
+      };
+      for (int q = 0; q < 3; ++q) {
+        Real dA = 0;
+        for (int d = 0; d < 3; ++d) dA += dadv[d] * deriv(F[q], d, adv[d]) + adv[d] * deriv(T[q], d, adv[d]);
+        const Lab& G = T[q];
+        const Real lap = G(ix,iy+1,iz) + G(ix,iy-1,iz) + G(ix+1,iy,iz) + G(ix-1,iy,iz) + G(ix,iy,iz-1) + G(ix,iy,iz+1) - G(ix,iy,iz) * 6;
+        const Real t = G(ix, iy, iz) + facA * dA + facD * lap;
+        outs[q][o] = bgs[q] ? 0.5 * (bgs[q][o] + t) : t;
+      }
+    }
+  });
+}
+
+// P applied to the fields (a,b,c) in place: the pipeline's RHS, periodic
+// Poisson solve and gradient correction on them (dt cancels in P; the
+// pressure field of the state is overwritten).
+void project_fields(OState& S, std::vector<Real>& a, std::vector<Real>& b, std::vector<Real>& c, double dt) {
+  std::swap(S.u, a);
+  std::swap(S.v, b);
+  std::swap(S.w, c);
+  op_pressure_rhs(S, dt);
+  op_pressure_projection(S, dt);
+  std::swap(S.u, a);
+  std::swap(S.v, b);
+  std::swap(S.w, c);
+}
+
 }  // namespace
 
 extern "C" {
@@ -872,6 +936,57 @@ void orc_diagnostics(void* hdl, double* out) {
         dmax = std::max(dmax, std::fabs(div));
       }
   out[0] = ke; out[1] = std::sqrt(d2); out[2] = dmax;
+}
+
+// Tangent-linear rollout (no obstacle): advances the state nsteps with the
+// given dt sequence and the tangent (du, dv, dw) along with it, in place.
+// Returns 1 if the state has an obstacle (not supported), else 0.
+int orc_tangent_run(void* hdl, int nsteps, const double* dts, double* du, double* dv, double* dw) {
+  OState* S = static_cast<OState*>(hdl);
+  if (S->has_sphere) return 1;
+  const size_t n = S->D.n();
+  std::vector<Real> tu(du, du + n), tv(dv, dv + n), tw(dw, dw + n);
+  std::vector<Real> u1(n), v1(n), w1(n), t1u(n), t1v(n), t1w(n);
+  for (int s = 0; s < nsteps; ++s) {
+    const double dt = dts[s];
+    S->dt = dt;
+    if (S->cfg.scheme == 1) {
+      // u1 = S(u), du1 = S'(u) du
+      upwind3_stage(*S, dt, S->u.data(), S->v.data(), S->w.data(), nullptr, nullptr, nullptr, u1.data(), v1.data(),
+                    w1.data());
+      stage_tangent(*S, dt, S->u.data(), S->v.data(), S->w.data(), tu.data(), tv.data(), tw.data(), nullptr, nullptr,
+                    nullptr, t1u.data(), t1v.data(), t1w.data());
+      // u* = 0.5 (u + S(u1)), du* = 0.5 (du + S'(u1) du1)
+      std::vector<Real> su(n), sv(n), sw(n);
+      stage_tangent(*S, dt, u1.data(), v1.data(), w1.data(), t1u.data(), t1v.data(), t1w.data(), tu.data(), tv.data(),
+                    tw.data(), su.data(), sv.data(), sw.data());
+      tu.swap(su);
+      tv.swap(sv);
+      tw.swap(sw);
+      upwind3_stage(*S, dt, u1.data(), v1.data(), w1.data(), S->u.data(), S->v.data(), S->w.data(), S->tmpU.data(),
+                    S->tmpV.data(), S->tmpW.data());
+    } else {
+      std::vector<Real> su(n), sv(n), sw(n);
+      stage_tangent(*S, dt, S->u.data(), S->v.data(), S->w.data(), tu.data(), tv.data(), tw.data(), nullptr, nullptr,
+                    nullptr, su.data(), sv.data(), sw.data());
+      tu.swap(su);
+      tv.swap(sv);
+      tw.swap(sw);
+      advect_diffuse_ref(*S, dt);
+    }
+    std::copy(S->tmpU.begin(), S->tmpU.end(), S->u.begin());
+    std::copy(S->tmpV.begin(), S->tmpV.end(), S->v.begin());
+    std::copy(S->tmpW.begin(), S->tmpW.end(), S->w.begin());
+    op_pressure_rhs(*S, dt);
+    op_pressure_projection(*S, dt);
+    project_fields(*S, tu, tv, tw, dt);
+    S->step++;
+    S->time += dt;
+  }
+  std::copy(tu.begin(), tu.end(), du);
+  std::copy(tv.begin(), tv.end(), dv);
+  std::copy(tw.begin(), tw.end(), dw);
+  return 0;
 }
 
 }  // extern "C"

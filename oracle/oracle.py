@@ -74,6 +74,8 @@ def lib():
         L.orc_lab_shift.argtypes = [dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_lab_shift.restype = C.c_int
         L.orc_diagnostics.argtypes = [C.c_void_p, dp]
+        L.orc_tangent_run.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp]
+        L.orc_tangent_run.restype = C.c_int
         L.orc_num_threads.restype = C.c_int
         L.orc_set_num_threads.argtypes = [C.c_int]
         _lib = L
@@ -155,6 +157,15 @@ class OracleSim:
             fx = np.ascontiguousarray(fixed_dts, dtype=np.float64)
         lib().orc_run(self._h, nsteps, _p(fx) if fx is not None else None, _p(dts))
         return dts
+
+    def tangent_run(self, dts, du, dv, dw):
+        """FP64 tangent-linear rollout with a fixed dt sequence: advances the state and
+        returns the propagated tangent (du, dv, dw)."""
+        dts = np.ascontiguousarray(dts, dtype=np.float64)
+        t = [np.ascontiguousarray(a, dtype=np.float64).copy() for a in (du, dv, dw)]
+        if lib().orc_tangent_run(self._h, len(dts), _p(dts), _p(t[0]), _p(t[1]), _p(t[2])) != 0:
+            raise ValueError("oracle: tangent rollout does not support obstacles")
+        return tuple(t)
 
     def stats(self) -> dict:
         out = np.zeros(21, dtype=np.float64)

@@ -161,3 +161,33 @@ def test_sphere_chi_and_penalization(oracle):
     assert st["force"].shape == (3,)
     assert np.all(np.isfinite(sim.stats()["force"]))
     assert dts[0] > 0
+
+
+@pytest.mark.parametrize("scheme", ["ref", "upwind3_rk2"])
+def test_tangent_linear_matches_central_differences(oracle, scheme):
+    # the FP64 tangent-linear model (checker of the GPU adjoint) against central
+    # differences of the oracle forward with the same fixed dt sequence. The
+    # upwind stencil switches with the sign of the advecting velocity, so its FD
+    # error is O(eps) from cells that flip direction: eps is taken small there.
+    from cubismup_3d_b200 import initial_conditions as ic
+    n, L, nsteps = 32, 2 * np.pi, (4 if scheme == "ref" else 2)
+    kw = dict(nu=5e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0, scheme=scheme)
+    u0 = ic.perturbed_taylor_green((n, n, n), L / n, seed=1)
+    base = oracle.OracleSim(n, n, n, L, **kw)
+    base.set_velocity(*u0)
+    dts = base.run(nsteps)
+    rng = np.random.default_rng(3)
+    d = [rng.standard_normal((n, n, n)) for _ in range(3)]
+    tl = oracle.OracleSim(n, n, n, L, **kw)
+    tl.set_velocity(*u0)
+    tang = tl.tangent_run(dts, *d)
+    eps = 1e-5 if scheme == "ref" else 1e-7
+    out = []
+    for sgn in (+1, -1):
+        s = oracle.OracleSim(n, n, n, L, **kw)
+        s.set_velocity(*[a + sgn * eps * b for a, b in zip(u0, d)])
+        s.run(nsteps, fixed_dts=dts)
+        out.append(s.velocity())
+    fd = [(a - b) / (2 * eps) for a, b in zip(*out)]
+    for a, b in zip(tang, fd):
+        assert rel_l2(a, b) < 1e-6
