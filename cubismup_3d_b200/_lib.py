@@ -104,6 +104,10 @@ SIGNATURES = {
     "cup_penalize": (C.c_int, [_H, C.c_double, _dp]),
     "cup_step": (C.c_int, [_H, C.c_double, C.POINTER(CupStepStats)]),
     "cup_run": (C.c_int, [_H, C.c_int, C.POINTER(CupStepStats)]),
+    "cup_adjoint_step": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]),
+    "cup_get_velocity_raw": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "cup_set_velocity_raw": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup_poisson_solve_field": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_int]),
     "cup_diagnostics": (C.c_int, [_H, _dp]),
     "cup_debug_shift": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),

@@ -55,6 +55,8 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
   constexpr bool BASE = AdvectTraits<SCHEME>::BASE;
   constexpr int ROWS = TY + 2 * G;
   constexpr int Q = 2 * G + 1;
+  // a G-row halo box starting at y0 - G (wrapped) stays inside [0, ny) only if y0 is a multiple of TY >= G
+  static_assert(TY >= G, "tile height must cover the halo depth");
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
   const int nx = g.nx, ny = g.ny, nz = g.nz;

@@ -18,6 +18,7 @@
 #include <utility>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "advect.cuh"
 #include "common.cuh"
 #include "dht.cuh"
@@ -407,6 +408,9 @@ struct cup_handle {
   DevState* hstate = nullptr;  // pinned host copy
   // per-step solve stats
   int last_n_solves = 0;
+  // discrete adjoint scratch (allocated on the first adjoint call)
+  void *au = nullptr, *av = nullptr, *aw = nullptr;
+  double* p_adj = nullptr;
   // launch accounting and optional per-kernel CUDA-event profiling
   long long launches = 0;
   bool prof_on = false;
@@ -919,6 +923,89 @@ int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance) {
   return CUP_OK;
 }
 
+// ---- discrete adjoint ------------------------------------------------------
+// Launches one k_adjoint_zq pass: out = alpha lam + beta S'(f)^T g.
+template <typename T, int SCHEME, bool LAM, int TY, int NS, int CPT>
+int launch_adjoint(cup_handle* H, const char* name, const void* const* f, const void* const* g, const void* const* lam,
+                   void* const* out, double alpha, double beta, DtArg dt) {
+  constexpr int G = SCHEME == 0 ? 1 : 2;
+  const int cells = TY * H->nx;
+  if (cells % CPT || cells / CPT > 512 || H->ny % TY)
+    return fail(H, CUP_ERR_ARG, "adjoint tile does not fit the grid");
+  AdjointMaps maps;
+  for (int q = 0; q < 3; ++q) {
+    int rc = make_map(H, &maps.main[q], f[q], tma_dtype<T>(), sizeof(T), H->nx, TY, 1);
+    if (!rc) rc = make_map(H, &maps.halo[q], f[q], tma_dtype<T>(), sizeof(T), H->nx, G, 1);
+    if (!rc) rc = make_map(H, &maps.main[3 + q], g[q], tma_dtype<T>(), sizeof(T), H->nx, TY, 1);
+    if (!rc) rc = make_map(H, &maps.halo[3 + q], g[q], tma_dtype<T>(), sizeof(T), H->nx, G, 1);
+    if (!rc) rc = make_map(H, &maps.lam[q], LAM ? lam[q] : g[q], tma_dtype<T>(), sizeof(T), H->nx, TY, 1);
+    if (rc) return rc;
+  }
+  const int zc = std::min(16, H->nz);
+  StreamGeom geo{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
+  const size_t smem = adjoint_smem_bytes<T, SCHEME, LAM, TY, NS, CPT>(H->nx) + 128;
+  auto kern = k_adjoint_zq<T, SCHEME, LAM, TY, NS, CPT>;
+  const int threads = cells / CPT;
+  int bpsm = 0;
+  int rc = prepare_kernel(H, kern, smem, threads, &bpsm);
+  if (rc) return rc;
+  const int grid = std::min(geo.n_items, bpsm * H->num_sms);
+  return launch_named(H, name, [&]() -> int {
+    kern<<<grid, threads, smem, H->stream>>>(maps, geo, (T*)out[0], (T*)out[1], (T*)out[2], (T)alpha, (T)beta, dt, H->h,
+                                             H->cfg.nu, H->uinf[0], H->uinf[1], H->uinf[2], H->derr);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+// The projection P = I - G L^+ D of the pipeline (PressureRHS, the periodic
+// FFT solve in FP64, the gradient correction) applied to the fields `in`,
+// result in `out` (may equal `in`). D = -G^T on the periodic grid and L = D G
+// is the wide-stencil Laplacian the spectral factor inverts, so P is
+// symmetric: the adjoint of the projection is P itself.
+template <typename T>
+int do_project_fields(cup_handle* H, void* const* in, void* const* out, double* pbuf, DtArg dt) {
+  int rc;
+  RowsRhs<T> prod{(const T*)in[0], (const T*)in[1], (const T*)in[2], dt, H->h, H->nx, H->ny, H->nz};
+  if ((rc = launch_rows<double>(H, "adjoint_rhs_dht_x", prod, RowsToArray<double>{H->rhs}, nullptr))) return rc;
+  if ((rc = fft_middle<double>(H, H->rhs, nullptr))) return rc;
+  if ((rc = launch_rows<double>(H, "adjoint_dht_x", RowsFromArray<double>{H->rhs}, RowsToArray<double>{pbuf}, nullptr)))
+    return rc;
+  const void* pf[1] = {pbuf};
+  OpGradP<T> op{(const T*)in[0], (const T*)in[1], (const T*)in[2], (T*)out[0], (T*)out[1], (T*)out[2],
+                partial(H, P_GRAD), dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, H->box, 0, H->nx, H->ny, H->nz};
+  int ngp = 0;
+  return launch_stream<double, 1, 1, 4, 4>(H, "adjoint_grad_p", pf, op, &ngp);
+}
+
+// Adjoint of one step u_{n+1} = P(H(u_n)) with the dt given, at the state un:
+// lam (dJ/du_{n+1}) becomes dJ/du_n.
+//   upwind3 + RK2:  lam* = P lam,  u1 = S(un),
+//                   mu = 1/2 S'(u1)^T lam*,  lam = 1/2 lam* + S'(un)^T mu
+//   central + Euler: lam = S'(un)^T (P lam)
+template <typename T>
+int do_adjoint_step(cup_handle* H, void* const* un, void* const* lam, DtArg dt) {
+  constexpr bool F32 = std::is_same<T, float>::value;
+  int rc;
+  void* mu[3] = {H->au, H->av, H->aw};
+  if (H->cfg.scheme == CUP_SCHEME_REF) {
+    if ((rc = do_project_fields<T>(H, lam, mu, H->p_adj, dt))) return rc;
+    if constexpr (F32) return launch_adjoint<T, 0, false, 4, 3, 2>(H, "adjoint_ref", un, mu, nullptr, lam, 0.0, 1.0, dt);
+    else return launch_adjoint<T, 0, false, 2, 3, 1>(H, "adjoint_ref", un, mu, nullptr, lam, 0.0, 1.0, dt);
+  }
+  void* st1[3] = {H->u1, H->v1, H->w1};
+  if ((rc = do_project_fields<T>(H, lam, lam, H->p_adj, dt))) return rc;
+  if constexpr (F32) {
+    if ((rc = launch_advect<T, 1, 4, 4, 2>(H, "adjoint_recompute_stage1", un, un, st1, dt))) return rc;
+    if ((rc = launch_adjoint<T, 1, false, 2, 3, 1>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt))) return rc;
+    return launch_adjoint<T, 1, true, 2, 3, 1>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
+  } else {
+    if ((rc = launch_advect<T, 1, 4, 3, 2>(H, "adjoint_recompute_stage1", un, un, st1, dt))) return rc;
+    if ((rc = launch_adjoint<T, 1, false, 2, 2, 1>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt))) return rc;
+    return launch_adjoint<T, 1, true, 2, 2, 1>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
+  }
+}
+
 template <typename T>
 int set_field(cup_handle* H, void* dst, const double* src, int where) {
   if (!H->fp32) {
@@ -1091,7 +1178,8 @@ int cup_destroy(cup_handle* H) {
   if (!H) return CUP_OK;
   cudaSetDevice(H->dev);
   if (H->stream) cudaStreamSynchronize(H->stream);
-  for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->chi, (void*)H->p, (void*)H->rhs,
+  for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->au, H->av, H->aw, (void*)H->p_adj,
+                  H->chi, (void*)H->p, (void*)H->rhs,
                   (void*)H->work32, (void*)H->partials, (void*)H->dstate, (void*)H->derr, (void*)H->cosx,
                   (void*)H->cosy, (void*)H->cosz, (void*)H->sp_dev})
     if (f) cudaFree(f);
@@ -1462,6 +1550,55 @@ int cup_step(cup_handle* H, double dt, cup_step_stats* stats) {
   H->time += dt;
   H->umax_fresh = true;
   if (stats) return fill_stats(H, stats);
+  return CUP_OK;
+}
+
+static int alloc_adjoint(cup_handle* H) {
+  if (H->p_adj) return CUP_OK;
+  const size_t es = H->fp32 ? sizeof(float) : sizeof(double);
+  for (void** f : {&H->au, &H->av, &H->aw}) CK(cudaMalloc(f, H->n * es));
+  CK(cudaMalloc(&H->p_adj, H->n * sizeof(double)));
+  return CUP_OK;
+}
+
+int cup_adjoint_step(cup_handle* H, const void* un, const void* vn, const void* wn, double dt, void* lu, void* lv,
+                     void* lw) {
+  REQUIRE_H(H);
+  if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
+  if (!un || !vn || !wn || !lu || !lv || !lw) return fail(H, CUP_ERR_ARG, "null field pointer");
+  if (H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_adjoint_step: the handle has an obstacle");
+  const void* st[3] = {un, vn, wn};
+  const void* lm[3] = {lu, lv, lw};
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      if (st[a] == lm[b]) return fail(H, CUP_ERR_ARG, "the state and the adjoint fields must not alias");
+      if (a < b && (lm[a] == lm[b] || st[a] == st[b])) return fail(H, CUP_ERR_ARG, "field pointers must be distinct");
+    }
+  int rc = alloc_adjoint(H);
+  if (rc) return rc;
+  void* s3[3] = {const_cast<void*>(un), const_cast<void*>(vn), const_cast<void*>(wn)};
+  void* l3[3] = {lu, lv, lw};
+  return DISPATCH_T(H, do_adjoint_step, s3, l3, DtArg{dt, nullptr});
+}
+
+int cup_get_velocity_raw(cup_handle* H, void* u, void* v, void* w) {
+  REQUIRE_H(H);
+  if (!u || !v || !w) return fail(H, CUP_ERR_ARG, "null field pointer");
+  const size_t bytes = H->n * (H->fp32 ? sizeof(float) : sizeof(double));
+  CK(cudaMemcpyAsync(u, H->u, bytes, cudaMemcpyDeviceToDevice, H->stream));
+  CK(cudaMemcpyAsync(v, H->v, bytes, cudaMemcpyDeviceToDevice, H->stream));
+  CK(cudaMemcpyAsync(w, H->w, bytes, cudaMemcpyDeviceToDevice, H->stream));
+  return CUP_OK;
+}
+
+int cup_set_velocity_raw(cup_handle* H, const void* u, const void* v, const void* w) {
+  REQUIRE_H(H);
+  if (!u || !v || !w) return fail(H, CUP_ERR_ARG, "null field pointer");
+  const size_t bytes = H->n * (H->fp32 ? sizeof(float) : sizeof(double));
+  CK(cudaMemcpyAsync(H->u, u, bytes, cudaMemcpyDeviceToDevice, H->stream));
+  CK(cudaMemcpyAsync(H->v, v, bytes, cudaMemcpyDeviceToDevice, H->stream));
+  CK(cudaMemcpyAsync(H->w, w, bytes, cudaMemcpyDeviceToDevice, H->stream));
+  H->umax_fresh = false;
   return CUP_OK;
 }
 

@@ -155,6 +155,9 @@ def _ptr(a: np.ndarray):
     return C.c_void_p(a.ctypes.data)
 
 
+_CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
+
+
 def _is_torch_cuda(a) -> bool:
     return hasattr(a, "is_cuda") and a.is_cuda
 
@@ -295,7 +298,19 @@ class Simulation:
         return self.sd
 
     def set_stream(self, stream_ptr: Optional[int]):
+        """Runs the handle's work on the CUDA stream ``stream_ptr`` (None: the
+        handle's own stream)."""
         L.check(L.lib().cup_set_stream(self._h, C.c_void_p(stream_ptr or 0)), self._h, "set_stream")
+        self._bound_stream = stream_ptr or None
+
+    def bind_torch_stream(self):
+        """Runs the handle's work on torch's current stream of its device, so that
+        torch tensors passed by pointer are ordered with it. torch reports the
+        legacy default stream as 0; the runtime's name for it is cudaStreamLegacy."""
+        import torch
+        ptr = torch.cuda.current_stream(self.sd.device).cuda_stream or _CUDA_STREAM_LEGACY
+        if getattr(self, "_bound_stream", None) != ptr:
+            self.set_stream(ptr)
 
     def sync(self):
         L.check(L.lib().cup_sync(self._h), self._h, "sync")
@@ -336,8 +351,50 @@ class Simulation:
 
     def velocity_into(self, u, v, w):
         """Copies the velocity into three FP64 CUDA torch tensors (device to device)."""
+        self.bind_torch_stream()
         L.check(L.lib().cup_get_velocity(self._h, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
                                          C.c_void_p(w.data_ptr()), L.CUP_WHERE_DEVICE), self._h, "velocity_into")
+
+    # -- raw device fields and the discrete adjoint (torch CUDA tensors) ---------
+    @property
+    def storage_dtype(self):
+        """torch dtype of the device fields: float64 (fp64) or float32 (fp32_dc)."""
+        import torch
+        return torch.float32 if self.sd.precision == "fp32_dc" else torch.float64
+
+    def _check_raw(self, t, what):
+        if not _is_torch_cuda(t) or t.dtype != self.storage_dtype or not t.is_contiguous() or \
+                tuple(t.shape) != (3,) + self.shape:
+            raise ValueError(f"{what}: expected a contiguous CUDA tensor of shape {(3,) + self.shape} "
+                             f"and dtype {self.storage_dtype}")
+
+    def velocity_raw(self, out=None):
+        """The velocity as one (3, nz, ny, nx) CUDA tensor in the storage dtype,
+        copied on the handle's stream."""
+        import torch
+        if out is None:
+            out = torch.empty((3,) + self.shape, dtype=self.storage_dtype, device=f"cuda:{self.sd.device}")
+        self._check_raw(out, "velocity_raw")
+        self.bind_torch_stream()
+        L.check(L.lib().cup_get_velocity_raw(self._h, *[C.c_void_p(out[i].data_ptr()) for i in range(3)]),
+                self._h, "velocity_raw")
+        return out
+
+    def set_velocity_raw(self, t):
+        """Sets the velocity from a (3, nz, ny, nx) CUDA tensor in the storage dtype."""
+        self._check_raw(t, "set_velocity_raw")
+        self.bind_torch_stream()
+        L.check(L.lib().cup_set_velocity_raw(self._h, *[C.c_void_p(t[i].data_ptr()) for i in range(3)]),
+                self._h, "set_velocity_raw")
+
+    def adjoint_step(self, state, dt: float, lam):
+        """Discrete adjoint of ``timestep(dt)`` taken from ``state``: ``lam``
+        (dJ/du after the step, (3, nz, ny, nx)) becomes dJ/du before it, in place."""
+        self._check_raw(state, "adjoint_step state")
+        self._check_raw(lam, "adjoint_step lam")
+        self.bind_torch_stream()
+        L.check(L.lib().cup_adjoint_step(self._h, *[C.c_void_p(state[i].data_ptr()) for i in range(3)], float(dt),
+                                         *[C.c_void_p(lam[i].data_ptr()) for i in range(3)]), self._h, "adjoint_step")
 
     def _get1(self, fn, what) -> np.ndarray:
         out = np.empty(self.shape, dtype=np.float64)

@@ -157,6 +157,22 @@ int cup_step(struct cup_handle* h, double dt, cup_step_stats* stats);
  * with dt computed on the device (no host round trip per step). */
 int cup_run(struct cup_handle* h, int nsteps, cup_step_stats* stats);
 
+/* Discrete adjoint of one cup_step with the given dt (no counterpart in the
+ * reference, which has no adjoint). un, vn, wn: the velocity at the start of the
+ * step; lu, lv, lw: on entry dJ/du after the step, on return dJ/du before it. All
+ * six are device arrays of nx*ny*nz elements in the handle's storage type (double
+ * for CUP_PREC_FP64, float for CUP_PREC_FP32_DC), x fastest; the adjoint fields
+ * must not alias the state. Upwind signs are frozen at the state; the projection
+ * is applied as the exact (FP64 FFT) symmetric projector. The handle's own
+ * velocity and pressure are untouched; its stage and RHS scratch are overwritten.
+ * Handles with an obstacle return CUP_ERR_ARG. Stream-ordered, no host sync. */
+int cup_adjoint_step(struct cup_handle* h, const void* un, const void* vn, const void* wn, double dt, void* lu,
+                     void* lv, void* lw);
+/* Device-to-device copies of the handle's velocity in its storage type (for
+ * checkpoints): get copies out to u, v, w; set copies in. Stream-ordered. */
+int cup_get_velocity_raw(struct cup_handle* h, void* u, void* v, void* w);
+int cup_set_velocity_raw(struct cup_handle* h, const void* u, const void* v, const void* w);
+
 /* Stand-alone Poisson solve: p = (wide-Laplacian)^+ rhs / h^3 on the handle's grid
  * (PoissonSolverPeriodic on an h^3-premultiplied RHS); rhs, p FP64. */
 int cup_poisson_solve_field(struct cup_handle* h, const double* rhs, double* p, int where);

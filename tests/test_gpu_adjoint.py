@@ -1,0 +1,241 @@
+"""Discrete adjoint of the step on the GPU, checked three ways:
+
+* dot-product test against the oracle's FP64 tangent-linear model:
+  <lam, TLM(du)> = <ADJ(lam), du> to rounding (FP64 handle);
+* directional derivatives of a rollout loss against central finite
+  differences of the GPU forward;
+* the FP32 adjoint against the FP64 tangent-linear model.
+
+The adjoint freezes the upwind switch at the forward state, the same
+convention as the oracle's tangent-linear model, so the dot-product identity
+is exact up to rounding.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def make_sim(cells, extent, precision="fp64", scheme="upwind3_rk2", nu=5e-3, uinf=(0.0, 0.0, 0.0), CFL=0.5):
+    import cubismup_3d_b200 as cup
+    sd = cup.SimulationData(CFL=CFL, cells=cells, uinf=uinf)
+    sd.extent, sd.nu, sd.rampup, sd.precision, sd.scheme = extent, nu, 0, precision, scheme
+    return cup.Simulation(sd)
+
+
+def make_oracle(oracle, cells, extent, scheme="upwind3_rk2", nu=5e-3, uinf=(0.0, 0.0, 0.0), CFL=0.5):
+    return oracle.OracleSim(*cells, extent, nu, CFL=CFL, lambda_=1e6, DLM=1.0, uinf=uinf, rampup=0, scheme=scheme)
+
+
+def initial_state(cells, h, seed, amplitude=0.05):
+    from cubismup_3d_b200.initial_conditions import perturbed_taylor_green
+    return perturbed_taylor_green(cells, h, seed, amplitude=amplitude, kmax=8)
+
+
+def to_dev(fields, dtype):
+    import torch
+    return torch.from_numpy(np.stack(fields)).to(device="cuda", dtype=dtype).contiguous()
+
+
+def dot(a, b):
+    return float(np.sum(np.asarray(a, dtype=np.float64) * np.asarray(b, dtype=np.float64)))
+
+
+@pytest.mark.parametrize("scheme,uinf", [("upwind3_rk2", (0.0, 0.0, 0.0)), ("upwind3_rk2", (0.3, -0.2, 0.1)),
+                                         ("ref", (0.0, 0.0, 0.0))])
+def test_adjoint_step_dot_product_vs_oracle_tlm(oracle, scheme, uinf):
+    import torch
+    cells = (32, 32, 32)
+    ext = 2 * np.pi
+    sim = make_sim(cells, ext, scheme=scheme, uinf=uinf)
+    orc = make_oracle(oracle, cells, ext, scheme=scheme, uinf=uinf)
+    u = initial_state(cells, sim.h, seed=1)
+    rng = np.random.default_rng(5)
+    du = [rng.standard_normal(sim.shape) for _ in range(3)]
+    lam = [rng.standard_normal(sim.shape) for _ in range(3)]
+    orc.set_velocity(*u)
+    dt = orc.calc_max_timestep()
+    tl = orc.tangent_run([dt], *du)
+    state = to_dev(u, torch.float64)
+    lam_d = to_dev(lam, torch.float64)
+    sim.adjoint_step(state, dt, lam_d)
+    adj = lam_d.cpu().numpy()
+    lhs = dot(np.stack(lam), np.stack(tl))
+    rhs = dot(adj, np.stack(du))
+    assert abs(lhs - rhs) <= 1e-11 * max(abs(lhs), np.linalg.norm(np.stack(lam)) * np.linalg.norm(np.stack(tl)))
+    # the state argument is read only
+    assert torch.equal(state, to_dev(u, torch.float64))
+
+
+def test_adjoint_step_leaves_handle_state(oracle):
+    import torch
+    cells = (32, 32, 16)
+    sim = make_sim(cells, 1.0)
+    u = initial_state(cells, sim.h, seed=3)
+    sim.set_velocity(*u)
+    before = sim.velocity_raw().clone()
+    lam = torch.randn((3,) + sim.shape, dtype=torch.float64, device="cuda")
+    sim.adjoint_step(to_dev(u, torch.float64), 1e-3, lam)
+    assert torch.equal(sim.velocity_raw(), before)
+
+
+def test_adjoint_argument_checks():
+    import torch
+    import cubismup_3d_b200 as cup
+    cells = (32, 32, 16)
+    sim = make_sim(cells, 1.0)
+    x = torch.zeros((3,) + sim.shape, dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError, match="alias"):
+        sim.adjoint_step(x, 1e-3, x)
+    with pytest.raises(ValueError):
+        sim.adjoint_step(x, 1e-3, torch.zeros((3,) + sim.shape, dtype=torch.float32, device="cuda"))
+    with pytest.raises(ValueError, match="dt"):
+        sim.adjoint_step(x, 0.0, x.clone())
+    sim.add_obstacle(cup.Sphere(radius=0.1, position=(0.5, 0.5, 0.25), enforcedVelocity=(1, 0, 0),
+                                bForcedInSimFrame=(True, True, True)))
+    with pytest.raises(ValueError, match="obstacle"):
+        sim.adjoint_step(x, 1e-3, x.clone())
+
+
+@pytest.mark.parametrize("scheme", ["upwind3_rk2", "ref"])
+def test_rollout_adjoint_vs_oracle_tlm(oracle, scheme):
+    """7 steps, checkpoints every 3 (a partial last segment): the gradient of
+    <w, u_T> against the oracle's FP64 tangent-linear rollout."""
+    import torch
+    from cubismup_3d_b200.adjoint import rollout
+    cells = (32, 32, 32)
+    ext = 2 * np.pi
+    sim = make_sim(cells, ext, scheme=scheme)
+    orc = make_oracle(oracle, cells, ext, scheme=scheme)
+    u = initial_state(cells, sim.h, seed=2)
+    orc.set_velocity(*u)
+    dt = orc.calc_max_timestep()
+    dts = [dt * (1 + 0.05 * i) for i in range(7)]
+    rng = np.random.default_rng(9)
+    du = [rng.standard_normal(sim.shape) for _ in range(3)]
+    wgt = [rng.standard_normal(sim.shape) for _ in range(3)]
+    tl = orc.tangent_run(dts, *du)
+    uT_orc = np.stack(orc.velocity())
+    u0 = to_dev(u, torch.float64).requires_grad_(True)
+    uT = rollout(sim, u0, dts, checkpoint_every=3)
+    assert rel_l2(uT.detach().cpu().numpy(), uT_orc) < 1e-10
+    (uT * to_dev(wgt, torch.float64)).sum().backward()
+    g = u0.grad.cpu().numpy()
+    lhs = dot(np.stack(wgt), np.stack(tl))
+    rhs = dot(g, np.stack(du))
+    assert abs(lhs - rhs) <= 1e-9 * abs(lhs) + 1e-13 * np.linalg.norm(np.stack(wgt)) * np.linalg.norm(np.stack(tl))
+
+
+@pytest.mark.parametrize("scheme,eps,tol", [("ref", 1e-6, 1e-8), ("upwind3_rk2", 1e-4, 1e-4)])
+def test_rollout_gradient_vs_central_differences_fp64(scheme, eps, tol):
+    """Central differences of the GPU forward. The central scheme is smooth, so
+    the FD error is O(eps^2) and the bar is tight; with upwind3 every advecting
+    velocity that changes sign inside [-eps, eps] along the path is a kink, and
+    the FD error levels off near 1e-5 independent of eps (the gradient itself
+    equals the tangent-linear value to rounding: see the dot-product tests)."""
+    import torch
+    from cubismup_3d_b200.adjoint import rollout
+    from cubismup_3d_b200.initial_conditions import random_solenoidal
+    cells = (32, 32, 32)
+    ext = 2 * np.pi
+    sim = make_sim(cells, ext, scheme=scheme)
+    u = initial_state(cells, sim.h, seed=1)
+    target = to_dev(initial_state(cells, sim.h, seed=2), torch.float64)
+    sim.set_velocity(*u)
+    dt = sim.calcMaxTimestep()
+    dts = [dt] * 10
+    u0 = to_dev(u, torch.float64)
+
+    def loss(x):
+        return 0.5 * ((rollout(sim, x, dts, checkpoint_every=4) - target) ** 2).sum()
+
+    x = u0.clone().requires_grad_(True)
+    loss(x).backward()
+    grad = x.grad
+    for seed in range(3):
+        d = to_dev(random_solenoidal(cells, 100 + seed, lambda k: np.ones_like(k), kmax=8, amplitude=1.0),
+                   torch.float64)
+        with torch.no_grad():
+            fd = (loss(u0 + eps * d) - loss(u0 - eps * d)).item() / (2 * eps)
+        ad = float((grad * d).sum())
+        assert abs(fd - ad) <= tol * abs(ad), (seed, fd, ad)
+
+
+def test_fp32_adjoint_vs_fp64_tlm(oracle):
+    import torch
+    from cubismup_3d_b200.adjoint import rollout
+    cells = (64, 64, 32)
+    ext = 2 * np.pi
+    sim = make_sim(cells, ext, precision="fp32_dc")
+    orc = make_oracle(oracle, cells, ext)
+    u = initial_state(cells, sim.h, seed=4)
+    orc.set_velocity(*u)
+    dt = orc.calc_max_timestep()
+    dts = [dt] * 6
+    rng = np.random.default_rng(21)
+    du = [rng.standard_normal(sim.shape) for _ in range(3)]
+    wgt = [rng.standard_normal(sim.shape) for _ in range(3)]
+    tl = orc.tangent_run(dts, *du)
+    u0 = to_dev(u, torch.float32).requires_grad_(True)
+    uT = rollout(sim, u0, dts, checkpoint_every=4)
+    (uT.double() * to_dev(wgt, torch.float64)).sum().backward()
+    g = u0.grad.double().cpu().numpy()
+    lhs = dot(np.stack(wgt), np.stack(tl))
+    rhs = dot(g, np.stack(du))
+    # FP32 storage and arithmetic: about 1e-6 relative per element
+    assert abs(lhs - rhs) <= 1e-4 * abs(lhs), (lhs, rhs)
+
+
+def test_adjoint_rollout_taylor_green_128(oracle):
+    """Perturbed Taylor-Green at 128^3 (perturbation amplitude 0.05, |k| <= 8,
+    seed 1), nu = 5e-3, 64 steps at the CFL-0.5 dt of the initial field,
+    checkpoints every 8; loss 0.5 ||u_T - u_target||^2 with u_target the
+    seed-2 field. Gradients w.r.t. u0 from the FP32 and FP64 forward are held
+    to 1e-4 of central FD (eps = 1e-4, FP64 forward) on 16 random solenoidal
+    directions (seeds 100..115), and to the oracle's FP64 tangent-linear
+    rollout on one of them."""
+    import torch
+    from cubismup_3d_b200.adjoint import rollout
+    from cubismup_3d_b200.initial_conditions import random_solenoidal
+    cells = (128, 128, 128)
+    ext = 2 * np.pi
+    nsteps, K, eps = 64, 8, 1e-4
+    s64 = make_sim(cells, ext)
+    s32 = make_sim(cells, ext, precision="fp32_dc")
+    u = initial_state(cells, s64.h, seed=1)
+    tgt_np = np.stack(initial_state(cells, s64.h, seed=2))
+    target = torch.from_numpy(tgt_np).cuda()
+    s64.set_velocity(*u)
+    dt = s64.calcMaxTimestep()
+    dts = [dt] * nsteps
+    u0 = to_dev(u, torch.float64)
+
+    def loss(sim, x):
+        return 0.5 * ((rollout(sim, x, dts, checkpoint_every=K).double() - target) ** 2).sum()
+
+    grads = {}
+    for name, sim, dtype in (("fp64", s64, torch.float64), ("fp32", s32, torch.float32)):
+        x = u0.to(dtype).clone().requires_grad_(True)
+        loss(sim, x).backward()
+        grads[name] = x.grad.double()
+    worst = {"fp64": 0.0, "fp32": 0.0}
+    d0 = None
+    for seed in range(100, 116):
+        d = to_dev(random_solenoidal(cells, seed, lambda k: np.ones_like(k), kmax=8, amplitude=1.0), torch.float64)
+        if d0 is None:
+            d0 = d
+        with torch.no_grad():
+            fd = (loss(s64, u0 + eps * d) - loss(s64, u0 - eps * d)).item() / (2 * eps)
+        for name, g in grads.items():
+            worst[name] = max(worst[name], abs(float((g * d).sum()) - fd) / abs(fd))
+    assert worst["fp64"] <= 1e-4 and worst["fp32"] <= 1e-4, worst
+    # FP64 tangent-linear rollout of the oracle along the first direction
+    orc = make_oracle(oracle, cells, ext)
+    orc.set_velocity(*u)
+    tl = np.stack(orc.tangent_run(dts, *d0.cpu().numpy()))
+    uT = np.stack(orc.velocity())
+    tlm = float(((uT - tgt_np) * tl).sum())
+    assert abs(float((grads["fp64"] * d0).sum()) - tlm) <= 1e-9 * abs(tlm)
+    assert abs(float((grads["fp32"] * d0).sum()) - tlm) <= 1e-4 * abs(tlm)
