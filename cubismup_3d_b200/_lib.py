@@ -69,7 +69,7 @@ class CupStepStats(C.Structure):
         ("dt", C.c_double), ("time", C.c_double), ("step", C.c_int),
         ("umax", C.c_double), ("kinetic_energy", C.c_double),
         ("force", C.c_double * 3), ("torque", C.c_double * 3),
-        ("n_solves", C.c_int), ("rel_residual", C.c_double),
+        ("n_solves", C.c_int), ("rel_residual", C.c_double), ("n_unconverged", C.c_int),
     ]
 
 

@@ -22,6 +22,7 @@
 #include "advect.cuh"
 #include "common.cuh"
 #include "dht.cuh"
+#include "pressure_zq.cuh"
 #include "ops.cuh"
 #include "stencil.cuh"
 
@@ -40,7 +41,8 @@ struct DevState {
   double cmean[8];  // parity-class means of p (the 8 null-mode components)
   double rmean[8];  // parity-class means of the first residual (the RHS's null parts)
   double res_hist[16];  // relative residual at each check of the last solve
-  int step, n_solves, converged, pad_;
+  int step, n_solves, converged;
+  int n_unconverged;  // steps whose defect correction missed the tolerance (cumulative)
 };
 
 enum PartialRegion { P_GRAD = 0, P_PEN, P_RHSOB, P_CHI, P_MAX, P_RES, P_DIAG, P_COUNT };
@@ -107,21 +109,22 @@ __global__ void k_set_dt(DevState* st, double dt, double DLM) {
 
 // End of step: umax (grid part outside the obstacle box, box part after
 // penalization), kinetic energy, force/torque; advances step and time.
-__global__ void k_finalize_step(const double* pgrad, int ngrad, const double* ppen, int npen, DevState* st,
-                                double h3, int advance) {
-  __shared__ double scratch[8 * 32];
+__global__ void k_finalize_step(const double* pgrad, int ngrad, int gstride, const double* ppen, int npen,
+                                DevState* st, double h3, int advance, int dc_final, double tol, int max_iter) {
+  __shared__ double scratch[9 * 32];
   double mx[1] = {0.0};
-  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   for (int i = threadIdx.x; i < ngrad; i += blockDim.x) {
-    mx[0] = fmax(mx[0], pgrad[2 * i]);
-    s[6] += pgrad[2 * i + 1];
+    mx[0] = fmax(mx[0], pgrad[gstride * i]);
+    s[6] += pgrad[gstride * i + 1];
+    if (dc_final) s[7] += pgrad[gstride * i + 2];
   }
   for (int i = threadIdx.x; i < npen; i += blockDim.x) {
     for (int k = 0; k < 6; ++k) s[k] += ppen[8 * i + k];
     mx[0] = fmax(mx[0], ppen[8 * i + 6]);
   }
-  block_reduce<7, false>(s, scratch);
-  block_reduce<1, true>(mx, scratch + 7 * 32);
+  block_reduce<8, false>(s, scratch);
+  block_reduce<1, true>(mx, scratch + 8 * 32);
   if (threadIdx.x == 0) {
     st->umax = mx[0];
     st->ke = s[6] * h3;
@@ -130,6 +133,17 @@ __global__ void k_finalize_step(const double* pgrad, int ngrad, const double* pp
         st->force[k] = s[k];
         st->torque[k] = s[3 + k];
       }
+    }
+    // final defect-correction check (fused into the gradient pass): it decides
+    // only when no earlier check converged, i.e. after max_iter solves
+    if (dc_final && st->converged == 0) {
+      const double res2 = s[7], b2 = st->b2;
+      const bool met = b2 == 0.0 || sqrt(res2) <= tol * sqrt(b2);
+      st->res2 = res2;
+      if (max_iter < 16) st->res_hist[max_iter] = b2 > 0 ? sqrt(res2 / b2) : 0.0;
+      st->n_solves = max_iter;
+      st->converged = met ? 1 : 2;
+      if (!met) st->n_unconverged += 1;
     }
     if (advance) {
       st->step += 1;
@@ -222,7 +236,10 @@ __global__ void k_finalize_residual(const double* p, int np, DevState* st, doubl
     const bool met = b2 == 0.0 || sqrt(res2) <= tol * sqrt(b2);
     st->n_solves = k;
     st->converged = (k >= min_iter && met) ? 1 : 0;
-    if (k >= max_iter) st->converged = met ? 1 : 2;  // 2: not converged after max_iter solves
+    if (k >= max_iter) {
+      st->converged = met ? 1 : 2;  // 2: not converged after max_iter solves
+      if (!met) st->n_unconverged += 1;
+    }
   }
 }
 
@@ -384,6 +401,13 @@ struct cup_handle {
   void *u1 = nullptr, *v1 = nullptr, *w1 = nullptr;
   void* chi = nullptr;
   double* p = nullptr;    // pressure (FP64)
+  // FP32_DC without obstacle: pressure of the previous step and the next
+  // step's warm start (extrapolated by the gradient pass); p_valid counts the
+  // valid levels among (p, p_old), pred_ready says p_pred holds a warm start
+  double* p_old = nullptr;
+  double* p_pred = nullptr;
+  int p_valid = 0;
+  bool pred_ready = false;
   double* rhs = nullptr;  // pressure RHS (FP64); FP64 mode: also the FFT work array
   float* work32 = nullptr;  // FP32_DC FFT work array
   double* partials = nullptr;
@@ -405,6 +429,7 @@ struct cup_handle {
   double uinf[3] = {0, 0, 0};
   bool umax_fresh = false;
   int n_grad_partials = 0, n_pen_partials = 0;
+  int grad_stride = 2;  // 4 when the gradient pass also carries the final residual check
   DevState* hstate = nullptr;  // pinned host copy
   // per-step solve stats
   int last_n_solves = 0;
@@ -666,6 +691,14 @@ int box_grid(const Box& b) {
   return (int)std::max<long long>(1, std::min<long long>(kBoxBlocksMax, (n + kBoxThreads - 1) / kBoxThreads));
 }
 
+// The warm-start history of the FP32 pressure stage is only valid along one
+// trajectory of cup_step/cup_run; anything else that sets the velocity or the
+// pressure restarts it.
+void reset_pressure_history(cup_handle* H) {
+  H->p_valid = 0;
+  H->pred_ready = false;
+}
+
 int check_dev_error(cup_handle* H) {
   int e = 0;
   CK(cudaMemcpy(&e, H->derr, sizeof(int), cudaMemcpyDeviceToHost));
@@ -783,6 +816,106 @@ int do_pressure_rhs(cup_handle* H, DtArg dt) {
   return CUP_OK;
 }
 
+double dc_tol(const cup_handle* H) { return H->cfg.dc_tol > 0 ? H->cfg.dc_tol : 1e-10; }
+int dc_max_iter(const cup_handle* H) { return H->cfg.dc_max_iter > 0 ? H->cfg.dc_max_iter : 4; }
+int dc_min_iter(const cup_handle* H) {
+  return std::min(dc_max_iter(H), H->cfg.dc_min_iter > 0 ? H->cfg.dc_min_iter : 1);
+}
+
+// Launches one k_pres_zq pass; returns the grid size (number of partials).
+template <typename T, int MODE, int TY, int NS, int CPT>
+int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
+               int* grid_out, const int* skip, int pred_order = 0, double* pred_out = nullptr) {
+  const int cells = TY * H->nx;
+  if (cells % CPT || cells / CPT > 512 || H->ny % TY)
+    return fail(H, CUP_ERR_ARG, "pressure tile does not fit the grid");
+  PzqMaps maps;
+  int rc = make_map(H, &maps.p_main, pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), H->nx, TY, 1);
+  if (!rc) rc = make_map(H, &maps.p_halo, pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), H->nx, 2, 1);
+  if (!rc) rc = make_map(H, &maps.h_main[0], pred_order >= 1 ? H->p : pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         sizeof(double), H->nx, TY, 1);
+  if (!rc) rc = make_map(H, &maps.h_main[1], pred_order >= 2 ? H->p_old : pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         sizeof(double), H->nx, TY, 1);
+  if (!rc) rc = make_map(H, &maps.b_main, H->rhs, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), H->nx, TY, 1);
+  const void* f[3] = {H->u, H->v, H->w};
+  for (int q = 0; q < 3 && !rc; ++q) rc = make_map(H, &maps.f_main[q], f[q], tma_dtype<T>(), sizeof(T), H->nx, TY, 1);
+  if (!rc) rc = make_map(H, &maps.v_halo, H->v, tma_dtype<T>(), sizeof(T), H->nx, 1, 1);
+  if (rc) return rc;
+  const int zc = std::min(16, H->nz);
+  StreamGeom geo{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
+  const size_t smem = pzq_smem_bytes_host<T, MODE, TY, NS>(H->nx) + 128;
+  auto kern = k_pres_zq<T, MODE, TY, NS, CPT>;
+  const int threads = cells / CPT;
+  int bpsm = 0;
+  if ((rc = prepare_kernel(H, kern, smem, threads, &bpsm))) return rc;
+  const int grid = std::min(geo.n_items, bpsm * H->num_sms);
+  if (grid > kPartialCap / 18) return fail(H, CUP_ERR_ARG, "too many CTAs for the partial buffers");
+  PzqParams prm{dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, pred_order, pred_out};
+  rc = launch_named(H, name, [&]() -> int {
+    kern<<<grid, threads, smem, H->stream>>>(maps, geo, (T*)H->u, (T*)H->v, (T*)H->w, H->rhs, H->work32, partials,
+                                             rmean, prm, H->derr, skip);
+    CKL();
+    return CUP_OK;
+  });
+  if (rc) return rc;
+  if (grid_out) *grid_out = grid;
+  return CUP_OK;
+}
+
+int launch_finalize_residual(cup_handle* H, int grid, int k) {
+  const double inv_class = 8.0 / (double)H->n;
+  return launch_named(H, "finalize_residual", [&]() -> int {
+    k_finalize_residual<<<1, 256, 0, H->stream>>>(partial(H, P_RES), grid, H->dstate, dc_tol(H), k, dc_min_iter(H),
+                                                  dc_max_iter(H), inv_class);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+// FP32 defect-correction pressure stage without obstacle, in z-queue passes:
+//   RHS + first residual (warm start p) -> [FP32 solve, residual check] ...
+//   -> last FP32 solve -> gradient correction + final residual check.
+// A check that meets the tolerance (after at least dc_min_iter solves) turns
+// every later solve and check into an exit at entry; the gradient pass always
+// runs and its check decides when no earlier one did.
+template <typename T>
+int do_pressure_dc_zq(cup_handle* H, DtArg dt) {
+  const int max_iter = dc_max_iter(H);
+  const int* conv = &H->dstate->converged;
+  double* W = H->p_pred;  // this step's pressure, starting from the warm start
+  if (!H->pred_ready) CK(cudaMemcpyAsync(W, H->p, H->n * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
+  int rc, grid = 0;
+  if ((rc = launch_pzq<T, PZQ_RHS_RES, 4, 4, 2>(H, "rhs_residual", W, partial(H, P_RES), nullptr, dt, &grid, nullptr)))
+    return rc;
+  if ((rc = launch_finalize_residual(H, grid, 0))) return rc;
+  for (int k = 1; k <= max_iter; ++k) {
+    if ((rc = launch_rows<float>(H, "dht_x", RowsFromArray<float>{H->work32}, RowsToArray<float>{H->work32}, conv)))
+      return rc;
+    if ((rc = fft_middle<float>(H, H->work32, conv))) return rc;
+    if ((rc = launch_rows<float>(H, "dht_x_update_p", RowsFromArray<float>{H->work32},
+                                 RowsUpdateP{W, H->dstate->cmean, H->nx, H->ny}, conv)))
+      return rc;
+    if (k == max_iter) break;
+    if ((rc = launch_pzq<T, PZQ_RES, 4, 4, 2>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid,
+                                              conv)))
+      return rc;
+    if ((rc = launch_finalize_residual(H, grid, k))) return rc;
+  }
+  // gradient correction + final check + next warm start (over p_old, point-wise)
+  const int order = H->p_valid;  // valid levels among (p, p_old) before this step
+  if ((rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 3, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
+                                                   &H->n_grad_partials, nullptr, order, H->p_old)))
+    return rc;
+  H->grad_stride = 4;
+  double* next_pred = H->p_old;
+  H->p_old = H->p;
+  H->p = W;
+  H->p_pred = next_pred;
+  H->p_valid = std::min(order + 1, 2);
+  H->pred_ready = true;
+  return CUP_OK;
+}
+
 // FP32 correction solve inside an FP64 defect-correction loop, warm-started
 // from the current p, on the RHS array b. Check k: the FP64 residual
 // r = b - h^3 L_2h p (TMA plane stream over p with a 2-ring halo), its norms
@@ -843,6 +976,7 @@ int do_grad(cup_handle* H, DtArg dt) {
   OpGradP<T> op{(const T*)H->u, (const T*)H->v, (const T*)H->w, (T*)H->u, (T*)H->v, (T*)H->w, partial(H, P_GRAD),
                 dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, H->box, H->has_sphere ? 1 : 0, H->nx, H->ny, H->nz};
   // p is FP64 in both forms: the stream runs over an FP64 field.
+  H->grad_stride = 2;
   return launch_stream<double, 1, 1, 4, 4>(H, "grad_p", pf, op, &H->n_grad_partials);
 }
 
@@ -904,17 +1038,20 @@ int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance) {
     if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
     if ((rc = do_poisson(H))) return rc;
   } else if (H->fp32) {
-    if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
-    if ((rc = do_poisson_dc(H))) return rc;
+    // RHS, defect correction and gradient correction in z-queue passes
+    if ((rc = do_pressure_dc_zq<T>(H, dt))) return rc;
   } else {
     if ((rc = do_poisson_fused_fp64<T>(H, dt))) return rc;
   }
-  if ((rc = do_grad<T>(H, dt))) return rc;
+  if (H->has_sphere || !H->fp32) {
+    if ((rc = do_grad<T>(H, dt))) return rc;
+  }
   if ((rc = do_penalize<T>(H, dt, lambda_dev))) return rc;
   {
     int rc_ = launch_named(H, "finalize_step", [&]() -> int {
-      k_finalize_step<<<1, 256, 0, H->stream>>>(partial(H, P_GRAD), H->n_grad_partials, partial(H, P_PEN),
-                                            H->n_pen_partials, H->dstate, H->h * H->h * H->h, advance);
+      k_finalize_step<<<1, 256, 0, H->stream>>>(partial(H, P_GRAD), H->n_grad_partials, H->grad_stride,
+                                            partial(H, P_PEN), H->n_pen_partials, H->dstate, H->h * H->h * H->h,
+                                            advance, H->grad_stride == 4 ? 1 : 0, dc_tol(H), dc_max_iter(H));
       CKL();
       return CUP_OK;
     });
@@ -1128,6 +1265,10 @@ int cup_create(const cup_config* cfg, cup_handle** out) {
     CK(cudaMalloc(&H->p, H->n * sizeof(double)));
     CK(cudaMalloc(&H->rhs, H->n * sizeof(double)));
     if (H->fp32) CK(cudaMalloc(&H->work32, H->n * sizeof(float)));
+    if (H->fp32) {
+      CK(cudaMalloc(&H->p_old, H->n * sizeof(double)));
+      CK(cudaMalloc(&H->p_pred, H->n * sizeof(double)));
+    }
     for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, (void*)H->p, (void*)H->rhs})
       CK(cudaMemsetAsync(f, 0, H->n * (f == (void*)H->p || f == (void*)H->rhs ? sizeof(double) : es), H->stream));
     CK(cudaMalloc(&H->partials, sizeof(double) * kPartialCap * P_COUNT));
@@ -1179,7 +1320,7 @@ int cup_destroy(cup_handle* H) {
   cudaSetDevice(H->dev);
   if (H->stream) cudaStreamSynchronize(H->stream);
   for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->au, H->av, H->aw, (void*)H->p_adj,
-                  H->chi, (void*)H->p, (void*)H->rhs,
+                  H->chi, (void*)H->p, (void*)H->p_old, (void*)H->p_pred, (void*)H->rhs,
                   (void*)H->work32, (void*)H->partials, (void*)H->dstate, (void*)H->derr, (void*)H->cosx,
                   (void*)H->cosy, (void*)H->cosz, (void*)H->sp_dev})
     if (f) cudaFree(f);
@@ -1228,6 +1369,7 @@ int cup_get_dims(const cup_handle* H, int cells[3], double* hgrid) {
 
 int cup_set_velocity(cup_handle* H, const double* u, const double* v, const double* w, int where) {
   REQUIRE_H(H);
+  reset_pressure_history(H);
   if (!u || !v || !w || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad velocity arguments");
   int rc;
   if ((rc = DISPATCH_T(H, set_field, H->u, u, where))) return rc;
@@ -1311,6 +1453,7 @@ int cup_global_to_blocks(const double* global, double* blocks, int nx, int ny, i
 
 int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
   REQUIRE_H(H);
+  reset_pressure_history(H);
   if (!s || !(s->radius > 0)) return fail(H, CUP_ERR_ARG, "sphere radius must be > 0");
   if (H->has_sphere) return fail(H, CUP_ERR_STATE, "only one obstacle is supported");
   bool anyForced = false;
@@ -1439,17 +1582,20 @@ int cup_calc_max_timestep(cup_handle* H, double* dt) {
 
 int cup_advect_diffuse(cup_handle* H, double dt) {
   REQUIRE_H(H);
+  reset_pressure_history(H);
   H->umax_fresh = false;
   return DISPATCH_T(H, do_advect_diffuse, DtArg{dt, nullptr});
 }
 
 int cup_pressure_rhs(cup_handle* H, double dt) {
   REQUIRE_H(H);
+  reset_pressure_history(H);
   return DISPATCH_T(H, do_pressure_rhs, DtArg{dt, nullptr});
 }
 
 int cup_poisson_solve(cup_handle* H, cup_solve_stats* stats) {
   REQUIRE_H(H);
+  reset_pressure_history(H);
   int rc = do_poisson(H);
   if (rc) return rc;
   if (stats) {
@@ -1469,6 +1615,7 @@ int cup_poisson_solve(cup_handle* H, cup_solve_stats* stats) {
 
 int cup_grad_correct(cup_handle* H, double dt) {
   REQUIRE_H(H);
+  reset_pressure_history(H);
   H->umax_fresh = false;
   return DISPATCH_T(H, do_grad, DtArg{dt, nullptr});
 }
@@ -1481,6 +1628,7 @@ int cup_pressure_projection(cup_handle* H, double dt, cup_solve_stats* stats) {
 
 int cup_penalize(cup_handle* H, double dt, double force_torque[6]) {
   REQUIRE_H(H);
+  reset_pressure_history(H);
   H->umax_fresh = false;
   if (!H->has_sphere) {
     if (force_torque) std::fill(force_torque, force_torque + 6, 0.0);
@@ -1521,6 +1669,7 @@ static int fill_stats(cup_handle* H, cup_step_stats* st) {
     st->torque[d] = s.torque[d];
   }
   st->n_solves = H->fp32 ? s.n_solves : 1;
+  st->n_unconverged = s.n_unconverged;
   st->rel_residual = H->fp32 && s.b2 > 0 ? std::sqrt(s.res2 / s.b2) : 0.0;
   if (H->fp32 && s.converged == 2)
     return fail(H, CUP_ERR_NOT_CONVERGED, "defect correction: relative residual %.3e after %d solves",
@@ -1593,6 +1742,7 @@ int cup_get_velocity_raw(cup_handle* H, void* u, void* v, void* w) {
 
 int cup_set_velocity_raw(cup_handle* H, const void* u, const void* v, const void* w) {
   REQUIRE_H(H);
+  reset_pressure_history(H);
   if (!u || !v || !w) return fail(H, CUP_ERR_ARG, "null field pointer");
   const size_t bytes = H->n * (H->fp32 ? sizeof(float) : sizeof(double));
   CK(cudaMemcpyAsync(H->u, u, bytes, cudaMemcpyDeviceToDevice, H->stream));
@@ -1636,6 +1786,7 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
 
 int cup_poisson_solve_field(cup_handle* H, const double* rhs, double* p, int where) {
   REQUIRE_H(H);
+  reset_pressure_history(H);
   if (!rhs || !p || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad poisson arguments");
   const cudaMemcpyKind in = where == CUP_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   const cudaMemcpyKind out = where == CUP_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;

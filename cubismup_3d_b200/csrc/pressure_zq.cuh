@@ -1,0 +1,355 @@
+// Pressure-stage kernels of the FP32 defect-correction step (no obstacle),
+// register z-queue form:
+//   RHS_RES    b = KernelPressureRHS(u*) (source/operators/PressureRHS.cpp:51-76)
+//              and the first FP64 residual r = b - h/4 L_2h p of the warm start,
+//              in one pass: b to HBM in FP64, r in FP32 for the FFT solve.
+//   RES        r = b - h/4 L_2h p between correction solves.
+//   GRAD_CHECK KernelGradP (source/operators/PressureProjection.cpp:38-50) on
+//              u* with the final p, fused with the final FP64 residual check
+//              (the divergence left by the projection is this residual) and
+//              with the warm start of the next step's solve: the polynomial
+//              extrapolation of p over the last three steps.
+// L_2h is the wide-stencil Laplacian (neighbours at +-2) the spectral solve
+// inverts; p is FP64 throughout.
+//
+// Structure as k_advect_zq: each thread owns CPT (x, y) columns of a TY x nx
+// row tile and marches down z; planes of p (TY + 4 rows: the +-2 halo in y)
+// arrive by TMA into a ring of NS slots, the centre values of the last 5
+// planes sit in a register queue (the z stencil), the x/y part of each plane
+// is computed on arrival and completed two planes later. The point-wise fields
+// of an output plane (b, u*) ride in the slot of the load that completes it.
+// Partial sums per CTA: RHS_RES and RES write the 18-value residual layout
+// (sum r^2, sum b^2, parity-class sums of p and of r); GRAD_CHECK writes
+// (max |u + uinf|, kinetic energy, sum of the null-free r^2, 0).
+#pragma once
+
+#include "common.cuh"
+#include "ops.cuh"
+#include "stencil.cuh"
+
+namespace cup {
+
+enum { PZQ_RHS_RES = 0, PZQ_RES = 1, PZQ_GRAD_CHECK = 2 };
+
+struct PzqMaps {
+  CUtensorMap p_main, p_halo;  // FP64 p: box {nx, TY, 1} and {nx, 2, 1}
+  CUtensorMap f_main[3];       // u, v, w (storage type): box {nx, TY, 1}
+  CUtensorMap v_halo;          // v: box {nx, 1, 1} (RHS_RES)
+  CUtensorMap b_main;          // FP64 b: box {nx, TY, 1} (RES, GRAD_CHECK)
+  CUtensorMap h_main[2];       // FP64 pressure history p_n, p_{n-1}: box {nx, TY, 1} (GRAD_CHECK)
+};
+
+struct PzqParams {
+  DtArg dt;
+  double h;
+  double uinf[3];
+  // GRAD_CHECK: extrapolation order (0, 1, 2) of the next step's warm start
+  // from the final p and the history (p_n, p_{n-1}); written over p_{n-1}
+  int pred_order;
+  double* pred_out;
+};
+
+// Byte layout of one ring slot (all parts multiples of 64 B for nx >= 16).
+template <typename T, int MODE, int TY>
+struct PzqSlot {
+  static constexpr int G = 2;
+  __host__ __device__ static size_t p_bytes(int nx) { return (size_t)(TY + 2 * G) * nx * sizeof(double); }
+  // RHS_RES: u [TY], v [TY + 2], w [TY] rows of T
+  __host__ __device__ static size_t u_off(int nx) { return p_bytes(nx); }
+  __host__ __device__ static size_t v_off(int nx) { return u_off(nx) + (size_t)TY * nx * sizeof(T); }
+  __host__ __device__ static size_t w_off(int nx) { return v_off(nx) + (size_t)(TY + 2) * nx * sizeof(T); }
+  // RES, GRAD_CHECK: b [TY] rows of double; GRAD_CHECK: then u, v, w [TY] rows of T
+  __host__ __device__ static size_t b_off(int nx) { return p_bytes(nx); }
+  __host__ __device__ static size_t f_off(int nx, int f) {
+    return b_off(nx) + (size_t)TY * nx * sizeof(double) + (size_t)f * TY * nx * sizeof(T);
+  }
+  // GRAD_CHECK: then the history rows p_n, p_{n-1} [TY] of double
+  __host__ __device__ static size_t h_off(int nx, int i) { return f_off(nx, 3) + (size_t)i * TY * nx * sizeof(double); }
+  __host__ __device__ static size_t bytes(int nx) {
+    size_t s = MODE == PZQ_RHS_RES ? w_off(nx) + (size_t)TY * nx * sizeof(T)
+               : MODE == PZQ_RES   ? b_off(nx) + (size_t)TY * nx * sizeof(double)
+                                   : h_off(nx, 2);
+    return (s + 127) / 128 * 128;
+  }
+};
+
+template <typename T, int MODE, int TY, int NS>
+constexpr size_t pzq_smem_bytes_host(int nx) {
+  return (size_t)NS * PzqSlot<T, MODE, TY>::bytes(nx) + NS * sizeof(uint64_t) + 18 * 32 * sizeof(double);
+}
+
+// blockDim.x * CPT == TY * nx (<= 512 threads), TY even.
+template <typename T, int MODE, int TY, int NS, int CPT>
+__global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps maps, const StreamGeom g,
+                                                T* __restrict__ ou, T* __restrict__ ov, T* __restrict__ ow,
+                                                double* __restrict__ bout, float* __restrict__ rout,
+                                                double* __restrict__ partials, const double* __restrict__ rmean,
+                                                const PzqParams prm, int* err, const int* skip) {
+  constexpr int G = 2;
+  constexpr int Q = 2 * G + 1;
+  constexpr int U = 10;  // lcm(Q, G)
+  static_assert(TY >= G && TY % 2 == 0, "tile height must cover the halo depth and keep the row parity");
+  using Slot = PzqSlot<T, MODE, TY>;
+  if (skip && *skip) return;  // converged defect correction: nothing to check
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw = smem_align128(smem_dyn);
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t slot_bytes = Slot::bytes(nx);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * slot_bytes);
+  double* scratch = reinterpret_cast<double*>(full + NS);
+  const int tid = threadIdx.x;
+  const int PL = g.zc + 2 * G;
+  const int my_items = blockIdx.x < g.n_items ? (g.n_items - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int L = my_items * PL;
+  const uint32_t p_bytes = (uint32_t)Slot::p_bytes(nx);
+  const uint32_t rowsT = (uint32_t)(TY * nx * sizeof(T));
+  const uint32_t rowsD = (uint32_t)(TY * nx * sizeof(double));
+
+  if (tid == 0) {
+    for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  auto issue = [&](int q) {
+    const int it = q / PL, j = q - it * PL;
+    const int item = blockIdx.x + it * gridDim.x;
+    const int ty = item % g.items_y, zi = item / g.items_y;
+    const int y0 = ty * TY, z0 = zi * g.zc;
+    int z = z0 - G + j;
+    z = z < 0 ? z + nz : (z >= nz ? z - nz : z);
+    const int s = q % NS;
+    unsigned char* dst = smem_raw + s * slot_bytes;
+    int ylo = y0 - G;
+    if (ylo < 0) ylo += ny;
+    int yhi = y0 + TY;
+    if (yhi >= ny) yhi -= ny;
+    uint32_t bytes = p_bytes;
+    const bool xy_plane = j >= G && j < G + g.zc;    // planes whose x/y part is computed
+    const bool w_plane = j >= 1 && j < PL - 1;        // planes at z0-1 .. z0+zc (w at z +- 1)
+    const bool out_plane = j >= 2 * G;                // completes output plane j - 2G
+    if constexpr (MODE == PZQ_RHS_RES) {
+      if (xy_plane) bytes += rowsT + (uint32_t)((TY + 2) * nx * sizeof(T));
+      if (w_plane) bytes += rowsT;
+    } else if constexpr (MODE == PZQ_RES) {
+      if (out_plane) bytes += rowsD;
+    } else {
+      if (out_plane) bytes += rowsD + 3 * rowsT + (prm.pred_order >= 1 ? rowsD : 0u) + (prm.pred_order >= 2 ? rowsD : 0u);
+    }
+    mbar_arrive_expect_tx(&full[s], bytes);
+    double* P = reinterpret_cast<double*>(dst);
+    tma_load_3d(P, &maps.p_halo, 0, ylo, z, &full[s]);
+    tma_load_3d(P + G * nx, &maps.p_main, 0, y0, z, &full[s]);
+    tma_load_3d(P + (G + TY) * nx, &maps.p_halo, 0, yhi, z, &full[s]);
+    if constexpr (MODE == PZQ_RHS_RES) {
+      if (xy_plane) {
+        tma_load_3d(dst + Slot::u_off(nx), &maps.f_main[0], 0, y0, z, &full[s]);
+        T* V = reinterpret_cast<T*>(dst + Slot::v_off(nx));
+        tma_load_3d(V, &maps.v_halo, 0, y0 == 0 ? ny - 1 : y0 - 1, z, &full[s]);
+        tma_load_3d(V + nx, &maps.f_main[1], 0, y0, z, &full[s]);
+        tma_load_3d(V + (TY + 1) * nx, &maps.v_halo, 0, yhi, z, &full[s]);
+      }
+      if (w_plane) tma_load_3d(dst + Slot::w_off(nx), &maps.f_main[2], 0, y0, z, &full[s]);
+    } else {
+      if (out_plane) {
+        const int zk = z0 + (j - 2 * G);  // output plane completed by this load (< nz)
+        tma_load_3d(dst + Slot::b_off(nx), &maps.b_main, 0, y0, zk, &full[s]);
+        if constexpr (MODE == PZQ_GRAD_CHECK) {
+#pragma unroll
+          for (int f = 0; f < 3; ++f) tma_load_3d(dst + Slot::f_off(nx, f), &maps.f_main[f], 0, y0, zk, &full[s]);
+          if (prm.pred_order >= 1) tma_load_3d(dst + Slot::h_off(nx, 0), &maps.h_main[0], 0, y0, zk, &full[s]);
+          if (prm.pred_order >= 2) tma_load_3d(dst + Slot::h_off(nx, 1), &maps.h_main[1], 0, y0, zk, &full[s]);
+        }
+      }
+    }
+  };
+
+  int q_issued = 0;
+  if (tid == 0)
+    for (; q_issued < min(L, NS); ++q_issued) issue(q_issued);
+
+  const int mask = nx - 1;
+  int cx[CPT], cy[CPT];
+#pragma unroll
+  for (int i = 0; i < CPT; ++i) {
+    const int c = tid + i * blockDim.x;
+    cx[i] = c & mask;
+    cy[i] = c >> g.log2nx;
+  }
+  const double dtv = prm.dt.get();
+  const double h = prm.h;
+  const double cL = 0.25 * h;           // h^3 / (4 h^2)
+  const double facB = 0.5 * h * h / dtv;  // KernelPressureRHS scaling
+  const double facG = -0.5 * dtv / h;     // KernelGradP scaling
+
+  double pq[Q][CPT];
+  T wq[Q][CPT];
+  double partL[G][CPT], partA[G][CPT], partB[G][CPT];
+  double pc[CPT][2], rc[CPT][2];  // parity-class sums of p and r by z parity
+  double acc0 = 0, acc1 = 0, accM = 0;
+#pragma unroll
+  for (int d = 0; d < Q; ++d)
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) {
+      pq[d][i] = 0.0;
+      wq[d][i] = (T)0;
+    }
+#pragma unroll
+  for (int d = 0; d < G; ++d)
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) partL[d][i] = partA[d][i] = partB[d][i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < CPT; ++i) pc[i][0] = pc[i][1] = rc[i][0] = rc[i][1] = 0.0;
+
+  bool ok = true;
+  int q = 0;
+  for (int it = 0; it < my_items; ++it) {
+    const int item = blockIdx.x + it * gridDim.x;
+    const int ty = item % g.items_y, zi = item / g.items_y;
+    const int y0 = ty * TY, z0 = zi * g.zc;
+    for (int j0 = 0; j0 < PL; j0 += U) {
+#pragma unroll
+      for (int jj = 0; jj < U; ++jj) {
+        const int j = j0 + jj;
+        const int s = q % NS;
+        if (ok) ok = mbar_wait(&full[s], (q / NS) & 1, err);
+        if (ok) {
+          const unsigned char* sl = smem_raw + s * slot_bytes;
+          const double* P = reinterpret_cast<const double*>(sl);
+          const int QN = jj % Q;
+#pragma unroll
+          for (int i = 0; i < CPT; ++i) pq[QN][i] = P[(G + cy[i]) * nx + cx[i]];
+          if constexpr (MODE == PZQ_RHS_RES) {
+            if (j >= 1 && j < PL - 1) {
+              const T* W = reinterpret_cast<const T*>(sl + Slot::w_off(nx));
+#pragma unroll
+              for (int i = 0; i < CPT; ++i) wq[QN][i] = W[cy[i] * nx + cx[i]];
+            }
+          }
+          // output plane k = j - 2G (z parity of k = jj parity: z0 and j0 are even)
+          if (j >= 2 * G) {
+            const int k = j - 2 * G;
+            const int QC = (jj + 3 * Q - G) % Q;
+            const int QM1 = (jj + 3 * Q - G - 1) % Q, QP1 = (jj + 3 * Q - G + 1) % Q;
+            const int QM2 = (jj + 3 * Q - G - 2) % Q, QP2 = (jj + 3 * Q - G + 2) % Q;
+            const int PS = jj % G;
+            const int zp = jj & 1;
+#pragma unroll
+            for (int i = 0; i < CPT; ++i) {
+              const size_t o = gidx(cx[i], y0 + cy[i], z0 + k, nx, ny);
+              const int cls = (cx[i] & 1) | ((cy[i] & 1) << 1) | (zp << 2);
+              const double p0 = pq[QC][i];
+              const double lap = partL[PS][i] + (pq[QP2][i] + pq[QM2][i] - 2 * p0);
+              if constexpr (MODE == PZQ_RHS_RES) {
+                const double b = partB[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
+                const double r = b - cL * lap;
+                bout[o] = b;
+                rout[o] = (float)r;
+                acc0 += r * r;
+                acc1 += b * b;
+                pc[i][zp] += p0;
+                rc[i][zp] += r;
+              } else {
+                const double* B = reinterpret_cast<const double*>(sl + Slot::b_off(nx));
+                const double b = B[cy[i] * nx + cx[i]];
+                const double r = b - cL * lap;
+                const double rp = rmean ? r - rmean[cls] : r;
+                acc0 += rp * rp;
+                if constexpr (MODE == PZQ_RES) {
+                  rout[o] = (float)rp;
+                  acc1 += b * b;
+                  pc[i][zp] += p0;
+                  rc[i][zp] += r;
+                } else {
+                  const T* F0 = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 0));
+                  const T* F1 = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 1));
+                  const T* F2 = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 2));
+                  const int c = cy[i] * nx + cx[i];
+                  const T tu = (T)((double)F0[c] + facG * partA[PS][i]);
+                  const T tv = (T)((double)F1[c] + facG * partB[PS][i]);
+                  const T tw = (T)((double)F2[c] + facG * (pq[QP1][i] - pq[QM1][i]));
+                  ou[o] = tu;
+                  ov[o] = tv;
+                  ow[o] = tw;
+                  // warm start of the next step: polynomial extrapolation in the step index
+                  const double* Hn = reinterpret_cast<const double*>(sl + Slot::h_off(nx, 0));
+                  const double* Hm = reinterpret_cast<const double*>(sl + Slot::h_off(nx, 1));
+                  double pred = p0;
+                  if (prm.pred_order == 1) pred = 2 * p0 - Hn[c];
+                  else if (prm.pred_order == 2) pred = 3 * (p0 - Hn[c]) + Hm[c];
+                  prm.pred_out[o] = pred;
+                  const double m = fmax(fmax(fabs((double)tu + prm.uinf[0]), fabs((double)tv + prm.uinf[1])),
+                                        fabs((double)tw + prm.uinf[2]));
+                  accM = fmax(accM, m);
+                  acc1 += 0.5 * ((double)tu * tu + (double)tv * tv + (double)tw * tw);
+                }
+              }
+            }
+          }
+          // x/y part of plane j (output plane j - G)
+          if (j >= G && j < G + g.zc) {
+            const int PS = jj % G;
+#pragma unroll
+            for (int i = 0; i < CPT; ++i) {
+              const int x = cx[i], r = G + cy[i];
+              const double p0 = pq[QN][i];
+              const double* Pr = P + r * nx;
+              partL[PS][i] = (Pr[(x + 2) & mask] + Pr[(x - 2) & mask] - 2 * p0) +
+                             (P[(r + 2) * nx + x] + P[(r - 2) * nx + x] - 2 * p0);
+              if constexpr (MODE == PZQ_RHS_RES) {
+                const T* Ur = reinterpret_cast<const T*>(sl + Slot::u_off(nx)) + cy[i] * nx;
+                const T* V = reinterpret_cast<const T*>(sl + Slot::v_off(nx));
+                partB[PS][i] = facB * (((double)Ur[(x + 1) & mask] - (double)Ur[(x - 1) & mask]) +
+                                       ((double)V[(cy[i] + 2) * nx + x] - (double)V[cy[i] * nx + x]));
+              } else if constexpr (MODE == PZQ_GRAD_CHECK) {
+                partA[PS][i] = Pr[(x + 1) & mask] - Pr[(x - 1) & mask];
+                partB[PS][i] = P[(r + 1) * nx + x] - P[(r - 1) * nx + x];
+              }
+            }
+          }
+        }
+        __syncthreads();  // slot s fully consumed
+        if (tid == 0 && ok && q_issued < L && q_issued == q + NS) issue(q_issued++);
+        ++q;
+      }
+    }
+  }
+  if (!ok && tid == 0) {
+    for (int r = q - NS < 0 ? 0 : q - NS; r < q_issued; ++r) mbar_wait(&full[r % NS], (r / NS) & 1, nullptr);
+  }
+  // per-CTA partial sums
+  if constexpr (MODE == PZQ_GRAD_CHECK) {
+    double mx[1] = {accM};
+    double sm[2] = {acc1, acc0};
+    block_reduce<1, true>(mx, scratch);
+    block_reduce<2, false>(sm, scratch + 32);
+    if (tid == 0) {
+      partials[4 * blockIdx.x + 0] = mx[0];
+      partials[4 * blockIdx.x + 1] = sm[0];
+      partials[4 * blockIdx.x + 2] = sm[1];
+      partials[4 * blockIdx.x + 3] = 0.0;
+    }
+  } else {
+    double v[18];
+#pragma unroll
+    for (int k = 0; k < 18; ++k) v[k] = 0.0;
+    v[0] = acc0;
+    v[1] = acc1;
+#pragma unroll
+    for (int i = 0; i < CPT; ++i)
+#pragma unroll
+      for (int zp = 0; zp < 2; ++zp) {
+        const int cls = (cx[i] & 1) | ((cy[i] & 1) << 1) | (zp << 2);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+          v[2 + c] += c == cls ? pc[i][zp] : 0.0;
+          v[10 + c] += c == cls ? rc[i][zp] : 0.0;
+        }
+      }
+    block_reduce<18, false>(v, scratch);
+    if (tid == 0)
+      for (int k = 0; k < 18; ++k) partials[18 * blockIdx.x + k] = v[k];
+  }
+}
+
+}  // namespace cup

@@ -240,11 +240,12 @@ class StepStats:
     torque: np.ndarray
     n_solves: int
     rel_residual: float
+    n_unconverged: int = 0
 
     @classmethod
     def from_c(cls, s: L.CupStepStats) -> "StepStats":
         return cls(s.dt, s.time, s.step, s.umax, s.kinetic_energy, np.array(s.force[:]), np.array(s.torque[:]),
-                   s.n_solves, s.rel_residual)
+                   s.n_solves, s.rel_residual, s.n_unconverged)
 
 
 class Simulation:

@@ -66,7 +66,10 @@ typedef struct cup_config {
   int precision;          /* CUP_PREC_* */
   int scheme;             /* CUP_SCHEME_* */
   double dc_tol;          /* FP32_DC: relative FP64 residual tolerance (default 1e-10 if <= 0) */
-  int dc_max_iter;        /* FP32_DC: max correction solves per step (default 4 if <= 0) */
+  int dc_max_iter;        /* FP32_DC: max correction solves per step (default 4 if <= 0). A residual
+                             check follows every solve; without an obstacle the check after the last
+                             solve runs inside the gradient pass, so dc_max_iter = 1 is one solve and
+                             one check per step, still verified against dc_tol */
   int dc_min_iter;        /* FP32_DC: solves always done per step (default 1 if <= 0) */
   int device;             /* CUDA device ordinal */
 } cup_config;
@@ -95,6 +98,7 @@ typedef struct cup_step_stats {
   double force[3], torque[3]; /* penalization force / torque on the sphere */
   int n_solves;
   double rel_residual;
+  int n_unconverged;       /* steps since cup_create whose defect correction missed dc_tol */
 } cup_step_stats;
 
 /* ---- lifetime (SimulationData ctor / Simulation ctor, source/Simulation.cpp:53-64) ---- */
