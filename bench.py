@@ -3,16 +3,22 @@
 
 Workload (default): decaying turbulence on [0, 2pi]^3 at 256^3, seeded random
 solenoidal velocity with E(k) ~ k^4 exp(-2 (k/4)^2), u_rms = 1, nu = 1e-3,
-CFL = 0.1, upwind3 + RK2 advection, periodic FFT pressure projection. Data
-are synthetic (generated here, seed 1234 + rank); each field is 134 MB (FP64)
-or 67 MB (FP32), so every pass streams well over L2 (126 MB) in total.
+CFL = 0.1, upwind3 + RK2 advection, periodic FFT pressure projection, in the
+chosen form: FP32 storage and advection, FP32 FFT correction solves inside an
+FP64 defect-correction loop (relative FP64 residual tolerance 1e-10, checked
+every step). Data are synthetic (generated here, seed 1234 + rank); each
+field is 67 MB (FP32) or 134 MB (FP64), so every pass streams well over L2
+(126 MB) in total.
 
 One JSON line on rank 0. `value` is device-timed (CUDA events on the
 solver's stream, inputs resident); `e2e` runs the same steps through the
 public API from pinned host buffers (velocity upload, per-step
 calcMaxTimestep + timestep with its stats read back, velocity download).
-`--impl reference` times the CPU oracle (the FP64 restatement of the
-reference's algorithm) on all host cores instead.
+Beside it: the FP64 plain step on the same workload and the relative L2
+velocity error of the FP32 form against it after the same steps, the
+defect-correction statistics, and the cost of one discrete-adjoint step
+against one forward step. `--impl reference` times the CPU oracle (the FP64
+restatement of the reference's algorithm) on all host cores instead.
 Multi-GPU: one process per GPU, each an independent replica (weak scaling).
 """
 from __future__ import annotations
@@ -41,19 +47,29 @@ def kernel_bytes(name: str, fp32: bool) -> float:
         "upwind3_stage1": 6 * s,
         "upwind3_stage2": 9 * s,
         "pressure_rhs": 3 * s + 8,
+        "rhs_dht_x": 3 * s + 8,          # FP64: u* in, RHS rows transformed in smem, x-transform out
         "dht_x": 2 * w,
         "dht_y": 2 * w,
         "dht_z_solve": 2 * w,
         "grad_p": 8 + 6 * s,
+        # FP32 defect-correction passes
+        "rhs_residual": 3 * s + 8 + 8 + 4,   # u*, p in; b (FP64), r (FP32) out
+        "dc_residual": 8 + 8 + 4,            # p, b in; r out
+        "dht_x_update_p": 4 + 8 + 8,         # correction rows in, p read-modify-write
+        "grad_p_check": 8 + 8 + 6 * s + 16 + 8,  # p, b, u* in, u out; p history in, warm start out
     }
     return float(table.get(name, 0.0))
 
 
-def step_bytes(fp32: bool, scheme: str) -> float:
-    ad = kernel_bytes("upwind3_stage1", fp32) + kernel_bytes("upwind3_stage2", fp32) if scheme == "upwind3_rk2" \
-        else kernel_bytes("advect_diffuse_ref", fp32)
-    return ad + kernel_bytes("pressure_rhs", fp32) + 2 * kernel_bytes("dht_x", fp32) + \
-        2 * kernel_bytes("dht_y", fp32) + kernel_bytes("dht_z_solve", fp32) + kernel_bytes("grad_p", fp32)
+def canonical_step_bytes(fp32: bool, scheme: str, n_solves: int = 1) -> float:
+    """Algorithmic bytes per cell-step of the hot path's canonical pass structure
+    (upwind3: 288 B FP64, 160 B FP32 with one correction solve, +64 B per
+    further solve; ref scheme: 216 / 124)."""
+    if scheme == "upwind3_rk2":
+        base = 160.0 if fp32 else 288.0
+    else:
+        base = 124.0 if fp32 else 216.0
+    return base + (64.0 * max(0, n_solves - 1) if fp32 else 0.0)
 
 
 def measured_peak():
@@ -177,6 +193,65 @@ def run_reference(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
+def make_sim(cup, n: int, precision: str, scheme: str, device: int):
+    sd = cup.SimulationData(CFL=0.1, cells=(n, n, n))
+    sd.extent, sd.nu, sd.rampup, sd.DLM, sd.lambda_ = 2 * np.pi, 1e-3, 0, 0.0, 1.0
+    sd.scheme, sd.precision, sd.device = scheme, precision, device
+    return cup.Simulation(sd)
+
+
+def timed_run(torch, sim, stream, steps: int, barrier):
+    """K device-chained steps bracketed by CUDA events on the solver's stream."""
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    st = sim.run_steps(steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    return ev0.elapsed_time(ev1), st
+
+
+def max_over_ranks(torch, world: int, dev, x: float) -> float:
+    if world == 1:
+        return x
+    t = torch.tensor([x], device=dev, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def adjoint_cost(torch, sim, stream, reps: int = 10) -> dict:
+    """One discrete-adjoint step (cup_adjoint_step: stage recompute, projection
+    of the adjoint field, two transposed stages) against one forward step with
+    the same fixed dt, both CUDA-event timed on the solver's stream."""
+    torch.cuda.set_stream(stream)
+    sim.bind_torch_stream()
+    dt = sim.calcMaxTimestep()
+    state = sim.velocity_raw()
+    lam = torch.randn_like(state)
+    for _ in range(2):
+        sim.timestep(dt, stats=False)
+        sim.adjoint_step(state, dt, lam)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    for _ in range(reps):
+        sim.timestep(dt, stats=False)
+    ev[1].record(stream)
+    ev[2].record(stream)
+    for _ in range(reps):
+        sim.adjoint_step(state, dt, lam)
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    fwd = ev[0].elapsed_time(ev[1]) / reps
+    adj = ev[2].elapsed_time(ev[3]) / reps
+    return {"forward_ms_per_step": fwd, "adjoint_ms_per_step": adj, "adjoint_over_forward": adj / fwd,
+            "note": "adjoint step = stage-1 recompute + adjoint projection + two transposed RK stages; "
+                    "a checkpointed rollout adds one forward recompute per step"}
+
+
 def run_ours(args, rank: int, world: int, local_rank: int):
     import ctypes as C
 
@@ -189,10 +264,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     dev = torch.device("cuda", local_rank)
     n = args.cells
     fp32 = args.precision == "fp32_dc"
-    sd = cup.SimulationData(CFL=0.1, cells=(n, n, n))
-    sd.extent, sd.nu, sd.rampup, sd.DLM, sd.lambda_ = 2 * np.pi, 1e-3, 0, 0.0, 1.0
-    sd.scheme, sd.precision, sd.device = args.scheme, args.precision, local_rank
-    sim = cup.Simulation(sd)
+    sim = make_sim(cup, n, args.precision, args.scheme, local_rank)
     stream = torch.cuda.Stream(device=dev)
     sim.set_stream(stream.cuda_stream)
     u, v, w = make_ic(n, 1234 + rank)
@@ -211,26 +283,15 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     # ---- device-timed region: K steps chained on the device ----
     launches0 = sim.launch_count()
     clocks = ClockSampler(local_rank)
-    barrier()
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
     w0 = time.time()
-    ev0.record(stream)
-    st = sim.run_steps(args.steps)
-    ev1.record(stream)
-    torch.cuda.synchronize()
+    ms, st = timed_run(torch, sim, stream, args.steps, barrier)
     w1 = time.time()
-    barrier()
     clocks.mark(w0, w1)
     clk = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
     launches = sim.launch_count() - launches0
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(torch, world, dev, ms)
     value = world * n ** 3 * args.steps / (ms * 1e-3)
+    u_final = sim.velocity() if (fp32 and not args.no_fp64_compare) else None
 
     # ---- per-kernel profile (separate run, CUDA events per launch) ----
     sim.profile(True)
@@ -254,18 +315,36 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
-    ems = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ems], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ems = float(t.item())
+    ems = max_over_ranks(torch, world, dev, e0.elapsed_time(e1))
     e2e = world * n ** 3 * sim_e2e_steps / (ems * 1e-3)
     field_bytes = 3 * n ** 3 * 8
     h2d = (field_bytes + sim_e2e_steps * 8) / sim_e2e_steps
     d2h = (field_bytes + sim_e2e_steps * (8 + 256)) / sim_e2e_steps
 
+    # ---- discrete adjoint against forward (same handle, fixed dt) ----
+    adj = adjoint_cost(torch, sim, stream) if not args.no_adjoint else None
+    sim.close()
+
+    # ---- FP64 plain step on the same workload: speed and the FP32 form's error ----
+    fp64 = None
+    if fp32 and not args.no_fp64_compare:
+        s64 = make_sim(cup, n, "fp64", args.scheme, local_rank)
+        s64.set_stream(stream.cuda_stream)
+        s64.set_velocity(*[p.numpy() for p in pinned])
+        for _ in range(args.warmup):
+            s64.run_steps(1)
+        ms64, st64 = timed_run(torch, s64, stream, args.steps, barrier)
+        ms64 = max_over_ranks(torch, world, dev, ms64)
+        v64 = world * n ** 3 * args.steps / (ms64 * 1e-3)
+        r64 = s64.velocity()
+        num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(u_final, r64))
+        den = sum(float(np.sum(b ** 2)) for b in r64)
+        fp64 = {"value": v64, "ms_per_step": ms64 / args.steps, "speedup_fp32_dc_over_fp64": value / v64,
+                "rel_l2_velocity_fp32_dc_vs_fp64": (num / den) ** 0.5,
+                "after_steps": args.warmup + args.steps, "time_fp32_dc": st.time, "time_fp64": st64.time}
+        s64.close()
+
     if rank != 0:
-        sim.close()
         return
 
     peak, peak_kind = measured_peak()
@@ -274,27 +353,37 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     for name, rec in prof.items():
         b = kernel_bytes(name, fp32)
         avg_ms = rec["ms"] / rec["count"]
-        kern.append((rec["ms"], name, avg_ms, b * n ** 3 / (avg_ms * 1e-3) / 1e9 if b else None))
+        kern.append((rec["ms"], name, avg_ms, b * n ** 3 / (avg_ms * 1e-3) / 1e9 if b else None, rec["count"]))
     kern.sort(reverse=True)
     top = next(k for k in kern if k[3] is not None)
     total_ms = sum(k[0] for k in kern)
+    n_solves = st.n_solves if fp32 else 1
+    cb = canonical_step_bytes(fp32, args.scheme, n_solves)
     roof = {"bound": "hbm", "kernel": top[1], "achieved": top[3], "peak": peak, "unit": "GB/s",
             "frac": top[3] / peak, "peak_kind": peak_kind, "traffic": None,
-            "step_achieved": step_bytes(fp32, args.scheme) * value / world / 1e9,
-            "step_frac": step_bytes(fp32, args.scheme) * value / world / 1e9 / peak}
+            "step_bytes_per_cell": cb,
+            "step_achieved": cb * value / world / 1e9,
+            "step_frac": cb * value / world / 1e9 / peak}
     line = {
         "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64" if fp32 else "f64", "data": "synthetic",
         "config": workload_config(args),
         "roofline": roof,
-        "kernels": {k[1]: {"share": k[0] / total_ms, "avg_ms": k[2], "GBps": k[3]} for k in kern},
+        "kernels": {k[1]: {"share": k[0] / total_ms, "avg_ms": k[2], "launches": k[4], "GBps": k[3]} for k in kern},
         "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "clocks": clk,
         "final_state": {"time": st.time, "kinetic_energy": st.kinetic_energy, "umax": st.umax},
     }
-    sim.close()
+    if fp32:
+        line["defect_correction"] = {"tol": 1e-10, "n_solves_last_step": st.n_solves,
+                                     "rel_residual_last_step": st.rel_residual,
+                                     "steps_missing_tol": st.n_unconverged}
+    if fp64 is not None:
+        line["fp64_plain"] = fp64
+    if adj is not None:
+        line["adjoint"] = adj
     if not args.no_cpu_baseline and world == 1:
         rate, el, thr = cpu_reference_rate(n, args.scheme, args.cpu_steps, 1, u, v, w)
         line["cpu_baseline"] = {"value": rate, "unit": "cell-steps/s", "cores": thr, "kind": "port",
@@ -309,11 +398,13 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_dc"])
+    ap.add_argument("--precision", default="fp32_dc", choices=["fp64", "fp32_dc"])
     ap.add_argument("--scheme", default="upwind3_rk2", choices=["upwind3_rk2", "ref"])
     ap.add_argument("--cells", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-compare", action="store_true", help="skip the FP64 plain run beside FP32_DC")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint-step timing")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -117,6 +117,13 @@ __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.comm
 // Waits until all committed bulk stores of this thread are complete.
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
+// Waits until the shared-memory sources of all but the N most recent committed
+// bulk-store groups of this thread have been read (the buffers may be reused).
+template <int N_>
+__device__ __forceinline__ void bulk_wait_read() {
+  asm volatile("cp.async.bulk.wait_group.read %0;" ::"n"(N_) : "memory");
+}
+
 // Orders this thread's generic-proxy shared-memory writes before subsequent
 // async-proxy (TMA / bulk) accesses.
 __device__ __forceinline__ void fence_proxy_async_smem() {

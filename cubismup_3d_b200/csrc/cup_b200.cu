@@ -102,9 +102,20 @@ __global__ void k_calc_dt(DevState* st, double h, double nu, double CFL, int ram
   if (DLM > 0) st->lambda = DLM / dt;
 }
 
-__global__ void k_set_dt(DevState* st, double dt, double DLM) {
-  st->dt = dt;
-  if (DLM > 0) st->lambda = DLM / dt;
+// Host-side scalars into the device state without a pageable copy (which
+// would serialise the host with the stream): bit 1 dt (and lambda = DLM/dt
+// when DLM > 0), bit 2 lambda (when DLM <= 0), bit 4 step and time.
+enum { SET_DT = 1, SET_LAMBDA = 2, SET_CLOCK = 4 };
+__global__ void k_set_state(DevState* st, int what, double dt, double DLM, double lambda, int step, double time) {
+  if (what & SET_DT) {
+    st->dt = dt;
+    if (DLM > 0) st->lambda = DLM / dt;
+  }
+  if ((what & SET_LAMBDA) && !(DLM > 0)) st->lambda = lambda;
+  if (what & SET_CLOCK) {
+    st->step = step;
+    st->time = time;
+  }
 }
 
 // End of step: umax (grid part outside the obstacle box, box part after
@@ -409,7 +420,8 @@ struct cup_handle {
   int p_valid = 0;
   bool pred_ready = false;
   double* rhs = nullptr;  // pressure RHS (FP64); FP64 mode: also the FFT work array
-  float* work32 = nullptr;  // FP32_DC FFT work array
+  float* work32 = nullptr;  // FP32_DC FFT work array (residual, forward x/y passes)
+  double* work64 = nullptr;  // FP32_DC FFT work array (z pass onwards, FP64)
   double* partials = nullptr;
   DevState* dstate = nullptr;
   int* derr = nullptr;
@@ -593,6 +605,7 @@ int launch_rows_M(cup_handle* H, const char* name, const Prod& prod, const Cons&
   const int lpc = 256 / TPL;
   const int nrows = H->ny * H->nz;
   const size_t smem = (size_t)lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
+                      (Cons::kAddBulk ? (size_t)lpc * N * sizeof(double) : 0) +
                       FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + 16 + 32 * 20 * sizeof(double) + 128;
   auto kern = k_dht_rows<M, R, Prod, Cons>;
   int bpsm = 0;
@@ -627,38 +640,44 @@ int rows_grid(const cup_handle* H) {
   return (H->ny * H->nz + lpc - 1) / lpc;
 }
 
-template <int M, typename R, int AXIS, bool DIVIDE>
-int launch_cols_M(cup_handle* H, R* buf, const int* skip) {
-  constexpr int N = 2 * M, TPL = M / 8;
-  const int W = std::min(256 / TPL, H->nx);
-  CUtensorMap map;
-  int rc = make_map(H, &map, buf, tma_dtype<R>(), sizeof(R), W, AXIS == 1 ? N : 1, AXIS == 2 ? N : 1);
+template <int M, typename R, int AXIS, bool DIVIDE, typename RIN = R>
+int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
+  // W x-columns per tile (FP32: 128-B rows of a tile, FP64: 128 B), NB = 3 tile buffers
+  constexpr int N = 2 * M, TPL = M / 8, NB = 3;
+  constexpr int W = sizeof(R) == 4 ? 32 : 16;
+  if (H->nx % W) return fail(H, CUP_ERR_ARG, "nx must be a multiple of %d for this precision", W);
+  CUtensorMap map_in, map_out;
+  int rc = make_map(H, &map_in, in, tma_dtype<RIN>(), sizeof(RIN), W, AXIS == 1 ? N : 1, AXIS == 2 ? N : 1);
+  if (!rc) rc = make_map(H, &map_out, out, tma_dtype<R>(), sizeof(R), W, AXIS == 1 ? N : 1, AXIS == 2 ? N : 1);
   if (rc) return rc;
-  const size_t smem = (size_t)N * W * sizeof(R) + FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + 16 + 128;
-  auto kern = k_dht_cols<M, R, AXIS, DIVIDE>;
+  const size_t smem = (size_t)NB * N * W * sizeof(R) + FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) +
+                      NB * sizeof(uint64_t) + 128;
+  auto kern = k_dht_cols_pipe<M, R, AXIS, DIVIDE, W, NB, RIN>;
+  const int threads = W * TPL;
   int bpsm = 0;
-  rc = prepare_kernel(H, kern, smem, W * TPL, &bpsm);
+  rc = prepare_kernel(H, kern, smem, threads, &bpsm);
   if (rc) return rc;
   const int ntx = H->nx / W;
-  const int grid = ntx * (AXIS == 1 ? H->nz : H->ny);
+  const int ntiles = ntx * (AXIS == 1 ? H->nz : H->ny);
+  const int grid = std::min(ntiles, bpsm * H->num_sms);
   SpectralParams sp{H->cosx, H->cosy, H->cosz, H->norm_factor, H->nx, H->ny, H->nz};
-  return launch_named(H, AXIS == 1 ? "dht_y" : "dht_z_solve", [&]() -> int {
-    kern<<<grid, W * TPL, smem, H->stream>>>(map, map, W, ntx, table<R>(H, AXIS), sp, H->derr, skip);
+  const char* name = AXIS == 1 ? "dht_y" : (sizeof(RIN) < sizeof(R) ? "dht_z_solve_mixed" : "dht_z_solve");
+  return launch_named(H, name, [&]() -> int {
+    kern<<<grid, threads, smem, H->stream>>>(map_in, map_out, ntx, ntiles, table<R>(H, AXIS), sp, H->derr, skip);
     CKL();
     return CUP_OK;
   });
 }
 
-template <typename R, int AXIS, bool DIVIDE>
-int launch_cols(cup_handle* H, R* buf, const int* skip) {
+template <typename R, int AXIS, bool DIVIDE, typename RIN = R>
+int launch_cols(cup_handle* H, RIN* in, R* out, const int* skip) {
   const int N = AXIS == 1 ? H->ny : H->nz;
   switch (N / 2) {
-    case 8: return launch_cols_M<8, R, AXIS, DIVIDE>(H, buf, skip);
-    case 16: return launch_cols_M<16, R, AXIS, DIVIDE>(H, buf, skip);
-    case 32: return launch_cols_M<32, R, AXIS, DIVIDE>(H, buf, skip);
-    case 64: return launch_cols_M<64, R, AXIS, DIVIDE>(H, buf, skip);
-    case 128: return launch_cols_M<128, R, AXIS, DIVIDE>(H, buf, skip);
-    case 256: return launch_cols_M<256, R, AXIS, DIVIDE>(H, buf, skip);
+    case 8: return launch_cols_M<8, R, AXIS, DIVIDE, RIN>(H, in, out, skip);
+    case 16: return launch_cols_M<16, R, AXIS, DIVIDE, RIN>(H, in, out, skip);
+    case 32: return launch_cols_M<32, R, AXIS, DIVIDE, RIN>(H, in, out, skip);
+    case 64: return launch_cols_M<64, R, AXIS, DIVIDE, RIN>(H, in, out, skip);
+    case 128: return launch_cols_M<128, R, AXIS, DIVIDE, RIN>(H, in, out, skip);
   }
   return fail(H, CUP_ERR_ARG, "unsupported line length %d", N);
 }
@@ -669,10 +688,29 @@ int launch_cols(cup_handle* H, R* buf, const int* skip) {
 template <typename R>
 int fft_middle(cup_handle* H, R* work, const int* skip) {
   int rc;
-  if ((rc = launch_cols<R, 1, false>(H, work, skip))) return rc;
-  if ((rc = launch_cols<R, 2, true>(H, work, skip))) return rc;
-  if ((rc = launch_cols<R, 1, false>(H, work, skip))) return rc;
+  if ((rc = launch_cols<R, 1, false>(H, work, work, skip))) return rc;
+  if ((rc = launch_cols<R, 2, true>(H, work, work, skip))) return rc;
+  if ((rc = launch_cols<R, 1, false>(H, work, work, skip))) return rc;
   return CUP_OK;
+}
+
+// Correction solve of the defect-correction loop, mixed precision: the x and y
+// forward transforms of the FP32 residual in FP32; the z pass widens to FP64
+// (forward, spectral divide, inverse); the y and x inverse transforms in FP64,
+// the last one adding the correction to p (minus the parity-class means of p
+// measured by the preceding residual pass). An FP32 inverse would leave white
+// rounding noise in the correction whose wide-Laplacian image is large next to
+// a smooth residual; with the inverse in FP64 one solve contracts the residual
+// by about 1e-7 whatever its spectrum.
+int dc_correction_solve(cup_handle* H, double* p, const int* skip) {
+  int rc;
+  if ((rc = launch_rows<float>(H, "dht_x", RowsFromArray<float>{H->work32}, RowsToArray<float>{H->work32}, skip)))
+    return rc;
+  if ((rc = launch_cols<float, 1, false>(H, H->work32, H->work32, skip))) return rc;
+  if ((rc = launch_cols<double, 2, true, float>(H, H->work32, H->work64, skip))) return rc;
+  if ((rc = launch_cols<double, 1, false>(H, H->work64, H->work64, skip))) return rc;
+  return launch_rows<double>(H, "dht_x_update_p", RowsFromArray<double>{H->work64},
+                             RowsAddToP{p, H->dstate->cmean, H->ny}, skip);
 }
 
 // p = H(f . H(work)) over the three axes, in place on `work`; the last x
@@ -817,7 +855,7 @@ int do_pressure_rhs(cup_handle* H, DtArg dt) {
 }
 
 double dc_tol(const cup_handle* H) { return H->cfg.dc_tol > 0 ? H->cfg.dc_tol : 1e-10; }
-int dc_max_iter(const cup_handle* H) { return H->cfg.dc_max_iter > 0 ? H->cfg.dc_max_iter : 4; }
+int dc_max_iter(const cup_handle* H) { return H->cfg.dc_max_iter > 0 ? H->cfg.dc_max_iter : 2; }
 int dc_min_iter(const cup_handle* H) {
   return std::min(dc_max_iter(H), H->cfg.dc_min_iter > 0 ? H->cfg.dc_min_iter : 1);
 }
@@ -889,12 +927,7 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt) {
     return rc;
   if ((rc = launch_finalize_residual(H, grid, 0))) return rc;
   for (int k = 1; k <= max_iter; ++k) {
-    if ((rc = launch_rows<float>(H, "dht_x", RowsFromArray<float>{H->work32}, RowsToArray<float>{H->work32}, conv)))
-      return rc;
-    if ((rc = fft_middle<float>(H, H->work32, conv))) return rc;
-    if ((rc = launch_rows<float>(H, "dht_x_update_p", RowsFromArray<float>{H->work32},
-                                 RowsUpdateP{W, H->dstate->cmean, H->nx, H->ny}, conv)))
-      return rc;
+    if ((rc = dc_correction_solve(H, W, conv))) return rc;
     if (k == max_iter) break;
     if ((rc = launch_pzq<T, PZQ_RES, 4, 4, 2>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid,
                                               conv)))
@@ -923,9 +956,9 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt) {
 // the device. Solve k: the five FFT passes in FP32, the last x pass adding the
 // correction to p in FP64. Kernels after convergence exit at entry.
 int do_poisson_dc(cup_handle* H) {
-  const double tol = H->cfg.dc_tol > 0 ? H->cfg.dc_tol : 1e-10;
-  const int max_iter = H->cfg.dc_max_iter > 0 ? H->cfg.dc_max_iter : 4;
-  const int min_iter = std::min(max_iter, H->cfg.dc_min_iter > 0 ? H->cfg.dc_min_iter : 1);
+  const double tol = dc_tol(H);
+  const int max_iter = dc_max_iter(H);
+  const int min_iter = dc_min_iter(H);
   const int* conv = &H->dstate->converged;
   const double inv_class = 8.0 / (double)H->n;
   int rc;
@@ -944,12 +977,7 @@ int do_poisson_dc(cup_handle* H) {
       if (rc_) return rc_;
     }
     if (k == max_iter) break;
-    if ((rc = launch_rows<float>(H, "dht_x", RowsFromArray<float>{H->work32}, RowsToArray<float>{H->work32}, conv)))
-      return rc;
-    if ((rc = fft_middle<float>(H, H->work32, conv))) return rc;
-    if ((rc = launch_rows<float>(H, "dht_x_update_p", RowsFromArray<float>{H->work32},
-                                 RowsUpdateP{H->p, H->dstate->cmean, H->nx, H->ny}, conv)))
-      return rc;
+    if ((rc = dc_correction_solve(H, H->p, conv))) return rc;
   }
   return CUP_OK;
 }
@@ -1265,6 +1293,7 @@ int cup_create(const cup_config* cfg, cup_handle** out) {
     CK(cudaMalloc(&H->p, H->n * sizeof(double)));
     CK(cudaMalloc(&H->rhs, H->n * sizeof(double)));
     if (H->fp32) CK(cudaMalloc(&H->work32, H->n * sizeof(float)));
+    if (H->fp32) CK(cudaMalloc(&H->work64, H->n * sizeof(double)));
     if (H->fp32) {
       CK(cudaMalloc(&H->p_old, H->n * sizeof(double)));
       CK(cudaMalloc(&H->p_pred, H->n * sizeof(double)));
@@ -1321,7 +1350,7 @@ int cup_destroy(cup_handle* H) {
   if (H->stream) cudaStreamSynchronize(H->stream);
   for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->au, H->av, H->aw, (void*)H->p_adj,
                   H->chi, (void*)H->p, (void*)H->p_old, (void*)H->p_pred, (void*)H->rhs,
-                  (void*)H->work32, (void*)H->partials, (void*)H->dstate, (void*)H->derr, (void*)H->cosx,
+                  (void*)H->work32, (void*)H->work64, (void*)H->partials, (void*)H->dstate, (void*)H->derr, (void*)H->cosx,
                   (void*)H->cosy, (void*)H->cosz, (void*)H->sp_dev})
     if (f) cudaFree(f);
   for (int d = 0; d < 3; ++d) {
@@ -1634,7 +1663,14 @@ int cup_penalize(cup_handle* H, double dt, double force_torque[6]) {
     if (force_torque) std::fill(force_torque, force_torque + 6, 0.0);
     return CUP_OK;
   }
-  CK(cudaMemcpyAsync(&H->dstate->lambda, &H->lambda, sizeof(double), cudaMemcpyHostToDevice, H->stream));
+  {
+    int rc_ = launch_named(H, "set_state", [&]() -> int {
+      k_set_state<<<1, 1, 0, H->stream>>>(H->dstate, SET_LAMBDA, 0.0, H->cfg.DLM, H->lambda, 0, 0.0);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
   int rc = DISPATCH_T(H, do_penalize, DtArg{dt, nullptr}, (const double*)nullptr);
   if (rc) return rc;
   {
@@ -1686,13 +1722,12 @@ int cup_step(cup_handle* H, double dt, cup_step_stats* stats) {
   // device dt/lambda follow the host values for this step
   {
     int rc_ = launch_named(H, "set_dt", [&]() -> int {
-      k_set_dt<<<1, 1, 0, H->stream>>>(H->dstate, dt, H->cfg.DLM);
+      k_set_state<<<1, 1, 0, H->stream>>>(H->dstate, SET_DT | SET_LAMBDA, dt, H->cfg.DLM, H->lambda, 0, 0.0);
       CKL();
       return CUP_OK;
     });
     if (rc_) return rc_;
   }
-  if (H->cfg.DLM <= 0) CK(cudaMemcpyAsync(&H->dstate->lambda, &H->lambda, sizeof(double), cudaMemcpyHostToDevice, H->stream));
   int rc = DISPATCH_T(H, do_step, DtArg{dt, nullptr}, (const double*)&H->dstate->lambda, 1);
   if (rc) return rc;
   H->step += 1;
@@ -1760,9 +1795,15 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
     if ((rc = DISPATCH_T(H, do_max_u))) return rc;
     H->umax_fresh = true;
   }
-  CK(cudaMemcpyAsync(&H->dstate->step, &H->step, sizeof(int), cudaMemcpyHostToDevice, H->stream));
-  CK(cudaMemcpyAsync(&H->dstate->time, &H->time, sizeof(double), cudaMemcpyHostToDevice, H->stream));
-  if (H->cfg.DLM <= 0) CK(cudaMemcpyAsync(&H->dstate->lambda, &H->lambda, sizeof(double), cudaMemcpyHostToDevice, H->stream));
+  {
+    int rc_ = launch_named(H, "set_state", [&]() -> int {
+      k_set_state<<<1, 1, 0, H->stream>>>(H->dstate, SET_LAMBDA | SET_CLOCK, 0.0, H->cfg.DLM, H->lambda, H->step,
+                                          H->time);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
   for (int i = 0; i < nsteps; ++i) {
     {
       int rc_ = launch_named(H, "calc_dt", [&]() -> int {

@@ -305,9 +305,30 @@ struct RowsFromArray {
 template <typename R>
 struct RowsToArray {
   static constexpr bool kBulk = true;
+  static constexpr bool kAddBulk = false;
   R* out;
   __device__ R* dst(int row0, int N) const { return out + (size_t)row0 * N; }
   __device__ void drain(const R*, int, int, int) const {}
+};
+
+// Consumer of the last x pass of a correction solve: p += rows - (parity-class
+// means of p measured by the preceding residual pass), in FP64. The p rows
+// arrive by bulk copy with the input rows and leave by one bulk store.
+struct RowsAddToP {
+  static constexpr bool kBulk = false;
+  static constexpr bool kAddBulk = true;
+  double* p;
+  const double* cmean;
+  int ny;
+  __device__ double* rows_of(int row0, int N) const { return p + (size_t)row0 * N; }
+  __device__ void add(double* ps, const double* rows, int row0, int nr, int N) const {
+    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) {
+      const int l = i / N, x = i - l * N;
+      const int r = row0 + l, y = r % ny, z = r / ny;
+      const int cls = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
+      ps[i] = ps[i] + rows[i] - cmean[cls];
+    }
+  }
 };
 
 template <int M, typename R, class Prod, class Cons>
@@ -319,17 +340,20 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
   constexpr int TL = FFTPlan<M>::table_len();
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
   constexpr int PPITCH = 2 * (M + M / 8);
+  constexpr bool ADD = Cons::kAddBulk;
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
   R* rows = reinterpret_cast<R*>(smem_raw);                        // lpc * N
   R* padb = rows + (size_t)lpc * N;                                // lpc * PPITCH
-  R2* tw = reinterpret_cast<R2*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));
+  double* prow = reinterpret_cast<double*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));  // lpc * N (ADD)
+  R2* tw = reinterpret_cast<R2*>(prow + (ADD ? (size_t)lpc * N : 0));
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
   double* scratch = reinterpret_cast<double*>(bar + 1);            // 32 * 20 doubles
   const int row0 = blockIdx.x * lpc;
   const int nr = min(lpc, nrows - row0);
   if (nr <= 0) return;
   const uint32_t bytes = (uint32_t)((size_t)nr * N * sizeof(R));
+  const uint32_t pbytes = ADD ? (uint32_t)((size_t)nr * N * sizeof(double)) : 0u;
   double acc[20];
 #pragma unroll
   for (int i = 0; i < 20; ++i) acc[i] = 0.0;
@@ -341,13 +365,15 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(bar, bytes);
+      mbar_arrive_expect_tx(bar, bytes + pbytes);
       bulk_load(rows, prod.src(row0, N), bytes, bar);
+      if constexpr (ADD) bulk_load(prow, cons.rows_of(row0, N), pbytes, bar);
     }
     load_table(tw, tw_g, TL);
     const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
     if (!ok) return;
   } else {
+    static_assert(!ADD, "the bulk read-modify-write consumer needs a bulk producer");
     load_table(tw, tw_g, TL);
     prod.fill(rows, row0, nr, N, acc);
     __syncthreads();
@@ -357,13 +383,24 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
   RowLines<R> A{rows, N};
   RowLinesPad<R> P{padb, PPITCH};
   dht_lines<M, PAD, R>(A, P, tw, l, t, active);
-  if constexpr (Cons::kBulk) {
-    fence_proxy_async_smem();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      bulk_store(cons.dst(row0, N), rows, bytes);
-      bulk_commit();
-      bulk_wait_all();
+  if constexpr (Cons::kBulk || ADD) {
+    if constexpr (ADD) {
+      cons.add(prow, rows, row0, nr, N);
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        bulk_store(cons.rows_of(row0, N), prow, pbytes);
+        bulk_commit();
+        bulk_wait_all();
+      }
+    } else {
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        bulk_store(cons.dst(row0, N), rows, bytes);
+        bulk_commit();
+        bulk_wait_all();
+      }
     }
   } else {
     cons.drain(rows, row0, nr, N);
@@ -441,6 +478,122 @@ __global__ void __launch_bounds__(256) k_dht_cols(const __grid_constant__ CUtens
     tma_store_3d(&map_out, x0, c1, c2, tile);
     bulk_commit();
     bulk_wait_all();
+  }
+}
+
+// Pipelined y / z pass: persistent CTAs walk the tiles (W consecutive x
+// columns by the whole line; tile t is x0 = (t % ntiles_x) W and the other
+// coordinate t / ntiles_x) through NB shared-memory tile buffers. The TMA
+// loads of the next NB-1 tiles and the store of the previous tile overlap the
+// transform of the current one; the twiddle table is loaded once per CTA.
+//
+// RIN = float with R = double (z pass of the mixed-precision correction
+// solve): the FP32 tile lands in the upper half of its FP64 buffer and is
+// widened in place (all reads, a barrier, then all writes) before the FP64
+// transforms; the tile is stored in FP64.
+template <int M, typename R, int AXIS, bool DIVIDE, int W, int NB, typename RIN = R>
+__global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_constant__ CUtensorMap map_in,
+                                                       const __grid_constant__ CUtensorMap map_out, int ntiles_x,
+                                                       int ntiles, const typename Cplx<R>::T* tw_g, SpectralParams sp,
+                                                       int* err, const int* skip) {
+  using R2 = typename Cplx<R>::T;
+  static_assert(NB >= 2, "need at least two tile buffers");
+  static_assert(sizeof(RIN) <= sizeof(R), "input may only be narrower than the transform type");
+  if (skip && *skip) return;
+  constexpr int N = 2 * M, TPL = M / 8;
+  constexpr int TL = FFTPlan<M>::table_len();
+  constexpr bool WIDEN = sizeof(RIN) < sizeof(R);
+  constexpr uint32_t TILE_BYTES = (uint32_t)(N * W * sizeof(RIN));
+  constexpr int PER_THREAD = (N * W + W * TPL - 1) / (W * TPL);
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw = smem_align128(smem_dyn);
+  R* tiles = reinterpret_cast<R*>(smem_raw);  // [NB][N][W]
+  R2* tw = reinterpret_cast<R2*>(tiles + (size_t)NB * N * W);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
+  const int tid = threadIdx.x;
+  const int my = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  if (tid == 0) {
+    for (int b = 0; b < NB; ++b) mbar_init(&bar[b], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto coords = [&](int i, int& x0, int& other) {
+    const int t = blockIdx.x + i * gridDim.x;
+    x0 = (t % ntiles_x) * W;
+    other = t / ntiles_x;  // z for AXIS 1, y for AXIS 2
+  };
+  auto issue = [&](int i) {
+    int x0, other;
+    coords(i, x0, other);
+    const int b = i % NB;
+    mbar_arrive_expect_tx(&bar[b], TILE_BYTES);
+    // widening: the narrow tile occupies the upper half of the buffer
+    unsigned char* dst = reinterpret_cast<unsigned char*>(tiles + (size_t)b * N * W) +
+                         (WIDEN ? (size_t)N * W * (sizeof(R) - sizeof(RIN)) : 0);
+    tma_load_3d(dst, &map_in, x0, AXIS == 1 ? 0 : other, AXIS == 1 ? other : 0, &bar[b]);
+  };
+  int issued = 0;
+  if (tid == 0)
+    for (; issued < min(NB - 1, my); ++issued) issue(issued);
+  load_table(tw, tw_g, TL);
+  __syncthreads();
+  const int l = tid % W, t = tid / W;
+  const bool active = t < TPL;
+  bool ok = true;
+  int done = 0;
+  for (int i = 0; i < my; ++i) {
+    // refill: tile i + NB - 1 goes into the buffer of tile i - 1, once the
+    // store of tile i - 1 has read it
+    if (tid == 0 && ok && issued < my) {
+      bulk_wait_read<0>();
+      issue(issued++);
+    }
+    const int b = i % NB;
+    ok = __syncthreads_and(ok && mbar_wait(&bar[b], (i / NB) & 1, err));
+    if (!ok) break;
+    int x0, other;
+    coords(i, x0, other);
+    R* tile = tiles + (size_t)b * N * W;
+    if constexpr (WIDEN) {
+      const RIN* narrow = reinterpret_cast<const RIN*>(reinterpret_cast<unsigned char*>(tile) +
+                                                       (size_t)N * W * (sizeof(R) - sizeof(RIN)));
+      R vals[PER_THREAD];
+#pragma unroll
+      for (int k = 0; k < PER_THREAD; ++k) {
+        const int e = tid + k * (int)blockDim.x;
+        vals[k] = e < N * W ? (R)narrow[e] : (R)0;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < PER_THREAD; ++k) {
+        const int e = tid + k * (int)blockDim.x;
+        if (e < N * W) tile[e] = vals[k];
+      }
+      __syncthreads();
+    }
+    ColLines<R> A{tile, W};
+    dht_lines<M, false, R>(A, A, tw, l, t, active);
+    if constexpr (DIVIDE) {
+      for (int k = tid; k < N * W; k += blockDim.x) {
+        const int n = k / W, w = k - n * W;
+        tile[k] = (R)((double)tile[k] * spectral_factor(sp, x0 + w, other, n));
+      }
+      __syncthreads();
+      dht_lines<M, false, R>(A, A, tw, l, t, active);
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tma_store_3d(&map_out, x0, AXIS == 1 ? 0 : other, AXIS == 1 ? other : 0, tile);
+      bulk_commit();
+    }
+    done = i + 1;
+  }
+  if (tid == 0) {
+    bulk_wait_all();
+    // after a timed-out wait: bounded drain of the loads still in flight
+    if (!ok)
+      for (int r = done; r < issued; ++r) mbar_wait(&bar[r % NB], (r / NB) & 1, nullptr);
   }
 }
 

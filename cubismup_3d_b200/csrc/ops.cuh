@@ -212,24 +212,6 @@ struct RowsRhs {
   __device__ void finish(double*, double*) const {}
 };
 
-// Consumer of the last x pass of a correction solve: p += delta - (parity-class
-// means of p measured by the preceding residual pass), in FP64.
-struct RowsUpdateP {
-  static constexpr bool kBulk = false;
-  double* p;
-  const double* cmean;
-  int nx, ny;
-  __device__ void drain(const float* rows, int row0, int nr, int N) const {
-    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) {
-      const int l = i / N, x = i - l * N;
-      const int r = row0 + l, y = r % ny, z = r / ny;
-      const size_t o = (size_t)r * N + x;
-      const int cls = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
-      p[o] = p[o] + (double)rows[i] - cmean[cls];
-    }
-  }
-};
-
 // Active box of the obstacle: cells [lo, lo+n) per dimension (global indices,
 // wrapped periodically). Outside it chi == 0 and the obstacle terms vanish.
 struct Box {

@@ -49,7 +49,7 @@ class SimulationData:
     precision: str = "fp64"  # "fp64" | "fp32_dc"
     scheme: str = "ref"      # "ref" | "upwind3_rk2"
     dc_tol: float = 1e-10
-    dc_max_iter: int = 4
+    dc_max_iter: int = 2
     dc_min_iter: int = 1
     device: int = 0
     verbose: bool = False

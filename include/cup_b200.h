@@ -66,7 +66,7 @@ typedef struct cup_config {
   int precision;          /* CUP_PREC_* */
   int scheme;             /* CUP_SCHEME_* */
   double dc_tol;          /* FP32_DC: relative FP64 residual tolerance (default 1e-10 if <= 0) */
-  int dc_max_iter;        /* FP32_DC: max correction solves per step (default 4 if <= 0). A residual
+  int dc_max_iter;        /* FP32_DC: max correction solves per step (default 2 if <= 0). A residual
                              check follows every solve; without an obstacle the check after the last
                              solve runs inside the gradient pass, so dc_max_iter = 1 is one solve and
                              one check per step, still verified against dc_tol */
