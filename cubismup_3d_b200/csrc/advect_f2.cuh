@@ -1,0 +1,215 @@
+// FP32 upwind3 + RK2 stages with Blackwell's packed FP32x2 arithmetic.
+//
+// Same streaming structure as k_advect_zq (TMA ring of planes, register
+// z-queues, x/y part on arrival, one block barrier per plane), but each
+// thread owns PPT pairs of x-adjacent cells and every arithmetic instruction
+// works on a pair (fma/add/mul .f32x2). The upwind term uses the branch-free
+// identity
+//   a up3(a; f) = 1/2 (a S(f) + |a| Q(f)),
+//   S = f-2 - 8 f-1 + 8 f+1 - f+2,  Q = f-2 - 4 f-1 + 6 f0 - 4 f+1 + f+2,
+// which is the same operator as the sign-selected stencil (at a = 0 both
+// give 0), so both cells of a pair follow one instruction stream.
+#pragma once
+
+#include "advect.cuh"
+
+namespace cup {
+
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 splat2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 abs2(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
+
+// 2 a up3(a; f) for a pair, given a and |a|.
+__device__ __forceinline__ float2 adv2(float2 a, float2 aa, float2 fm2, float2 fm1, float2 f0, float2 fp1, float2 fp2) {
+  const float2 S = fma2(splat2(8.f), sub2(fp1, fm1), sub2(fm2, fp2));
+  const float2 Q = fma2(splat2(6.f), f0, fma2(splat2(-4.f), add2(fm1, fp1), add2(fm2, fp2)));
+  return fma2(aa, Q, mul2(a, S));
+}
+
+// STAGE2 false: out = f + dt A(f); true: out = 1/2 (f^n + f1 + dt A(f1)).
+// blockDim.x * PPT * 2 == TY * nx (<= 512 threads).
+template <bool STAGE2, int TY, int NS, int PPT>
+__global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ AdvectMaps maps, const StreamGeom g,
+                                                     float* __restrict__ ou, float* __restrict__ ov,
+                                                     float* __restrict__ ow, DtArg dt, double h, double nu, double ux,
+                                                     double uy, double uz, int* err) {
+  constexpr int G = 2;
+  constexpr int ROWS = TY + 2 * G;
+  constexpr int Q = 2 * G + 1;
+  constexpr int U = 10;  // lcm(Q, G)
+  static_assert(TY >= G, "tile height must cover the halo depth");
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw = smem_align128(smem_dyn);
+  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const size_t field_elems = (size_t)ROWS * nx;
+  const size_t stencil_elems = 3 * field_elems;
+  const size_t slot_elems = stencil_elems + (STAGE2 ? (size_t)3 * TY * nx : 0);
+  float* slots = reinterpret_cast<float*>(smem_raw);
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * slot_elems * sizeof(float));
+  const int tid = threadIdx.x;
+  const int PL = g.zc + 2 * G;
+  const int my_items = blockIdx.x < g.n_items ? (g.n_items - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int L = my_items * PL;
+  const uint32_t stencil_bytes = (uint32_t)(stencil_elems * sizeof(float));
+  const uint32_t base_bytes = (uint32_t)(3 * TY * nx * sizeof(float));
+
+  if (tid == 0) {
+    for (int s = 0; s < NS; ++s) mbar_init(&full[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  auto issue = [&](int q) {
+    const int it = q / PL, j = q - it * PL;
+    const int item = blockIdx.x + it * gridDim.x;
+    const int ty = item % g.items_y, zi = item / g.items_y;
+    const int y0 = ty * TY, z0 = zi * g.zc;
+    int z = z0 - G + j;
+    z = z < 0 ? z + nz : (z >= nz ? z - nz : z);
+    const int s = q % NS;
+    float* dst = slots + s * slot_elems;
+    int ylo = y0 - G;
+    if (ylo < 0) ylo += ny;
+    int yhi = y0 + TY;
+    if (yhi >= ny) yhi -= ny;
+    const bool with_base = STAGE2 && j >= 2 * G;
+    mbar_arrive_expect_tx(&full[s], stencil_bytes + (with_base ? base_bytes : 0u));
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      float* fd = dst + f * field_elems;
+      tma_load_3d(fd, &maps.halo[f], 0, ylo, z, &full[s]);
+      tma_load_3d(fd + G * nx, &maps.main[f], 0, y0, z, &full[s]);
+      tma_load_3d(fd + (G + TY) * nx, &maps.halo[f], 0, yhi, z, &full[s]);
+    }
+    if (with_base) {
+      const int zk = z0 + (j - 2 * G);
+#pragma unroll
+      for (int f = 0; f < 3; ++f) tma_load_3d(dst + stencil_elems + f * TY * nx, &maps.base[f], 0, y0, zk, &full[s]);
+    }
+  };
+
+  int q_issued = 0;
+  if (tid == 0)
+    for (; q_issued < min(L, NS); ++q_issued) issue(q_issued);
+
+  const int mask = nx - 1;
+  const int half = nx >> 1;
+  int px[PPT], cy[PPT];  // even x of the pair, tile row
+#pragma unroll
+  for (int i = 0; i < PPT; ++i) {
+    const int pi = tid + i * blockDim.x;
+    px[i] = (pi % half) * 2;
+    cy[i] = pi / half;
+  }
+  const double dtv = dt.get();
+  const float2 facA = splat2((float)(-dtv / (12 * h)));  // the 1/2 of the symmetric form folded in
+  const float2 facD = splat2((float)((nu / h) * (dtv / h)));
+  const float2 uinf[3] = {splat2((float)ux), splat2((float)uy), splat2((float)uz)};
+
+  float2 qv[3][Q][PPT];
+  float2 part[3][G][PPT];
+#pragma unroll
+  for (int f = 0; f < 3; ++f)
+#pragma unroll
+    for (int d = 0; d < Q; ++d)
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) qv[f][d][i] = splat2(0.f);
+#pragma unroll
+  for (int f = 0; f < 3; ++f)
+#pragma unroll
+    for (int d = 0; d < G; ++d)
+#pragma unroll
+      for (int i = 0; i < PPT; ++i) part[f][d][i] = splat2(0.f);
+
+  bool ok = true;
+  int q = 0;
+  for (int it = 0; it < my_items; ++it) {
+    const int item = blockIdx.x + it * gridDim.x;
+    const int ty = item % g.items_y, zi = item / g.items_y;
+    const int y0 = ty * TY, z0 = zi * g.zc;
+    for (int j0 = 0; j0 < PL; j0 += U) {
+#pragma unroll
+      for (int jj = 0; jj < U; ++jj) {
+        const int j = j0 + jj;
+        const int s = q % NS;
+        if (ok) ok = mbar_wait(&full[s], (q / NS) & 1, err);
+        if (ok) {
+          const float* sl = slots + s * slot_elems;
+          const int QN = jj % Q;
+#pragma unroll
+          for (int f = 0; f < 3; ++f)
+#pragma unroll
+            for (int i = 0; i < PPT; ++i)
+              qv[f][QN][i] = *reinterpret_cast<const float2*>(sl + f * field_elems + (G + cy[i]) * nx + px[i]);
+          if (j >= 2 * G) {
+            const int k = j - 2 * G;
+            const int QC = (jj + 3 * Q - G) % Q;
+            const int QM1 = (jj + 3 * Q - G - 1) % Q, QP1 = (jj + 3 * Q - G + 1) % Q;
+            const int QM2 = (jj + 3 * Q - G - 2) % Q, QP2 = (jj + 3 * Q - G + 2) % Q;
+            const int PS = jj % G;
+#pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+              const size_t o = gidx(px[i], y0 + cy[i], z0 + k, nx, ny);
+              const float2 ww = add2(qv[2][QC][i], uinf[2]);
+              const float2 aw = abs2(ww);
+              float2 outv[3];
+#pragma unroll
+              for (int f = 0; f < 3; ++f) {
+                const float2 f0 = qv[f][QC][i];
+                const float2 az = adv2(ww, aw, qv[f][QM2][i], qv[f][QM1][i], f0, qv[f][QP1][i], qv[f][QP2][i]);
+                const float2 lz = fma2(splat2(-6.f), f0, add2(qv[f][QM1][i], qv[f][QP1][i]));
+                outv[f] = fma2(facD, lz, fma2(facA, az, add2(f0, part[f][PS][i])));
+              }
+              if constexpr (STAGE2) {
+                const float* bs = sl + stencil_elems + cy[i] * nx + px[i];
+#pragma unroll
+                for (int f = 0; f < 3; ++f)
+                  outv[f] = mul2(splat2(0.5f), add2(*reinterpret_cast<const float2*>(bs + f * TY * nx), outv[f]));
+              }
+              *reinterpret_cast<float2*>(ou + o) = outv[0];
+              *reinterpret_cast<float2*>(ov + o) = outv[1];
+              *reinterpret_cast<float2*>(ow + o) = outv[2];
+            }
+          }
+          if (j >= G && j < G + g.zc) {
+            const int PS = jj % G;
+#pragma unroll
+            for (int i = 0; i < PPT; ++i) {
+              const float2 uu = add2(qv[0][QN][i], uinf[0]), vv = add2(qv[1][QN][i], uinf[1]);
+              const float2 au = abs2(uu), av = abs2(vv);
+              const int x = px[i], r = G + cy[i];
+              const int xl = (x - 2) & mask, xr = (x + 2) & mask;
+#pragma unroll
+              for (int f = 0; f < 3; ++f) {
+                const float* F = sl + f * field_elems;
+                const float2 c0 = qv[f][QN][i];
+                const float2 A = *reinterpret_cast<const float2*>(F + r * nx + xl);
+                const float2 B = *reinterpret_cast<const float2*>(F + r * nx + xr);
+                const float2 xm1 = make_float2(A.y, c0.x), xp1 = make_float2(c0.y, B.x);
+                const float2 ym2 = *reinterpret_cast<const float2*>(F + (r - 2) * nx + x);
+                const float2 ym1 = *reinterpret_cast<const float2*>(F + (r - 1) * nx + x);
+                const float2 yp1 = *reinterpret_cast<const float2*>(F + (r + 1) * nx + x);
+                const float2 yp2 = *reinterpret_cast<const float2*>(F + (r + 2) * nx + x);
+                const float2 ax = adv2(uu, au, A, xm1, c0, xp1, B);
+                const float2 ay = adv2(vv, av, ym2, ym1, c0, yp1, yp2);
+                const float2 nb = add2(add2(xm1, xp1), add2(ym1, yp1));
+                part[f][PS][i] = fma2(facD, nb, mul2(facA, add2(ax, ay)));
+              }
+            }
+          }
+        }
+        __syncthreads();  // slot s fully consumed
+        if (tid == 0 && ok && q_issued < L && q_issued == q + NS) issue(q_issued++);
+        ++q;
+      }
+    }
+  }
+  if (!ok && tid == 0) {
+    for (int r = q - NS < 0 ? 0 : q - NS; r < q_issued; ++r) mbar_wait(&full[r % NS], (r / NS) & 1, nullptr);
+  }
+}
+
+}  // namespace cup
