@@ -121,22 +121,21 @@ __global__ void k_set_state(DevState* st, int what, double dt, double DLM, doubl
 
 // End of step: umax (grid part outside the obstacle box, box part after
 // penalization), kinetic energy, force/torque; advances step and time.
-__global__ void k_finalize_step(const double* pgrad, int ngrad, int gstride, const double* ppen, int npen,
-                                DevState* st, double h3, int advance, int dc_final, double tol, int max_iter) {
-  __shared__ double scratch[9 * 32];
+__global__ void k_finalize_step(const double* pgrad, int ngrad, int gstride, int max_off, int ke_off,
+                                const double* ppen, int npen, DevState* st, double h3, int advance) {
+  __shared__ double scratch[8 * 32];
   double mx[1] = {0.0};
-  double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
   for (int i = threadIdx.x; i < ngrad; i += blockDim.x) {
-    mx[0] = fmax(mx[0], pgrad[gstride * i]);
-    s[6] += pgrad[gstride * i + 1];
-    if (dc_final) s[7] += pgrad[gstride * i + 2];
+    mx[0] = fmax(mx[0], pgrad[gstride * i + max_off]);
+    s[6] += pgrad[gstride * i + ke_off];
   }
   for (int i = threadIdx.x; i < npen; i += blockDim.x) {
     for (int k = 0; k < 6; ++k) s[k] += ppen[8 * i + k];
     mx[0] = fmax(mx[0], ppen[8 * i + 6]);
   }
-  block_reduce<8, false>(s, scratch);
-  block_reduce<1, true>(mx, scratch + 8 * 32);
+  block_reduce<7, false>(s, scratch);
+  block_reduce<1, true>(mx, scratch + 7 * 32);
   if (threadIdx.x == 0) {
     st->umax = mx[0];
     st->ke = s[6] * h3;
@@ -145,17 +144,6 @@ __global__ void k_finalize_step(const double* pgrad, int ngrad, int gstride, con
         st->force[k] = s[k];
         st->torque[k] = s[3 + k];
       }
-    }
-    // final defect-correction check (fused into the gradient pass): it decides
-    // only when no earlier check converged, i.e. after max_iter solves
-    if (dc_final && st->converged == 0) {
-      const double res2 = s[7], b2 = st->b2;
-      const bool met = b2 == 0.0 || sqrt(res2) <= tol * sqrt(b2);
-      st->res2 = res2;
-      if (max_iter < 16) st->res_hist[max_iter] = b2 > 0 ? sqrt(res2 / b2) : 0.0;
-      st->n_solves = max_iter;
-      st->converged = met ? 1 : 2;
-      if (!met) st->n_unconverged += 1;
     }
     if (advance) {
       st->step += 1;
@@ -217,14 +205,14 @@ __global__ void k_finalize_com(const double* p, int np, DevState* st, SpherePara
 // reachable by any pressure: the spectral factor is zero there), the
 // parity-class means of p, and the decision |r| <= tol |b| (from check
 // min_iter on; check max_iter is final).
-__global__ void k_finalize_residual(const double* p, int np, DevState* st, double tol, int k, int min_iter,
-                                    int max_iter, double inv_class_cells) {
+__global__ void k_finalize_residual(const double* p, int stride, int np, DevState* st, double tol, int k,
+                                    int min_iter, int max_iter, double inv_class_cells) {
   __shared__ double scratch[18 * 32];
   if (k > 0 && st->converged) return;
   double s[18];
   for (int j = 0; j < 18; ++j) s[j] = 0.0;
   for (int i = threadIdx.x; i < np; i += blockDim.x)
-    for (int j = 0; j < 18; ++j) s[j] += p[18 * i + j];
+    for (int j = 0; j < 18; ++j) s[j] += p[(size_t)stride * i + j];
   block_reduce<18, false>(s, scratch);
   if (threadIdx.x == 0) {
     double res2, b2;
@@ -442,7 +430,8 @@ struct cup_handle {
   double uinf[3] = {0, 0, 0};
   bool umax_fresh = false;
   int n_grad_partials = 0, n_pen_partials = 0;
-  int grad_stride = 2;  // 4 when the gradient pass also carries the final residual check
+  // layout of the gradient pass's partials: values per CTA, offsets of max |u| and the kinetic energy
+  int grad_stride = 2, grad_max_off = 0, grad_ke_off = 1;
   DevState* hstate = nullptr;  // pinned host copy
   // per-step solve stats
   int last_n_solves = 0;
@@ -458,7 +447,7 @@ struct cup_handle {
   };
   std::vector<Pending> pending;
   std::vector<cudaEvent_t> ev_pool;
-  std::map<std::string, std::pair<long long, double>> prof;  // name -> (count, ms)
+  std::map<std::string, std::vector<float>> prof;  // name -> duration (ms) of each launch
 };
 
 namespace {
@@ -507,9 +496,7 @@ void prof_flush(cup_handle* H) {
   for (auto& p : H->pending) {
     float ms = 0;
     cudaEventElapsedTime(&ms, p.a, p.b);
-    auto& e = H->prof[p.name];
-    e.first += 1;
-    e.second += ms;
+    H->prof[p.name].push_back(ms);
     H->ev_pool.push_back(p.a);
     H->ev_pool.push_back(p.b);
   }
@@ -634,6 +621,45 @@ int launch_rows(cup_handle* H, const char* name, const Prod& prod, const Cons& c
   return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
 }
 
+// Pipelined x pass (k_dht_rows_pipe): rows of `in` transformed into `out`,
+// or with ADD added to p (minus cmean). FP32: three tile buffers; FP64: two.
+template <int M, typename R, bool ADD>
+int launch_rows_pipe_M(cup_handle* H, const char* name, const R* in, R* out, double* p, const double* cmean,
+                       const int* skip) {
+  constexpr int N = 2 * M, TPL = M / 8;
+  constexpr bool PAD = FFTPlan<M>::nstages > 1;
+  constexpr int NB = sizeof(R) == 4 ? 3 : 2;
+  const int lpc = 256 / TPL;
+  const int nrows = H->ny * H->nz;
+  const size_t smem = (size_t)NB * lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
+                      FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + NB * sizeof(uint64_t) + 128;
+  auto kern = k_dht_rows_pipe<M, R, ADD, NB>;
+  int bpsm = 0;
+  int rc = prepare_kernel(H, kern, smem, 256, &bpsm);
+  if (rc) return rc;
+  const int ntiles = (nrows + lpc - 1) / lpc;
+  const int grid = std::min(ntiles, bpsm * H->num_sms);
+  return launch_named(H, name, [&]() -> int {
+    kern<<<grid, 256, smem, H->stream>>>(in, out, p, cmean, H->ny, nrows, lpc, table<R>(H, 0), H->derr, skip);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+template <typename R, bool ADD>
+int launch_rows_pipe(cup_handle* H, const char* name, const R* in, R* out, double* p, const double* cmean,
+                     const int* skip) {
+  switch (H->nx / 2) {
+    case 8: return launch_rows_pipe_M<8, R, ADD>(H, name, in, out, p, cmean, skip);
+    case 16: return launch_rows_pipe_M<16, R, ADD>(H, name, in, out, p, cmean, skip);
+    case 32: return launch_rows_pipe_M<32, R, ADD>(H, name, in, out, p, cmean, skip);
+    case 64: return launch_rows_pipe_M<64, R, ADD>(H, name, in, out, p, cmean, skip);
+    case 128: return launch_rows_pipe_M<128, R, ADD>(H, name, in, out, p, cmean, skip);
+    case 256: return launch_rows_pipe_M<256, R, ADD>(H, name, in, out, p, cmean, skip);
+  }
+  return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
+}
+
 // number of CTAs of a rows pass (= partials written by a reducing producer)
 int rows_grid(const cup_handle* H) {
   const int TPL = std::max(1, H->nx / 16);
@@ -662,7 +688,9 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   const int ntiles = ntx * (AXIS == 1 ? H->nz : H->ny);
   const int grid = std::min(ntiles, bpsm * H->num_sms);
   SpectralParams sp{H->cosx, H->cosy, H->cosz, H->norm_factor, H->nx, H->ny, H->nz};
-  const char* name = AXIS == 1 ? "dht_y" : (sizeof(RIN) < sizeof(R) ? "dht_z_solve_mixed" : "dht_z_solve");
+  const bool inv64 = H->fp32 && sizeof(R) == 8;  // FP64 inverse pass of a mixed-precision correction solve
+  const char* name = AXIS == 1 ? (inv64 ? "dht_y_f64" : "dht_y")
+                               : (sizeof(RIN) < sizeof(R) ? "dht_z_solve_mixed" : "dht_z_solve");
   return launch_named(H, name, [&]() -> int {
     kern<<<grid, threads, smem, H->stream>>>(map_in, map_out, ntx, ntiles, table<R>(H, AXIS), sp, H->derr, skip);
     CKL();
@@ -705,8 +733,7 @@ int fft_middle(cup_handle* H, R* work, const int* skip) {
 // by about 1e-7 whatever its spectrum.
 int dc_correction_solve(cup_handle* H, double* p, const int* skip) {
   int rc;
-  if ((rc = launch_rows<float>(H, "dht_x", RowsFromArray<float>{H->work32}, RowsToArray<float>{H->work32}, skip)))
-    return rc;
+  if ((rc = launch_rows_pipe<float, false>(H, "dht_x", H->work32, H->work32, nullptr, nullptr, skip))) return rc;
   if ((rc = launch_cols<float, 1, false>(H, H->work32, H->work32, skip))) return rc;
   if ((rc = launch_cols<double, 2, true, float>(H, H->work32, H->work64, skip))) return rc;
   if ((rc = launch_cols<double, 1, false>(H, H->work64, H->work64, skip))) return rc;
@@ -719,10 +746,9 @@ int dc_correction_solve(cup_handle* H, double* p, const int* skip) {
 template <typename R>
 int fft_poisson(cup_handle* H, R* work, R* out, const int* skip = nullptr) {
   int rc;
-  if ((rc = launch_rows<R>(H, "dht_x", RowsFromArray<R>{work}, RowsToArray<R>{work}, skip))) return rc;
+  if ((rc = launch_rows_pipe<R, false>(H, "dht_x", work, work, nullptr, nullptr, skip))) return rc;
   if ((rc = fft_middle<R>(H, work, skip))) return rc;
-  if ((rc = launch_rows<R>(H, "dht_x", RowsFromArray<R>{work}, RowsToArray<R>{out}, skip))) return rc;
-  return CUP_OK;
+  return launch_rows_pipe<R, false>(H, "dht_x", work, out, nullptr, nullptr, skip);
 }
 
 int box_grid(const Box& b) {
@@ -909,16 +935,15 @@ int dc_min_iter(const cup_handle* H) {
 // Launches one k_pres_zq pass; returns the grid size (number of partials).
 template <typename T, int MODE, int TY, int NS, int CPT>
 int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
-               int* grid_out, const int* skip, int pred_order = 0, double* pred_out = nullptr) {
+               int* grid_out, const int* skip, int pred_order = -1, double* pred_out = nullptr,
+               void* const* out = nullptr) {
   const int cells = TY * H->nx;
   if (cells % CPT || cells / CPT > 512 || H->ny % TY)
     return fail(H, CUP_ERR_ARG, "pressure tile does not fit the grid");
   PzqMaps maps;
   int rc = make_map(H, &maps.p_main, pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), H->nx, TY, 1);
   if (!rc) rc = make_map(H, &maps.p_halo, pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), H->nx, 2, 1);
-  if (!rc) rc = make_map(H, &maps.h_main[0], pred_order >= 1 ? H->p : pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-                         sizeof(double), H->nx, TY, 1);
-  if (!rc) rc = make_map(H, &maps.h_main[1], pred_order >= 2 ? H->p_old : pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+  if (!rc) rc = make_map(H, &maps.h_main, pred_order >= 1 ? H->p : pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                          sizeof(double), H->nx, TY, 1);
   if (!rc) rc = make_map(H, &maps.b_main, H->rhs, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), H->nx, TY, 1);
   const void* f[3] = {H->u, H->v, H->w};
@@ -933,11 +958,15 @@ int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, co
   int bpsm = 0;
   if ((rc = prepare_kernel(H, kern, smem, threads, &bpsm))) return rc;
   const int grid = std::min(geo.n_items, bpsm * H->num_sms);
-  if (grid > kPartialCap / 18) return fail(H, CUP_ERR_ARG, "too many CTAs for the partial buffers");
+  if (grid > kPartialCap / pzq_partials_per_cta<MODE>())
+    return fail(H, CUP_ERR_ARG, "too many CTAs for the partial buffers");
   PzqParams prm{dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, pred_order, pred_out};
+  T* o[3] = {nullptr, nullptr, nullptr};
+  if (out)
+    for (int q = 0; q < 3; ++q) o[q] = (T*)out[q];
   rc = launch_named(H, name, [&]() -> int {
-    kern<<<grid, threads, smem, H->stream>>>(maps, geo, (T*)H->u, (T*)H->v, (T*)H->w, H->rhs, H->work32, partials,
-                                             rmean, prm, H->derr, skip);
+    kern<<<grid, threads, smem, H->stream>>>(maps, geo, o[0], o[1], o[2], H->rhs, H->work32, partials, rmean, prm,
+                                             H->derr, skip);
     CKL();
     return CUP_OK;
   });
@@ -946,22 +975,28 @@ int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, co
   return CUP_OK;
 }
 
-int launch_finalize_residual(cup_handle* H, int grid, int k) {
+int launch_finalize_residual(cup_handle* H, const double* partials, int stride, int grid, int k) {
   const double inv_class = 8.0 / (double)H->n;
   return launch_named(H, "finalize_residual", [&]() -> int {
-    k_finalize_residual<<<1, 256, 0, H->stream>>>(partial(H, P_RES), grid, H->dstate, dc_tol(H), k, dc_min_iter(H),
+    k_finalize_residual<<<1, 256, 0, H->stream>>>(partials, stride, grid, H->dstate, dc_tol(H), k, dc_min_iter(H),
                                                   dc_max_iter(H), inv_class);
     CKL();
     return CUP_OK;
   });
 }
 
-// FP32 defect-correction pressure stage without obstacle, in z-queue passes:
-//   RHS + first residual (warm start p) -> [FP32 solve, residual check] ...
-//   -> last FP32 solve -> gradient correction + final residual check.
-// A check that meets the tolerance (after at least dc_min_iter solves) turns
-// every later solve and check into an exit at entry; the gradient pass always
-// runs and its check decides when no earlier one did.
+// FP32 defect-correction pressure stage without obstacle, in z-queue passes.
+// Check k measures the FP64 residual of p after k correction solves; from
+// k = 1 on the check is fused with the gradient correction, which writes
+// u = u* - dt grad p to the spare velocity buffer, so the usual step (one
+// solve meets the tolerance) is
+//   RHS + check 0 (warm start p) -> FP32 solve -> gradient + check 1.
+// When check k misses the tolerance, a residual pass writes the FP32 residual
+// again, solve k + 1 refines p and the gradient pass runs again from u* (still
+// intact). A check that meets the tolerance (after at least dc_min_iter
+// solves) turns every later kernel of the loop into an exit at entry, so the
+// loop needs no host round trip. Only the first gradient pass writes the next
+// step's warm start.
 template <typename T>
 int do_pressure_dc_zq(cup_handle* H, DtArg dt) {
   const int max_iter = dc_max_iter(H);
@@ -971,26 +1006,34 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt) {
   int rc, grid = 0;
   if ((rc = launch_pzq<T, PZQ_RHS_RES, 4, 4, 2>(H, "rhs_residual", W, partial(H, P_RES), nullptr, dt, &grid, nullptr)))
     return rc;
-  if ((rc = launch_finalize_residual(H, grid, 0))) return rc;
+  if ((rc = launch_finalize_residual(H, partial(H, P_RES), 18, grid, 0))) return rc;
+  const int order = std::min(H->p_valid, 1);  // valid levels among (p) before this step
+  void* unew[3] = {H->tu, H->tv, H->tw};      // u^n is dead after the advection stages
+  constexpr int kGradStride = pzq_partials_per_cta<PZQ_GRAD_CHECK>();
   for (int k = 1; k <= max_iter; ++k) {
+    if (k > 1) {
+      if ((rc = launch_pzq<T, PZQ_RES, 4, 4, 2>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid,
+                                                conv)))
+        return rc;
+    }
     if ((rc = dc_correction_solve(H, W, conv))) return rc;
-    if (k == max_iter) break;
-    if ((rc = launch_pzq<T, PZQ_RES, 4, 4, 2>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid,
-                                              conv)))
+    if ((rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 3, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
+                                                     &H->n_grad_partials, k > 1 ? conv : nullptr,
+                                                     k == 1 ? order : -1, H->p_old, unew)))
       return rc;
-    if ((rc = launch_finalize_residual(H, grid, k))) return rc;
+    if ((rc = launch_finalize_residual(H, partial(H, P_GRAD), kGradStride, H->n_grad_partials, k))) return rc;
   }
-  // gradient correction + final check + next warm start (over p_old, point-wise)
-  const int order = H->p_valid;  // valid levels among (p, p_old) before this step
-  if ((rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 3, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
-                                                   &H->n_grad_partials, nullptr, order, H->p_old)))
-    return rc;
-  H->grad_stride = 4;
+  H->grad_stride = kGradStride;
+  H->grad_max_off = 18;
+  H->grad_ke_off = 19;
+  std::swap(H->u, H->tu);
+  std::swap(H->v, H->tv);
+  std::swap(H->w, H->tw);
   double* next_pred = H->p_old;
   H->p_old = H->p;
   H->p = W;
   H->p_pred = next_pred;
-  H->p_valid = std::min(order + 1, 2);
+  H->p_valid = std::min(order + 1, 1);
   H->pred_ready = true;
   return CUP_OK;
 }
@@ -1015,7 +1058,7 @@ int do_poisson_dc(cup_handle* H) {
     if ((rc = launch_stream<double, 1, 2, 4, 6>(H, "dc_residual", pf, op, &grid, k > 0 ? conv : nullptr))) return rc;
     {
       int rc_ = launch_named(H, "finalize_residual", [&]() -> int {
-        k_finalize_residual<<<1, 256, 0, H->stream>>>(partial(H, P_RES), grid, H->dstate, tol, k, min_iter, max_iter,
+        k_finalize_residual<<<1, 256, 0, H->stream>>>(partial(H, P_RES), 18, grid, H->dstate, tol, k, min_iter, max_iter,
                                                       inv_class);
         CKL();
         return CUP_OK;
@@ -1035,7 +1078,7 @@ int do_poisson_fused_fp64(cup_handle* H, DtArg dt) {
   RowsRhs<T> prod{(const T*)H->u, (const T*)H->v, (const T*)H->w, dt, H->h, H->nx, H->ny, H->nz};
   if ((rc = launch_rows<double>(H, "rhs_dht_x", prod, RowsToArray<double>{H->rhs}, nullptr))) return rc;
   if ((rc = fft_middle<double>(H, H->rhs, nullptr))) return rc;
-  return launch_rows<double>(H, "dht_x", RowsFromArray<double>{H->rhs}, RowsToArray<double>{H->p}, nullptr);
+  return launch_rows_pipe<double, false>(H, "dht_x", H->rhs, H->p, nullptr, nullptr, nullptr);
 }
 
 // Poisson solve of the RHS array (operator-by-operator path, obstacles).
@@ -1051,6 +1094,8 @@ int do_grad(cup_handle* H, DtArg dt) {
                 dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, H->box, H->has_sphere ? 1 : 0, H->nx, H->ny, H->nz};
   // p is FP64 in both forms: the stream runs over an FP64 field.
   H->grad_stride = 2;
+  H->grad_max_off = 0;
+  H->grad_ke_off = 1;
   return launch_stream<double, 1, 1, 4, 4>(H, "grad_p", pf, op, &H->n_grad_partials);
 }
 
@@ -1124,8 +1169,8 @@ int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance) {
   {
     int rc_ = launch_named(H, "finalize_step", [&]() -> int {
       k_finalize_step<<<1, 256, 0, H->stream>>>(partial(H, P_GRAD), H->n_grad_partials, H->grad_stride,
-                                            partial(H, P_PEN), H->n_pen_partials, H->dstate, H->h * H->h * H->h,
-                                            advance, H->grad_stride == 4 ? 1 : 0, dc_tol(H), dc_max_iter(H));
+                                            H->grad_max_off, H->grad_ke_off, partial(H, P_PEN), H->n_pen_partials,
+                                            H->dstate, H->h * H->h * H->h, advance);
       CKL();
       return CUP_OK;
     });
@@ -1180,8 +1225,7 @@ int do_project_fields(cup_handle* H, void* const* in, void* const* out, double* 
   RowsRhs<T> prod{(const T*)in[0], (const T*)in[1], (const T*)in[2], dt, H->h, H->nx, H->ny, H->nz};
   if ((rc = launch_rows<double>(H, "adjoint_rhs_dht_x", prod, RowsToArray<double>{H->rhs}, nullptr))) return rc;
   if ((rc = fft_middle<double>(H, H->rhs, nullptr))) return rc;
-  if ((rc = launch_rows<double>(H, "adjoint_dht_x", RowsFromArray<double>{H->rhs}, RowsToArray<double>{pbuf}, nullptr)))
-    return rc;
+  if ((rc = launch_rows_pipe<double, false>(H, "adjoint_dht_x", H->rhs, pbuf, nullptr, nullptr, nullptr))) return rc;
   const void* pf[1] = {pbuf};
   OpGradP<T> op{(const T*)in[0], (const T*)in[1], (const T*)in[2], (T*)out[0], (T*)out[1], (T*)out[2],
                 partial(H, P_GRAD), dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, H->box, 0, H->nx, H->ny, H->nz};
@@ -2011,9 +2055,23 @@ int cup_profile_report(cup_handle* H, char* buf, size_t len, int reset) {
   std::string js = "{";
   bool first = true;
   for (const auto& kv : H->prof) {
-    char item[256];
-    snprintf(item, sizeof item, "%s\"%s\": {\"count\": %lld, \"ms\": %.6f}", first ? "" : ", ", kv.first.c_str(),
-             kv.second.first, kv.second.second);
+    // launches that did the pass's work: longer than a quarter of the longest
+    // (the later kernels of a converged defect-correction loop exit at entry)
+    double total = 0, tmax = 0, work = 0;
+    long long nwork = 0;
+    for (float d : kv.second) {
+      total += d;
+      tmax = std::max(tmax, (double)d);
+    }
+    for (float d : kv.second)
+      if (d >= 0.25 * tmax) {
+        work += d;
+        nwork += 1;
+      }
+    char item[320];
+    snprintf(item, sizeof item,
+             "%s\"%s\": {\"count\": %lld, \"ms\": %.6f, \"work_count\": %lld, \"work_ms\": %.6f}",
+             first ? "" : ", ", kv.first.c_str(), (long long)kv.second.size(), total, nwork, work);
     js += item;
     first = false;
   }

@@ -212,11 +212,22 @@ __device__ __forceinline__ void fft_stage(const In& in, const Out& out, const R2
   __syncthreads();
 }
 
+// No scaling after the forward transform.
+struct NoScale {
+  static constexpr bool kOn = false;
+  __device__ double operator()(int) const { return 1.0; }
+};
+
 // Even/odd split of the packed M-point FFT Z into the Hartley transform H of
 // the length-2M real line, in place (task k handles Z[k], Z[M-k] and writes
-// H[k], H[N-k], H[M-k], H[M+k]).
-template <int M, typename R, typename R2, class Acc>
-__device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int t, bool active) {
+// H[k], H[N-k], H[M-k], H[M+k]). With a scaler, the four outputs of task k are
+// multiplied by scale(k): for the wide Laplacian (eigenvalue a function of
+// cos(4 pi k / N), which has period N/2 and is even) the four indices k, N-k,
+// M-k, M+k share one eigenvalue, so the spectral divide costs one factor per
+// four values.
+template <int M, typename R, typename R2, class Acc, class Scale = NoScale>
+__device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int t, bool active,
+                                         const Scale& scale = Scale()) {
   constexpr int TPL = M / 8;
   constexpr int NT = (M / 2 + 1 + TPL - 1) / TPL;
   constexpr int N = 2 * M;
@@ -239,19 +250,33 @@ __device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int
       if (k > M / 2) continue;
       const R2 A = A_[i], B = B_[i];
       if (k == 0) {
-        a.str(l, 0, A.x + A.y);
-        a.str(l, M, A.x - A.y);
+        R h0 = A.x + A.y, hM = A.x - A.y;
+        if constexpr (Scale::kOn) {
+          const double f = scale(0);
+          h0 = (R)((double)h0 * f);
+          hM = (R)((double)hM * f);
+        }
+        a.str(l, 0, h0);
+        a.str(l, M, hM);
       } else {
         const R2 W = twp[k];
         const R half = (R)0.5;
         const R Er = (A.x + B.x) * half, Ei = (A.y - B.y) * half;
         const R Or = (A.y + B.y) * half, Oi = (B.x - A.x) * half;
         const R Xr = Er + (W.x * Or - W.y * Oi), Xi = Ei + (W.x * Oi + W.y * Or);
-        a.str(l, k, Xr - Xi);
-        a.str(l, N - k, Xr + Xi);
         const R X2r = Er - W.x * Or + W.y * Oi, X2i = -Ei + W.x * Oi + W.y * Or;
-        a.str(l, M - k, X2r - X2i);
-        a.str(l, M + k, X2r + X2i);
+        R hk = Xr - Xi, hNk = Xr + Xi, hMk = X2r - X2i, hMpk = X2r + X2i;
+        if constexpr (Scale::kOn) {
+          const double f = scale(k);
+          hk = (R)((double)hk * f);
+          hNk = (R)((double)hNk * f);
+          hMk = (R)((double)hMk * f);
+          hMpk = (R)((double)hMpk * f);
+        }
+        a.str(l, k, hk);
+        a.str(l, N - k, hNk);
+        a.str(l, M - k, hMk);
+        a.str(l, M + k, hMpk);
       }
     }
   }
@@ -260,9 +285,9 @@ __device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int
 
 // Full in-place Hartley transform of the lines of `a` (pad: scratch for the
 // first stage's output when USE_PAD). Thread `t` of line `l`, M/8 per line.
-template <int M, bool USE_PAD, typename R, class Acc, class P>
+template <int M, bool USE_PAD, typename R, class Acc, class P, class Scale = NoScale>
 __device__ __forceinline__ void dht_lines(const Acc& a, const P& pad, const typename Cplx<R>::T* tw, int l, int t,
-                                          bool active) {
+                                          bool active, const Scale& scale = Scale()) {
   using R2 = typename Cplx<R>::T;
   using Pl = FFTPlan<M>;
   if constexpr (Pl::nstages == 1) {
@@ -276,7 +301,7 @@ __device__ __forceinline__ void dht_lines(const Acc& a, const P& pad, const type
     fft_stage<M, Pl::radix(1), 8, true, R2>(a, a, tw + Pl::tw_off(1), l, t, active);
     if constexpr (Pl::nstages == 3) fft_stage<M, Pl::radix(2), 64, true, R2>(a, a, tw + Pl::tw_off(2), l, t, active);
   }
-  dht_post<M, R, R2>(a, tw + Pl::post_off(), l, t, active);
+  dht_post<M, R, R2>(a, tw + Pl::post_off(), l, t, active, scale);
 }
 
 template <typename R2>
@@ -408,6 +433,123 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
   if constexpr (!Prod::kBulk) prod.finish(acc, scratch);
 }
 
+// Pipelined x pass: persistent CTAs walk tiles of lpc consecutive rows
+// (tile i of a CTA: rows (blockIdx.x + i gridDim.x) lpc ...) through NB
+// shared-memory buffers. The 1-D bulk loads of the next NB-1 tiles and the
+// bulk store of the previous tile overlap the transform of the current one;
+// the twiddle table is loaded once per CTA.
+// ADD (last pass of a correction solve, R = double): the transformed rows are
+// added to p minus the parity-class means of p measured by the preceding
+// residual pass, p += rows - cmean; the p values of a tile are loaded into
+// registers before its transform (their latency hides behind it) and written
+// back with coalesced stores, so the tile needs no second buffer.
+template <int M, typename R, bool ADD, int NB>
+__global__ void __launch_bounds__(256, 2) k_dht_rows_pipe(const R* __restrict__ in, R* __restrict__ out,
+                                                       double* __restrict__ p, const double* __restrict__ cmean,
+                                                       int ny, int nrows, int lpc,
+                                                       const typename Cplx<R>::T* tw_g, int* err, const int* skip) {
+  using R2 = typename Cplx<R>::T;
+  static_assert(NB >= 2, "need at least two tile buffers");
+  static_assert(!ADD || sizeof(R) == sizeof(double), "p is FP64");
+  if (skip && *skip) return;
+  constexpr int N = 2 * M, TPL = M / 8;
+  constexpr int TL = FFTPlan<M>::table_len();
+  constexpr bool PAD = FFTPlan<M>::nstages > 1;
+  constexpr int PPITCH = 2 * (M + M / 8);
+  constexpr int EPT = 16;  // elements per thread of a full tile: lpc * N = (2048 / M) * 2M = 4096 over 256 threads
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw = smem_align128(smem_dyn);
+  R* bufs = reinterpret_cast<R*>(smem_raw);                 // NB * lpc * N
+  R* padb = bufs + (size_t)NB * lpc * N;                     // lpc * PPITCH
+  R2* tw = reinterpret_cast<R2*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
+  const int tid = threadIdx.x;
+  const int ntiles = (nrows + lpc - 1) / lpc;
+  const int my = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  if (tid == 0) {
+    for (int b = 0; b < NB; ++b) mbar_init(&bar[b], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto rows_of = [&](int i, int& row0, int& nr) {
+    row0 = (blockIdx.x + i * gridDim.x) * lpc;
+    nr = min(lpc, nrows - row0);
+  };
+  auto issue = [&](int i) {
+    int row0, nr;
+    rows_of(i, row0, nr);
+    const int b = i % NB;
+    const uint32_t bytes = (uint32_t)((size_t)nr * N * sizeof(R));
+    mbar_arrive_expect_tx(&bar[b], bytes);
+    bulk_load(bufs + (size_t)b * lpc * N, in + (size_t)row0 * N, bytes, &bar[b]);
+  };
+  int issued = 0;
+  if (tid == 0)
+    for (; issued < min(NB - 1, my); ++issued) issue(issued);
+  load_table(tw, tw_g, TL);
+  double cm[8];
+  if constexpr (ADD) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) cm[c] = cmean[c];
+  }
+  __syncthreads();
+  const int l = tid / TPL, t = tid % TPL;
+  RowLinesPad<R> P{padb, PPITCH};
+  bool ok = true;
+  int done = 0;
+  for (int i = 0; i < my; ++i) {
+    // refill: tile i + NB - 1 goes into the buffer of tile i - 1, once its
+    // store has read it (ADD: once every thread is past its add loop)
+    if (tid == 0 && ok && issued < my) {
+      if constexpr (!ADD) bulk_wait_read<0>();
+      issue(issued++);
+    }
+    int row0, nr;
+    rows_of(i, row0, nr);
+    double pv[ADD ? EPT : 1];
+    if constexpr (ADD) {
+#pragma unroll
+      for (int k = 0; k < EPT; ++k) {
+        const int e = tid + k * 256;
+        pv[k] = e < nr * N ? p[(size_t)row0 * N + e] : 0.0;
+      }
+    }
+    const int b = i % NB;
+    ok = __syncthreads_and(ok && mbar_wait(&bar[b], (i / NB) & 1, err));
+    if (!ok) break;
+    R* rows = bufs + (size_t)b * lpc * N;
+    RowLines<R> A{rows, N};
+    dht_lines<M, PAD, R>(A, P, tw, l, t, l < nr);
+    if constexpr (ADD) {
+#pragma unroll
+      for (int k = 0; k < EPT; ++k) {
+        const int e = tid + k * 256;
+        if (e < nr * N) {
+          const int rl = e / N, x = e - rl * N;
+          const int r = row0 + rl, y = r % ny, z = r / ny;
+          const int cls = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
+          p[(size_t)row0 * N + e] = pv[k] + (double)rows[e] - cm[cls];
+        }
+      }
+      __syncthreads();
+    } else {
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        bulk_store(out + (size_t)row0 * N, rows, (uint32_t)((size_t)nr * N * sizeof(R)));
+        bulk_commit();
+      }
+    }
+    done = i + 1;
+  }
+  if (tid == 0) {
+    bulk_wait_all();
+    // after a timed-out wait: bounded drain of the loads still in flight
+    if (!ok)
+      for (int r = done; r < issued; ++r) mbar_wait(&bar[r % NB], (r / NB) & 1, nullptr);
+  }
+}
+
 // Spectral factor of PoissonSolverPeriodic::_solve (grid-consistent branch,
 // source/poisson/PoissonSolverPeriodic.cpp:23-61): cx/cy/cz hold
 // cos(4 pi k / N) evaluated on the host exactly as the reference does.
@@ -419,66 +561,29 @@ struct SpectralParams {
   int nx, ny, nz;
 };
 
-__device__ __forceinline__ double spectral_factor(const SpectralParams& sp, int kx, int ky, int kz) {
-  const bool null_mode = (kx == 0 || kx == sp.nx / 2) && (ky == 0 || ky == sp.ny / 2) && (kz == 0 || kz == sp.nz / 2);
-  if (null_mode) return 0.0;
-  const double D = sp.cx[kx] + sp.cy[ky] + sp.cz[kz];
-  return sp.norm_factor / (2 * D - 6);
-}
+// Scaler of the z pass: the factor of column (kx, ky) at z index k,
+// nf / (2 (cos_x + cos_y + cos_z) - 6), zero on the 8 null modes (kx in
+// {0, Nx/2}, ky in {0, Ny/2}, kz in {0, Nz/2}); the z indices 0 and Nz/2 are
+// both handled by task k = 0.
+struct ZColumnFactor {
+  double cxy;  // cos_x[kx] + cos_y[ky]
+  const double* cz;
+  double nf;
+  bool null_col;
+  static constexpr bool kOn = true;
+  __device__ __forceinline__ double operator()(int k) const {
+    if (k == 0 && null_col) return 0.0;
+    return nf / (2 * (cxy + __ldg(cz + k)) - 6);
+  }
+};
 
-// y / z pass: a tile of W consecutive x columns by the whole line length,
-// moved with TMA tiled loads/stores. AXIS 1: box {W, Ny, 1} at (x0, 0, z);
-// AXIS 2: box {W, 1, Nz} at (x0, y, 0). With DIVIDE (z pass only) the tile is
-// transformed, multiplied by the spectral factor and transformed back.
-template <int M, typename R, int AXIS, bool DIVIDE>
-__global__ void __launch_bounds__(256) k_dht_cols(const __grid_constant__ CUtensorMap map_in,
-                                                  const __grid_constant__ CUtensorMap map_out, int W, int ntiles_x,
-                                                  const typename Cplx<R>::T* tw_g, SpectralParams sp, int* err,
-                                                  const int* skip) {
-  using R2 = typename Cplx<R>::T;
-  if (skip && *skip) return;
-  constexpr int N = 2 * M, TPL = M / 8;
-  constexpr int TL = FFTPlan<M>::table_len();
-  extern __shared__ __align__(128) unsigned char smem_dyn[];
-  unsigned char* smem_raw = smem_align128(smem_dyn);
-  R* tile = reinterpret_cast<R*>(smem_raw);  // [N][W]
-  R2* tw = reinterpret_cast<R2*>(tile + (size_t)N * W);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
-  const int x0 = (blockIdx.x % ntiles_x) * W;
-  const int other = blockIdx.x / ntiles_x;  // z for AXIS 1, y for AXIS 2
-  const int c1 = AXIS == 1 ? 0 : other, c2 = AXIS == 1 ? other : 0;
-  // the barrier must be initialised before any thread waits on it
-  if (threadIdx.x == 0) {
-    mbar_init(bar, 1);
-    mbar_fence_init();
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    mbar_arrive_expect_tx(bar, (uint32_t)((size_t)N * W * sizeof(R)));
-    tma_load_3d(tile, &map_in, x0, c1, c2, bar);
-  }
-  load_table(tw, tw_g, TL);
-  const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
-  if (!ok) return;
-  const int l = threadIdx.x % W, t = threadIdx.x / W;
-  const bool active = t < TPL;
-  ColLines<R> A{tile, W};
-  dht_lines<M, false, R>(A, A, tw, l, t, active);
-  if constexpr (DIVIDE) {
-    for (int i = threadIdx.x; i < N * W; i += blockDim.x) {
-      const int n = i / W, w = i - n * W;
-      tile[i] = (R)((double)tile[i] * spectral_factor(sp, x0 + w, other, n));
-    }
-    __syncthreads();
-    dht_lines<M, false, R>(A, A, tw, l, t, active);
-  }
-  fence_proxy_async_smem();
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    tma_store_3d(&map_out, x0, c1, c2, tile);
-    bulk_commit();
-    bulk_wait_all();
-  }
+__device__ __forceinline__ ZColumnFactor z_column_factor(const SpectralParams& sp, int kx, int ky) {
+  ZColumnFactor f;
+  f.cxy = __ldg(sp.cx + kx) + __ldg(sp.cy + ky);
+  f.cz = sp.cz;
+  f.nf = sp.norm_factor;
+  f.null_col = (kx == 0 || kx == sp.nx / 2) && (ky == 0 || ky == sp.ny / 2);
+  return f;
 }
 
 // Pipelined y / z pass: persistent CTAs walk the tiles (W consecutive x
@@ -572,13 +677,11 @@ __global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_cons
       __syncthreads();
     }
     ColLines<R> A{tile, W};
-    dht_lines<M, false, R>(A, A, tw, l, t, active);
     if constexpr (DIVIDE) {
-      for (int k = tid; k < N * W; k += blockDim.x) {
-        const int n = k / W, w = k - n * W;
-        tile[k] = (R)((double)tile[k] * spectral_factor(sp, x0 + w, other, n));
-      }
-      __syncthreads();
+      // forward, spectral divide fused into the even/odd split, inverse
+      dht_lines<M, false, R>(A, A, tw, l, t, active, z_column_factor(sp, x0 + l, other));
+      dht_lines<M, false, R>(A, A, tw, l, t, active);
+    } else {
       dht_lines<M, false, R>(A, A, tw, l, t, active);
     }
     fence_proxy_async_smem();

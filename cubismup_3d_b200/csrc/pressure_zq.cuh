@@ -3,24 +3,33 @@
 //   RHS_RES    b = KernelPressureRHS(u*) (source/operators/PressureRHS.cpp:51-76)
 //              and the first FP64 residual r = b - h/4 L_2h p of the warm start,
 //              in one pass: b to HBM in FP64, r in FP32 for the FFT solve.
-//   RES        r = b - h/4 L_2h p between correction solves.
+//   RES        r = b - h/4 L_2h p before a further correction solve, minus the
+//              class means of b (its null-mode part), in FP32.
 //   GRAD_CHECK KernelGradP (source/operators/PressureProjection.cpp:38-50) on
-//              u* with the final p, fused with the final FP64 residual check
-//              (the divergence left by the projection is this residual) and
-//              with the warm start of the next step's solve: the polynomial
-//              extrapolation of p over the last three steps.
+//              u* with the current p, written to a separate buffer so that it
+//              can be redone, fused with the residual check of that p (the
+//              divergence left by the projection is this residual) and, on
+//              the first check of a step, with the warm start of the next
+//              step's solve: the linear extrapolation 2 p_{n+1} - p_n. (The
+//              unpredictable part of b is the white FP32 rounding noise of the
+//              stored velocity; a quadratic extrapolation amplifies it more
+//              than it gains on the smooth part.)
 // L_2h is the wide-stencil Laplacian (neighbours at +-2) the spectral solve
-// inverts; p is FP64 throughout.
+// inverts; p is FP64 throughout. (Storing b costs 16 B/cell against
+// recomputing it from u* in every pass, but the gradient pass is
+// instruction-bound and measured faster reading b.)
 //
 // Structure as k_advect_zq: each thread owns CPT (x, y) columns of a TY x nx
 // row tile and marches down z; planes of p (TY + 4 rows: the +-2 halo in y)
 // arrive by TMA into a ring of NS slots, the centre values of the last 5
 // planes sit in a register queue (the z stencil), the x/y part of each plane
 // is computed on arrival and completed two planes later. The point-wise fields
-// of an output plane (b, u*) ride in the slot of the load that completes it.
-// Partial sums per CTA: RHS_RES and RES write the 18-value residual layout
-// (sum r^2, sum b^2, parity-class sums of p and of r); GRAD_CHECK writes
-// (max |u + uinf|, kinetic energy, sum of the null-free r^2, 0).
+// of an output plane (b, u*, the previous p) ride in the slot of the load that
+// completes it.
+// Partial sums per CTA: the 18-value residual layout (sum r^2 with the null
+// parts removed after check 0, sum b^2 and the class sums of r at check 0,
+// class sums of p); GRAD_CHECK then adds max |u + uinf| and the kinetic
+// energy: 20 per CTA.
 #pragma once
 
 #include "common.cuh"
@@ -33,18 +42,25 @@ enum { PZQ_RHS_RES = 0, PZQ_RES = 1, PZQ_GRAD_CHECK = 2 };
 
 struct PzqMaps {
   CUtensorMap p_main, p_halo;  // FP64 p: box {nx, TY, 1} and {nx, 2, 1}
-  CUtensorMap f_main[3];       // u, v, w (storage type): box {nx, TY, 1}
-  CUtensorMap v_halo;          // v: box {nx, 1, 1} (RHS_RES)
+  CUtensorMap f_main[3];       // u*, v*, w* (storage type): box {nx, TY, 1}
+  CUtensorMap v_halo;          // v*: box {nx, 1, 1} (RHS_RES)
   CUtensorMap b_main;          // FP64 b: box {nx, TY, 1} (RES, GRAD_CHECK)
-  CUtensorMap h_main[2];       // FP64 pressure history p_n, p_{n-1}: box {nx, TY, 1} (GRAD_CHECK)
+  CUtensorMap h_main;          // FP64 pressure of the previous step p_n: box {nx, TY, 1} (GRAD_CHECK)
 };
+
+// Values per CTA in the partial-sum buffer.
+template <int MODE>
+constexpr int pzq_partials_per_cta() {
+  return MODE == 2 ? 20 : 18;
+}
 
 struct PzqParams {
   DtArg dt;
   double h;
   double uinf[3];
-  // GRAD_CHECK: extrapolation order (0, 1, 2) of the next step's warm start
-  // from the final p and the history (p_n, p_{n-1}); written over p_{n-1}
+  // GRAD_CHECK: extrapolation order of the next step's warm start from the
+  // current p and the previous step's p_n (0: p, 1: 2 p - p_n; negative: the
+  // warm start is not written)
   int pred_order;
   double* pred_out;
 };
@@ -63,12 +79,12 @@ struct PzqSlot {
   __host__ __device__ static size_t f_off(int nx, int f) {
     return b_off(nx) + (size_t)TY * nx * sizeof(double) + (size_t)f * TY * nx * sizeof(T);
   }
-  // GRAD_CHECK: then the history rows p_n, p_{n-1} [TY] of double
-  __host__ __device__ static size_t h_off(int nx, int i) { return f_off(nx, 3) + (size_t)i * TY * nx * sizeof(double); }
+  // GRAD_CHECK: then the rows of the previous step's p [TY] of double
+  __host__ __device__ static size_t h_off(int nx) { return f_off(nx, 3); }
   __host__ __device__ static size_t bytes(int nx) {
     size_t s = MODE == PZQ_RHS_RES ? w_off(nx) + (size_t)TY * nx * sizeof(T)
                : MODE == PZQ_RES   ? b_off(nx) + (size_t)TY * nx * sizeof(double)
-                                   : h_off(nx, 2);
+                                   : h_off(nx) + (size_t)TY * nx * sizeof(double);
     return (s + 127) / 128 * 128;
   }
 };
@@ -134,7 +150,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     } else if constexpr (MODE == PZQ_RES) {
       if (out_plane) bytes += rowsD;
     } else {
-      if (out_plane) bytes += rowsD + 3 * rowsT + (prm.pred_order >= 1 ? rowsD : 0u) + (prm.pred_order >= 2 ? rowsD : 0u);
+      if (out_plane) bytes += rowsD + 3 * rowsT + (prm.pred_order >= 1 ? rowsD : 0u);
     }
     mbar_arrive_expect_tx(&full[s], bytes);
     double* P = reinterpret_cast<double*>(dst);
@@ -157,8 +173,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
         if constexpr (MODE == PZQ_GRAD_CHECK) {
 #pragma unroll
           for (int f = 0; f < 3; ++f) tma_load_3d(dst + Slot::f_off(nx, f), &maps.f_main[f], 0, y0, zk, &full[s]);
-          if (prm.pred_order >= 1) tma_load_3d(dst + Slot::h_off(nx, 0), &maps.h_main[0], 0, y0, zk, &full[s]);
-          if (prm.pred_order >= 2) tma_load_3d(dst + Slot::h_off(nx, 1), &maps.h_main[1], 0, y0, zk, &full[s]);
+          if (prm.pred_order >= 1) tma_load_3d(dst + Slot::h_off(nx), &maps.h_main, 0, y0, zk, &full[s]);
         }
       }
     }
@@ -169,13 +184,25 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     for (; q_issued < min(L, NS); ++q_issued) issue(q_issued);
 
   const int mask = nx - 1;
+  // per column: its cell, the shared-memory offsets of its x/y neighbours in
+  // a slot, and (after check 0) the class means of b at both z parities
   int cx[CPT], cy[CPT];
+  int xm1[CPT], xp1[CPT], xm2[CPT], xp2[CPT];
+  double rm[CPT][2];
 #pragma unroll
   for (int i = 0; i < CPT; ++i) {
     const int c = tid + i * blockDim.x;
     cx[i] = c & mask;
     cy[i] = c >> g.log2nx;
+    xm1[i] = (cx[i] - 1) & mask;
+    xp1[i] = (cx[i] + 1) & mask;
+    xm2[i] = (cx[i] - 2) & mask;
+    xp2[i] = (cx[i] + 2) & mask;
+#pragma unroll
+    for (int zp = 0; zp < 2; ++zp)
+      rm[i][zp] = MODE == PZQ_RHS_RES ? 0.0 : rmean[(cx[i] & 1) | ((cy[i] & 1) << 1) | (zp << 2)];
   }
+  const size_t plane = (size_t)nx * ny;
   const double dtv = prm.dt.get();
   const double h = prm.h;
   const double cL = 0.25 * h;           // h^3 / (4 h^2)
@@ -184,9 +211,21 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
 
   double pq[Q][CPT];
   T wq[Q][CPT];
-  double partL[G][CPT], partA[G][CPT], partB[G][CPT];
+  // x/y parts of the planes in flight (G of them): Laplacian, divergence and
+  // (GRAD_CHECK) the gradient of p and the u*, v* centre values
+  double partL[G][CPT], partB[G][CPT];  // partB: divergence (RHS_RES) or y-gradient (GRAD_CHECK)
+  double gA[G][CPT];                     // x-gradient (GRAD_CHECK)
   double pc[CPT][2], rc[CPT][2];  // parity-class sums of p and r by z parity
-  double acc0 = 0, acc1 = 0, accM = 0;
+  double acc0 = 0, acc1 = 0;
+  // extremes of each corrected velocity component: max |u + uinf| over the
+  // cells is max(|umax + uinf|, |umin + uinf|), so the FP64 max needs no
+  // per-cell conversion
+  T vmax[3], vmin[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    vmax[c] = (T)-INFINITY;
+    vmin[c] = (T)INFINITY;
+  }
 #pragma unroll
   for (int d = 0; d < Q; ++d)
 #pragma unroll
@@ -197,7 +236,9 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
 #pragma unroll
   for (int d = 0; d < G; ++d)
 #pragma unroll
-    for (int i = 0; i < CPT; ++i) partL[d][i] = partA[d][i] = partB[d][i] = 0.0;
+    for (int i = 0; i < CPT; ++i) {
+      partL[d][i] = partB[d][i] = gA[d][i] = 0.0;
+    }
 #pragma unroll
   for (int i = 0; i < CPT; ++i) pc[i][0] = pc[i][1] = rc[i][0] = rc[i][1] = 0.0;
 
@@ -207,6 +248,9 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     const int item = blockIdx.x + it * gridDim.x;
     const int ty = item % g.items_y, zi = item / g.items_y;
     const int y0 = ty * TY, z0 = zi * g.zc;
+    size_t obase[CPT];  // output index of plane z0
+#pragma unroll
+    for (int i = 0; i < CPT; ++i) obase[i] = gidx(cx[i], y0 + cy[i], z0, nx, ny);
     for (int j0 = 0; j0 < PL; j0 += U) {
 #pragma unroll
       for (int jj = 0; jj < U; ++jj) {
@@ -236,52 +280,48 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
             const int zp = jj & 1;
 #pragma unroll
             for (int i = 0; i < CPT; ++i) {
-              const size_t o = gidx(cx[i], y0 + cy[i], z0 + k, nx, ny);
-              const int cls = (cx[i] & 1) | ((cy[i] & 1) << 1) | (zp << 2);
+              const size_t o = obase[i] + (size_t)k * plane;
+              const int c = cy[i] * nx + cx[i];
               const double p0 = pq[QC][i];
               const double lap = partL[PS][i] + (pq[QP2][i] + pq[QM2][i] - 2 * p0);
+              pc[i][zp] += p0;
               if constexpr (MODE == PZQ_RHS_RES) {
                 const double b = partB[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
                 const double r = b - cL * lap;
+                rc[i][zp] += r;  // the class means of b (only check 0 needs them)
                 bout[o] = b;
                 rout[o] = (float)r;
                 acc0 += r * r;
                 acc1 += b * b;
-                pc[i][zp] += p0;
-                rc[i][zp] += r;
               } else {
-                const double* B = reinterpret_cast<const double*>(sl + Slot::b_off(nx));
-                const double b = B[cy[i] * nx + cx[i]];
+                const double b = reinterpret_cast<const double*>(sl + Slot::b_off(nx))[c];
                 const double r = b - cL * lap;
-                const double rp = rmean ? r - rmean[cls] : r;
+                const double rp = r - rm[i][zp];
                 acc0 += rp * rp;
                 if constexpr (MODE == PZQ_RES) {
                   rout[o] = (float)rp;
-                  acc1 += b * b;
-                  pc[i][zp] += p0;
-                  rc[i][zp] += r;
                 } else {
-                  const T* F0 = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 0));
-                  const T* F1 = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 1));
-                  const T* F2 = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 2));
-                  const int c = cy[i] * nx + cx[i];
-                  const T tu = (T)((double)F0[c] + facG * partA[PS][i]);
-                  const T tv = (T)((double)F1[c] + facG * partB[PS][i]);
-                  const T tw = (T)((double)F2[c] + facG * (pq[QP1][i] - pq[QM1][i]));
+                  // the FP64 correction rounded once to the storage type, then added
+                  const T tu = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 0))[c] + (T)(facG * gA[PS][i]);
+                  const T tv = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 1))[c] + (T)(facG * partB[PS][i]);
+                  const T tw = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 2))[c] +
+                               (T)(facG * (pq[QP1][i] - pq[QM1][i]));
                   ou[o] = tu;
                   ov[o] = tv;
                   ow[o] = tw;
-                  // warm start of the next step: polynomial extrapolation in the step index
-                  const double* Hn = reinterpret_cast<const double*>(sl + Slot::h_off(nx, 0));
-                  const double* Hm = reinterpret_cast<const double*>(sl + Slot::h_off(nx, 1));
-                  double pred = p0;
-                  if (prm.pred_order == 1) pred = 2 * p0 - Hn[c];
-                  else if (prm.pred_order == 2) pred = 3 * (p0 - Hn[c]) + Hm[c];
-                  prm.pred_out[o] = pred;
-                  const double m = fmax(fmax(fabs((double)tu + prm.uinf[0]), fabs((double)tv + prm.uinf[1])),
-                                        fabs((double)tw + prm.uinf[2]));
-                  accM = fmax(accM, m);
-                  acc1 += 0.5 * ((double)tu * tu + (double)tv * tv + (double)tw * tw);
+                  // warm start of the next step: linear extrapolation in the step index
+                  if (prm.pred_order >= 0) {
+                    const double* Hn = reinterpret_cast<const double*>(sl + Slot::h_off(nx));
+                    prm.pred_out[o] = prm.pred_order == 1 ? 2 * p0 - Hn[c] : p0;
+                  }
+                  vmax[0] = fmax(vmax[0], tu);
+                  vmin[0] = fmin(vmin[0], tu);
+                  vmax[1] = fmax(vmax[1], tv);
+                  vmin[1] = fmin(vmin[1], tv);
+                  vmax[2] = fmax(vmax[2], tw);
+                  vmin[2] = fmin(vmin[2], tw);
+                  // kinetic energy: squares in the storage type, FP64 sum
+                  acc1 += (double)(tu * tu + tv * tv + tw * tw);
                 }
               }
             }
@@ -291,19 +331,18 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
             const int PS = jj % G;
 #pragma unroll
             for (int i = 0; i < CPT; ++i) {
-              const int x = cx[i], r = G + cy[i];
+              const int x = cx[i];
               const double p0 = pq[QN][i];
-              const double* Pr = P + r * nx;
-              partL[PS][i] = (Pr[(x + 2) & mask] + Pr[(x - 2) & mask] - 2 * p0) +
-                             (P[(r + 2) * nx + x] + P[(r - 2) * nx + x] - 2 * p0);
+              const double* Pc = P + (G + cy[i]) * nx;  // this column's row of p
+              partL[PS][i] = (Pc[xp2[i]] + Pc[xm2[i]] - 2 * p0) + (Pc[2 * nx + x] + Pc[x - 2 * nx] - 2 * p0);
               if constexpr (MODE == PZQ_RHS_RES) {
-                const T* Ur = reinterpret_cast<const T*>(sl + Slot::u_off(nx)) + cy[i] * nx;
-                const T* V = reinterpret_cast<const T*>(sl + Slot::v_off(nx));
-                partB[PS][i] = facB * (((double)Ur[(x + 1) & mask] - (double)Ur[(x - 1) & mask]) +
-                                       ((double)V[(cy[i] + 2) * nx + x] - (double)V[cy[i] * nx + x]));
+                const T* Urow = reinterpret_cast<const T*>(sl + Slot::u_off(nx)) + cy[i] * nx;
+                const T* Vc = reinterpret_cast<const T*>(sl + Slot::v_off(nx)) + (cy[i] + 1) * nx;  // row of v*
+                partB[PS][i] = facB * (((double)Urow[xp1[i]] - (double)Urow[xm1[i]]) +
+                                       ((double)Vc[nx + x] - (double)Vc[x - nx]));
               } else if constexpr (MODE == PZQ_GRAD_CHECK) {
-                partA[PS][i] = Pr[(x + 1) & mask] - Pr[(x - 1) & mask];
-                partB[PS][i] = P[(r + 1) * nx + x] - P[(r - 1) * nx + x];
+                gA[PS][i] = Pc[xp1[i]] - Pc[xm1[i]];
+                partB[PS][i] = Pc[nx + x] - Pc[x - nx];
               }
             }
           }
@@ -318,23 +357,13 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     for (int r = q - NS < 0 ? 0 : q - NS; r < q_issued; ++r) mbar_wait(&full[r % NS], (r / NS) & 1, nullptr);
   }
   // per-CTA partial sums
-  if constexpr (MODE == PZQ_GRAD_CHECK) {
-    double mx[1] = {accM};
-    double sm[2] = {acc1, acc0};
-    block_reduce<1, true>(mx, scratch);
-    block_reduce<2, false>(sm, scratch + 32);
-    if (tid == 0) {
-      partials[4 * blockIdx.x + 0] = mx[0];
-      partials[4 * blockIdx.x + 1] = sm[0];
-      partials[4 * blockIdx.x + 2] = sm[1];
-      partials[4 * blockIdx.x + 3] = 0.0;
-    }
-  } else {
+  {
+    constexpr int NPV = pzq_partials_per_cta<MODE>();
     double v[18];
 #pragma unroll
     for (int k = 0; k < 18; ++k) v[k] = 0.0;
     v[0] = acc0;
-    v[1] = acc1;
+    v[1] = MODE == PZQ_GRAD_CHECK ? 0.0 : acc1;
 #pragma unroll
     for (int i = 0; i < CPT; ++i)
 #pragma unroll
@@ -347,8 +376,24 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
         }
       }
     block_reduce<18, false>(v, scratch);
+    if constexpr (MODE == PZQ_GRAD_CHECK) {
+      double accM = 0.0;
+      if (vmax[0] >= vmin[0]) {  // this thread corrected at least one cell
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          accM = fmax(accM, fmax(fabs((double)vmax[c] + prm.uinf[c]), fabs((double)vmin[c] + prm.uinf[c])));
+      }
+      double mx[1] = {accM};
+      double ke[1] = {acc1};
+      block_reduce<1, true>(mx, scratch);
+      block_reduce<1, false>(ke, scratch + 32);
+      if (tid == 0) {
+        partials[NPV * blockIdx.x + 18] = mx[0];
+        partials[NPV * blockIdx.x + 19] = ke[0];
+      }
+    }
     if (tid == 0)
-      for (int k = 0; k < 18; ++k) partials[18 * blockIdx.x + k] = v[k];
+      for (int k = 0; k < 18; ++k) partials[NPV * blockIdx.x + k] = v[k];
   }
 }
 

@@ -219,7 +219,10 @@ int cup_dc_history(struct cup_handle* h, double* out, int n, int* n_checks);
  * as CUDA-event ranges per kernel) ---- */
 /* Turns per-kernel CUDA-event timing on or off (off by default; no host sync while on). */
 int cup_profile_enable(struct cup_handle* h, int on);
-/* Writes {"kernel": {"count": n, "ms": total}, ...} as JSON into buf; reset != 0 clears the totals. */
+/* Writes {"kernel": {"count": n, "ms": total, "work_count": m, "work_ms": t}, ...} as JSON into buf:
+ * all launches, and those that did the pass's work (at least a quarter of the
+ * longest launch of that kernel; the kernels of a converged defect-correction
+ * loop's later solves exit at entry). reset != 0 clears the records. */
 int cup_profile_report(struct cup_handle* h, char* buf, size_t len, int reset);
 /* Number of kernels this handle has launched so far. */
 int cup_launch_count(const struct cup_handle* h, long long* n);
