@@ -278,8 +278,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
             torch.distributed.barrier()
 
     # warm-up (also builds the per-kernel launch configuration caches)
+    st_w = None
     for _ in range(args.warmup):
-        sim.run_steps(1)
+        st_w = sim.run_steps(1)
     sim.sync()
 
     # ---- device-timed region: K steps chained on the device ----
@@ -385,7 +386,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     if fp32:
         line["defect_correction"] = {"tol": 1e-10, "n_solves_last_step": st.n_solves,
                                      "rel_residual_last_step": st.rel_residual,
-                                     "steps_missing_tol": st.n_unconverged}
+                                     "steps_missing_tol": st.n_unconverged,
+                                     "solves_per_step_timed":
+                                         (st.n_solves_total - (st_w.n_solves_total if st_w else 0)) / args.steps}
     if fp64 is not None:
         line["fp64_plain"] = fp64
     if adj is not None:

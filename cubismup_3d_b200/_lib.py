@@ -70,6 +70,7 @@ class CupStepStats(C.Structure):
         ("umax", C.c_double), ("kinetic_energy", C.c_double),
         ("force", C.c_double * 3), ("torque", C.c_double * 3),
         ("n_solves", C.c_int), ("rel_residual", C.c_double), ("n_unconverged", C.c_int),
+        ("n_solves_total", C.c_longlong),
     ]
 
 

@@ -44,6 +44,7 @@ struct DevState {
   double res_hist[16];  // relative residual at each check of the last solve
   int step, n_solves, converged;
   int n_unconverged;  // steps whose defect correction missed the tolerance (cumulative)
+  long long solves_total;  // correction solves of all decided defect corrections (cumulative)
 };
 
 enum PartialRegion { P_GRAD = 0, P_PEN, P_RHSOB, P_CHI, P_MAX, P_RES, P_DIAG, P_COUNT };
@@ -240,6 +241,7 @@ __global__ void k_finalize_residual(const double* p, int stride, int np, DevStat
       st->converged = met ? 1 : 2;  // 2: not converged after max_iter solves
       if (!met) st->n_unconverged += 1;
     }
+    if (st->converged) st->solves_total += k;
   }
 }
 
@@ -660,13 +662,6 @@ int launch_rows_pipe(cup_handle* H, const char* name, const R* in, R* out, doubl
   return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
 }
 
-// number of CTAs of a rows pass (= partials written by a reducing producer)
-int rows_grid(const cup_handle* H) {
-  const int TPL = std::max(1, H->nx / 16);
-  const int lpc = 256 / TPL;
-  return (H->ny * H->nz + lpc - 1) / lpc;
-}
-
 template <int M, typename R, int AXIS, bool DIVIDE, typename RIN = R>
 int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   // W x-columns per tile (FP32: 128-B rows of a tile, FP64: 128 B), NB = 3 tile buffers
@@ -677,7 +672,9 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   int rc = make_map(H, &map_in, in, tma_dtype<RIN>(), sizeof(RIN), W, AXIS == 1 ? N : 1, AXIS == 2 ? N : 1);
   if (!rc) rc = make_map(H, &map_out, out, tma_dtype<R>(), sizeof(R), W, AXIS == 1 ? N : 1, AXIS == 2 ? N : 1);
   if (rc) return rc;
+  constexpr bool WIDEN = sizeof(RIN) < sizeof(R);
   const size_t smem = (size_t)NB * N * W * sizeof(R) + FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) +
+                      (WIDEN ? FFTPlan<M>::table_len() * sizeof(typename Cplx<RIN>::T) : 0) +
                       NB * sizeof(uint64_t) + 128;
   auto kern = k_dht_cols_pipe<M, R, AXIS, DIVIDE, W, NB, RIN>;
   const int threads = W * TPL;
@@ -692,7 +689,8 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   const char* name = AXIS == 1 ? (inv64 ? "dht_y_f64" : "dht_y")
                                : (sizeof(RIN) < sizeof(R) ? "dht_z_solve_mixed" : "dht_z_solve");
   return launch_named(H, name, [&]() -> int {
-    kern<<<grid, threads, smem, H->stream>>>(map_in, map_out, ntx, ntiles, table<R>(H, AXIS), sp, H->derr, skip);
+    kern<<<grid, threads, smem, H->stream>>>(map_in, map_out, ntx, ntiles, table<R>(H, AXIS), table<RIN>(H, AXIS),
+                                             sp, H->derr, skip);
     CKL();
     return CUP_OK;
   });
@@ -1796,6 +1794,7 @@ static int fill_stats(cup_handle* H, cup_step_stats* st) {
   }
   st->n_solves = H->fp32 ? s.n_solves : 1;
   st->n_unconverged = s.n_unconverged;
+  st->n_solves_total = H->fp32 ? s.solves_total : 0;
   st->rel_residual = H->fp32 && s.b2 > 0 ? std::sqrt(s.res2 / s.b2) : 0.0;
   if (H->fp32 && s.converged == 2)
     return fail(H, CUP_ERR_NOT_CONVERGED, "defect correction: relative residual %.3e after %d solves",

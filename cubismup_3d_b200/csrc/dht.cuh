@@ -135,6 +135,7 @@ struct FFTPlan {
 // Row lines: line l starts at base + l*pitch (reals), complex m at reals 2m, 2m+1.
 template <typename R>
 struct RowLines {
+  using elem = R;
   using R2 = typename Cplx<R>::T;
   R* base;
   int pitch;
@@ -147,6 +148,7 @@ struct RowLines {
 // stage's stride-8 stores free of bank conflicts.
 template <typename R>
 struct RowLinesPad {
+  using elem = R;
   using R2 = typename Cplx<R>::T;
   R* base;
   int pitch;  // reals per line (>= 2*(M + M/8))
@@ -160,6 +162,7 @@ struct RowLinesPad {
 // Column lines of a tile [n][W]: element n of line l at n*W + l.
 template <typename R>
 struct ColLines {
+  using elem = R;
   using R2 = typename Cplx<R>::T;
   R* base;
   int W;
@@ -225,9 +228,14 @@ struct NoScale {
 // cos(4 pi k / N), which has period N/2 and is even) the four indices k, N-k,
 // M-k, M+k share one eigenvalue, so the spectral divide costs one factor per
 // four values.
-template <int M, typename R, typename R2, class Acc, class Scale = NoScale>
-__device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int t, bool active,
-                                         const Scale& scale = Scale()) {
+// The outputs go to `ao`; all inputs are read before a block barrier and the
+// outputs written after it, so `ao` may alias `a` even with a wider element
+// type (the z pass of the mixed-precision solve reads FP32 lines and writes
+// FP64 ones over the same bytes).
+template <int M, typename R, typename R2, class Acc, class AccO, class Scale>
+__device__ __forceinline__ void dht_post_to(const Acc& a, const AccO& ao, const R2* twp, int l, int t, bool active,
+                                            const Scale& scale) {
+  using RO = typename AccO::elem;
   constexpr int TPL = M / 8;
   constexpr int NT = (M / 2 + 1 + TPL - 1) / TPL;
   constexpr int N = 2 * M;
@@ -250,14 +258,14 @@ __device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int
       if (k > M / 2) continue;
       const R2 A = A_[i], B = B_[i];
       if (k == 0) {
-        R h0 = A.x + A.y, hM = A.x - A.y;
+        RO h0 = (RO)(A.x + A.y), hM = (RO)(A.x - A.y);
         if constexpr (Scale::kOn) {
           const double f = scale(0);
-          h0 = (R)((double)h0 * f);
-          hM = (R)((double)hM * f);
+          h0 = (RO)((double)h0 * f);
+          hM = (RO)((double)hM * f);
         }
-        a.str(l, 0, h0);
-        a.str(l, M, hM);
+        ao.str(l, 0, h0);
+        ao.str(l, M, hM);
       } else {
         const R2 W = twp[k];
         const R half = (R)0.5;
@@ -265,29 +273,36 @@ __device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int
         const R Or = (A.y + B.y) * half, Oi = (B.x - A.x) * half;
         const R Xr = Er + (W.x * Or - W.y * Oi), Xi = Ei + (W.x * Oi + W.y * Or);
         const R X2r = Er - W.x * Or + W.y * Oi, X2i = -Ei + W.x * Oi + W.y * Or;
-        R hk = Xr - Xi, hNk = Xr + Xi, hMk = X2r - X2i, hMpk = X2r + X2i;
+        RO hk = (RO)(Xr - Xi), hNk = (RO)(Xr + Xi), hMk = (RO)(X2r - X2i), hMpk = (RO)(X2r + X2i);
         if constexpr (Scale::kOn) {
           const double f = scale(k);
-          hk = (R)((double)hk * f);
-          hNk = (R)((double)hNk * f);
-          hMk = (R)((double)hMk * f);
-          hMpk = (R)((double)hMpk * f);
+          hk = (RO)((double)hk * f);
+          hNk = (RO)((double)hNk * f);
+          hMk = (RO)((double)hMk * f);
+          hMpk = (RO)((double)hMpk * f);
         }
-        a.str(l, k, hk);
-        a.str(l, N - k, hNk);
-        a.str(l, M - k, hMk);
-        a.str(l, M + k, hMpk);
+        ao.str(l, k, hk);
+        ao.str(l, N - k, hNk);
+        ao.str(l, M - k, hMk);
+        ao.str(l, M + k, hMpk);
       }
     }
   }
   __syncthreads();
 }
 
+template <int M, typename R, typename R2, class Acc, class Scale = NoScale>
+__device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int t, bool active,
+                                         const Scale& scale = Scale()) {
+  dht_post_to<M, R, R2>(a, a, twp, l, t, active, scale);
+}
+
 // Full in-place Hartley transform of the lines of `a` (pad: scratch for the
 // first stage's output when USE_PAD). Thread `t` of line `l`, M/8 per line.
-template <int M, bool USE_PAD, typename R, class Acc, class P, class Scale = NoScale>
-__device__ __forceinline__ void dht_lines(const Acc& a, const P& pad, const typename Cplx<R>::T* tw, int l, int t,
-                                          bool active, const Scale& scale = Scale()) {
+// The packed complex FFT stages of dht_lines (no even/odd split).
+template <int M, bool USE_PAD, typename R, class Acc, class P>
+__device__ __forceinline__ void fft_stages(const Acc& a, const P& pad, const typename Cplx<R>::T* tw, int l, int t,
+                                           bool active) {
   using R2 = typename Cplx<R>::T;
   using Pl = FFTPlan<M>;
   if constexpr (Pl::nstages == 1) {
@@ -301,7 +316,14 @@ __device__ __forceinline__ void dht_lines(const Acc& a, const P& pad, const type
     fft_stage<M, Pl::radix(1), 8, true, R2>(a, a, tw + Pl::tw_off(1), l, t, active);
     if constexpr (Pl::nstages == 3) fft_stage<M, Pl::radix(2), 64, true, R2>(a, a, tw + Pl::tw_off(2), l, t, active);
   }
-  dht_post<M, R, R2>(a, tw + Pl::post_off(), l, t, active, scale);
+}
+
+template <int M, bool USE_PAD, typename R, class Acc, class P, class Scale = NoScale>
+__device__ __forceinline__ void dht_lines(const Acc& a, const P& pad, const typename Cplx<R>::T* tw, int l, int t,
+                                          bool active, const Scale& scale = Scale()) {
+  using R2 = typename Cplx<R>::T;
+  fft_stages<M, USE_PAD, R>(a, pad, tw, l, t, active);
+  dht_post<M, R, R2>(a, tw + FFTPlan<M>::post_off(), l, t, active, scale);
 }
 
 template <typename R2>
@@ -593,15 +615,19 @@ __device__ __forceinline__ ZColumnFactor z_column_factor(const SpectralParams& s
 // transform of the current one; the twiddle table is loaded once per CTA.
 //
 // RIN = float with R = double (z pass of the mixed-precision correction
-// solve): the FP32 tile lands in the upper half of its FP64 buffer and is
-// widened in place (all reads, a barrier, then all writes) before the FP64
-// transforms; the tile is stored in FP64.
+// solve): the FP32 tile lands in the upper half of its FP64 buffer; the
+// forward transform runs in FP32 on it (like the x and y forward passes) and
+// its even/odd split writes the divided spectrum in FP64 over the whole
+// buffer (all reads before a barrier, all writes after it); the inverse runs
+// in FP64 and the tile is stored in FP64. tw_in_g: the FP32 table.
 template <int M, typename R, int AXIS, bool DIVIDE, int W, int NB, typename RIN = R>
 __global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_constant__ CUtensorMap map_in,
                                                        const __grid_constant__ CUtensorMap map_out, int ntiles_x,
-                                                       int ntiles, const typename Cplx<R>::T* tw_g, SpectralParams sp,
+                                                       int ntiles, const typename Cplx<R>::T* tw_g,
+                                                       const typename Cplx<RIN>::T* tw_in_g, SpectralParams sp,
                                                        int* err, const int* skip) {
   using R2 = typename Cplx<R>::T;
+  using RI2 = typename Cplx<RIN>::T;
   static_assert(NB >= 2, "need at least two tile buffers");
   static_assert(sizeof(RIN) <= sizeof(R), "input may only be narrower than the transform type");
   if (skip && *skip) return;
@@ -609,12 +635,12 @@ __global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_cons
   constexpr int TL = FFTPlan<M>::table_len();
   constexpr bool WIDEN = sizeof(RIN) < sizeof(R);
   constexpr uint32_t TILE_BYTES = (uint32_t)(N * W * sizeof(RIN));
-  constexpr int PER_THREAD = (N * W + W * TPL - 1) / (W * TPL);
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
   R* tiles = reinterpret_cast<R*>(smem_raw);  // [NB][N][W]
   R2* tw = reinterpret_cast<R2*>(tiles + (size_t)NB * N * W);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
+  RI2* tw_in = reinterpret_cast<RI2*>(tw + TL);  // (WIDEN only)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw_in + (WIDEN ? TL : 0));
   const int tid = threadIdx.x;
   const int my = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   if (tid == 0) {
@@ -641,6 +667,7 @@ __global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_cons
   if (tid == 0)
     for (; issued < min(NB - 1, my); ++issued) issue(issued);
   load_table(tw, tw_g, TL);
+  if constexpr (WIDEN) load_table(tw_in, tw_in_g, TL);
   __syncthreads();
   const int l = tid % W, t = tid / W;
   const bool active = t < TPL;
@@ -659,25 +686,20 @@ __global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_cons
     int x0, other;
     coords(i, x0, other);
     R* tile = tiles + (size_t)b * N * W;
-    if constexpr (WIDEN) {
-      const RIN* narrow = reinterpret_cast<const RIN*>(reinterpret_cast<unsigned char*>(tile) +
-                                                       (size_t)N * W * (sizeof(R) - sizeof(RIN)));
-      R vals[PER_THREAD];
-#pragma unroll
-      for (int k = 0; k < PER_THREAD; ++k) {
-        const int e = tid + k * (int)blockDim.x;
-        vals[k] = e < N * W ? (R)narrow[e] : (R)0;
-      }
-      __syncthreads();
-#pragma unroll
-      for (int k = 0; k < PER_THREAD; ++k) {
-        const int e = tid + k * (int)blockDim.x;
-        if (e < N * W) tile[e] = vals[k];
-      }
-      __syncthreads();
-    }
     ColLines<R> A{tile, W};
-    if constexpr (DIVIDE) {
+    if constexpr (WIDEN) {
+      ColLines<RIN> An{reinterpret_cast<RIN*>(reinterpret_cast<unsigned char*>(tile) +
+                                              (size_t)N * W * (sizeof(R) - sizeof(RIN))),
+                       W};
+      fft_stages<M, false, RIN>(An, An, tw_in, l, t, active);
+      if constexpr (DIVIDE) {
+        dht_post_to<M, RIN, RI2>(An, A, tw_in + FFTPlan<M>::post_off(), l, t, active,
+                                 z_column_factor(sp, x0 + l, other));
+        dht_lines<M, false, R>(A, A, tw, l, t, active);
+      } else {
+        dht_post_to<M, RIN, RI2>(An, A, tw_in + FFTPlan<M>::post_off(), l, t, active, NoScale());
+      }
+    } else if constexpr (DIVIDE) {
       // forward, spectral divide fused into the even/odd split, inverse
       dht_lines<M, false, R>(A, A, tw, l, t, active, z_column_factor(sp, x0 + l, other));
       dht_lines<M, false, R>(A, A, tw, l, t, active);

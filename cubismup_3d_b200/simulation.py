@@ -241,11 +241,12 @@ class StepStats:
     n_solves: int
     rel_residual: float
     n_unconverged: int = 0
+    n_solves_total: int = 0
 
     @classmethod
     def from_c(cls, s: L.CupStepStats) -> "StepStats":
         return cls(s.dt, s.time, s.step, s.umax, s.kinetic_energy, np.array(s.force[:]), np.array(s.torque[:]),
-                   s.n_solves, s.rel_residual, s.n_unconverged)
+                   s.n_solves, s.rel_residual, s.n_unconverged, s.n_solves_total)
 
 
 class Simulation:

@@ -99,6 +99,7 @@ typedef struct cup_step_stats {
   int n_solves;
   double rel_residual;
   int n_unconverged;       /* steps since cup_create whose defect correction missed dc_tol */
+  long long n_solves_total; /* FP32 correction solves since cup_create (FP32_DC) */
 } cup_step_stats;
 
 /* ---- lifetime (SimulationData ctor / Simulation ctor, source/Simulation.cpp:53-64) ---- */
