@@ -592,17 +592,21 @@ template <int M, typename R, class Prod, class Cons>
 int launch_rows_M(cup_handle* H, const char* name, const Prod& prod, const Cons& cons, const int* skip) {
   constexpr int N = 2 * M, TPL = M / 8;
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
-  const int lpc = 256 / TPL;
+  // the read-modify-write of p runs on half tiles (128 threads): more CTAs per
+  // SM overlap one CTA's bulk copies with another's transform
+  const int lpc = (Cons::kAddBulk && TPL <= 16 ? 128 : 256) / TPL;
   const int nrows = H->ny * H->nz;
+  // reduction scratch only for producers that compute rows (and may reduce)
+  const size_t scratch = Prod::kBulk ? 0 : 32 * 20 * sizeof(double);
   const size_t smem = (size_t)lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
                       (Cons::kAddBulk ? (size_t)lpc * N * sizeof(double) : 0) +
-                      FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + 16 + 32 * 20 * sizeof(double) + 128;
+                      FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + 16 + scratch + 128;
   auto kern = k_dht_rows<M, R, Prod, Cons>;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, lpc * TPL, &bpsm);
   if (rc) return rc;
   const int grid = (nrows + lpc - 1) / lpc;
-  if (grid > kPartialCap / 20) return fail(H, CUP_ERR_ARG, "too many row tiles for the partial buffers");
+  if (!Prod::kBulk && grid > kPartialCap / 20) return fail(H, CUP_ERR_ARG, "too many row tiles for the partial buffers");
   return launch_named(H, name, [&]() -> int {
     kern<<<grid, lpc * TPL, smem, H->stream>>>(prod, cons, nrows, lpc, table<R>(H, 0), H->derr, skip);
     CKL();
