@@ -63,6 +63,15 @@ def kernel_bytes(name: str, fp32: bool) -> float:
     return float(table.get(name, 0.0))
 
 
+# DRAM traffic per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum
+# of an ncu capture of the 256^3 FP32-DC step, profiles/step_fp32dc_upwind3_256_kernels_full.md),
+# scaled by the cells of the run; traffic grows with the cells streamed.
+MEASURED_DRAM_BYTES_PER_CELL_FP32DC = {
+    "grad_p_check": 55.3, "upwind3_stage1": 23.3, "upwind3_stage2": 34.9, "rhs_residual": 30.5,
+    "dht_x_update_p": 21.5, "dht_z_solve_mixed": 8.7, "dht_y_f64": 12.5, "dht_x": 4.8, "dht_y": 4.5,
+}
+
+
 def canonical_step_bytes(fp32: bool, scheme: str, n_solves: int = 1) -> float:
     """Algorithmic bytes per cell-step of the hot path's canonical pass structure
     (upwind3: 288 B FP64, 160 B FP32 with one correction solve, +64 B per
@@ -365,8 +374,13 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     total_ms = sum(k[0] for k in kern)
     n_solves = st.n_solves if fp32 else 1
     cb = canonical_step_bytes(fp32, args.scheme, n_solves)
+    traffic = None
+    if fp32 and args.scheme == "upwind3_rk2" and top[1] in MEASURED_DRAM_BYTES_PER_CELL_FP32DC:
+        traffic = MEASURED_DRAM_BYTES_PER_CELL_FP32DC[top[1]] * n ** 3
     roof = {"bound": "hbm", "kernel": top[1], "achieved": top[3], "peak": peak, "unit": "GB/s",
-            "frac": top[3] / peak, "peak_kind": peak_kind, "traffic": None,
+            "frac": top[3] / peak, "peak_kind": peak_kind, "traffic": traffic,
+            "traffic_source": "ncu capture at 256^3 scaled by cells" if traffic else None,
+            "algorithmic_bytes": kernel_bytes(top[1], fp32) * n ** 3,
             "step_bytes_per_cell": cb,
             "step_achieved": cb * value / world / 1e9,
             "step_frac": cb * value / world / 1e9 / peak}
