@@ -232,13 +232,47 @@ struct NoScale {
 // outputs written after it, so `ao` may alias `a` even with a wider element
 // type (the z pass of the mixed-precision solve reads FP32 lines and writes
 // FP64 ones over the same bytes).
+// Split task k of one line: Z[k] = A, Z[M-k] = B -> H[k], H[N-k], H[M-k],
+// H[M+k] (task 0: H[0], H[M] from A = Z[0]), times scale(k).
+template <int M, typename R, typename R2, class AccO, class Scale>
+__device__ __forceinline__ void split_task(const AccO& ao, int l, int k, R2 A, R2 B, R2 W, const Scale& scale) {
+  using RO = typename AccO::elem;
+  constexpr int N = 2 * M;
+  if (k == 0) {
+    RO h0 = (RO)(A.x + A.y), hM = (RO)(A.x - A.y);
+    if constexpr (Scale::kOn) {
+      const double f = scale(0);
+      h0 = (RO)((double)h0 * f);
+      hM = (RO)((double)hM * f);
+    }
+    ao.str(l, 0, h0);
+    ao.str(l, M, hM);
+  } else {
+    const R half = (R)0.5;
+    const R Er = (A.x + B.x) * half, Ei = (A.y - B.y) * half;
+    const R Or = (A.y + B.y) * half, Oi = (B.x - A.x) * half;
+    const R Xr = Er + (W.x * Or - W.y * Oi), Xi = Ei + (W.x * Oi + W.y * Or);
+    const R X2r = Er - W.x * Or + W.y * Oi, X2i = -Ei + W.x * Oi + W.y * Or;
+    RO hk = (RO)(Xr - Xi), hNk = (RO)(Xr + Xi), hMk = (RO)(X2r - X2i), hMpk = (RO)(X2r + X2i);
+    if constexpr (Scale::kOn) {
+      const double f = scale(k);
+      hk = (RO)((double)hk * f);
+      hNk = (RO)((double)hNk * f);
+      hMk = (RO)((double)hMk * f);
+      hMpk = (RO)((double)hMpk * f);
+    }
+    ao.str(l, k, hk);
+    ao.str(l, N - k, hNk);
+    ao.str(l, M - k, hMk);
+    ao.str(l, M + k, hMpk);
+  }
+}
+
 template <int M, typename R, typename R2, class Acc, class AccO, class Scale>
 __device__ __forceinline__ void dht_post_to(const Acc& a, const AccO& ao, const R2* twp, int l, int t, bool active,
                                             const Scale& scale) {
-  using RO = typename AccO::elem;
   constexpr int TPL = M / 8;
   constexpr int NT = (M / 2 + 1 + TPL - 1) / TPL;
-  constexpr int N = 2 * M;
   R2 A_[NT], B_[NT];
   if (active) {
 #pragma unroll
@@ -256,36 +290,60 @@ __device__ __forceinline__ void dht_post_to(const Acc& a, const AccO& ao, const 
     for (int i = 0; i < NT; ++i) {
       const int k = t + i * TPL;
       if (k > M / 2) continue;
-      const R2 A = A_[i], B = B_[i];
-      if (k == 0) {
-        RO h0 = (RO)(A.x + A.y), hM = (RO)(A.x - A.y);
-        if constexpr (Scale::kOn) {
-          const double f = scale(0);
-          h0 = (RO)((double)h0 * f);
-          hM = (RO)((double)hM * f);
-        }
-        ao.str(l, 0, h0);
-        ao.str(l, M, hM);
-      } else {
-        const R2 W = twp[k];
-        const R half = (R)0.5;
-        const R Er = (A.x + B.x) * half, Ei = (A.y - B.y) * half;
-        const R Or = (A.y + B.y) * half, Oi = (B.x - A.x) * half;
-        const R Xr = Er + (W.x * Or - W.y * Oi), Xi = Ei + (W.x * Oi + W.y * Or);
-        const R X2r = Er - W.x * Or + W.y * Oi, X2i = -Ei + W.x * Oi + W.y * Or;
-        RO hk = (RO)(Xr - Xi), hNk = (RO)(Xr + Xi), hMk = (RO)(X2r - X2i), hMpk = (RO)(X2r + X2i);
-        if constexpr (Scale::kOn) {
-          const double f = scale(k);
-          hk = (RO)((double)hk * f);
-          hNk = (RO)((double)hNk * f);
-          hMk = (RO)((double)hMk * f);
-          hMpk = (RO)((double)hMpk * f);
-        }
-        ao.str(l, k, hk);
-        ao.str(l, N - k, hNk);
-        ao.str(l, M - k, hMk);
-        ao.str(l, M + k, hMpk);
-      }
+      split_task<M, R, R2>(ao, l, k, A_[i], B_[i], twp[k], scale);
+    }
+  }
+  __syncthreads();
+}
+
+// 128-point FFT (256-long lines): its last Stockham stage (radix 2, Ns = 64)
+// fused with the even/odd split. Butterfly j (0..63) takes Z'[j] and
+// W128^j Z'[j+64] and gives Z[j] = a + b, Z[j+64] = a - b. Split task k
+// (0..64) needs Z[k] and Z[128-k], which come from butterflies k and 64-k
+// (mod 64), so a thread that owns both does the stage and both tasks in
+// registers: one shared-memory round trip less per transform. Thread t < 15
+// owns butterflies t+1, 63-t (tasks t+1, 63-t) and t+17, 47-t (tasks t+17,
+// 47-t); thread 15 owns 16, 48 (tasks 16, 48), 0 (tasks 0 and 64) and 32
+// (task 32). All inputs are read before a block barrier, all outputs
+// written after it (`ao` may alias `a`, also with a wider element type).
+template <typename R, typename R2, class Acc, class AccO, class Scale>
+__device__ __forceinline__ void dht128_tail(const Acc& a, const AccO& ao, const R2* tw3, const R2* twp, int l, int t,
+                                            bool active, const Scale& scale) {
+  constexpr int M = 128;
+  int bj[4];
+  if (t < 15) {
+    bj[0] = t + 1;
+    bj[1] = 63 - t;
+    bj[2] = t + 17;
+    bj[3] = 47 - t;
+  } else {
+    bj[0] = 16;
+    bj[1] = 48;
+    bj[2] = 0;
+    bj[3] = 32;
+  }
+  R2 lo[4], hi[4];
+  if (active) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const R2 x0 = a.ld(l, bj[q]);
+      const R2 x1 = cmul(a.ld(l, bj[q] + 64), tw3[64 + bj[q]]);
+      lo[q] = cadd(x0, x1);  // Z[bj]
+      hi[q] = csub(x0, x1);  // Z[bj + 64]
+    }
+  }
+  __syncthreads();
+  if (active) {
+    // pair (bj[0], bj[1] = 64 - bj[0]): tasks bj[0] and bj[1]
+    split_task<M, R, R2>(ao, l, bj[0], lo[0], hi[1], twp[bj[0]], scale);
+    split_task<M, R, R2>(ao, l, bj[1], lo[1], hi[0], twp[bj[1]], scale);
+    if (t < 15) {
+      split_task<M, R, R2>(ao, l, bj[2], lo[2], hi[3], twp[bj[2]], scale);
+      split_task<M, R, R2>(ao, l, bj[3], lo[3], hi[2], twp[bj[3]], scale);
+    } else {
+      split_task<M, R, R2>(ao, l, 0, lo[2], lo[2], twp[0], scale);     // Z[0]
+      split_task<M, R, R2>(ao, l, 64, hi[2], hi[2], twp[64], scale);   // Z[64], Z[128 - 64]
+      split_task<M, R, R2>(ao, l, 32, lo[3], hi[3], twp[32], scale);   // Z[32], Z[96]
     }
   }
   __syncthreads();
@@ -299,7 +357,8 @@ __device__ __forceinline__ void dht_post(const Acc& a, const R2* twp, int l, int
 
 // Full in-place Hartley transform of the lines of `a` (pad: scratch for the
 // first stage's output when USE_PAD). Thread `t` of line `l`, M/8 per line.
-// The packed complex FFT stages of dht_lines (no even/odd split).
+// The packed complex FFT stages of dht_lines (for M = 128 all but the last,
+// which dht_tail_to fuses with the even/odd split).
 template <int M, bool USE_PAD, typename R, class Acc, class P>
 __device__ __forceinline__ void fft_stages(const Acc& a, const P& pad, const typename Cplx<R>::T* tw, int l, int t,
                                            bool active) {
@@ -310,20 +369,37 @@ __device__ __forceinline__ void fft_stages(const Acc& a, const P& pad, const typ
   } else if constexpr (USE_PAD) {
     fft_stage<M, 8, 1, false, R2>(a, pad, tw, l, t, active);
     fft_stage<M, Pl::radix(1), 8, false, R2>(pad, a, tw + Pl::tw_off(1), l, t, active);
-    if constexpr (Pl::nstages == 3) fft_stage<M, Pl::radix(2), 64, true, R2>(a, a, tw + Pl::tw_off(2), l, t, active);
+    if constexpr (Pl::nstages == 3 && M != 128)
+      fft_stage<M, Pl::radix(2), 64, true, R2>(a, a, tw + Pl::tw_off(2), l, t, active);
   } else {
     fft_stage<M, 8, 1, true, R2>(a, a, tw, l, t, active);
     fft_stage<M, Pl::radix(1), 8, true, R2>(a, a, tw + Pl::tw_off(1), l, t, active);
-    if constexpr (Pl::nstages == 3) fft_stage<M, Pl::radix(2), 64, true, R2>(a, a, tw + Pl::tw_off(2), l, t, active);
+    if constexpr (Pl::nstages == 3 && M != 128)
+      fft_stage<M, Pl::radix(2), 64, true, R2>(a, a, tw + Pl::tw_off(2), l, t, active);
+  }
+}
+
+// The rest of the transform after fft_stages: for M = 128 the last Stockham
+// stage fused with the even/odd split, otherwise the split alone; outputs to
+// `ao` (may alias `a`).
+template <int M, typename R, class Acc, class AccO, class Scale>
+__device__ __forceinline__ void dht_tail_to(const Acc& a, const AccO& ao, const typename Cplx<R>::T* tw, int l, int t,
+                                            bool active, const Scale& scale) {
+  using R2 = typename Cplx<R>::T;
+  using Pl = FFTPlan<M>;
+  if constexpr (M == 128) {
+    static_assert(Pl::nstages == 3 && Pl::radix(2) == 2, "the fused tail needs a final radix-2 stage");
+    dht128_tail<R, R2>(a, ao, tw + Pl::tw_off(2), tw + Pl::post_off(), l, t, active, scale);
+  } else {
+    dht_post_to<M, R, R2>(a, ao, tw + Pl::post_off(), l, t, active, scale);
   }
 }
 
 template <int M, bool USE_PAD, typename R, class Acc, class P, class Scale = NoScale>
 __device__ __forceinline__ void dht_lines(const Acc& a, const P& pad, const typename Cplx<R>::T* tw, int l, int t,
                                           bool active, const Scale& scale = Scale()) {
-  using R2 = typename Cplx<R>::T;
   fft_stages<M, USE_PAD, R>(a, pad, tw, l, t, active);
-  dht_post<M, R, R2>(a, tw + FFTPlan<M>::post_off(), l, t, active, scale);
+  dht_tail_to<M, R>(a, a, tw, l, t, active, scale);
 }
 
 template <typename R2>
@@ -693,11 +769,10 @@ __global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_cons
                        W};
       fft_stages<M, false, RIN>(An, An, tw_in, l, t, active);
       if constexpr (DIVIDE) {
-        dht_post_to<M, RIN, RI2>(An, A, tw_in + FFTPlan<M>::post_off(), l, t, active,
-                                 z_column_factor(sp, x0 + l, other));
+        dht_tail_to<M, RIN>(An, A, tw_in, l, t, active, z_column_factor(sp, x0 + l, other));
         dht_lines<M, false, R>(A, A, tw, l, t, active);
       } else {
-        dht_post_to<M, RIN, RI2>(An, A, tw_in + FFTPlan<M>::post_off(), l, t, active, NoScale());
+        dht_tail_to<M, RIN>(An, A, tw_in, l, t, active, NoScale());
       }
     } else if constexpr (DIVIDE) {
       // forward, spectral divide fused into the even/odd split, inverse
