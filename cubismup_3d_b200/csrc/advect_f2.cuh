@@ -98,12 +98,17 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
   const int mask = nx - 1;
   const int half = nx >> 1;
   int px[PPT], cy[PPT];  // even x of the pair, tile row
+  int ctr[PPT], xl[PPT], xr[PPT];  // slot offsets: centre row, pairs at x -+ 2 in that row
 #pragma unroll
   for (int i = 0; i < PPT; ++i) {
     const int pi = tid + i * blockDim.x;
     px[i] = (pi % half) * 2;
     cy[i] = pi / half;
+    ctr[i] = (G + cy[i]) * nx + px[i];
+    xl[i] = (G + cy[i]) * nx + ((px[i] - 2) & mask);
+    xr[i] = (G + cy[i]) * nx + ((px[i] + 2) & mask);
   }
+  const size_t plane = (size_t)nx * ny;
   const double dtv = dt.get();
   const float2 facA = splat2((float)(-dtv / (12 * h)));  // the 1/2 of the symmetric form folded in
   const float2 facD = splat2((float)((nu / h) * (dtv / h)));
@@ -130,6 +135,9 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
     const int item = blockIdx.x + it * gridDim.x;
     const int ty = item % g.items_y, zi = item / g.items_y;
     const int y0 = ty * TY, z0 = zi * g.zc;
+    size_t obase[PPT];  // output index of the pair in plane z0
+#pragma unroll
+    for (int i = 0; i < PPT; ++i) obase[i] = gidx(px[i], y0 + cy[i], z0, nx, ny);
     for (int j0 = 0; j0 < PL; j0 += U) {
 #pragma unroll
       for (int jj = 0; jj < U; ++jj) {
@@ -143,7 +151,7 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
           for (int f = 0; f < 3; ++f)
 #pragma unroll
             for (int i = 0; i < PPT; ++i)
-              qv[f][QN][i] = *reinterpret_cast<const float2*>(sl + f * field_elems + (G + cy[i]) * nx + px[i]);
+              qv[f][QN][i] = *reinterpret_cast<const float2*>(sl + f * field_elems + ctr[i]);
           if (j >= 2 * G) {
             const int k = j - 2 * G;
             const int QC = (jj + 3 * Q - G) % Q;
@@ -152,7 +160,7 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
             const int PS = jj % G;
 #pragma unroll
             for (int i = 0; i < PPT; ++i) {
-              const size_t o = gidx(px[i], y0 + cy[i], z0 + k, nx, ny);
+              const size_t o = obase[i] + (size_t)k * plane;
               const float2 ww = add2(qv[2][QC][i], uinf[2]);
               const float2 aw = abs2(ww);
               float2 outv[3];
@@ -180,19 +188,18 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
             for (int i = 0; i < PPT; ++i) {
               const float2 uu = add2(qv[0][QN][i], uinf[0]), vv = add2(qv[1][QN][i], uinf[1]);
               const float2 au = abs2(uu), av = abs2(vv);
-              const int x = px[i], r = G + cy[i];
-              const int xl = (x - 2) & mask, xr = (x + 2) & mask;
 #pragma unroll
               for (int f = 0; f < 3; ++f) {
                 const float* F = sl + f * field_elems;
+                const float* Fc = F + ctr[i];
                 const float2 c0 = qv[f][QN][i];
-                const float2 A = *reinterpret_cast<const float2*>(F + r * nx + xl);
-                const float2 B = *reinterpret_cast<const float2*>(F + r * nx + xr);
+                const float2 A = *reinterpret_cast<const float2*>(F + xl[i]);
+                const float2 B = *reinterpret_cast<const float2*>(F + xr[i]);
                 const float2 xm1 = make_float2(A.y, c0.x), xp1 = make_float2(c0.y, B.x);
-                const float2 ym2 = *reinterpret_cast<const float2*>(F + (r - 2) * nx + x);
-                const float2 ym1 = *reinterpret_cast<const float2*>(F + (r - 1) * nx + x);
-                const float2 yp1 = *reinterpret_cast<const float2*>(F + (r + 1) * nx + x);
-                const float2 yp2 = *reinterpret_cast<const float2*>(F + (r + 2) * nx + x);
+                const float2 ym2 = *reinterpret_cast<const float2*>(Fc - 2 * nx);
+                const float2 ym1 = *reinterpret_cast<const float2*>(Fc - nx);
+                const float2 yp1 = *reinterpret_cast<const float2*>(Fc + nx);
+                const float2 yp2 = *reinterpret_cast<const float2*>(Fc + 2 * nx);
                 const float2 ax = adv2(uu, au, A, xm1, c0, xp1, B);
                 const float2 ay = adv2(vv, av, ym2, ym1, c0, yp1, yp2);
                 const float2 nb = add2(add2(xm1, xp1), add2(ym1, yp1));
