@@ -740,7 +740,7 @@ int dc_correction_solve(cup_handle* H, double* p, const int* skip) {
   if ((rc = launch_cols<double, 2, true, float>(H, H->work32, H->work64, skip))) return rc;
   if ((rc = launch_cols<double, 1, false>(H, H->work64, H->work64, skip))) return rc;
   return launch_rows<double>(H, "dht_x_update_p", RowsFromArray<double>{H->work64},
-                             RowsAddToP{p, H->dstate->cmean, H->ny}, skip);
+                             RowsAddToP{p, H->dstate->cmean, ilog2(H->ny)}, skip);
 }
 
 // p = H(f . H(work)) over the three axes, in place on `work`; the last x

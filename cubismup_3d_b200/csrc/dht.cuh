@@ -442,13 +442,13 @@ struct RowsAddToP {
   static constexpr bool kAddBulk = true;
   double* p;
   const double* cmean;
-  int ny;
+  int log2ny;  // ny is a power of two: row r is (y, z) = (r & (ny-1), r >> log2ny)
   __device__ double* rows_of(int row0, int N) const { return p + (size_t)row0 * N; }
   __device__ void add(double* ps, const double* rows, int row0, int nr, int N) const {
     for (int i = threadIdx.x; i < nr * N; i += blockDim.x) {
       const int l = i / N, x = i - l * N;
-      const int r = row0 + l, y = r % ny, z = r / ny;
-      const int cls = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
+      const int r = row0 + l;
+      const int cls = (x & 1) | ((r & 1) << 1) | (((r >> log2ny) & 1) << 2);
       ps[i] = ps[i] + rows[i] - cmean[cls];
     }
   }
