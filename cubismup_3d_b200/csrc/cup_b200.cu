@@ -370,6 +370,9 @@ void build_table_M(std::vector<double2>& t64, std::vector<float2>& t32) {
       for (int j = 0; j < Ns; ++j) put(off + r * Ns + j, -2.0L * PI * r * j / ((long double)Ns * R));
   }
   for (int k = 0; k <= M / 2; ++k) put(Pl::post_off() + k, -2.0L * PI * k / (2.0L * M));
+  if (M == 128)
+    for (int r = 0; r < 8; ++r)
+      for (int j = 0; j < 16; ++j) put(Pl::r16_off() + 16 * r + j, -2.0L * PI * r * j / (long double)M);
 }
 
 void build_table(int N, std::vector<double2>& t64, std::vector<float2>& t32) {
@@ -600,7 +603,7 @@ int launch_rows_M(cup_handle* H, const char* name, const Prod& prod, const Cons&
   const size_t scratch = Prod::kBulk ? 0 : 32 * 20 * sizeof(double);
   const size_t smem = (size_t)lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
                       (Cons::kAddBulk ? (size_t)lpc * N * sizeof(double) : 0) +
-                      FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + 16 + scratch + 128;
+                      FFTPlan<M>::rows_table_len() * sizeof(typename Cplx<R>::T) + 16 + scratch + 128;
   auto kern = k_dht_rows<M, R, Prod, Cons>;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, lpc * TPL, &bpsm);
@@ -638,7 +641,7 @@ int launch_rows_pipe_M(cup_handle* H, const char* name, const R* in, R* out, dou
   const int lpc = 256 / TPL;
   const int nrows = H->ny * H->nz;
   const size_t smem = (size_t)NB * lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
-                      FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) + NB * sizeof(uint64_t) + 128;
+                      FFTPlan<M>::rows_table_len() * sizeof(typename Cplx<R>::T) + NB * sizeof(uint64_t) + 128;
   auto kern = k_dht_rows_pipe<M, R, ADD, NB>;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, 256, &bpsm);
@@ -669,7 +672,10 @@ int launch_rows_pipe(cup_handle* H, const char* name, const R* in, R* out, doubl
 template <int M, typename R, int AXIS, bool DIVIDE, typename RIN = R>
 int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   // W x-columns per tile (FP32: 128-B rows of a tile, FP64: 128 B), NB = 3 tile buffers
-  constexpr int N = 2 * M, TPL = M / 8, NB = 3;
+  // 256-long FP32 lines: the 8-thread plan (radix 16, then radix 8 fused with the
+  // split); measured slower than the 16-thread plan for FP64 tiles (fewer CTAs fit)
+  constexpr bool T8 = M == 128 && sizeof(R) == 4;
+  constexpr int N = 2 * M, TPL = T8 ? 8 : M / 8, NB = 3;
   constexpr int W = sizeof(R) == 4 ? 32 : 16;
   if (H->nx % W) return fail(H, CUP_ERR_ARG, "nx must be a multiple of %d for this precision", W);
   CUtensorMap map_in, map_out;
@@ -680,7 +686,7 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   const size_t smem = (size_t)NB * N * W * sizeof(R) + FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) +
                       (WIDEN ? FFTPlan<M>::table_len() * sizeof(typename Cplx<RIN>::T) : 0) +
                       NB * sizeof(uint64_t) + 128;
-  auto kern = k_dht_cols_pipe<M, R, AXIS, DIVIDE, W, NB, RIN>;
+  auto kern = k_dht_cols_pipe<M, R, AXIS, DIVIDE, W, NB, RIN, T8>;
   const int threads = W * TPL;
   int bpsm = 0;
   rc = prepare_kernel(H, kern, smem, threads, &bpsm);

@@ -111,6 +111,49 @@ struct DFT<8, R2> {
   }
 };
 
+// 16-point forward DFT as 4 x 4: X[k1 + 4 k2] =
+//   sum_n2 W4^(n2 k2) W16^(n2 k1) sum_n1 x[4 n1 + n2] W4^(n1 k1).
+template <typename R2>
+struct DFT<16, R2> {
+  __device__ __forceinline__ static R2 cm(R2 a, double re, double im) {
+    using S = decltype(a.x);
+    R2 r;
+    r.x = a.x * (S)re - a.y * (S)im;
+    r.y = a.x * (S)im + a.y * (S)re;
+    return r;
+  }
+  __device__ __forceinline__ static void run(R2* v) {
+    constexpr double c1 = 0.92387953251128675613;  // cos(pi/8)
+    constexpr double s1 = 0.38268343236508977173;  // sin(pi/8)
+    constexpr double h = 0.70710678118654752440;   // sqrt(2)/2
+    R2 y[4][4];
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) {
+      R2 t[4] = {v[n2], v[4 + n2], v[8 + n2], v[12 + n2]};
+      DFT<4, R2>::run(t);
+#pragma unroll
+      for (int k1 = 0; k1 < 4; ++k1) y[n2][k1] = t[k1];
+    }
+    // twiddles W16^(n2 k1) = cos(2 pi m / 16) - i sin(2 pi m / 16), m = n2 k1
+    y[1][1] = cm(y[1][1], c1, -s1);
+    y[1][2] = cm(y[1][2], h, -h);
+    y[1][3] = cm(y[1][3], s1, -c1);
+    y[2][1] = cm(y[2][1], h, -h);
+    y[2][2] = cmul_mi(y[2][2]);
+    y[2][3] = cm(y[2][3], -h, -h);
+    y[3][1] = cm(y[3][1], s1, -c1);
+    y[3][2] = cm(y[3][2], -h, -h);
+    y[3][3] = cm(y[3][3], -c1, s1);
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      R2 t[4] = {y[0][k1], y[1][k1], y[2][k1], y[3][k1]};
+      DFT<4, R2>::run(t);
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[k2];
+    }
+  }
+};
+
 // Radix plan of an M-point complex FFT: radix-8 stages then one 2 or 4.
 template <int M>
 struct FFTPlan {
@@ -128,7 +171,12 @@ struct FFTPlan {
   }
   // post-processing table W_N^k, k = 0..M/2, follows the stage tables
   static constexpr int post_off() { return tw_stage_total(); }
-  static constexpr int table_len() { return tw_stage_total() + M / 2 + 1; }
+  // M = 128 only: W128^(r j), r < 8, j < 16 (index 16 r + j) of the 8-thread
+  // plan (radix 16, then radix 8 over Ns = 16), after the post table
+  static constexpr int r16_off() { return tw_stage_total() + M / 2 + 1; }
+  static constexpr int table_len() { return tw_stage_total() + M / 2 + 1 + (M == 128 ? 128 : 0); }
+  // the row passes use the 16-thread plan only: stage and post tables
+  static constexpr int rows_table_len() { return tw_stage_total() + M / 2 + 1; }
 };
 
 // ---- line accessors -------------------------------------------------------
@@ -379,6 +427,74 @@ __device__ __forceinline__ void fft_stages(const Acc& a, const P& pad, const typ
   }
 }
 
+// 256-long lines with 8 threads per line (t = 0..7), two shared-memory round
+// trips per transform instead of three:
+//   A: radix-16 over m = t + 8 r (r < 16), outputs to 16 t + r (Stockham, Ns = 1);
+//   B: radix-8 butterflies j (inputs Z'[j + 16 r] times W128^(r j), outputs
+//      Z[j + 16 r]) fused with the even/odd split. Split task k needs Z[k] and
+//      Z[128 - k]; Z[j + 16 r] pairs with Z[(16 - j) + 16 (7 - r)], so thread t
+//      owns butterflies t and 16 - t (t = 0: 0 and 8, each its own partner)
+//      and does their split tasks in registers.
+// Meant for column tiles (ColLines), where stage A's 16-strided writes fall in
+// different columns across a warp. `ao` may alias `a` (see dht_post_to).
+template <typename R, class Acc, class AccO, class Scale>
+__device__ __forceinline__ void dht128_t8_to(const Acc& a, const AccO& ao, const typename Cplx<R>::T* tw, int l,
+                                             int t, bool active, const Scale& scale) {
+  using R2 = typename Cplx<R>::T;
+  using Pl = FFTPlan<128>;
+  constexpr int M = 128;
+  const R2* twB = tw + Pl::r16_off();
+  const R2* twp = tw + Pl::post_off();
+  R2 v[16];
+  // stage A (in place: all reads, barrier, all writes)
+  if (active) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = a.ld(l, t + 8 * r);
+    DFT<16, R2>::run(v);
+  }
+  __syncthreads();
+  if (active) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) a.st(l, 16 * t + r, v[r]);
+  }
+  __syncthreads();
+  // stage B + split
+  const int j0 = t == 0 ? 0 : t, j1 = t == 0 ? 8 : 16 - t;
+  R2 z0[8], z1[8];
+  if (active) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      z0[r] = a.ld(l, j0 + 16 * r);
+      z1[r] = a.ld(l, j1 + 16 * r);
+      if (r > 0) {
+        z0[r] = cmul(z0[r], twB[16 * r + j0]);
+        z1[r] = cmul(z1[r], twB[16 * r + j1]);
+      }
+    }
+    DFT<8, R2>::run(z0);
+    DFT<8, R2>::run(z1);
+  }
+  __syncthreads();
+  if (active) {
+    if (t == 0) {
+      // butterfly 0: Z[16 r] pairs with Z[16 (8 - r)]; tasks 0, 16, 32, 48, 64
+      split_task<M, R, R2>(ao, l, 0, z0[0], z0[0], twp[0], scale);
+#pragma unroll
+      for (int r = 1; r <= 4; ++r) split_task<M, R, R2>(ao, l, 16 * r, z0[r], z0[8 - r], twp[16 * r], scale);
+      // butterfly 8: Z[8 + 16 r] pairs with Z[8 + 16 (7 - r)]; tasks 8, 24, 40, 56
+#pragma unroll
+      for (int r = 0; r < 4; ++r) split_task<M, R, R2>(ao, l, 8 + 16 * r, z1[r], z1[7 - r], twp[8 + 16 * r], scale);
+    } else {
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        split_task<M, R, R2>(ao, l, j0 + 16 * r, z0[r], z1[7 - r], twp[j0 + 16 * r], scale);
+        split_task<M, R, R2>(ao, l, j1 + 16 * r, z1[r], z0[7 - r], twp[j1 + 16 * r], scale);
+      }
+    }
+  }
+  __syncthreads();
+}
+
 // The rest of the transform after fft_stages: for M = 128 the last Stockham
 // stage fused with the even/odd split, otherwise the split alone; outputs to
 // `ao` (may alias `a`).
@@ -460,7 +576,7 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
   using R2 = typename Cplx<R>::T;
   if (skip && *skip) return;
   constexpr int N = 2 * M, TPL = M / 8;
-  constexpr int TL = FFTPlan<M>::table_len();
+  constexpr int TL = FFTPlan<M>::rows_table_len();
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
   constexpr int PPITCH = 2 * (M + M / 8);
   constexpr bool ADD = Cons::kAddBulk;
@@ -551,7 +667,7 @@ __global__ void __launch_bounds__(256, 2) k_dht_rows_pipe(const R* __restrict__ 
   static_assert(!ADD || sizeof(R) == sizeof(double), "p is FP64");
   if (skip && *skip) return;
   constexpr int N = 2 * M, TPL = M / 8;
-  constexpr int TL = FFTPlan<M>::table_len();
+  constexpr int TL = FFTPlan<M>::rows_table_len();
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
   constexpr int PPITCH = 2 * (M + M / 8);
   constexpr int EPT = 16;  // elements per thread of a full tile: lpc * N = (2048 / M) * 2M = 4096 over 256 threads
@@ -696,8 +812,8 @@ __device__ __forceinline__ ZColumnFactor z_column_factor(const SpectralParams& s
 // its even/odd split writes the divided spectrum in FP64 over the whole
 // buffer (all reads before a barrier, all writes after it); the inverse runs
 // in FP64 and the tile is stored in FP64. tw_in_g: the FP32 table.
-template <int M, typename R, int AXIS, bool DIVIDE, int W, int NB, typename RIN = R>
-__global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_constant__ CUtensorMap map_in,
+template <int M, typename R, int AXIS, bool DIVIDE, int W, int NB, typename RIN = R, bool T8 = false>
+__global__ void __launch_bounds__(W * (T8 ? 8 : M / 8)) k_dht_cols_pipe(const __grid_constant__ CUtensorMap map_in,
                                                        const __grid_constant__ CUtensorMap map_out, int ntiles_x,
                                                        int ntiles, const typename Cplx<R>::T* tw_g,
                                                        const typename Cplx<RIN>::T* tw_in_g, SpectralParams sp,
@@ -706,8 +822,9 @@ __global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_cons
   using RI2 = typename Cplx<RIN>::T;
   static_assert(NB >= 2, "need at least two tile buffers");
   static_assert(sizeof(RIN) <= sizeof(R), "input may only be narrower than the transform type");
+  static_assert(!T8 || M == 128, "the 8-thread plan is for 256-long lines");
   if (skip && *skip) return;
-  constexpr int N = 2 * M, TPL = M / 8;
+  constexpr int N = 2 * M, TPL = T8 ? 8 : M / 8;
   constexpr int TL = FFTPlan<M>::table_len();
   constexpr bool WIDEN = sizeof(RIN) < sizeof(R);
   constexpr uint32_t TILE_BYTES = (uint32_t)(N * W * sizeof(RIN));
@@ -763,7 +880,24 @@ __global__ void __launch_bounds__(W * (M / 8)) k_dht_cols_pipe(const __grid_cons
     coords(i, x0, other);
     R* tile = tiles + (size_t)b * N * W;
     ColLines<R> A{tile, W};
-    if constexpr (WIDEN) {
+    if constexpr (T8) {
+      if constexpr (WIDEN) {
+        ColLines<RIN> An{reinterpret_cast<RIN*>(reinterpret_cast<unsigned char*>(tile) +
+                                                (size_t)N * W * (sizeof(R) - sizeof(RIN))),
+                         W};
+        if constexpr (DIVIDE) {
+          dht128_t8_to<RIN>(An, A, tw_in, l, t, active, z_column_factor(sp, x0 + l, other));
+          dht128_t8_to<R>(A, A, tw, l, t, active, NoScale());
+        } else {
+          dht128_t8_to<RIN>(An, A, tw_in, l, t, active, NoScale());
+        }
+      } else if constexpr (DIVIDE) {
+        dht128_t8_to<R>(A, A, tw, l, t, active, z_column_factor(sp, x0 + l, other));
+        dht128_t8_to<R>(A, A, tw, l, t, active, NoScale());
+      } else {
+        dht128_t8_to<R>(A, A, tw, l, t, active, NoScale());
+      }
+    } else if constexpr (WIDEN) {
       ColLines<RIN> An{reinterpret_cast<RIN*>(reinterpret_cast<unsigned char*>(tile) +
                                               (size_t)N * W * (sizeof(R) - sizeof(RIN))),
                        W};
