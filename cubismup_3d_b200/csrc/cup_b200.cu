@@ -675,7 +675,7 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   // 256-long FP32 lines: the 8-thread plan (radix 16, then radix 8 fused with the
   // split); measured slower than the 16-thread plan for FP64 tiles (fewer CTAs fit)
   constexpr bool T8 = M == 128;
-  constexpr int N = 2 * M, TPL = T8 ? 8 : M / 8, NB = (T8 && sizeof(R) == 8) ? 2 : 3;
+  constexpr int N = 2 * M, TPL = T8 ? 8 : M / 8, NB = T8 ? 2 : 3;
   constexpr int W = sizeof(R) == 4 ? 32 : 16;
   if (H->nx % W) return fail(H, CUP_ERR_ARG, "nx must be a multiple of %d for this precision", W);
   CUtensorMap map_in, map_out;
