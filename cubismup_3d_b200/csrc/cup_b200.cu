@@ -603,7 +603,8 @@ int launch_rows_M(cup_handle* H, const char* name, const Prod& prod, const Cons&
   const size_t scratch = Prod::kBulk ? 0 : 32 * 20 * sizeof(double);
   const size_t smem = (size_t)lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
                       (Cons::kAddBulk ? (size_t)lpc * N * sizeof(double) : 0) +
-                      FFTPlan<M>::rows_table_len() * sizeof(typename Cplx<R>::T) + 16 + scratch + 128;
+                      FFTPlan<M>::rows_table_len() * sizeof(typename Cplx<R>::T) + 16 +
+                      (Cons::kAddBulk ? 8 * sizeof(double) : 0) + scratch + 128;
   auto kern = k_dht_rows<M, R, Prod, Cons>;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, lpc * TPL, &bpsm);
@@ -630,11 +631,10 @@ int launch_rows(cup_handle* H, const char* name, const Prod& prod, const Cons& c
   return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
 }
 
-// Pipelined x pass (k_dht_rows_pipe): rows of `in` transformed into `out`,
-// or with ADD added to p (minus cmean). FP32: three tile buffers; FP64: two.
-template <int M, typename R, bool ADD>
-int launch_rows_pipe_M(cup_handle* H, const char* name, const R* in, R* out, double* p, const double* cmean,
-                       const int* skip) {
+// Pipelined x pass (k_dht_rows_pipe): rows of `in` transformed into `out`.
+// FP32: three tile buffers; FP64: two.
+template <int M, typename R>
+int launch_rows_pipe_M(cup_handle* H, const char* name, const R* in, R* out, const int* skip) {
   constexpr int N = 2 * M, TPL = M / 8;
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
   constexpr int NB = sizeof(R) == 4 ? 3 : 2;
@@ -642,29 +642,29 @@ int launch_rows_pipe_M(cup_handle* H, const char* name, const R* in, R* out, dou
   const int nrows = H->ny * H->nz;
   const size_t smem = (size_t)NB * lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
                       FFTPlan<M>::rows_table_len() * sizeof(typename Cplx<R>::T) + NB * sizeof(uint64_t) + 128;
-  auto kern = k_dht_rows_pipe<M, R, ADD, NB>;
+  auto kern = k_dht_rows_pipe<M, R, NB>;
+  const int threads = lpc * TPL;
   int bpsm = 0;
-  int rc = prepare_kernel(H, kern, smem, 256, &bpsm);
+  int rc = prepare_kernel(H, kern, smem, threads, &bpsm);
   if (rc) return rc;
   const int ntiles = (nrows + lpc - 1) / lpc;
   const int grid = std::min(ntiles, bpsm * H->num_sms);
   return launch_named(H, name, [&]() -> int {
-    kern<<<grid, 256, smem, H->stream>>>(in, out, p, cmean, H->ny, nrows, lpc, table<R>(H, 0), H->derr, skip);
+    kern<<<grid, threads, smem, H->stream>>>(in, out, nrows, lpc, table<R>(H, 0), H->derr, skip);
     CKL();
     return CUP_OK;
   });
 }
 
-template <typename R, bool ADD>
-int launch_rows_pipe(cup_handle* H, const char* name, const R* in, R* out, double* p, const double* cmean,
-                     const int* skip) {
+template <typename R>
+int launch_rows_pipe(cup_handle* H, const char* name, const R* in, R* out, const int* skip) {
   switch (H->nx / 2) {
-    case 8: return launch_rows_pipe_M<8, R, ADD>(H, name, in, out, p, cmean, skip);
-    case 16: return launch_rows_pipe_M<16, R, ADD>(H, name, in, out, p, cmean, skip);
-    case 32: return launch_rows_pipe_M<32, R, ADD>(H, name, in, out, p, cmean, skip);
-    case 64: return launch_rows_pipe_M<64, R, ADD>(H, name, in, out, p, cmean, skip);
-    case 128: return launch_rows_pipe_M<128, R, ADD>(H, name, in, out, p, cmean, skip);
-    case 256: return launch_rows_pipe_M<256, R, ADD>(H, name, in, out, p, cmean, skip);
+    case 8: return launch_rows_pipe_M<8, R>(H, name, in, out, skip);
+    case 16: return launch_rows_pipe_M<16, R>(H, name, in, out, skip);
+    case 32: return launch_rows_pipe_M<32, R>(H, name, in, out, skip);
+    case 64: return launch_rows_pipe_M<64, R>(H, name, in, out, skip);
+    case 128: return launch_rows_pipe_M<128, R>(H, name, in, out, skip);
+    case 256: return launch_rows_pipe_M<256, R>(H, name, in, out, skip);
   }
   return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
 }
@@ -741,7 +741,7 @@ int fft_middle(cup_handle* H, R* work, const int* skip) {
 // by about 1e-7 whatever its spectrum.
 int dc_correction_solve(cup_handle* H, double* p, const int* skip) {
   int rc;
-  if ((rc = launch_rows_pipe<float, false>(H, "dht_x", H->work32, H->work32, nullptr, nullptr, skip))) return rc;
+  if ((rc = launch_rows_pipe<float>(H, "dht_x", H->work32, H->work32, skip))) return rc;
   if ((rc = launch_cols<float, 1, false>(H, H->work32, H->work32, skip))) return rc;
   if ((rc = launch_cols<double, 2, true, float>(H, H->work32, H->work64, skip))) return rc;
   if ((rc = launch_cols<double, 1, false>(H, H->work64, H->work64, skip))) return rc;
@@ -754,9 +754,9 @@ int dc_correction_solve(cup_handle* H, double* p, const int* skip) {
 template <typename R>
 int fft_poisson(cup_handle* H, R* work, R* out, const int* skip = nullptr) {
   int rc;
-  if ((rc = launch_rows_pipe<R, false>(H, "dht_x", work, work, nullptr, nullptr, skip))) return rc;
+  if ((rc = launch_rows_pipe<R>(H, "dht_x", work, work, skip))) return rc;
   if ((rc = fft_middle<R>(H, work, skip))) return rc;
-  return launch_rows_pipe<R, false>(H, "dht_x", work, out, nullptr, nullptr, skip);
+  return launch_rows_pipe<R>(H, "dht_x", work, out, skip);
 }
 
 int box_grid(const Box& b) {
@@ -1086,7 +1086,7 @@ int do_poisson_fused_fp64(cup_handle* H, DtArg dt) {
   RowsRhs<T> prod{(const T*)H->u, (const T*)H->v, (const T*)H->w, dt, H->h, H->nx, H->ny, H->nz};
   if ((rc = launch_rows<double>(H, "rhs_dht_x", prod, RowsToArray<double>{H->rhs}, nullptr))) return rc;
   if ((rc = fft_middle<double>(H, H->rhs, nullptr))) return rc;
-  return launch_rows_pipe<double, false>(H, "dht_x", H->rhs, H->p, nullptr, nullptr, nullptr);
+  return launch_rows_pipe<double>(H, "dht_x", H->rhs, H->p, nullptr);
 }
 
 // Poisson solve of the RHS array (operator-by-operator path, obstacles).
@@ -1233,7 +1233,7 @@ int do_project_fields(cup_handle* H, void* const* in, void* const* out, double* 
   RowsRhs<T> prod{(const T*)in[0], (const T*)in[1], (const T*)in[2], dt, H->h, H->nx, H->ny, H->nz};
   if ((rc = launch_rows<double>(H, "adjoint_rhs_dht_x", prod, RowsToArray<double>{H->rhs}, nullptr))) return rc;
   if ((rc = fft_middle<double>(H, H->rhs, nullptr))) return rc;
-  if ((rc = launch_rows_pipe<double, false>(H, "adjoint_dht_x", H->rhs, pbuf, nullptr, nullptr, nullptr))) return rc;
+  if ((rc = launch_rows_pipe<double>(H, "adjoint_dht_x", H->rhs, pbuf, nullptr))) return rc;
   const void* pf[1] = {pbuf};
   OpGradP<T> op{(const T*)in[0], (const T*)in[1], (const T*)in[2], (T*)out[0], (T*)out[1], (T*)out[2],
                 partial(H, P_GRAD), dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, H->box, 0, H->nx, H->ny, H->nz};

@@ -311,8 +311,12 @@ __device__ __forceinline__ void split_task(const AccO& ao, int l, int k, R2 A, R
     }
     ao.str(l, k, hk);
     ao.str(l, N - k, hNk);
-    ao.str(l, M - k, hMk);
-    ao.str(l, M + k, hMpk);
+    // k = M/2: M - k = k and M + k = N - k (same values); write each index
+    // once, so that an accumulating accessor adds it once
+    if (2 * k != M) {
+      ao.str(l, M - k, hMk);
+      ao.str(l, M + k, hMpk);
+    }
   }
 }
 
@@ -437,9 +441,11 @@ __device__ __forceinline__ void fft_stages(const Acc& a, const P& pad, const typ
 //      and does their split tasks in registers.
 // Meant for column tiles (ColLines), where stage A's 16-strided writes fall in
 // different columns across a warp. `ao` may alias `a` (see dht_post_to).
-template <typename R, class Acc, class AccO, class Scale>
-__device__ __forceinline__ void dht128_t8_to(const Acc& a, const AccO& ao, const typename Cplx<R>::T* tw, int l,
-                                             int t, bool active, const Scale& scale) {
+// Stage A writes to `pa` and stage B reads from it (column tiles: `a` itself).
+template <typename R, class Acc, class PAcc, class AccO, class Scale>
+__device__ __forceinline__ void dht128_t8_to(const Acc& a, const PAcc& pa, const AccO& ao,
+                                             const typename Cplx<R>::T* tw, int l, int t, bool active,
+                                             const Scale& scale) {
   using R2 = typename Cplx<R>::T;
   using Pl = FFTPlan<128>;
   constexpr int M = 128;
@@ -455,7 +461,7 @@ __device__ __forceinline__ void dht128_t8_to(const Acc& a, const AccO& ao, const
   __syncthreads();
   if (active) {
 #pragma unroll
-    for (int r = 0; r < 16; ++r) a.st(l, 16 * t + r, v[r]);
+    for (int r = 0; r < 16; ++r) pa.st(l, 16 * t + r, v[r]);
   }
   __syncthreads();
   // stage B + split
@@ -464,8 +470,8 @@ __device__ __forceinline__ void dht128_t8_to(const Acc& a, const AccO& ao, const
   if (active) {
 #pragma unroll
     for (int r = 0; r < 8; ++r) {
-      z0[r] = a.ld(l, j0 + 16 * r);
-      z1[r] = a.ld(l, j1 + 16 * r);
+      z0[r] = pa.ld(l, j0 + 16 * r);
+      z1[r] = pa.ld(l, j1 + 16 * r);
       if (r > 0) {
         z0[r] = cmul(z0[r], twB[16 * r + j0]);
         z1[r] = cmul(z1[r], twB[16 * r + j1]);
@@ -552,7 +558,8 @@ struct RowsToArray {
 
 // Consumer of the last x pass of a correction solve: p += rows - (parity-class
 // means of p measured by the preceding residual pass), in FP64. The p rows
-// arrive by bulk copy with the input rows and leave by one bulk store.
+// arrive by bulk copy with the input rows and leave by one bulk store; the
+// transform's last step adds into them directly (AddToPRows).
 struct RowsAddToP {
   static constexpr bool kBulk = false;
   static constexpr bool kAddBulk = true;
@@ -560,13 +567,20 @@ struct RowsAddToP {
   const double* cmean;
   int log2ny;  // ny is a power of two: row r is (y, z) = (r & (ny-1), r >> log2ny)
   __device__ double* rows_of(int row0, int N) const { return p + (size_t)row0 * N; }
-  __device__ void add(double* ps, const double* rows, int row0, int nr, int N) const {
-    for (int i = threadIdx.x; i < nr * N; i += blockDim.x) {
-      const int l = i / N, x = i - l * N;
-      const int r = row0 + l;
-      const int cls = (x & 1) | ((r & 1) << 1) | (((r >> log2ny) & 1) << 2);
-      ps[i] = ps[i] + rows[i] - cmean[cls];
-    }
+};
+
+// Output accessor of the transform's last step for RowsAddToP: element n of
+// line l is added to the shared-memory p row, minus the class mean of p.
+struct AddToPRows {
+  using elem = double;
+  double* prow;
+  const double* cm;  // the 8 class means (shared memory)
+  int N, row0, log2ny;
+  __device__ __forceinline__ void str(int l, int n, double v) const {
+    const int r = row0 + l;
+    const int cls = (n & 1) | ((r & 1) << 1) | (((r >> log2ny) & 1) << 2);
+    double* q = prow + l * N + n;
+    *q = *q + v - cm[cls];
   }
 };
 
@@ -587,7 +601,8 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
   double* prow = reinterpret_cast<double*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));  // lpc * N (ADD)
   R2* tw = reinterpret_cast<R2*>(prow + (ADD ? (size_t)lpc * N : 0));
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
-  double* scratch = reinterpret_cast<double*>(bar + 1);            // 32 * 20 doubles
+  double* cms = reinterpret_cast<double*>(bar + 1);                // 8 class means (ADD)
+  double* scratch = cms + (ADD ? 8 : 0);                           // 32 * 20 doubles (computing producers)
   const int row0 = blockIdx.x * lpc;
   const int nr = min(lpc, nrows - row0);
   if (nr <= 0) return;
@@ -608,6 +623,8 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
       bulk_load(rows, prod.src(row0, N), bytes, bar);
       if constexpr (ADD) bulk_load(prow, cons.rows_of(row0, N), pbytes, bar);
     }
+    if constexpr (ADD)
+      if (threadIdx.x < 8) cms[threadIdx.x] = cons.cmean[threadIdx.x];
     load_table(tw, tw_g, TL);
     const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
     if (!ok) return;
@@ -621,10 +638,14 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
   const bool active = l < nr;
   RowLines<R> A{rows, N};
   RowLinesPad<R> P{padb, PPITCH};
-  dht_lines<M, PAD, R>(A, P, tw, l, t, active);
+  if constexpr (ADD) {
+    fft_stages<M, PAD, R>(A, P, tw, l, t, active);
+    dht_tail_to<M, R>(A, AddToPRows{prow, cms, N, row0, cons.log2ny}, tw, l, t, active, NoScale());
+  } else {
+    dht_lines<M, PAD, R>(A, P, tw, l, t, active);
+  }
   if constexpr (Cons::kBulk || ADD) {
     if constexpr (ADD) {
-      cons.add(prow, rows, row0, nr, N);
       fence_proxy_async_smem();
       __syncthreads();
       if (threadIdx.x == 0) {
@@ -651,26 +672,20 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
 // (tile i of a CTA: rows (blockIdx.x + i gridDim.x) lpc ...) through NB
 // shared-memory buffers. The 1-D bulk loads of the next NB-1 tiles and the
 // bulk store of the previous tile overlap the transform of the current one;
-// the twiddle table is loaded once per CTA.
-// ADD (last pass of a correction solve, R = double): the transformed rows are
-// added to p minus the parity-class means of p measured by the preceding
-// residual pass, p += rows - cmean; the p values of a tile are loaded into
-// registers before its transform (their latency hides behind it) and written
-// back with coalesced stores, so the tile needs no second buffer.
-template <int M, typename R, bool ADD, int NB>
-__global__ void __launch_bounds__(256, 2) k_dht_rows_pipe(const R* __restrict__ in, R* __restrict__ out,
-                                                       double* __restrict__ p, const double* __restrict__ cmean,
-                                                       int ny, int nrows, int lpc,
-                                                       const typename Cplx<R>::T* tw_g, int* err, const int* skip) {
+// the twiddle table is loaded once per CTA. (The 8-thread plan of the column
+// passes measured slower on rows: 16-strided stage-A writes need a padded
+// buffer and fewer threads share a row tile.)
+template <int M, typename R, int NB>
+__global__ void __launch_bounds__(256, 2) k_dht_rows_pipe(const R* __restrict__ in, R* __restrict__ out, int nrows,
+                                                          int lpc, const typename Cplx<R>::T* tw_g, int* err,
+                                                          const int* skip) {
   using R2 = typename Cplx<R>::T;
   static_assert(NB >= 2, "need at least two tile buffers");
-  static_assert(!ADD || sizeof(R) == sizeof(double), "p is FP64");
   if (skip && *skip) return;
   constexpr int N = 2 * M, TPL = M / 8;
   constexpr int TL = FFTPlan<M>::rows_table_len();
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
   constexpr int PPITCH = 2 * (M + M / 8);
-  constexpr int EPT = 16;  // elements per thread of a full tile: lpc * N = (2048 / M) * 2M = 4096 over 256 threads
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
   R* bufs = reinterpret_cast<R*>(smem_raw);                 // NB * lpc * N
@@ -701,11 +716,6 @@ __global__ void __launch_bounds__(256, 2) k_dht_rows_pipe(const R* __restrict__ 
   if (tid == 0)
     for (; issued < min(NB - 1, my); ++issued) issue(issued);
   load_table(tw, tw_g, TL);
-  double cm[8];
-  if constexpr (ADD) {
-#pragma unroll
-    for (int c = 0; c < 8; ++c) cm[c] = cmean[c];
-  }
   __syncthreads();
   const int l = tid / TPL, t = tid % TPL;
   RowLinesPad<R> P{padb, PPITCH};
@@ -713,46 +723,24 @@ __global__ void __launch_bounds__(256, 2) k_dht_rows_pipe(const R* __restrict__ 
   int done = 0;
   for (int i = 0; i < my; ++i) {
     // refill: tile i + NB - 1 goes into the buffer of tile i - 1, once its
-    // store has read it (ADD: once every thread is past its add loop)
+    // store has read it
     if (tid == 0 && ok && issued < my) {
-      if constexpr (!ADD) bulk_wait_read<0>();
+      bulk_wait_read<0>();
       issue(issued++);
     }
     int row0, nr;
     rows_of(i, row0, nr);
-    double pv[ADD ? EPT : 1];
-    if constexpr (ADD) {
-#pragma unroll
-      for (int k = 0; k < EPT; ++k) {
-        const int e = tid + k * 256;
-        pv[k] = e < nr * N ? p[(size_t)row0 * N + e] : 0.0;
-      }
-    }
     const int b = i % NB;
     ok = __syncthreads_and(ok && mbar_wait(&bar[b], (i / NB) & 1, err));
     if (!ok) break;
     R* rows = bufs + (size_t)b * lpc * N;
     RowLines<R> A{rows, N};
     dht_lines<M, PAD, R>(A, P, tw, l, t, l < nr);
-    if constexpr (ADD) {
-#pragma unroll
-      for (int k = 0; k < EPT; ++k) {
-        const int e = tid + k * 256;
-        if (e < nr * N) {
-          const int rl = e / N, x = e - rl * N;
-          const int r = row0 + rl, y = r % ny, z = r / ny;
-          const int cls = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
-          p[(size_t)row0 * N + e] = pv[k] + (double)rows[e] - cm[cls];
-        }
-      }
-      __syncthreads();
-    } else {
-      fence_proxy_async_smem();
-      __syncthreads();
-      if (tid == 0) {
-        bulk_store(out + (size_t)row0 * N, rows, (uint32_t)((size_t)nr * N * sizeof(R)));
-        bulk_commit();
-      }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      bulk_store(out + (size_t)row0 * N, rows, (uint32_t)((size_t)nr * N * sizeof(R)));
+      bulk_commit();
     }
     done = i + 1;
   }
@@ -886,16 +874,16 @@ __global__ void __launch_bounds__(W * (T8 ? 8 : M / 8)) k_dht_cols_pipe(const __
                                                 (size_t)N * W * (sizeof(R) - sizeof(RIN))),
                          W};
         if constexpr (DIVIDE) {
-          dht128_t8_to<RIN>(An, A, tw_in, l, t, active, z_column_factor(sp, x0 + l, other));
-          dht128_t8_to<R>(A, A, tw, l, t, active, NoScale());
+          dht128_t8_to<RIN>(An, An, A, tw_in, l, t, active, z_column_factor(sp, x0 + l, other));
+          dht128_t8_to<R>(A, A, A, tw, l, t, active, NoScale());
         } else {
-          dht128_t8_to<RIN>(An, A, tw_in, l, t, active, NoScale());
+          dht128_t8_to<RIN>(An, An, A, tw_in, l, t, active, NoScale());
         }
       } else if constexpr (DIVIDE) {
-        dht128_t8_to<R>(A, A, tw, l, t, active, z_column_factor(sp, x0 + l, other));
-        dht128_t8_to<R>(A, A, tw, l, t, active, NoScale());
+        dht128_t8_to<R>(A, A, A, tw, l, t, active, z_column_factor(sp, x0 + l, other));
+        dht128_t8_to<R>(A, A, A, tw, l, t, active, NoScale());
       } else {
-        dht128_t8_to<R>(A, A, tw, l, t, active, NoScale());
+        dht128_t8_to<R>(A, A, A, tw, l, t, active, NoScale());
       }
     } else if constexpr (WIDEN) {
       ColLines<RIN> An{reinterpret_cast<RIN*>(reinterpret_cast<unsigned char*>(tile) +
