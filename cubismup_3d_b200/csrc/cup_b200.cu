@@ -857,12 +857,12 @@ int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* con
 // depth and pairs per thread measured best at 256^3: stage 1 126 us
 // (TY 8, NS 3, 2 pairs), stage 2 152 us (TY 4, NS 3, 1 pair).
 int upwind_stage1_f32(cup_handle* H, const char* name, void* const* in, void* const* out, DtArg dt) {
-  if (H->ny % 8 == 0 && 4 * H->nx <= 512 * 2) return launch_advect_f2<false, 8, 3, 2>(H, name, in, in, out, dt);
+  if (H->ny % 8 == 0 && 4 * H->nx <= 512 * 2) return launch_advect_f2<false, 8, 4, 2>(H, name, in, in, out, dt);
   return launch_advect_f2<false, 4, 4, 1>(H, name, in, in, out, dt);
 }
 int upwind_stage2_f32(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out,
                       DtArg dt) {
-  return launch_advect_f2<true, 4, 3, 1>(H, name, in, base, out, dt);
+  return launch_advect_f2<true, 4, 4, 1>(H, name, in, base, out, dt);
 }
 
 template <typename T>
@@ -1025,7 +1025,7 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt) {
         return rc;
     }
     if ((rc = dc_correction_solve(H, W, conv))) return rc;
-    if ((rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 3, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
+    if ((rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
                                                      &H->n_grad_partials, k > 1 ? conv : nullptr,
                                                      k == 1 ? order : -1, H->p_old, unew)))
       return rc;
