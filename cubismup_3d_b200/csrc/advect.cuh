@@ -235,15 +235,28 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
             }
           }
         }
-        __syncthreads();  // slot s fully consumed
-        if (tid == 0 && ok && q_issued < L && q_issued == q + NS) issue(q_issued++);
+        // rings of 4+ slots: one block barrier per two planes (slots of loads
+        // q-1 and q fully consumed, refill both; PL is even, so a pair never
+        // straddles items); shallower rings keep one barrier per plane
+        if constexpr (NS >= 4) {
+          if (q & 1) {
+            __syncthreads();
+            if (tid == 0 && ok)
+              for (int r = q - 1 + NS; r <= q + NS && r < L; ++r)
+                if (r == q_issued) issue(q_issued++);
+          }
+        } else {
+          __syncthreads();  // slot s fully consumed
+          if (tid == 0 && ok && q_issued < L && q_issued == q + NS) issue(q_issued++);
+        }
         ++q;
       }
     }
   }
   if (!ok && tid == 0) {
-    // bounded drain of this CTA's loads still in flight
-    for (int r = q - NS < 0 ? 0 : q - NS; r < q_issued; ++r) mbar_wait(&full[r % NS], (r / NS) & 1, nullptr);
+    // bounded drain of this CTA's loads still in flight (at most the last NS issued)
+    for (int r = q_issued - NS < 0 ? 0 : q_issued - NS; r < q_issued; ++r)
+      mbar_wait(&full[r % NS], (r / NS) & 1, nullptr);
   }
 }
 
