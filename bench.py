@@ -67,8 +67,8 @@ def kernel_bytes(name: str, fp32: bool) -> float:
 # of an ncu capture of the 256^3 FP32-DC step, profiles/step_fp32dc_upwind3_256_kernels_full.md),
 # scaled by the cells of the run; traffic grows with the cells streamed.
 MEASURED_DRAM_BYTES_PER_CELL_FP32DC = {
-    "grad_p_check": 55.3, "upwind3_stage1": 23.3, "upwind3_stage2": 34.9, "rhs_residual": 30.5,
-    "dht_x_update_p": 21.5, "dht_z_solve_mixed": 8.7, "dht_y_f64": 12.5, "dht_x": 4.8, "dht_y": 4.5,
+    "grad_p_check": 55.3, "upwind3_stage1": 23.4, "upwind3_stage2": 35.1, "rhs_residual": 30.8,
+    "dht_x_update_p": 21.4, "dht_z_solve_mixed": 8.5, "dht_y_f64": 12.8, "dht_x": 4.6, "dht_y": 4.6,
 }
 
 
