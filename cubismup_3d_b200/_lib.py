@@ -117,6 +117,10 @@ SIGNATURES = {
     "cup_dc_history": (C.c_int, [_H, _dp, C.c_int, C.POINTER(C.c_int)]),
     "cup_profile_enable": (C.c_int, [_H, C.c_int]),
     "cup_profile_report": (C.c_int, [_H, C.c_char_p, C.c_size_t, C.c_int]),
+    "cup_adjoint_step_obstacle": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                            C.c_void_p, C.c_void_p, _dp, C.c_void_p, C.c_void_p]),
+    "cup_set_chi": (C.c_int, [_H, C.c_void_p, C.c_int]),
+    "cup_set_sphere_velocity": (C.c_int, [_H, _dp]),
     "cup_launch_count": (C.c_int, [_H, C.POINTER(C.c_longlong)]),
 }
 

@@ -16,7 +16,11 @@ for n steps and checkpoint interval K, so long rollouts fit in HBM.
 The fixed-dt convention makes the rollout a smooth function of u0 except where
 an upwind switch flips sign; the adjoint freezes the switch at the forward
 state (the derivative from either side at a kink is the one-sided one).
-Obstacles are not supported by the adjoint.
+With the sphere, ``obstacle_gradients`` gives the gradients of
+J = <g, u_T> + sum over steps of w . F_n (F_n the penalization force of step n,
+e.g. w = (1/n, 0, 0) for the time-averaged drag) with respect to the initial
+velocity, the characteristic function chi and the sphere's target velocity
+(``cup_adjoint_step_obstacle``), with the same checkpointing.
 """
 from __future__ import annotations
 
@@ -73,6 +77,47 @@ class Rollout(torch.autograd.Function):
         _set_clock(sim, *ctx.end_clock)
         ctx.ckpts = None
         return lam.to(ctx.in_dtype), None, None, None
+
+
+def obstacle_gradients(sim: Simulation, u0: torch.Tensor, dts: Sequence[float], w_force, grad_uT=None,
+                       checkpoint_every: int = 8):
+    """Gradients of J = <grad_uT, u_T> + sum_n w_force . F_n over ``len(dts)``
+    steps of ``sim`` (which has the sphere) from ``u0`` (3, nz, ny, nx):
+    returns (dJ/du0, dJ/dchi, dJ/dU) as CUDA tensors (storage dtype, FP64 of the
+    grid's shape, FP64 of 3), plus the list of forces F_n of the forward."""
+    if not sim.obstacles:
+        raise ValueError("obstacle_gradients: the simulation has no obstacle")
+    K = int(checkpoint_every)
+    if K < 1:
+        raise ValueError("checkpoint_every must be >= 1")
+    dts = [float(d) for d in dts]
+    n = len(dts)
+    sim.bind_torch_stream()
+    clock = (sim.step, sim.time)
+    sim.set_velocity_raw(u0.detach().to(sim.storage_dtype).contiguous())
+    ckpts, forces = [], []
+    for s, dt in enumerate(dts):
+        if s % K == 0:
+            ckpts.append(sim.velocity_raw())
+        forces.append(sim.timestep(dt).force.copy())
+    end_clock = (sim.step, sim.time)
+    dev = u0.device
+    lam = (torch.zeros((3,) + sim.shape, dtype=sim.storage_dtype, device=dev) if grad_uT is None
+           else grad_uT.detach().to(sim.storage_dtype).contiguous().clone())
+    g_chi = torch.zeros(sim.shape, dtype=torch.float64, device=dev)
+    g_vel = torch.zeros(3, dtype=torch.float64, device=dev)
+    for seg in reversed(range(len(ckpts))):
+        s0, s1 = seg * K, min(n, seg * K + K)
+        _set_clock(sim, clock[0] + s0, clock[1] + sum(dts[:s0]))
+        sim.set_velocity_raw(ckpts[seg])
+        states = [ckpts[seg]]
+        for s in range(s0, s1 - 1):
+            sim.timestep(dts[s], stats=False)
+            states.append(sim.velocity_raw())
+        for s in reversed(range(s0, s1)):
+            sim.adjoint_step_obstacle(states[s - s0], dts[s], lam, w_force, g_chi, g_vel)
+    _set_clock(sim, *end_clock)
+    return lam, g_chi, g_vel, forces
 
 
 def _set_clock(sim: Simulation, step: int, time: float):

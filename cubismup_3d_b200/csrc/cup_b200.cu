@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "adjoint.cuh"
+#include "adjoint_obstacle.cuh"
 #include "advect.cuh"
 #include "advect_f2.cuh"
 #include "common.cuh"
@@ -42,6 +43,7 @@ struct DevState {
   double cmean[8];  // parity-class means of p (the 8 null-mode components)
   double rmean[8];  // parity-class means of the first residual (the RHS's null parts)
   double res_hist[16];  // relative residual at each check of the last solve
+  double adj_sq;        // obstacle adjoint: sum over the corrected surface cells of b1 q
   int step, n_solves, converged;
   int n_unconverged;  // steps whose defect correction missed the tolerance (cumulative)
   long long solves_total;  // correction solves of all decided defect corrections (cumulative)
@@ -443,6 +445,10 @@ struct cup_handle {
   // discrete adjoint scratch (allocated on the first adjoint call)
   void *au = nullptr, *av = nullptr, *aw = nullptr;
   double* p_adj = nullptr;
+  // obstacle adjoint scratch: the velocity before penalization u** (T) and the
+  // RHS before its obstacle terms b0 (FP64), recomputed per adjoint step
+  void *aus = nullptr, *avs = nullptr, *aws = nullptr;
+  double* ab0 = nullptr;
   // launch accounting and optional per-kernel CUDA-event profiling
   long long launches = 0;
   bool prof_on = false;
@@ -895,13 +901,17 @@ int do_advect_diffuse(cup_handle* H, DtArg dt) {
 }
 
 template <typename T>
-int do_pressure_rhs(cup_handle* H, DtArg dt) {
+int do_pressure_rhs(cup_handle* H, DtArg dt, void* const* fields = nullptr, double* save_b0 = nullptr) {
   int rc;
   const void* uvw[3] = {H->u, H->v, H->w};
+  if (fields)
+    for (int q = 0; q < 3; ++q) uvw[q] = fields[q];
   OpPressureRHS<T> op{H->rhs, dt, H->h, H->nx, H->ny};
   if (H->fp32) rc = launch_stream<T, 3, 1, 8, 4>(H, "pressure_rhs", uvw, op);
   else rc = launch_stream<T, 3, 1, 4, 4>(H, "pressure_rhs", uvw, op);
   if (rc) return rc;
+  // the RHS before its obstacle terms (the obstacle adjoint linearises them there)
+  if (save_b0) CK(cudaMemcpyAsync(save_b0, H->rhs, H->n * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
   if (H->has_sphere) {
     const int gb = box_grid(H->box);
     {
@@ -1228,17 +1238,29 @@ int launch_adjoint(cup_handle* H, const char* name, const void* const* f, const 
 // is the wide-stencil Laplacian the spectral factor inverts, so P is
 // symmetric: the adjoint of the projection is P itself.
 template <typename T>
-int do_project_fields(cup_handle* H, void* const* in, void* const* out, double* pbuf, DtArg dt) {
+int do_solve_rhs_of(cup_handle* H, void* const* in, double* pbuf, DtArg dt) {
   int rc;
   RowsRhs<T> prod{(const T*)in[0], (const T*)in[1], (const T*)in[2], dt, H->h, H->nx, H->ny, H->nz};
   if ((rc = launch_rows<double>(H, "adjoint_rhs_dht_x", prod, RowsToArray<double>{H->rhs}, nullptr))) return rc;
   if ((rc = fft_middle<double>(H, H->rhs, nullptr))) return rc;
-  if ((rc = launch_rows_pipe<double>(H, "adjoint_dht_x", H->rhs, pbuf, nullptr))) return rc;
+  return launch_rows_pipe<double>(H, "adjoint_dht_x", H->rhs, pbuf, nullptr);
+}
+
+// out = in - dt/(2h) grad_c p (KernelGradP on given fields; out may equal in).
+template <typename T>
+int do_grad_fields(cup_handle* H, const char* name, void* const* in, void* const* out, const double* pbuf, DtArg dt) {
   const void* pf[1] = {pbuf};
   OpGradP<T> op{(const T*)in[0], (const T*)in[1], (const T*)in[2], (T*)out[0], (T*)out[1], (T*)out[2],
                 partial(H, P_GRAD), dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, H->box, 0, H->nx, H->ny, H->nz};
   int ngp = 0;
-  return launch_stream<double, 1, 1, 4, 4>(H, "adjoint_grad_p", pf, op, &ngp);
+  return launch_stream<double, 1, 1, 4, 4>(H, name, pf, op, &ngp);
+}
+
+template <typename T>
+int do_project_fields(cup_handle* H, void* const* in, void* const* out, double* pbuf, DtArg dt) {
+  int rc;
+  if ((rc = do_solve_rhs_of<T>(H, in, pbuf, dt))) return rc;
+  return do_grad_fields<T>(H, "adjoint_grad_p", in, out, pbuf, dt);
 }
 
 // Adjoint of one step u_{n+1} = P(H(u_n)) with the dt given, at the state un:
@@ -1264,6 +1286,90 @@ int do_adjoint_step(cup_handle* H, void* const* un, void* const* lam, DtArg dt) 
     return launch_adjoint<T, 1, true, 2, 3, 1>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
   } else {
     if ((rc = launch_advect<T, 1, 4, 3, 2>(H, "adjoint_recompute_stage1", un, un, st1, dt))) return rc;
+    if ((rc = launch_adjoint<T, 1, false, 2, 2, 1>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt))) return rc;
+    return launch_adjoint<T, 1, true, 2, 2, 1>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
+  }
+}
+
+// Adjoint of one step with the sphere (penalization, its force and the
+// obstacle terms of the RHS; adjoint_obstacle.cuh): lam (dJ/du_{n+1}) becomes
+// dJ/du_n for J = <g, u_T> + sum_n wF . F_n, and dJ/dchi, dJ/dU (the sphere's
+// penalization target velocity) are added to g_chi, g_vel. The step is
+// recomputed from un up to the velocity before penalization (projection by
+// the FP64 FFT solve), then
+//   lam** = Pen^T lam (- force term),  q = L^+ RHS(lam**),  q' = M^T q,
+//   lam* = lam** - dt/(2h) grad_c q',  then the advection transposes.
+template <typename T>
+int do_adjoint_step_obstacle(cup_handle* H, void* const* un, void* const* lam, DtArg dt, const double* wF,
+                             double* g_chi, double* g_vel) {
+  constexpr bool F32 = std::is_same<T, float>::value;
+  int rc;
+  void* mu[3] = {H->au, H->av, H->aw};
+  void* us[3] = {H->aus, H->avs, H->aws};
+  void* st1[3] = {H->u1, H->v1, H->w1};
+  const double dtv = dt.host;
+  // 1. forward recompute: advection, RHS with its obstacle terms, solve, gradient
+  if (H->cfg.scheme == CUP_SCHEME_REF) {
+    if constexpr (F32) rc = launch_advect<T, 0, 8, 5, 4>(H, "adjoint_recompute_ref", un, un, us, dt);
+    else rc = launch_advect<T, 0, 4, 5, 2>(H, "adjoint_recompute_ref", un, un, us, dt);
+    if (rc) return rc;
+  } else if constexpr (F32) {
+    if ((rc = upwind_stage1_f32(H, "adjoint_recompute_stage1", un, st1, dt))) return rc;
+    if ((rc = upwind_stage2_f32(H, "adjoint_recompute_stage2", st1, un, us, dt))) return rc;
+  } else {
+    if ((rc = launch_advect<T, 1, 4, 3, 2>(H, "adjoint_recompute_stage1", un, un, st1, dt))) return rc;
+    if ((rc = launch_advect<T, 2, 2, 4, 1>(H, "adjoint_recompute_stage2", st1, un, us, dt))) return rc;
+  }
+  if ((rc = do_pressure_rhs<T>(H, dt, us, H->ab0))) return rc;
+  if ((rc = fft_poisson<double>(H, H->rhs, H->p_adj))) return rc;
+  if ((rc = do_grad_fields<T>(H, "adjoint_recompute_grad_p", us, us, H->p_adj, dt))) return rc;
+  // 2. penalization and force
+  const int gb = box_grid(H->box);
+  const double lambda = H->cfg.DLM > 0 ? H->cfg.DLM / dtv : H->lambda;
+  {
+    int rc_ = launch_named(H, "adjoint_penalize", [&]() -> int {
+      k_adj_penalize<T><<<gb, kBoxThreads, 0, H->stream>>>(
+          (T*)lam[0], (T*)lam[1], (T*)lam[2], (const T*)us[0], (const T*)us[1], (const T*)us[2], (const T*)H->chi,
+          H->sp_dev, H->box, H->nx, H->ny, H->nz, H->h, dtv, lambda, H->cfg.bImplicitPenalization, wF[0], wF[1],
+          wF[2], g_chi, partial(H, P_PEN));
+      CKL();
+      k_adj_accumulate<<<1, 256, 0, H->stream>>>(partial(H, P_PEN), gb, 3, 3, g_vel);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  // 3. projection with the transposed obstacle RHS terms
+  if ((rc = do_solve_rhs_of<T>(H, lam, H->p_adj, dt))) return rc;
+  const double kappa = dtv * dtv / (H->h * H->h * H->h);  // dJ/db2 = kappa q
+  {
+    int rc_ = launch_named(H, "adjoint_rhs_obstacle", [&]() -> int {
+      CK(cudaMemsetAsync(&H->dstate->adj_sq, 0, sizeof(double), H->stream));
+      k_adj_rhs_sum<T><<<gb, kBoxThreads, 0, H->stream>>>(H->p_adj, H->ab0, (const T*)H->chi, H->box, H->nx, H->ny,
+                                                         H->nz, H->dstate->rhs_sums, &H->dstate->corr,
+                                                         partial(H, P_RHSOB));
+      CKL();
+      k_adj_accumulate<<<1, 256, 0, H->stream>>>(partial(H, P_RHSOB), gb, 1, 1, &H->dstate->adj_sq);
+      CKL();
+      k_adj_rhs_apply<T><<<gb, kBoxThreads, 0, H->stream>>>(H->p_adj, H->ab0, (const T*)H->chi, H->box, H->nx,
+                                                           H->ny, H->nz, H->dstate->rhs_sums, &H->dstate->corr,
+                                                           &H->dstate->adj_sq, kappa, g_chi);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  // 4. gradient correction, then the advection transposes
+  if (H->cfg.scheme == CUP_SCHEME_REF) {
+    if ((rc = do_grad_fields<T>(H, "adjoint_grad_p", lam, mu, H->p_adj, dt))) return rc;
+    if constexpr (F32) return launch_adjoint<T, 0, false, 4, 3, 2>(H, "adjoint_ref", un, mu, nullptr, lam, 0.0, 1.0, dt);
+    else return launch_adjoint<T, 0, false, 2, 3, 1>(H, "adjoint_ref", un, mu, nullptr, lam, 0.0, 1.0, dt);
+  }
+  if ((rc = do_grad_fields<T>(H, "adjoint_grad_p", lam, lam, H->p_adj, dt))) return rc;
+  if constexpr (F32) {
+    if ((rc = launch_adjoint<T, 1, false, 2, 3, 1>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt))) return rc;
+    return launch_adjoint<T, 1, true, 2, 3, 1>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
+  } else {
     if ((rc = launch_adjoint<T, 1, false, 2, 2, 1>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt))) return rc;
     return launch_adjoint<T, 1, true, 2, 2, 1>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
   }
@@ -1446,6 +1552,8 @@ int cup_destroy(cup_handle* H) {
   if (!H) return CUP_OK;
   cudaSetDevice(H->dev);
   if (H->stream) cudaStreamSynchronize(H->stream);
+  for (void* f : {H->aus, H->avs, H->aws, (void*)H->ab0})
+    if (f) cudaFree(f);
   for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->au, H->av, H->aw, (void*)H->p_adj,
                   H->chi, (void*)H->p, (void*)H->p_old, (void*)H->p_pred, (void*)H->rhs,
                   (void*)H->work32, (void*)H->work64, (void*)H->partials, (void*)H->dstate, (void*)H->derr, (void*)H->cosx,
@@ -1844,12 +1952,9 @@ static int alloc_adjoint(cup_handle* H) {
   return CUP_OK;
 }
 
-int cup_adjoint_step(cup_handle* H, const void* un, const void* vn, const void* wn, double dt, void* lu, void* lv,
-                     void* lw) {
-  REQUIRE_H(H);
-  if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
+static int check_adjoint_fields(cup_handle* H, const void* un, const void* vn, const void* wn, void* lu, void* lv,
+                                void* lw) {
   if (!un || !vn || !wn || !lu || !lv || !lw) return fail(H, CUP_ERR_ARG, "null field pointer");
-  if (H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_adjoint_step: the handle has an obstacle");
   const void* st[3] = {un, vn, wn};
   const void* lm[3] = {lu, lv, lw};
   for (int a = 0; a < 3; ++a)
@@ -1857,11 +1962,58 @@ int cup_adjoint_step(cup_handle* H, const void* un, const void* vn, const void* 
       if (st[a] == lm[b]) return fail(H, CUP_ERR_ARG, "the state and the adjoint fields must not alias");
       if (a < b && (lm[a] == lm[b] || st[a] == st[b])) return fail(H, CUP_ERR_ARG, "field pointers must be distinct");
     }
-  int rc = alloc_adjoint(H);
+  return CUP_OK;
+}
+
+int cup_adjoint_step(cup_handle* H, const void* un, const void* vn, const void* wn, double dt, void* lu, void* lv,
+                     void* lw) {
+  REQUIRE_H(H);
+  if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
+  if (H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_adjoint_step: the handle has an obstacle (use cup_adjoint_step_obstacle)");
+  int rc = check_adjoint_fields(H, un, vn, wn, lu, lv, lw);
+  if (!rc) rc = alloc_adjoint(H);
   if (rc) return rc;
   void* s3[3] = {const_cast<void*>(un), const_cast<void*>(vn), const_cast<void*>(wn)};
   void* l3[3] = {lu, lv, lw};
   return DISPATCH_T(H, do_adjoint_step, s3, l3, DtArg{dt, nullptr});
+}
+
+int cup_adjoint_step_obstacle(cup_handle* H, const void* un, const void* vn, const void* wn, double dt, void* lu,
+                              void* lv, void* lw, const double w_force[3], double* g_chi, double* g_vel) {
+  REQUIRE_H(H);
+  if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
+  if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_adjoint_step_obstacle: the handle has no obstacle");
+  if (!w_force || !g_chi || !g_vel) return fail(H, CUP_ERR_ARG, "null w_force / g_chi / g_vel");
+  int rc = check_adjoint_fields(H, un, vn, wn, lu, lv, lw);
+  if (!rc) rc = alloc_adjoint(H);
+  if (rc) return rc;
+  if (!H->ab0) {
+    const size_t es = H->fp32 ? sizeof(float) : sizeof(double);
+    for (void** f : {&H->aus, &H->avs, &H->aws}) CK(cudaMalloc(f, H->n * es));
+    CK(cudaMalloc(&H->ab0, H->n * sizeof(double)));
+  }
+  void* s3[3] = {const_cast<void*>(un), const_cast<void*>(vn), const_cast<void*>(wn)};
+  void* l3[3] = {lu, lv, lw};
+  const double wF[3] = {w_force[0], w_force[1], w_force[2]};
+  return DISPATCH_T(H, do_adjoint_step_obstacle, s3, l3, DtArg{dt, nullptr}, wF, g_chi, g_vel);
+}
+
+int cup_set_chi(cup_handle* H, const double* chi, int where) {
+  REQUIRE_H(H);
+  if (!H->has_sphere || !H->chi) return fail(H, CUP_ERR_ARG, "cup_set_chi: the handle has no obstacle");
+  if (!chi || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad chi arguments");
+  return DISPATCH_T(H, set_field, H->chi, chi, where);
+}
+
+int cup_set_sphere_velocity(cup_handle* H, const double vel[3]) {
+  REQUIRE_H(H);
+  if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_set_sphere_velocity: the handle has no obstacle");
+  if (!vel) return fail(H, CUP_ERR_ARG, "null velocity");
+  // SphereParams::transVel only (the device copy is read by every penalization)
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(H->sp_dev) + offsetof(SphereParams, transVel), vel, 3 * sizeof(double),
+                     cudaMemcpyHostToDevice, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  return CUP_OK;
 }
 
 int cup_get_velocity_raw(cup_handle* H, void* u, void* v, void* w) {

@@ -398,6 +398,36 @@ class Simulation:
         L.check(L.lib().cup_adjoint_step(self._h, *[C.c_void_p(state[i].data_ptr()) for i in range(3)], float(dt),
                                          *[C.c_void_p(lam[i].data_ptr()) for i in range(3)]), self._h, "adjoint_step")
 
+    def adjoint_step_obstacle(self, state, dt: float, lam, w_force, g_chi, g_vel):
+        """Discrete adjoint of ``timestep(dt)`` of a handle with the sphere, taken
+        from ``state``, for J = <g, u_T> + sum over steps of w_force . F (F the
+        penalization force): ``lam`` becomes dJ/du before the step (in place);
+        dJ/dchi is added to ``g_chi`` (FP64 CUDA tensor of the grid's shape) and
+        dJ/dU for the sphere's target velocity (uinf fixed) to ``g_vel`` (3 FP64)."""
+        import torch
+        self._check_raw(state, "adjoint_step_obstacle state")
+        self._check_raw(lam, "adjoint_step_obstacle lam")
+        for t, shape, what in ((g_chi, self.shape, "g_chi"), (g_vel, (3,), "g_vel")):
+            if not _is_torch_cuda(t) or t.dtype != torch.float64 or not t.is_contiguous() or tuple(t.shape) != shape:
+                raise ValueError(f"adjoint_step_obstacle: {what} must be a contiguous FP64 CUDA tensor of shape {shape}")
+        self.bind_torch_stream()
+        w = (C.c_double * 3)(*[float(x) for x in w_force])
+        L.check(L.lib().cup_adjoint_step_obstacle(self._h, *[C.c_void_p(state[i].data_ptr()) for i in range(3)],
+                                                  float(dt), *[C.c_void_p(lam[i].data_ptr()) for i in range(3)], w,
+                                                  C.c_void_p(g_chi.data_ptr()), C.c_void_p(g_vel.data_ptr())),
+                self._h, "adjoint_step_obstacle")
+
+    def set_chi(self, chi):
+        """Replaces the obstacle's characteristic function (host array of the
+        grid's shape; only the obstacle's active box is read by the step)."""
+        a = _as_host_f64(chi, self.shape)
+        L.check(L.lib().cup_set_chi(self._h, _ptr(a), L.CUP_WHERE_HOST), self._h, "set_chi")
+
+    def set_sphere_velocity(self, vel):
+        """Sets the sphere's penalization target velocity (uinf unchanged)."""
+        v = (C.c_double * 3)(*[float(x) for x in vel])
+        L.check(L.lib().cup_set_sphere_velocity(self._h, v), self._h, "set_sphere_velocity")
+
     def _get1(self, fn, what) -> np.ndarray:
         out = np.empty(self.shape, dtype=np.float64)
         L.check(fn(self._h, _ptr(out), L.CUP_WHERE_HOST), self._h, what)

@@ -173,6 +173,25 @@ int cup_run(struct cup_handle* h, int nsteps, cup_step_stats* stats);
  * Handles with an obstacle return CUP_ERR_ARG. Stream-ordered, no host sync. */
 int cup_adjoint_step(struct cup_handle* h, const void* un, const void* vn, const void* wn, double dt, void* lu,
                      void* lv, void* lw);
+/* Discrete adjoint of one cup_step of a handle with the sphere (no counterpart
+ * in the reference): the same transposes as cup_adjoint_step plus those of the
+ * Brinkman penalization (Penalization.cpp:40-98), of its force (:101-123) and of
+ * the obstacle terms of the pressure RHS (PressureRHS.cpp:78-112, 215-256,
+ * 322-343), for J = <g, u_T> + sum over steps of w_force . F_n (F_n the
+ * penalization force of step n). un..lw as in cup_adjoint_step; w_force: 3 host
+ * doubles; g_chi (device, nx*ny*nz doubles) += dJ/dchi on the obstacle's active
+ * box (the derivative from the chi >= 0 side); g_vel (device, 3 doubles) +=
+ * dJ/dU for the sphere's penalization target velocity U with uinf held fixed.
+ * The step is recomputed from un (projection by the FP64 FFT solve); the surface
+ * set and the sign of the RHS correction are frozen at it. Stream-ordered. */
+int cup_adjoint_step_obstacle(struct cup_handle* h, const void* un, const void* vn, const void* wn, double dt,
+                              void* lu, void* lv, void* lw, const double w_force[3], double* g_chi, double* g_vel);
+/* Replaces the obstacle's characteristic function (FP64, nx*ny*nz; only cells in
+ * the obstacle's active box are read by the step). The centre of mass is kept. */
+int cup_set_chi(struct cup_handle* h, const double* chi, int where);
+/* Sets the sphere's penalization target velocity (transVel) without touching
+ * uinf. */
+int cup_set_sphere_velocity(struct cup_handle* h, const double vel[3]);
 /* Device-to-device copies of the handle's velocity in its storage type (for
  * checkpoints): get copies out to u, v, w; set copies in. Stream-ordered. */
 int cup_get_velocity_raw(struct cup_handle* h, void* u, void* v, void* w);

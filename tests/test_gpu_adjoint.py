@@ -239,3 +239,119 @@ def test_adjoint_rollout_taylor_green_128(oracle):
     tlm = float(((uT - tgt_np) * tl).sum())
     assert abs(float((grads["fp64"] * d0).sum()) - tlm) <= 1e-9 * abs(tlm)
     assert abs(float((grads["fp32"] * d0).sum()) - tlm) <= 1e-4 * abs(tlm)
+
+
+# ---- obstacle: penalization, its force and the RHS obstacle terms ----------
+
+# off the grid's symmetry planes: a cell whose central chi differences cancel by
+# symmetry is not a surface cell, and any perturbation would make it one (the
+# RHS surface set is piecewise constant in chi)
+OBST_SPHERE = dict(radius=0.25, position=(0.52, 0.49, 0.505), enforcedVelocity=(1.0, 0.0, 0.0),
+                   bForcedInSimFrame=(True, True, True), bFixFrameOfRef=(True, True, True))
+
+
+def make_obstacle_sim(precision="fp64", scheme="ref"):
+    import cubismup_3d_b200 as cup
+    sd = cup.SimulationData(CFL=0.1, cells=(32, 16, 16))
+    sd.extent, sd.nu, sd.rampup, sd.DLM, sd.lambda_ = 2.0, 2e-3, 0, 0.0, 1e6
+    sd.bImplicitPenalization, sd.precision, sd.scheme = True, precision, scheme
+    sim = cup.Simulation(sd)
+    sim.add_obstacle(cup.Sphere(**OBST_SPHERE))
+    return sim
+
+
+def obstacle_case(sim, seed=5):
+    import torch
+    from cubismup_3d_b200.initial_conditions import random_solenoidal
+    u = random_solenoidal(sim.shape[::-1], seed, lambda k: k ** 2 * np.exp(-(k / 2.0) ** 2), rms=0.3)
+    u0 = to_dev(u, torch.float64)
+    rng = np.random.default_rng(seed + 1)
+    g = to_dev([rng.standard_normal(sim.shape) for _ in range(3)], torch.float64)
+    return u0, g
+
+
+def obstacle_loss(sim, u0, g, dts, w, chi=None, vel=None):
+    import torch
+    if chi is not None:
+        sim.set_chi(chi)
+    if vel is not None:
+        sim.set_sphere_velocity(vel)
+    sim.set_velocity_raw(u0.to(sim.storage_dtype).contiguous())
+    J = 0.0
+    for dt in dts:
+        J += float(np.dot(w, sim.timestep(dt).force))
+    uT = sim.velocity_raw().double()
+    return J + float((uT * g).sum())
+
+
+def test_obstacle_adjoint_vs_central_differences():
+    """dJ/du0, dJ/dchi (8 random directions on the cells of the smoothed
+    interface, 0 < chi < 1) and dJ/dU of J = <g, u_T> + time-averaged drag over
+    4 steps, FP64, against central finite differences of the GPU forward."""
+    import torch
+    from cubismup_3d_b200.adjoint import obstacle_gradients
+    sim = make_obstacle_sim()
+    u0, g = obstacle_case(sim)
+    dts = [0.01] * 4
+    w = np.array([1.0 / len(dts), 0.0, 0.0])
+    chi0 = sim.chi()
+    vel0 = np.array(OBST_SPHERE["enforcedVelocity"])
+    lam, g_chi, g_vel, forces = obstacle_gradients(sim, u0, dts, w, grad_uT=g, checkpoint_every=2)
+    assert abs(forces[-1][0]) > 0
+    g_u0 = lam.double().cpu().numpy()
+    g_chi = g_chi.cpu().numpy()
+    g_vel = g_vel.cpu().numpy()
+    rng = np.random.default_rng(11)
+    # initial velocity
+    d = rng.standard_normal((3,) + sim.shape)
+    eps = 1e-6  # the white-noise direction makes the rollout strongly nonlinear
+    dd = torch.from_numpy(d).cuda()
+    fd = (obstacle_loss(sim, u0 + eps * dd, g, dts, w, chi0, vel0) -
+          obstacle_loss(sim, u0 - eps * dd, g, dts, w, chi0, vel0)) / (2 * eps)
+    ad = float(np.sum(g_u0 * d))
+    assert abs(fd - ad) <= 1e-6 * abs(ad) + 1e-9, ("u0", fd, ad)
+    # characteristic function: directions on the interface cells (inside the
+    # body, chi = 1 and b1 = 0: the surface set changes with the sign of a
+    # perturbation there, a kink)
+    body = (chi0 > 1e-3) & (chi0 < 1 - 1e-3)
+    for k in range(8):
+        dc = np.where(body, rng.standard_normal(sim.shape), 0.0)
+        e = 1e-6
+        fd = (obstacle_loss(sim, u0, g, dts, w, chi0 + e * dc, vel0) -
+              obstacle_loss(sim, u0, g, dts, w, chi0 - e * dc, vel0)) / (2 * e)
+        ad = float(np.sum(g_chi * dc))
+        assert abs(fd - ad) <= 1e-5 * abs(ad) + 1e-9, ("chi", k, fd, ad)
+    # target velocity (x)
+    e = 1e-6
+    fd = (obstacle_loss(sim, u0, g, dts, w, chi0, vel0 + [e, 0, 0]) -
+          obstacle_loss(sim, u0, g, dts, w, chi0, vel0 - [e, 0, 0])) / (2 * e)
+    assert abs(fd - g_vel[0]) <= 1e-5 * abs(g_vel[0]) + 1e-9, ("U", fd, g_vel[0])
+
+
+def test_obstacle_adjoint_fp32_tracks_fp64():
+    """The FP32-storage obstacle adjoint against the FP64 one (same gradients to
+    FP32 accuracy)."""
+    from cubismup_3d_b200.adjoint import obstacle_gradients
+    dts = [0.01] * 3
+    w = np.array([1.0 / len(dts), 0.0, 0.0])
+    out = {}
+    for prec in ("fp64", "fp32_dc"):
+        sim = make_obstacle_sim(prec)
+        u0, g = obstacle_case(sim)
+        lam, g_chi, g_vel, _ = obstacle_gradients(sim, u0, dts, w, grad_uT=g, checkpoint_every=2)
+        out[prec] = (lam.double().cpu().numpy(), g_chi.cpu().numpy(), g_vel.cpu().numpy())
+        sim.close()
+    for a, b in zip(out["fp32_dc"], out["fp64"]):
+        assert rel_l2(a, b) < 1e-3, rel_l2(a, b)
+
+
+def test_obstacle_adjoint_argument_checks():
+    import torch
+    sim = make_obstacle_sim()
+    z = torch.zeros((3,) + sim.shape, dtype=torch.float64, device="cuda")
+    lam = torch.zeros_like(z)
+    with pytest.raises(ValueError):
+        sim.adjoint_step(z, 0.01, lam)  # the plain adjoint refuses a handle with an obstacle
+    with pytest.raises(ValueError):
+        sim.adjoint_step_obstacle(z, 0.01, lam, (1, 0, 0), torch.zeros(3, device="cuda"),
+                                  torch.zeros(3, dtype=torch.float64, device="cuda"))
