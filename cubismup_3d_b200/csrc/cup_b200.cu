@@ -44,6 +44,7 @@ struct DevState {
   double rmean[8];  // parity-class means of the first residual (the RHS's null parts)
   double res_hist[16];  // relative residual at each check of the last solve
   double adj_sq;        // obstacle adjoint: sum over the corrected surface cells of b1 q
+  int err_word;         // device error word (kDevErr* bits), read back with the state
   int step, n_solves, converged;
   int n_unconverged;  // steps whose defect correction missed the tolerance (cumulative)
   long long solves_total;  // correction solves of all decided defect corrections (cumulative)
@@ -92,7 +93,9 @@ __global__ void k_finalize_max(const double* partials, int np, DevState* st) {
 }
 
 // Simulation::calcMaxTimestep (source/Simulation.cpp:403-424) on the device.
-__global__ void k_calc_dt(DevState* st, double h, double nu, double CFL, int rampup, double DLM) {
+// step >= 0: the host's step counter, stored first (the ramp-up reads it).
+__global__ void k_calc_dt(DevState* st, double h, double nu, double CFL, int rampup, double DLM, int step = -1) {
+  if (step >= 0) st->step = step;
   const double hMin = h;
   const double dtDif = hMin * hMin / nu;
   const double dtAdv = hMin / (st->umax + 1e-8);
@@ -778,18 +781,23 @@ void reset_pressure_history(cup_handle* H) {
   H->pred_ready = false;
 }
 
-int check_dev_error(cup_handle* H) {
-  int e = 0;
-  CK(cudaMemcpy(&e, H->derr, sizeof(int), cudaMemcpyDeviceToHost));
+int dev_error_status(cup_handle* H, int e) {
   if (e & kDevErrMbarTimeout) return fail(H, CUP_ERR_TIMEOUT, "device wait timed out (mbarrier)");
   if (e & kDevErrBulkTimeout) return fail(H, CUP_ERR_TIMEOUT, "device wait timed out (bulk store)");
   return CUP_OK;
 }
 
+int check_dev_error(cup_handle* H) {
+  int e = 0;
+  CK(cudaMemcpy(&e, H->derr, sizeof(int), cudaMemcpyDeviceToHost));
+  return dev_error_status(H, e);
+}
+
+// One stream-ordered read of the device state (the error word included).
 int read_state(cup_handle* H) {
   CK(cudaMemcpyAsync(H->hstate, H->dstate, sizeof(DevState), cudaMemcpyDeviceToHost, H->stream));
   CK(cudaStreamSynchronize(H->stream));
-  return check_dev_error(H);
+  return dev_error_status(H, H->hstate->err_word);
 }
 
 // ---- typed pipeline pieces -------------------------------------------------
@@ -1507,8 +1515,7 @@ int cup_create(const cup_config* cfg, cup_handle** out) {
     CK(cudaMalloc(&H->partials, sizeof(double) * kPartialCap * P_COUNT));
     CK(cudaMalloc(&H->dstate, sizeof(DevState)));
     CK(cudaMemsetAsync(H->dstate, 0, sizeof(DevState), H->stream));
-    CK(cudaMalloc(&H->derr, sizeof(int)));
-    CK(cudaMemsetAsync(H->derr, 0, sizeof(int), H->stream));
+    H->derr = &H->dstate->err_word;  // zeroed with the state
     CK(cudaMallocHost(&H->hstate, sizeof(DevState)));
     // FFT tables per axis, spectral cosines exactly as PoissonSolverPeriodic::_solve
     // computes them (source/poisson/PoissonSolverPeriodic.cpp:23-33).
@@ -1556,7 +1563,7 @@ int cup_destroy(cup_handle* H) {
     if (f) cudaFree(f);
   for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->au, H->av, H->aw, (void*)H->p_adj,
                   H->chi, (void*)H->p, (void*)H->p_old, (void*)H->p_pred, (void*)H->rhs,
-                  (void*)H->work32, (void*)H->work64, (void*)H->partials, (void*)H->dstate, (void*)H->derr, (void*)H->cosx,
+                  (void*)H->work32, (void*)H->work64, (void*)H->partials, (void*)H->dstate, (void*)H->cosx,
                   (void*)H->cosy, (void*)H->cosz, (void*)H->sp_dev})
     if (f) cudaFree(f);
   for (int d = 0; d < 3; ++d) {
@@ -1798,11 +1805,10 @@ int cup_calc_max_timestep(cup_handle* H, double* dt) {
     if ((rc = DISPATCH_T(H, do_max_u))) return rc;
     H->umax_fresh = true;
   }
-  // the device keeps its own step counter in sync with the host mirror
-  CK(cudaMemcpyAsync(&H->dstate->step, &H->step, sizeof(int), cudaMemcpyHostToDevice, H->stream));
   {
+    // the device keeps its own step counter in sync with the host mirror
     int rc_ = launch_named(H, "calc_dt", [&]() -> int {
-      k_calc_dt<<<1, 1, 0, H->stream>>>(H->dstate, H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM);
+      k_calc_dt<<<1, 1, 0, H->stream>>>(H->dstate, H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM, H->step);
       CKL();
       return CUP_OK;
     });
