@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
 #pragma unroll
       for (int jj = 0; jj < U; ++jj) {
         const int j = j0 + jj;
+        if (j >= PL) break;  // items of PL planes, PL not a multiple of U (zc = 8)
         const int s = q % NS;
         if (ok) ok = mbar_wait(&full[s], (q / NS) & 1, err);
         if (ok) {

@@ -836,8 +836,11 @@ int launch_advect(cup_handle* H, const char* name, void* const* in, void* const*
 
 // Launches one packed-FP32 upwind3 stage (k_advect_zq_f2): `in` stencil
 // fields, `base` the stage-2 point-wise u^n, `out` the result.
+// zmax: z planes per work item (at most; nz when smaller): a tall tile (TY 8)
+// uses 8 so that the items spread evenly over the SMs.
 template <bool STAGE2, int TY, int NS, int PPT>
-int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out, DtArg dt) {
+int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out, DtArg dt,
+                     int zmax = 16) {
   constexpr int G = 2;
   const int pairs = TY * H->nx / 2;
   if (pairs % PPT || pairs / PPT > 512 || H->ny % TY) return fail(H, CUP_ERR_ARG, "advection tile does not fit the grid");
@@ -849,7 +852,7 @@ int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* con
                            H->nx, TY, 1);
     if (rc) return rc;
   }
-  const int zc = std::min(16, H->nz);
+  const int zc = std::min(zmax, H->nz);
   StreamGeom g{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
   const size_t smem = advect_smem_bytes<float, STAGE2 ? 2 : 1, TY, NS, 1>(H->nx) + 128;
   auto kern = k_advect_zq_f2<STAGE2, TY, NS, PPT>;
@@ -871,7 +874,7 @@ int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* con
 // depth and pairs per thread measured best at 256^3: stage 1 126 us
 // (TY 8, NS 3, 2 pairs), stage 2 152 us (TY 4, NS 3, 1 pair).
 int upwind_stage1_f32(cup_handle* H, const char* name, void* const* in, void* const* out, DtArg dt) {
-  if (H->ny % 8 == 0 && 4 * H->nx <= 512 * 2) return launch_advect_f2<false, 8, 4, 2>(H, name, in, in, out, dt);
+  if (H->ny % 8 == 0 && 4 * H->nx <= 512 * 2) return launch_advect_f2<false, 8, 4, 2>(H, name, in, in, out, dt, 8);
   return launch_advect_f2<false, 4, 4, 1>(H, name, in, in, out, dt);
 }
 int upwind_stage2_f32(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out,
