@@ -989,7 +989,7 @@ int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, co
   const int grid = std::min(geo.n_items, bpsm * H->num_sms);
   if (grid > kPartialCap / pzq_partials_per_cta<MODE>())
     return fail(H, CUP_ERR_ARG, "too many CTAs for the partial buffers");
-  PzqParams prm{dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, pred_order, pred_out};
+  PzqParams prm{dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, pred_order, pred_out, H->box};
   T* o[3] = {nullptr, nullptr, nullptr};
   if (out)
     for (int q = 0; q < 3; ++q) o[q] = (T*)out[q];
@@ -1026,15 +1026,17 @@ int launch_finalize_residual(cup_handle* H, const double* partials, int stride, 
 // solves) turns every later kernel of the loop into an exit at entry, so the
 // loop needs no host round trip. Only the first gradient pass writes the next
 // step's warm start.
+// rhs_given: b (with the obstacle terms) is already in H->rhs; check 0 reads it.
 template <typename T>
-int do_pressure_dc_zq(cup_handle* H, DtArg dt) {
+int do_pressure_dc_zq(cup_handle* H, DtArg dt, bool rhs_given = false) {
   const int max_iter = dc_max_iter(H);
   const int* conv = &H->dstate->converged;
   double* W = H->p_pred;  // this step's pressure, starting from the warm start
   if (!H->pred_ready) CK(cudaMemcpyAsync(W, H->p, H->n * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
   int rc, grid = 0;
-  if ((rc = launch_pzq<T, PZQ_RHS_RES, 4, 4, 2>(H, "rhs_residual", W, partial(H, P_RES), nullptr, dt, &grid, nullptr)))
-    return rc;
+  if (rhs_given) rc = launch_pzq<T, PZQ_RES0, 4, 4, 2>(H, "dc_residual0", W, partial(H, P_RES), nullptr, dt, &grid, nullptr);
+  else rc = launch_pzq<T, PZQ_RHS_RES, 4, 4, 2>(H, "rhs_residual", W, partial(H, P_RES), nullptr, dt, &grid, nullptr);
+  if (rc) return rc;
   if ((rc = launch_finalize_residual(H, partial(H, P_RES), 18, grid, 0))) return rc;
   const int order = std::min(H->p_valid, 1);  // valid levels among (p) before this step
   void* unew[3] = {H->tu, H->tv, H->tw};      // u^n is dead after the advection stages
@@ -1046,10 +1048,15 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt) {
         return rc;
     }
     if ((rc = dc_correction_solve(H, W, conv))) return rc;
-    if ((rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
-                                                     &H->n_grad_partials, k > 1 ? conv : nullptr,
-                                                     k == 1 ? order : -1, H->p_old, unew)))
-      return rc;
+    const int* skip = k > 1 ? conv : nullptr;
+    const int pred = k == 1 ? order : -1;
+    if (H->has_sphere)
+      rc = launch_pzq<T, PZQ_GRAD_CHECK_BOX, 4, 4, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
+                                                      &H->n_grad_partials, skip, pred, H->p_old, unew);
+    else
+      rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
+                                                  &H->n_grad_partials, skip, pred, H->p_old, unew);
+    if (rc) return rc;
     if ((rc = launch_finalize_residual(H, partial(H, P_GRAD), kGradStride, H->n_grad_partials, k))) return rc;
   }
   H->grad_stride = kGradStride;
@@ -1181,8 +1188,12 @@ template <typename T>
 int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance) {
   int rc;
   if ((rc = do_advect_diffuse<T>(H, dt))) return rc;
-  if (H->has_sphere) {
-    // the obstacle terms need global sums over the RHS first: unfused path
+  if (H->has_sphere && H->fp32) {
+    // the obstacle terms need global sums over the RHS first: RHS pass, then
+    // the z-queue defect correction on the given RHS
+    if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
+    if ((rc = do_pressure_dc_zq<T>(H, dt, true))) return rc;
+  } else if (H->has_sphere) {
     if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
     if ((rc = do_poisson(H))) return rc;
   } else if (H->fp32) {
@@ -1191,7 +1202,7 @@ int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance) {
   } else {
     if ((rc = do_poisson_fused_fp64<T>(H, dt))) return rc;
   }
-  if (H->has_sphere || !H->fp32) {
+  if (!H->fp32) {
     if ((rc = do_grad<T>(H, dt))) return rc;
   }
   if ((rc = do_penalize<T>(H, dt, lambda_dev))) return rc;

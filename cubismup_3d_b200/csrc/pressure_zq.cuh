@@ -5,6 +5,8 @@
 //              in one pass: b to HBM in FP64, r in FP32 for the FFT solve.
 //   RES        r = b - h/4 L_2h p before a further correction solve, minus the
 //              class means of b (its null-mode part), in FP32.
+//   RES0       check 0 on a given b (the RHS with its obstacle terms, which need
+//              global sums first): RES's loads, RHS_RES's outputs.
 //   GRAD_CHECK KernelGradP (source/operators/PressureProjection.cpp:38-50) on
 //              u* with the current p, written to a separate buffer so that it
 //              can be redone, fused with the residual check of that p (the
@@ -38,7 +40,14 @@
 
 namespace cup {
 
-enum { PZQ_RHS_RES = 0, PZQ_RES = 1, PZQ_GRAD_CHECK = 2 };
+// GRAD_CHECK_BOX: GRAD_CHECK with an obstacle (the max |u + uinf| leaves out
+// the obstacle's box, which the penalization pass covers)
+enum { PZQ_RHS_RES = 0, PZQ_RES = 1, PZQ_GRAD_CHECK = 2, PZQ_RES0 = 3, PZQ_GRAD_CHECK_BOX = 4 };
+
+template <int MODE>
+constexpr bool pzq_grad() {
+  return MODE == PZQ_GRAD_CHECK || MODE == PZQ_GRAD_CHECK_BOX;
+}
 
 struct PzqMaps {
   CUtensorMap p_main, p_halo;  // FP64 p: box {nx, TY, 1} and {nx, 2, 1}
@@ -51,7 +60,7 @@ struct PzqMaps {
 // Values per CTA in the partial-sum buffer.
 template <int MODE>
 constexpr int pzq_partials_per_cta() {
-  return MODE == 2 ? 20 : 18;
+  return pzq_grad<MODE>() ? 20 : 18;
 }
 
 struct PzqParams {
@@ -63,6 +72,7 @@ struct PzqParams {
   // warm start is not written)
   int pred_order;
   double* pred_out;
+  Box box;  // GRAD_CHECK_BOX: the obstacle's box
 };
 
 // Byte layout of one ring slot (all parts multiples of 64 B for nx >= 16).
@@ -83,7 +93,7 @@ struct PzqSlot {
   __host__ __device__ static size_t h_off(int nx) { return f_off(nx, 3); }
   __host__ __device__ static size_t bytes(int nx) {
     size_t s = MODE == PZQ_RHS_RES ? w_off(nx) + (size_t)TY * nx * sizeof(T)
-               : MODE == PZQ_RES   ? b_off(nx) + (size_t)TY * nx * sizeof(double)
+               : (MODE == PZQ_RES || MODE == PZQ_RES0) ? b_off(nx) + (size_t)TY * nx * sizeof(double)
                                    : h_off(nx) + (size_t)TY * nx * sizeof(double);
     return (s + 127) / 128 * 128;
   }
@@ -147,7 +157,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     if constexpr (MODE == PZQ_RHS_RES) {
       if (xy_plane) bytes += rowsT + (uint32_t)((TY + 2) * nx * sizeof(T));
       if (w_plane) bytes += rowsT;
-    } else if constexpr (MODE == PZQ_RES) {
+    } else if constexpr (MODE == PZQ_RES || MODE == PZQ_RES0) {
       if (out_plane) bytes += rowsD;
     } else {
       if (out_plane) bytes += rowsD + 3 * rowsT + (prm.pred_order >= 1 ? rowsD : 0u);
@@ -170,7 +180,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
       if (out_plane) {
         const int zk = z0 + (j - 2 * G);  // output plane completed by this load (< nz)
         tma_load_3d(dst + Slot::b_off(nx), &maps.b_main, 0, y0, zk, &full[s]);
-        if constexpr (MODE == PZQ_GRAD_CHECK) {
+        if constexpr (pzq_grad<MODE>()) {
 #pragma unroll
           for (int f = 0; f < 3; ++f) tma_load_3d(dst + Slot::f_off(nx, f), &maps.f_main[f], 0, y0, zk, &full[s]);
           if (prm.pred_order >= 1) tma_load_3d(dst + Slot::h_off(nx), &maps.h_main, 0, y0, zk, &full[s]);
@@ -200,7 +210,8 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     xp2[i] = (cx[i] + 2) & mask;
 #pragma unroll
     for (int zp = 0; zp < 2; ++zp)
-      rm[i][zp] = MODE == PZQ_RHS_RES ? 0.0 : rmean[(cx[i] & 1) | ((cy[i] & 1) << 1) | (zp << 2)];
+      rm[i][zp] = (MODE == PZQ_RHS_RES || MODE == PZQ_RES0) ? 0.0
+                                                            : rmean[(cx[i] & 1) | ((cy[i] & 1) << 1) | (zp << 2)];
   }
   const size_t plane = (size_t)nx * ny;
   const double dtv = prm.dt.get();
@@ -285,11 +296,16 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
               const double p0 = pq[QC][i];
               const double lap = partL[PS][i] + (pq[QP2][i] + pq[QM2][i] - 2 * p0);
               pc[i][zp] += p0;
-              if constexpr (MODE == PZQ_RHS_RES) {
-                const double b = partB[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
+              if constexpr (MODE == PZQ_RHS_RES || MODE == PZQ_RES0) {
+                double b;
+                if constexpr (MODE == PZQ_RHS_RES) {
+                  b = partB[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
+                  bout[o] = b;
+                } else {
+                  b = reinterpret_cast<const double*>(sl + Slot::b_off(nx))[c];
+                }
                 const double r = b - cL * lap;
                 rc[i][zp] += r;  // the class means of b (only check 0 needs them)
-                bout[o] = b;
                 rout[o] = (float)r;
                 acc0 += r * r;
                 acc1 += b * b;
@@ -314,14 +330,16 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
                     const double* Hn = reinterpret_cast<const double*>(sl + Slot::h_off(nx));
                     prm.pred_out[o] = prm.pred_order == 1 ? 2 * p0 - Hn[c] : p0;
                   }
-                  vmax[0] = fmax(vmax[0], tu);
-                  vmin[0] = fmin(vmin[0], tu);
-                  vmax[1] = fmax(vmax[1], tv);
-                  vmin[1] = fmin(vmin[1], tv);
-                  vmax[2] = fmax(vmax[2], tw);
-                  vmin[2] = fmin(vmin[2], tw);
-                  // kinetic energy: squares in the storage type, FP64 sum
-                  acc1 += (double)(tu * tu + tv * tv + tw * tw);
+                  if (MODE != PZQ_GRAD_CHECK_BOX || !prm.box.contains(cx[i], y0 + cy[i], z0 + k, nx, ny, nz)) {
+                    vmax[0] = fmax(vmax[0], tu);
+                    vmin[0] = fmin(vmin[0], tu);
+                    vmax[1] = fmax(vmax[1], tv);
+                    vmin[1] = fmin(vmin[1], tv);
+                    vmax[2] = fmax(vmax[2], tw);
+                    vmin[2] = fmin(vmin[2], tw);
+                  }
+                  // kinetic energy |u|^2/2: squares in the storage type, FP64 sum
+                  acc1 += 0.5 * (double)(tu * tu + tv * tv + tw * tw);
                 }
               }
             }
@@ -340,7 +358,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
                 const T* Vc = reinterpret_cast<const T*>(sl + Slot::v_off(nx)) + (cy[i] + 1) * nx;  // row of v*
                 partB[PS][i] = facB * (((double)Urow[xp1[i]] - (double)Urow[xm1[i]]) +
                                        ((double)Vc[nx + x] - (double)Vc[x - nx]));
-              } else if constexpr (MODE == PZQ_GRAD_CHECK) {
+              } else if constexpr (pzq_grad<MODE>()) {
                 gA[PS][i] = Pc[xp1[i]] - Pc[xm1[i]];
                 partB[PS][i] = Pc[nx + x] - Pc[x - nx];
               }
@@ -378,7 +396,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
 #pragma unroll
     for (int k = 0; k < 18; ++k) v[k] = 0.0;
     v[0] = acc0;
-    v[1] = MODE == PZQ_GRAD_CHECK ? 0.0 : acc1;
+    v[1] = pzq_grad<MODE>() ? 0.0 : acc1;
 #pragma unroll
     for (int i = 0; i < CPT; ++i)
 #pragma unroll
@@ -391,7 +409,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
         }
       }
     block_reduce<18, false>(v, scratch);
-    if constexpr (MODE == PZQ_GRAD_CHECK) {
+    if constexpr (pzq_grad<MODE>()) {
       double accM = 0.0;
       if (vmax[0] >= vmin[0]) {  // this thread corrected at least one cell
 #pragma unroll

@@ -278,6 +278,10 @@ def test_fp32_dc_taylor_green_error_vs_fp64_oracle(oracle):
         for a, b in zip(sim.velocity(), orc.velocity()):
             worst = max(worst, rel_l2(a, b))
     assert worst < 1e-6, worst
+    # the step's FP64 reductions of the FP32 fields: kinetic energy and max |u|
+    assert st.kinetic_energy == pytest.approx(orc.diagnostics()["ke"], rel=1e-5)
+    umax = max(np.abs(f).max() for f in orc.velocity())
+    assert st.umax == pytest.approx(umax, rel=1e-5)
 
 
 def test_fp32_dc_not_converged_is_reported():
