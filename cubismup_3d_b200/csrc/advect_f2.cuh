@@ -22,11 +22,33 @@ __device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b
 __device__ __forceinline__ float2 splat2(float a) { return make_float2(a, a); }
 __device__ __forceinline__ float2 abs2(float2 a) { return make_float2(fabsf(a.x), fabsf(a.y)); }
 
-// 2 a up3(a; f) for a pair, given a and |a|.
-__device__ __forceinline__ float2 adv2(float2 a, float2 aa, float2 fm2, float2 fm1, float2 f0, float2 fp1, float2 fp2) {
-  const float2 S = fma2(splat2(8.f), sub2(fp1, fm1), sub2(fm2, fp2));
-  const float2 Q = fma2(splat2(6.f), f0, fma2(splat2(-4.f), add2(fm1, fp1), add2(fm2, fp2)));
-  return fma2(aa, Q, mul2(a, S));
+// The five weights of one direction of the update, for a pair: with
+// facA = -dt / (12 h) and facD = nu dt / h^2,
+//   facA (a S(f) + |a| Q(f)) + facD (f-1 + f+1 - 2 f0) = m2 f-2 + m1 f-1 + c0 f0 + p1 f+1 + p2 f+2,
+//   m2 = A1 + A2, p2 = A2 - A1, m1 = -8 A1 - 4 A2 + facD, p1 = 8 A1 - 4 A2 + facD,
+//   c0 = 6 A2 - 2 facD,  A1 = facA a, A2 = facA |a|.
+// They depend on the advecting velocity only, so the three components of a
+// cell share them (five FMAs per component and direction).
+struct Weights5 {
+  float2 m2, m1, c0, p1, p2;
+};
+__device__ __forceinline__ Weights5 weights5(float2 a, float2 facA, float2 facD, float2 m2FacD) {
+  const float2 A1 = mul2(facA, a), A2 = mul2(facA, abs2(a));
+  const float2 t = fma2(splat2(-4.f), A2, facD);
+  Weights5 k;
+  k.m2 = add2(A1, A2);
+  k.p2 = sub2(A2, A1);
+  k.m1 = fma2(splat2(-8.f), A1, t);
+  k.p1 = fma2(splat2(8.f), A1, t);
+  k.c0 = fma2(splat2(6.f), A2, m2FacD);
+  return k;
+}
+__device__ __forceinline__ float2 apply5(const Weights5& k, float2 fm2, float2 fm1, float2 f0, float2 fp1, float2 fp2,
+                                         float2 acc) {
+  return fma2(k.m2, fm2, fma2(k.m1, fm1, fma2(k.c0, f0, fma2(k.p1, fp1, fma2(k.p2, fp2, acc)))));
+}
+__device__ __forceinline__ float2 apply5(const Weights5& k, float2 fm2, float2 fm1, float2 f0, float2 fp1, float2 fp2) {
+  return fma2(k.m2, fm2, fma2(k.m1, fm1, fma2(k.c0, f0, fma2(k.p1, fp1, mul2(k.p2, fp2)))));
 }
 
 // STAGE2 false: out = f + dt A(f); true: out = 1/2 (f^n + f1 + dt A(f1)).
@@ -112,6 +134,7 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
   const double dtv = dt.get();
   const float2 facA = splat2((float)(-dtv / (12 * h)));  // the 1/2 of the symmetric form folded in
   const float2 facD = splat2((float)((nu / h) * (dtv / h)));
+  const float2 m2facD = splat2(-2.f * (float)((nu / h) * (dtv / h)));
   const float2 uinf[3] = {splat2((float)ux), splat2((float)uy), splat2((float)uz)};
 
   float2 qv[3][Q][PPT];
@@ -162,15 +185,13 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
 #pragma unroll
             for (int i = 0; i < PPT; ++i) {
               const size_t o = obase[i] + (size_t)k * plane;
-              const float2 ww = add2(qv[2][QC][i], uinf[2]);
-              const float2 aw = abs2(ww);
+              const Weights5 kz = weights5(add2(qv[2][QC][i], uinf[2]), facA, facD, m2facD);
               float2 outv[3];
 #pragma unroll
               for (int f = 0; f < 3; ++f) {
                 const float2 f0 = qv[f][QC][i];
-                const float2 az = adv2(ww, aw, qv[f][QM2][i], qv[f][QM1][i], f0, qv[f][QP1][i], qv[f][QP2][i]);
-                const float2 lz = fma2(splat2(-6.f), f0, add2(qv[f][QM1][i], qv[f][QP1][i]));
-                outv[f] = fma2(facD, lz, fma2(facA, az, add2(f0, part[f][PS][i])));
+                outv[f] = apply5(kz, qv[f][QM2][i], qv[f][QM1][i], f0, qv[f][QP1][i], qv[f][QP2][i],
+                                 add2(f0, part[f][PS][i]));
               }
               if constexpr (STAGE2) {
                 const float* bs = sl + stencil_elems + cy[i] * nx + px[i];
@@ -187,8 +208,8 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
             const int PS = jj % G;
 #pragma unroll
             for (int i = 0; i < PPT; ++i) {
-              const float2 uu = add2(qv[0][QN][i], uinf[0]), vv = add2(qv[1][QN][i], uinf[1]);
-              const float2 au = abs2(uu), av = abs2(vv);
+              const Weights5 kx = weights5(add2(qv[0][QN][i], uinf[0]), facA, facD, m2facD);
+              const Weights5 ky = weights5(add2(qv[1][QN][i], uinf[1]), facA, facD, m2facD);
 #pragma unroll
               for (int f = 0; f < 3; ++f) {
                 const float* F = sl + f * field_elems;
@@ -201,10 +222,7 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
                 const float2 ym1 = *reinterpret_cast<const float2*>(Fc - nx);
                 const float2 yp1 = *reinterpret_cast<const float2*>(Fc + nx);
                 const float2 yp2 = *reinterpret_cast<const float2*>(Fc + 2 * nx);
-                const float2 ax = adv2(uu, au, A, xm1, c0, xp1, B);
-                const float2 ay = adv2(vv, av, ym2, ym1, c0, yp1, yp2);
-                const float2 nb = add2(add2(xm1, xp1), add2(ym1, yp1));
-                part[f][PS][i] = fma2(facD, nb, mul2(facA, add2(ax, ay)));
+                part[f][PS][i] = apply5(kx, A, xm1, c0, xp1, B, apply5(ky, ym2, ym1, c0, yp1, yp2));
               }
             }
           }
