@@ -53,7 +53,11 @@ __device__ __forceinline__ float2 apply5(const Weights5& k, float2 fm2, float2 f
 
 // STAGE2 false: out = f + dt A(f); true: out = 1/2 (f^n + f1 + dt A(f1)).
 // blockDim.x * PPT * 2 == TY * nx (<= 512 threads).
-template <bool STAGE2, int TY, int NS, int PPT>
+// NXC, ZCC: nx and the planes per work item fixed at compile time (0: read
+// from g). Fixed, every shared-memory offset of the stencil is an immediate
+// on a per-thread base register and each item's planes unroll completely
+// (ring slot and z-queue position known per plane).
+template <bool STAGE2, int TY, int NS, int PPT, int NXC = 0, int ZCC = 0>
 __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ AdvectMaps maps, const StreamGeom g,
                                                      float* __restrict__ ou, float* __restrict__ ov,
                                                      float* __restrict__ ow, DtArg dt, double h, double nu, double ux,
@@ -61,18 +65,21 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
   constexpr int G = 2;
   constexpr int ROWS = TY + 2 * G;
   constexpr int Q = 2 * G + 1;
-  constexpr int U = 10;  // lcm(Q, G)
+  constexpr int U = ZCC ? ZCC + 2 * G : 10;  // planes per unrolled chunk: a whole item, or lcm(Q, G)
+  constexpr bool SLOT_CT = ZCC != 0 && (ZCC + 2 * G) % NS == 0;  // ring slot of plane j is j % NS
+  static_assert(ZCC == 0 || ZCC % 2 == 0, "paired barriers need an even plane count");
   static_assert(TY >= G, "tile height must cover the halo depth");
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nx = NXC ? NXC : g.nx, ny = g.ny, nz = g.nz;
+  const int zc = ZCC ? ZCC : g.zc;
   const size_t field_elems = (size_t)ROWS * nx;
   const size_t stencil_elems = 3 * field_elems;
   const size_t slot_elems = stencil_elems + (STAGE2 ? (size_t)3 * TY * nx : 0);
   float* slots = reinterpret_cast<float*>(smem_raw);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * slot_elems * sizeof(float));
   const int tid = threadIdx.x;
-  const int PL = g.zc + 2 * G;
+  const int PL = zc + 2 * G;
   const int my_items = blockIdx.x < g.n_items ? (g.n_items - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int L = my_items * PL;
   const uint32_t stencil_bytes = (uint32_t)(stencil_elems * sizeof(float));
@@ -88,7 +95,7 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
     const int it = q / PL, j = q - it * PL;
     const int item = blockIdx.x + it * gridDim.x;
     const int ty = item % g.items_y, zi = item / g.items_y;
-    const int y0 = ty * TY, z0 = zi * g.zc;
+    const int y0 = ty * TY, z0 = zi * zc;
     int z = z0 - G + j;
     z = z < 0 ? z + nz : (z >= nz ? z - nz : z);
     const int s = q % NS;
@@ -157,17 +164,19 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
   for (int it = 0; it < my_items; ++it) {
     const int item = blockIdx.x + it * gridDim.x;
     const int ty = item % g.items_y, zi = item / g.items_y;
-    const int y0 = ty * TY, z0 = zi * g.zc;
+    const int y0 = ty * TY, z0 = zi * zc;
     size_t obase[PPT];  // output index of the pair in plane z0
 #pragma unroll
     for (int i = 0; i < PPT; ++i) obase[i] = gidx(px[i], y0 + cy[i], z0, nx, ny);
+    const int q0 = q;  // first load of the item (a multiple of NS when SLOT_CT)
     for (int j0 = 0; j0 < PL; j0 += U) {
 #pragma unroll
       for (int jj = 0; jj < U; ++jj) {
         const int j = j0 + jj;
         if (j >= PL) break;  // items of PL planes, PL not a multiple of U (zc = 8)
-        const int s = q % NS;
-        if (ok) ok = mbar_wait(&full[s], (q / NS) & 1, err);
+        const int s = SLOT_CT ? jj % NS : q % NS;
+        const uint32_t phase = SLOT_CT ? ((q0 / NS + jj / NS) & 1) : ((q / NS) & 1);
+        if (ok) ok = mbar_wait(&full[s], phase, err);
         if (ok) {
           const float* sl = slots + s * slot_elems;
           const int QN = jj % Q;
@@ -204,7 +213,7 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
               *reinterpret_cast<float2*>(ow + o) = outv[2];
             }
           }
-          if (j >= G && j < G + g.zc) {
+          if (j >= G && j < G + zc) {
             const int PS = jj % G;
 #pragma unroll
             for (int i = 0; i < PPT; ++i) {
@@ -217,12 +226,16 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
                 const float2 c0 = qv[f][QN][i];
                 const float2 A = *reinterpret_cast<const float2*>(F + xl[i]);
                 const float2 B = *reinterpret_cast<const float2*>(F + xr[i]);
-                const float2 xm1 = make_float2(A.y, c0.x), xp1 = make_float2(c0.y, B.x);
                 const float2 ym2 = *reinterpret_cast<const float2*>(Fc - 2 * nx);
                 const float2 ym1 = *reinterpret_cast<const float2*>(Fc - nx);
                 const float2 yp1 = *reinterpret_cast<const float2*>(Fc + nx);
                 const float2 yp2 = *reinterpret_cast<const float2*>(Fc + 2 * nx);
-                part[f][PS][i] = apply5(kx, A, xm1, c0, xp1, B, apply5(ky, ym2, ym1, c0, yp1, yp2));
+                // x: the pairs at x -+ 1 straddle A|c0 and c0|B, so their two
+                // weights go in as scalar FMAs (no register shuffle)
+                float2 acc = fma2(kx.m2, A, fma2(kx.c0, c0, fma2(kx.p2, B, apply5(ky, ym2, ym1, c0, yp1, yp2))));
+                acc.x = fmaf(kx.m1.x, A.y, fmaf(kx.p1.x, c0.y, acc.x));
+                acc.y = fmaf(kx.m1.y, c0.x, fmaf(kx.p1.y, B.x, acc.y));
+                part[f][PS][i] = acc;
               }
             }
           }

@@ -838,7 +838,9 @@ int launch_advect(cup_handle* H, const char* name, void* const* in, void* const*
 // fields, `base` the stage-2 point-wise u^n, `out` the result.
 // zmax: z planes per work item (at most; nz when smaller): a tall tile (TY 8)
 // uses 8 so that the items spread evenly over the SMs.
-template <bool STAGE2, int TY, int NS, int PPT>
+// NXC, ZCC: compile-time nx and planes per item (0: runtime); the caller
+// picks them only when they equal H->nx and min(zmax, nz).
+template <bool STAGE2, int TY, int NS, int PPT, int NXC = 0, int ZCC = 0>
 int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out, DtArg dt,
                      int zmax = 16) {
   constexpr int G = 2;
@@ -853,9 +855,10 @@ int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* con
     if (rc) return rc;
   }
   const int zc = std::min(zmax, H->nz);
+  if ((NXC && NXC != H->nx) || (ZCC && ZCC != zc)) return fail(H, CUP_ERR_ARG, "advection specialisation mismatch");
   StreamGeom g{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
   const size_t smem = advect_smem_bytes<float, STAGE2 ? 2 : 1, TY, NS, 1>(H->nx) + 128;
-  auto kern = k_advect_zq_f2<STAGE2, TY, NS, PPT>;
+  auto kern = k_advect_zq_f2<STAGE2, TY, NS, PPT, NXC, ZCC>;
   const int threads = pairs / PPT;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, threads, &bpsm);
@@ -873,13 +876,28 @@ int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* con
 // the adjoint's stage recompute, so both see the same u1). Tile height, ring
 // depth and pairs per thread measured best at 256^3: stage 1 126 us
 // (TY 8, NS 3, 2 pairs), stage 2 152 us (TY 4, NS 3, 1 pair).
+// Grids of nx 64, 128 or 256 with nz >= ZC take the compile-time-size
+// kernels; other shapes the same kernel with runtime sizes.
+template <bool STAGE2, int TY, int NS, int PPT, int ZC>
+int launch_advect_f2_sized(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out,
+                           DtArg dt) {
+  if (H->nz >= ZC) {
+    switch (H->nx) {
+      case 64: return launch_advect_f2<STAGE2, TY, NS, PPT, 64, ZC>(H, name, in, base, out, dt, ZC);
+      case 128: return launch_advect_f2<STAGE2, TY, NS, PPT, 128, ZC>(H, name, in, base, out, dt, ZC);
+      case 256: return launch_advect_f2<STAGE2, TY, NS, PPT, 256, ZC>(H, name, in, base, out, dt, ZC);
+      default: break;
+    }
+  }
+  return launch_advect_f2<STAGE2, TY, NS, PPT>(H, name, in, base, out, dt, ZC);
+}
 int upwind_stage1_f32(cup_handle* H, const char* name, void* const* in, void* const* out, DtArg dt) {
-  if (H->ny % 8 == 0 && 4 * H->nx <= 512 * 2) return launch_advect_f2<false, 8, 4, 2>(H, name, in, in, out, dt, 8);
+  if (H->ny % 8 == 0 && 4 * H->nx <= 512 * 2) return launch_advect_f2_sized<false, 8, 4, 2, 8>(H, name, in, in, out, dt);
   return launch_advect_f2<false, 4, 4, 1>(H, name, in, in, out, dt);
 }
 int upwind_stage2_f32(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out,
                       DtArg dt) {
-  return launch_advect_f2<true, 4, 4, 1>(H, name, in, base, out, dt);
+  return launch_advect_f2_sized<true, 4, 4, 1, 16>(H, name, in, base, out, dt);
 }
 
 template <typename T>
