@@ -980,10 +980,9 @@ int dc_min_iter(const cup_handle* H) {
 }
 
 // Launches one k_pres_zq pass; returns the grid size (number of partials).
-template <typename T, int MODE, int TY, int NS, int CPT>
-int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
-               int* grid_out, const int* skip, int pred_order = -1, double* pred_out = nullptr,
-               void* const* out = nullptr) {
+template <typename T, int MODE, int TY, int NS, int CPT, int NXC, int ZCC>
+int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
+                     int* grid_out, const int* skip, int pred_order, double* pred_out, void* const* out) {
   const int cells = TY * H->nx;
   if (cells % CPT || cells / CPT > 512 || H->ny % TY)
     return fail(H, CUP_ERR_ARG, "pressure tile does not fit the grid");
@@ -998,9 +997,10 @@ int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, co
   if (!rc) rc = make_map(H, &maps.v_halo, H->v, tma_dtype<T>(), sizeof(T), H->nx, 1, 1);
   if (rc) return rc;
   const int zc = std::min(16, H->nz);
+  if ((NXC && NXC != H->nx) || (ZCC && ZCC != zc)) return fail(H, CUP_ERR_ARG, "pressure specialisation mismatch");
   StreamGeom geo{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
   const size_t smem = pzq_smem_bytes_host<T, MODE, TY, NS>(H->nx) + 128;
-  auto kern = k_pres_zq<T, MODE, TY, NS, CPT>;
+  auto kern = k_pres_zq<T, MODE, TY, NS, CPT, NXC, ZCC>;
   const int threads = cells / CPT;
   int bpsm = 0;
   if ((rc = prepare_kernel(H, kern, smem, threads, &bpsm))) return rc;
@@ -1020,6 +1020,30 @@ int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, co
   if (rc) return rc;
   if (grid_out) *grid_out = grid;
   return CUP_OK;
+}
+
+// Grids of nx 64, 128 or 256 with nz >= 16 take the compile-time-size
+// kernels; other shapes the same kernel with runtime sizes.
+template <typename T, int MODE, int TY, int NS, int CPT>
+int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
+               int* grid_out, const int* skip, int pred_order = -1, double* pred_out = nullptr,
+               void* const* out = nullptr) {
+  if (H->nz >= 16) {
+    switch (H->nx) {
+      case 64:
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 64, 16>(H, name, pw, partials, rmean, dt, grid_out, skip,
+                                                              pred_order, pred_out, out);
+      case 128:
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 128, 16>(H, name, pw, partials, rmean, dt, grid_out, skip,
+                                                               pred_order, pred_out, out);
+      case 256:
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 256, 16>(H, name, pw, partials, rmean, dt, grid_out, skip,
+                                                               pred_order, pred_out, out);
+      default: break;
+    }
+  }
+  return launch_pzq_sized<T, MODE, TY, NS, CPT, 0, 0>(H, name, pw, partials, rmean, dt, grid_out, skip, pred_order,
+                                                      pred_out, out);
 }
 
 int launch_finalize_residual(cup_handle* H, const double* partials, int stride, int grid, int k) {

@@ -105,7 +105,10 @@ constexpr size_t pzq_smem_bytes_host(int nx) {
 }
 
 // blockDim.x * CPT == TY * nx (<= 512 threads), TY even.
-template <typename T, int MODE, int TY, int NS, int CPT>
+// NXC, ZCC: nx and the planes per work item fixed at compile time (0: read
+// from g); fixed, the stencil's shared-memory offsets are immediates and the
+// ring slot of each plane is known.
+template <typename T, int MODE, int TY, int NS, int CPT, int NXC = 0, int ZCC = 0>
 __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps maps, const StreamGeom g,
                                                 T* __restrict__ ou, T* __restrict__ ov, T* __restrict__ ow,
                                                 double* __restrict__ bout, float* __restrict__ rout,
@@ -113,18 +116,21 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
                                                 const PzqParams prm, int* err, const int* skip) {
   constexpr int G = 2;
   constexpr int Q = 2 * G + 1;
-  constexpr int U = 10;  // lcm(Q, G)
+  constexpr int U = ZCC ? ZCC + 2 * G : 10;  // planes per unrolled chunk: a whole item, or lcm(Q, G)
+  constexpr bool SLOT_CT = ZCC != 0 && (ZCC + 2 * G) % NS == 0;  // ring slot of plane j is j % NS
   static_assert(TY >= G && TY % 2 == 0, "tile height must cover the halo depth and keep the row parity");
+  static_assert(ZCC % 2 == 0, "paired barriers and the z parity need an even plane count");
   using Slot = PzqSlot<T, MODE, TY>;
   if (skip && *skip) return;  // converged defect correction: nothing to check
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nx = NXC ? NXC : g.nx, ny = g.ny, nz = g.nz;
+  const int zc = ZCC ? ZCC : g.zc;
   const size_t slot_bytes = Slot::bytes(nx);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * slot_bytes);
   double* scratch = reinterpret_cast<double*>(full + NS);
   const int tid = threadIdx.x;
-  const int PL = g.zc + 2 * G;
+  const int PL = zc + 2 * G;
   const int my_items = blockIdx.x < g.n_items ? (g.n_items - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int L = my_items * PL;
   const uint32_t p_bytes = (uint32_t)Slot::p_bytes(nx);
@@ -141,7 +147,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     const int it = q / PL, j = q - it * PL;
     const int item = blockIdx.x + it * gridDim.x;
     const int ty = item % g.items_y, zi = item / g.items_y;
-    const int y0 = ty * TY, z0 = zi * g.zc;
+    const int y0 = ty * TY, z0 = zi * zc;
     int z = z0 - G + j;
     z = z < 0 ? z + nz : (z >= nz ? z - nz : z);
     const int s = q % NS;
@@ -151,7 +157,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     int yhi = y0 + TY;
     if (yhi >= ny) yhi -= ny;
     uint32_t bytes = p_bytes;
-    const bool xy_plane = j >= G && j < G + g.zc;    // planes whose x/y part is computed
+    const bool xy_plane = j >= G && j < G + zc;    // planes whose x/y part is computed
     const bool w_plane = j >= 1 && j < PL - 1;        // planes at z0-1 .. z0+zc (w at z +- 1)
     const bool out_plane = j >= 2 * G;                // completes output plane j - 2G
     if constexpr (MODE == PZQ_RHS_RES) {
@@ -203,7 +209,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
   for (int i = 0; i < CPT; ++i) {
     const int c = tid + i * blockDim.x;
     cx[i] = c & mask;
-    cy[i] = c >> g.log2nx;
+    cy[i] = NXC ? c / NXC : c >> g.log2nx;
     xm1[i] = (cx[i] - 1) & mask;
     xp1[i] = (cx[i] + 1) & mask;
     xm2[i] = (cx[i] - 2) & mask;
@@ -258,16 +264,19 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
   for (int it = 0; it < my_items; ++it) {
     const int item = blockIdx.x + it * gridDim.x;
     const int ty = item % g.items_y, zi = item / g.items_y;
-    const int y0 = ty * TY, z0 = zi * g.zc;
+    const int y0 = ty * TY, z0 = zi * zc;
     size_t obase[CPT];  // output index of plane z0
 #pragma unroll
     for (int i = 0; i < CPT; ++i) obase[i] = gidx(cx[i], y0 + cy[i], z0, nx, ny);
+    const int q0 = q;  // first load of the item (a multiple of NS when SLOT_CT)
     for (int j0 = 0; j0 < PL; j0 += U) {
 #pragma unroll
       for (int jj = 0; jj < U; ++jj) {
         const int j = j0 + jj;
-        const int s = q % NS;
-        if (ok) ok = mbar_wait(&full[s], (q / NS) & 1, err);
+        if (j >= PL) break;  // items of PL planes, PL not a multiple of U
+        const int s = SLOT_CT ? jj % NS : q % NS;
+        const uint32_t phase = SLOT_CT ? ((q0 / NS + jj / NS) & 1) : ((q / NS) & 1);
+        if (ok) ok = mbar_wait(&full[s], phase, err);
         if (ok) {
           const unsigned char* sl = smem_raw + s * slot_bytes;
           const double* P = reinterpret_cast<const double*>(sl);
@@ -345,7 +354,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
             }
           }
           // x/y part of plane j (output plane j - G)
-          if (j >= G && j < G + g.zc) {
+          if (j >= G && j < G + zc) {
             const int PS = jj % G;
 #pragma unroll
             for (int i = 0; i < CPT; ++i) {
