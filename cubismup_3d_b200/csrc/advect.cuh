@@ -47,7 +47,10 @@ constexpr size_t advect_smem_bytes(int nx) {
 }
 
 // blockDim.x * CPT must equal TY * nx (<= 512 threads).
-template <typename T, int SCHEME, int TY, int NS, int CPT>
+// NXC, ZCC: nx and the planes per work item fixed at compile time (0: read
+// from g); fixed, the stencil's shared-memory offsets are immediates and the
+// ring slot of each plane is known when NS divides the item's plane count.
+template <typename T, int SCHEME, int TY, int NS, int CPT, int NXC = 0, int ZCC = 0>
 __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ AdvectMaps maps, const StreamGeom g,
                                                   T* __restrict__ ou, T* __restrict__ ov, T* __restrict__ ow, DtArg dt,
                                                   double h, double nu, double ux, double uy, double uz, int* err) {
@@ -59,14 +62,15 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
   static_assert(TY >= G, "tile height must cover the halo depth");
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
-  const int nx = g.nx, ny = g.ny, nz = g.nz;
+  const int nx = NXC ? NXC : g.nx, ny = g.ny, nz = g.nz;
+  const int zc = ZCC ? ZCC : g.zc;
   const size_t field_elems = (size_t)ROWS * nx;
   const size_t stencil_elems = 3 * field_elems;
   const size_t slot_elems = stencil_elems + (BASE ? (size_t)3 * TY * nx : 0);
   T* slots = reinterpret_cast<T*>(smem_raw);
   uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw + NS * slot_elems * sizeof(T));
   const int tid = threadIdx.x;
-  const int PL = g.zc + 2 * G;
+  const int PL = zc + 2 * G;
   const int my_items = blockIdx.x < g.n_items ? (g.n_items - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int L = my_items * PL;
   const uint32_t stencil_bytes = (uint32_t)(stencil_elems * sizeof(T));
@@ -82,7 +86,7 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
     const int it = q / PL, j = q - it * PL;
     const int item = blockIdx.x + it * gridDim.x;
     const int ty = item % g.items_y, zi = item / g.items_y;
-    const int y0 = ty * TY, z0 = zi * g.zc;
+    const int y0 = ty * TY, z0 = zi * zc;
     int z = z0 - G + j;
     z = z < 0 ? z + nz : (z >= nz ? z - nz : z);
     const int s = q % NS;
@@ -117,7 +121,7 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
   for (int i = 0; i < CPT; ++i) {
     const int c = tid + i * blockDim.x;
     cx[i] = c & mask;
-    cy[i] = c >> g.log2nx;
+    cy[i] = NXC ? c / NXC : c >> g.log2nx;
   }
   const double dtv = dt.get();
   const T facA = (T)(SCHEME == 0 ? -dtv / (2 * h) : -dtv / (6 * h));
@@ -129,7 +133,9 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
   // (the partial of load j in slot j % G). The plane loop is unrolled by
   // U = lcm(Q, G) and every item's PL = ZC + 2G planes is a multiple of U, so
   // all ring indices fold to constants: no register shuffling.
-  constexpr int U = (G == 1) ? 3 : 10;
+  constexpr int U = ZCC ? ZCC + 2 * G : ((G == 1) ? 3 : 10);
+  constexpr bool SLOT_CT = ZCC != 0 && (ZCC + 2 * G) % NS == 0;  // ring slot of plane j is j % NS
+  static_assert(ZCC % 2 == 0, "paired barriers need an even plane count");
   T qv[3][Q][CPT];
   T part[3][G][CPT];
 #pragma unroll
@@ -154,13 +160,15 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
   for (int it = 0; it < my_items; ++it) {
     const int item = blockIdx.x + it * gridDim.x;
     const int ty = item % g.items_y, zi = item / g.items_y;
-    const int y0 = ty * TY, z0 = zi * g.zc;
+    const int y0 = ty * TY, z0 = zi * zc;
+    const int q0 = q;  // first load of the item (a multiple of NS when SLOT_CT)
     for (int j0 = 0; j0 < PL; j0 += U) {
 #pragma unroll
       for (int jj = 0; jj < U; ++jj) {
         const int j = j0 + jj;
-        const int s = q % NS;
-        if (ok) ok = mbar_wait(&full[s], (q / NS) & 1, err);
+        const int s = SLOT_CT ? jj % NS : q % NS;
+        const uint32_t phase = SLOT_CT ? ((q0 / NS + jj / NS) & 1) : ((q / NS) & 1);
+        if (ok) ok = mbar_wait(&full[s], phase, err);
         if (ok) {
           const T* sl = slots + s * slot_elems;
           const int QN = jj % Q;  // slot of the newest plane
@@ -208,7 +216,7 @@ __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ Advec
             }
           }
           // 3. x/y partial of plane j (output plane j - G), into slot j % G
-          if (j >= G && j < G + g.zc) {
+          if (j >= G && j < G + zc) {
             const int PS = jj % G;
 #pragma unroll
             for (int i = 0; i < CPT; ++i) {

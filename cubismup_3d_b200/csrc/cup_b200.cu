@@ -803,8 +803,9 @@ int read_state(cup_handle* H) {
 // ---- typed pipeline pieces -------------------------------------------------
 // Launches one k_advect_zq pass: fields `in` (stencil), `base` (stage-2
 // point-wise u^n, else unused), output `out`.
-template <typename T, int SCHEME, int TY, int NS, int CPT>
-int launch_advect(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out, DtArg dt) {
+template <typename T, int SCHEME, int TY, int NS, int CPT, int NXC, int ZCC>
+int launch_advect_sized(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out,
+                        DtArg dt) {
   constexpr int G = AdvectTraits<SCHEME>::G;
   const int cells = TY * H->nx;
   if (cells % CPT || cells / CPT > 512 || H->ny % TY)
@@ -818,9 +819,10 @@ int launch_advect(cup_handle* H, const char* name, void* const* in, void* const*
     if (rc) return rc;
   }
   const int zc = std::min(16, H->nz);
+  if ((NXC && NXC != H->nx) || (ZCC && ZCC != zc)) return fail(H, CUP_ERR_ARG, "advection specialisation mismatch");
   StreamGeom g{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
   const size_t smem = advect_smem_bytes<T, SCHEME, TY, NS, CPT>(H->nx) + 128;
-  auto kern = k_advect_zq<T, SCHEME, TY, NS, CPT>;
+  auto kern = k_advect_zq<T, SCHEME, TY, NS, CPT, NXC, ZCC>;
   const int threads = cells / CPT;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, threads, &bpsm);
@@ -832,6 +834,21 @@ int launch_advect(cup_handle* H, const char* name, void* const* in, void* const*
     CKL();
     return CUP_OK;
   });
+}
+
+// Grids of nx 64, 128 or 256 take the compile-time-nx kernels; other
+// shapes the same kernel with runtime sizes. (The planes per item stay a
+// runtime count here: unrolling a whole 20-plane item measured slower for
+// the FP64 stages than the 10-plane loop.)
+template <typename T, int SCHEME, int TY, int NS, int CPT>
+int launch_advect(cup_handle* H, const char* name, void* const* in, void* const* base, void* const* out, DtArg dt) {
+  switch (H->nx) {
+    case 64: return launch_advect_sized<T, SCHEME, TY, NS, CPT, 64, 0>(H, name, in, base, out, dt);
+    case 128: return launch_advect_sized<T, SCHEME, TY, NS, CPT, 128, 0>(H, name, in, base, out, dt);
+    case 256: return launch_advect_sized<T, SCHEME, TY, NS, CPT, 256, 0>(H, name, in, base, out, dt);
+    default: break;
+  }
+  return launch_advect_sized<T, SCHEME, TY, NS, CPT, 0, 0>(H, name, in, base, out, dt);
 }
 
 // Launches one packed-FP32 upwind3 stage (k_advect_zq_f2): `in` stencil
