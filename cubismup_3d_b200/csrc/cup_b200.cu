@@ -997,7 +997,7 @@ int dc_min_iter(const cup_handle* H) {
 }
 
 // Launches one k_pres_zq pass; returns the grid size (number of partials).
-template <typename T, int MODE, int TY, int NS, int CPT, int NXC, int ZCC>
+template <typename T, int MODE, int TY, int NS, int CPT, int NXC, int ZCC, bool BU>
 int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
                      int* grid_out, const int* skip, int pred_order, double* pred_out, void* const* out) {
   const int cells = TY * H->nx;
@@ -1016,8 +1016,8 @@ int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partia
   const int zc = std::min(16, H->nz);
   if ((NXC && NXC != H->nx) || (ZCC && ZCC != zc)) return fail(H, CUP_ERR_ARG, "pressure specialisation mismatch");
   StreamGeom geo{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
-  const size_t smem = pzq_smem_bytes_host<T, MODE, TY, NS>(H->nx) + 128;
-  auto kern = k_pres_zq<T, MODE, TY, NS, CPT, NXC, ZCC>;
+  const size_t smem = pzq_smem_bytes_host<T, MODE, TY, NS, BU>(H->nx) + 128;
+  auto kern = k_pres_zq<T, MODE, TY, NS, CPT, NXC, ZCC, BU>;
   const int threads = cells / CPT;
   int bpsm = 0;
   if ((rc = prepare_kernel(H, kern, smem, threads, &bpsm))) return rc;
@@ -1040,26 +1040,27 @@ int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partia
 }
 
 // Grids of nx 64, 128 or 256 with nz >= 16 take the compile-time-size
-// kernels; other shapes the same kernel with runtime sizes.
-template <typename T, int MODE, int TY, int NS, int CPT>
+// kernels; other shapes the same kernel with runtime sizes. BU: b from u*
+// (not stored).
+template <typename T, int MODE, int TY, int NS, int CPT, bool BU = false>
 int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
                int* grid_out, const int* skip, int pred_order = -1, double* pred_out = nullptr,
                void* const* out = nullptr) {
   if (H->nz >= 16) {
     switch (H->nx) {
       case 64:
-        return launch_pzq_sized<T, MODE, TY, NS, CPT, 64, 16>(H, name, pw, partials, rmean, dt, grid_out, skip,
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 64, 16, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
                                                               pred_order, pred_out, out);
       case 128:
-        return launch_pzq_sized<T, MODE, TY, NS, CPT, 128, 16>(H, name, pw, partials, rmean, dt, grid_out, skip,
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 128, 16, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
                                                                pred_order, pred_out, out);
       case 256:
-        return launch_pzq_sized<T, MODE, TY, NS, CPT, 256, 16>(H, name, pw, partials, rmean, dt, grid_out, skip,
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 256, 16, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
                                                                pred_order, pred_out, out);
       default: break;
     }
   }
-  return launch_pzq_sized<T, MODE, TY, NS, CPT, 0, 0>(H, name, pw, partials, rmean, dt, grid_out, skip, pred_order,
+  return launch_pzq_sized<T, MODE, TY, NS, CPT, 0, 0, BU>(H, name, pw, partials, rmean, dt, grid_out, skip, pred_order,
                                                       pred_out, out);
 }
 
@@ -1093,8 +1094,11 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt, bool rhs_given = false) {
   double* W = H->p_pred;  // this step's pressure, starting from the warm start
   if (!H->pred_ready) CK(cudaMemcpyAsync(W, H->p, H->n * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
   int rc, grid = 0;
+  // without a given RHS, b = div u* is recomputed in every pass (not stored)
   if (rhs_given) rc = launch_pzq<T, PZQ_RES0, 4, 4, 2>(H, "dc_residual0", W, partial(H, P_RES), nullptr, dt, &grid, nullptr);
-  else rc = launch_pzq<T, PZQ_RHS_RES, 4, 4, 2>(H, "rhs_residual", W, partial(H, P_RES), nullptr, dt, &grid, nullptr);
+  else
+    rc = launch_pzq<T, PZQ_RHS_RES, 4, 4, 2, true>(H, "rhs_residual", W, partial(H, P_RES), nullptr, dt, &grid,
+                                                   nullptr);
   if (rc) return rc;
   if ((rc = launch_finalize_residual(H, partial(H, P_RES), 18, grid, 0))) return rc;
   const int order = std::min(H->p_valid, 1);  // valid levels among (p) before this step
@@ -1102,9 +1106,12 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt, bool rhs_given = false) {
   constexpr int kGradStride = pzq_partials_per_cta<PZQ_GRAD_CHECK>();
   for (int k = 1; k <= max_iter; ++k) {
     if (k > 1) {
-      if ((rc = launch_pzq<T, PZQ_RES, 4, 4, 2>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid,
-                                                conv)))
-        return rc;
+      if (rhs_given)
+        rc = launch_pzq<T, PZQ_RES, 4, 4, 2>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid, conv);
+      else
+        rc = launch_pzq<T, PZQ_RES, 4, 4, 2, true>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid,
+                                                   conv);
+      if (rc) return rc;
     }
     if ((rc = dc_correction_solve(H, W, conv))) return rc;
     const int* skip = k > 1 ? conv : nullptr;
@@ -1112,9 +1119,12 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt, bool rhs_given = false) {
     if (H->has_sphere)
       rc = launch_pzq<T, PZQ_GRAD_CHECK_BOX, 4, 4, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
                                                       &H->n_grad_partials, skip, pred, H->p_old, unew);
-    else
+    else if (rhs_given)
       rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
                                                   &H->n_grad_partials, skip, pred, H->p_old, unew);
+    else
+      rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2, true>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
+                                                        &H->n_grad_partials, skip, pred, H->p_old, unew);
     if (rc) return rc;
     if ((rc = launch_finalize_residual(H, partial(H, P_GRAD), kGradStride, H->n_grad_partials, k))) return rc;
   }

@@ -75,40 +75,55 @@ struct PzqParams {
   Box box;  // GRAD_CHECK_BOX: the obstacle's box
 };
 
+// Whether a pass computes b from u* (RHS_RES always; RES and GRAD_CHECK when
+// BU: b is not stored) or reads the stored b (RES0, GRAD_CHECK_BOX: the RHS
+// with its obstacle terms; RES and GRAD_CHECK without BU).
+template <int MODE, bool BU>
+constexpr bool pzq_div() {
+  return MODE == PZQ_RHS_RES || BU;
+}
+
 // Byte layout of one ring slot (all parts multiples of 64 B for nx >= 16).
-template <typename T, int MODE, int TY>
+template <typename T, int MODE, int TY, bool BU>
 struct PzqSlot {
   static constexpr int G = 2;
+  static constexpr bool DIV = pzq_div<MODE, BU>();
+  static constexpr bool READ_B = !DIV;
   __host__ __device__ static size_t p_bytes(int nx) { return (size_t)(TY + 2 * G) * nx * sizeof(double); }
-  // RHS_RES: u [TY], v [TY + 2], w [TY] rows of T
+  // b from u*: u [TY], v [TY + 2], w [TY] rows of T
   __host__ __device__ static size_t u_off(int nx) { return p_bytes(nx); }
   __host__ __device__ static size_t v_off(int nx) { return u_off(nx) + (size_t)TY * nx * sizeof(T); }
   __host__ __device__ static size_t w_off(int nx) { return v_off(nx) + (size_t)(TY + 2) * nx * sizeof(T); }
-  // RES, GRAD_CHECK: b [TY] rows of double; GRAD_CHECK: then u, v, w [TY] rows of T
-  __host__ __device__ static size_t b_off(int nx) { return p_bytes(nx); }
-  __host__ __device__ static size_t f_off(int nx, int f) {
-    return b_off(nx) + (size_t)TY * nx * sizeof(double) + (size_t)f * TY * nx * sizeof(T);
+  __host__ __device__ static size_t div_end(int nx) {
+    return DIV ? w_off(nx) + (size_t)TY * nx * sizeof(T) : p_bytes(nx);
   }
+  // stored b: b [TY] rows of double
+  __host__ __device__ static size_t b_off(int nx) { return div_end(nx); }
+  __host__ __device__ static size_t b_end(int nx) {
+    return b_off(nx) + (READ_B ? (size_t)TY * nx * sizeof(double) : 0);
+  }
+  // GRAD_CHECK: u*, v*, w* [TY] rows of T of the output plane
+  __host__ __device__ static size_t f_off(int nx, int f) { return b_end(nx) + (size_t)f * TY * nx * sizeof(T); }
   // GRAD_CHECK: then the rows of the previous step's p [TY] of double
   __host__ __device__ static size_t h_off(int nx) { return f_off(nx, 3); }
   __host__ __device__ static size_t bytes(int nx) {
-    size_t s = MODE == PZQ_RHS_RES ? w_off(nx) + (size_t)TY * nx * sizeof(T)
-               : (MODE == PZQ_RES || MODE == PZQ_RES0) ? b_off(nx) + (size_t)TY * nx * sizeof(double)
-                                   : h_off(nx) + (size_t)TY * nx * sizeof(double);
+    size_t s = pzq_grad<MODE>() ? h_off(nx) + (size_t)TY * nx * sizeof(double) : b_end(nx);
     return (s + 127) / 128 * 128;
   }
 };
 
-template <typename T, int MODE, int TY, int NS>
+template <typename T, int MODE, int TY, int NS, bool BU = false>
 constexpr size_t pzq_smem_bytes_host(int nx) {
-  return (size_t)NS * PzqSlot<T, MODE, TY>::bytes(nx) + NS * sizeof(uint64_t) + 18 * 32 * sizeof(double);
+  return (size_t)NS * PzqSlot<T, MODE, TY, BU>::bytes(nx) + NS * sizeof(uint64_t) + 18 * 32 * sizeof(double);
 }
 
 // blockDim.x * CPT == TY * nx (<= 512 threads), TY even.
 // NXC, ZCC: nx and the planes per work item fixed at compile time (0: read
 // from g); fixed, the stencil's shared-memory offsets are immediates and the
 // ring slot of each plane is known.
-template <typename T, int MODE, int TY, int NS, int CPT, int NXC = 0, int ZCC = 0>
+// BU: b recomputed from u* in every pass instead of stored by RHS_RES (no
+// obstacle: the RHS is the divergence alone).
+template <typename T, int MODE, int TY, int NS, int CPT, int NXC = 0, int ZCC = 0, bool BU = false>
 __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps maps, const StreamGeom g,
                                                 T* __restrict__ ou, T* __restrict__ ov, T* __restrict__ ow,
                                                 double* __restrict__ bout, float* __restrict__ rout,
@@ -120,7 +135,10 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
   constexpr bool SLOT_CT = ZCC != 0 && (ZCC + 2 * G) % NS == 0;  // ring slot of plane j is j % NS
   static_assert(TY >= G && TY % 2 == 0, "tile height must cover the halo depth and keep the row parity");
   static_assert(ZCC % 2 == 0, "paired barriers and the z parity need an even plane count");
-  using Slot = PzqSlot<T, MODE, TY>;
+  using Slot = PzqSlot<T, MODE, TY, BU>;
+  constexpr bool DIV = Slot::DIV;
+  static_assert(!BU || MODE == PZQ_RHS_RES || MODE == PZQ_RES || MODE == PZQ_GRAD_CHECK,
+                "obstacle passes read the stored RHS");
   if (skip && *skip) return;  // converged defect correction: nothing to check
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
@@ -160,20 +178,22 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     const bool xy_plane = j >= G && j < G + zc;    // planes whose x/y part is computed
     const bool w_plane = j >= 1 && j < PL - 1;        // planes at z0-1 .. z0+zc (w at z +- 1)
     const bool out_plane = j >= 2 * G;                // completes output plane j - 2G
-    if constexpr (MODE == PZQ_RHS_RES) {
+    if constexpr (DIV) {
       if (xy_plane) bytes += rowsT + (uint32_t)((TY + 2) * nx * sizeof(T));
       if (w_plane) bytes += rowsT;
-    } else if constexpr (MODE == PZQ_RES || MODE == PZQ_RES0) {
+    }
+    if constexpr (Slot::READ_B) {
       if (out_plane) bytes += rowsD;
-    } else {
-      if (out_plane) bytes += rowsD + 3 * rowsT + (prm.pred_order >= 1 ? rowsD : 0u);
+    }
+    if constexpr (pzq_grad<MODE>()) {
+      if (out_plane) bytes += 3 * rowsT + (prm.pred_order >= 1 ? rowsD : 0u);
     }
     mbar_arrive_expect_tx(&full[s], bytes);
     double* P = reinterpret_cast<double*>(dst);
     tma_load_3d(P, &maps.p_halo, 0, ylo, z, &full[s]);
     tma_load_3d(P + G * nx, &maps.p_main, 0, y0, z, &full[s]);
     tma_load_3d(P + (G + TY) * nx, &maps.p_halo, 0, yhi, z, &full[s]);
-    if constexpr (MODE == PZQ_RHS_RES) {
+    if constexpr (DIV) {
       if (xy_plane) {
         tma_load_3d(dst + Slot::u_off(nx), &maps.f_main[0], 0, y0, z, &full[s]);
         T* V = reinterpret_cast<T*>(dst + Slot::v_off(nx));
@@ -182,15 +202,14 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
         tma_load_3d(V + (TY + 1) * nx, &maps.v_halo, 0, yhi, z, &full[s]);
       }
       if (w_plane) tma_load_3d(dst + Slot::w_off(nx), &maps.f_main[2], 0, y0, z, &full[s]);
-    } else {
-      if (out_plane) {
-        const int zk = z0 + (j - 2 * G);  // output plane completed by this load (< nz)
-        tma_load_3d(dst + Slot::b_off(nx), &maps.b_main, 0, y0, zk, &full[s]);
-        if constexpr (pzq_grad<MODE>()) {
+    }
+    if (out_plane) {
+      const int zk = z0 + (j - 2 * G);  // output plane completed by this load (< nz)
+      if constexpr (Slot::READ_B) tma_load_3d(dst + Slot::b_off(nx), &maps.b_main, 0, y0, zk, &full[s]);
+      if constexpr (pzq_grad<MODE>()) {
 #pragma unroll
-          for (int f = 0; f < 3; ++f) tma_load_3d(dst + Slot::f_off(nx, f), &maps.f_main[f], 0, y0, zk, &full[s]);
-          if (prm.pred_order >= 1) tma_load_3d(dst + Slot::h_off(nx), &maps.h_main, 0, y0, zk, &full[s]);
-        }
+        for (int f = 0; f < 3; ++f) tma_load_3d(dst + Slot::f_off(nx, f), &maps.f_main[f], 0, y0, zk, &full[s]);
+        if (prm.pred_order >= 1) tma_load_3d(dst + Slot::h_off(nx), &maps.h_main, 0, y0, zk, &full[s]);
       }
     }
   };
@@ -230,8 +249,9 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
   T wq[Q][CPT];
   // x/y parts of the planes in flight (G of them): Laplacian, divergence and
   // (GRAD_CHECK) the gradient of p and the u*, v* centre values
-  double partL[G][CPT], partB[G][CPT];  // partB: divergence (RHS_RES) or y-gradient (GRAD_CHECK)
-  double gA[G][CPT];                     // x-gradient (GRAD_CHECK)
+  double partL[G][CPT];
+  double partD[G][CPT];          // x/y part of the divergence (b from u*)
+  double gA[G][CPT], gB[G][CPT];  // x- and y-gradient of p (GRAD_CHECK)
   double pc[CPT][2], rc[CPT][2];  // parity-class sums of p and r by z parity
   double acc0 = 0, acc1 = 0;
   // extremes of each corrected velocity component: max |u + uinf| over the
@@ -254,7 +274,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
   for (int d = 0; d < G; ++d)
 #pragma unroll
     for (int i = 0; i < CPT; ++i) {
-      partL[d][i] = partB[d][i] = gA[d][i] = 0.0;
+      partL[d][i] = partD[d][i] = gA[d][i] = gB[d][i] = 0.0;
     }
 #pragma unroll
   for (int i = 0; i < CPT; ++i) pc[i][0] = pc[i][1] = rc[i][0] = rc[i][1] = 0.0;
@@ -283,7 +303,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
           const int QN = jj % Q;
 #pragma unroll
           for (int i = 0; i < CPT; ++i) pq[QN][i] = P[(G + cy[i]) * nx + cx[i]];
-          if constexpr (MODE == PZQ_RHS_RES) {
+          if constexpr (DIV) {
             if (j >= 1 && j < PL - 1) {
               const T* W = reinterpret_cast<const T*>(sl + Slot::w_off(nx));
 #pragma unroll
@@ -305,21 +325,21 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
               const double p0 = pq[QC][i];
               const double lap = partL[PS][i] + (pq[QP2][i] + pq[QM2][i] - 2 * p0);
               pc[i][zp] += p0;
+              // b: from u* (x/y part on arrival, z part here) or the stored RHS
+              double b;
+              if constexpr (DIV) {
+                b = partD[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
+              } else {
+                b = reinterpret_cast<const double*>(sl + Slot::b_off(nx))[c];
+              }
               if constexpr (MODE == PZQ_RHS_RES || MODE == PZQ_RES0) {
-                double b;
-                if constexpr (MODE == PZQ_RHS_RES) {
-                  b = partB[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
-                  bout[o] = b;
-                } else {
-                  b = reinterpret_cast<const double*>(sl + Slot::b_off(nx))[c];
-                }
+                if constexpr (MODE == PZQ_RHS_RES && !BU) bout[o] = b;
                 const double r = b - cL * lap;
                 rc[i][zp] += r;  // the class means of b (only check 0 needs them)
                 rout[o] = (float)r;
                 acc0 += r * r;
                 acc1 += b * b;
               } else {
-                const double b = reinterpret_cast<const double*>(sl + Slot::b_off(nx))[c];
                 const double r = b - cL * lap;
                 const double rp = r - rm[i][zp];
                 acc0 += rp * rp;
@@ -328,7 +348,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
                 } else {
                   // the FP64 correction rounded once to the storage type, then added
                   const T tu = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 0))[c] + (T)(facG * gA[PS][i]);
-                  const T tv = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 1))[c] + (T)(facG * partB[PS][i]);
+                  const T tv = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 1))[c] + (T)(facG * gB[PS][i]);
                   const T tw = reinterpret_cast<const T*>(sl + Slot::f_off(nx, 2))[c] +
                                (T)(facG * (pq[QP1][i] - pq[QM1][i]));
                   ou[o] = tu;
@@ -362,14 +382,15 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
               const double p0 = pq[QN][i];
               const double* Pc = P + (G + cy[i]) * nx;  // this column's row of p
               partL[PS][i] = (Pc[xp2[i]] + Pc[xm2[i]] - 2 * p0) + (Pc[2 * nx + x] + Pc[x - 2 * nx] - 2 * p0);
-              if constexpr (MODE == PZQ_RHS_RES) {
+              if constexpr (DIV) {
                 const T* Urow = reinterpret_cast<const T*>(sl + Slot::u_off(nx)) + cy[i] * nx;
                 const T* Vc = reinterpret_cast<const T*>(sl + Slot::v_off(nx)) + (cy[i] + 1) * nx;  // row of v*
-                partB[PS][i] = facB * (((double)Urow[xp1[i]] - (double)Urow[xm1[i]]) +
+                partD[PS][i] = facB * (((double)Urow[xp1[i]] - (double)Urow[xm1[i]]) +
                                        ((double)Vc[nx + x] - (double)Vc[x - nx]));
-              } else if constexpr (pzq_grad<MODE>()) {
+              }
+              if constexpr (pzq_grad<MODE>()) {
                 gA[PS][i] = Pc[xp1[i]] - Pc[xm1[i]];
-                partB[PS][i] = Pc[nx + x] - Pc[x - nx];
+                gB[PS][i] = Pc[nx + x] - Pc[x - nx];
               }
             }
           }
