@@ -92,10 +92,16 @@ __global__ void k_finalize_max(const double* partials, int np, DevState* st) {
   if (threadIdx.x == 0) st->umax = m[0];
 }
 
-// Simulation::calcMaxTimestep (source/Simulation.cpp:403-424) on the device.
-// step >= 0: the host's step counter, stored first (the ramp-up reads it).
-__global__ void k_calc_dt(DevState* st, double h, double nu, double CFL, int rampup, double DLM, int step = -1) {
-  if (step >= 0) st->step = step;
+// Simulation::calcMaxTimestep (source/Simulation.cpp:403-424) on the device,
+// from st->umax and st->step.
+struct CflParams {
+  double h, nu, CFL;
+  int rampup;
+  double DLM;
+};
+__device__ __forceinline__ void calc_dt_device(DevState* st, const CflParams& c) {
+  const double h = c.h, nu = c.nu, CFL = c.CFL, DLM = c.DLM;
+  const int rampup = c.rampup;
   const double hMin = h;
   const double dtDif = hMin * hMin / nu;
   const double dtAdv = hMin / (st->umax + 1e-8);
@@ -107,6 +113,12 @@ __global__ void k_calc_dt(DevState* st, double h, double nu, double CFL, int ram
   }
   st->dt = dt;
   if (DLM > 0) st->lambda = DLM / dt;
+}
+
+// step >= 0: the host's step counter, stored first (the ramp-up reads it).
+__global__ void k_calc_dt(DevState* st, double h, double nu, double CFL, int rampup, double DLM, int step = -1) {
+  if (step >= 0) st->step = step;
+  calc_dt_device(st, CflParams{h, nu, CFL, rampup, DLM});
 }
 
 // Host-side scalars into the device state without a pageable copy (which
@@ -127,8 +139,11 @@ __global__ void k_set_state(DevState* st, int what, double dt, double DLM, doubl
 
 // End of step: umax (grid part outside the obstacle box, box part after
 // penalization), kinetic energy, force/torque; advances step and time.
+// next_dt: then the CFL time step of the next step (what k_calc_dt would
+// compute before it), saving its launch in a run of steps.
 __global__ void k_finalize_step(const double* pgrad, int ngrad, int gstride, int max_off, int ke_off,
-                                const double* ppen, int npen, DevState* st, double h3, int advance) {
+                                const double* ppen, int npen, DevState* st, double h3, int advance, int next_dt,
+                                CflParams cfl) {
   __shared__ double scratch[8 * 32];
   double mx[1] = {0.0};
   double s[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -155,6 +170,7 @@ __global__ void k_finalize_step(const double* pgrad, int ngrad, int gstride, int
       st->step += 1;
       st->time += st->dt;
     }
+    if (next_dt) calc_dt_device(st, cfl);
   }
 }
 
@@ -1254,7 +1270,8 @@ int do_max_u(cup_handle* H) {
 // AdvectionDiffusion -> PressureRHS -> PressureProjection -> UpdateObstacles
 // (forced sphere: no-op) -> Penalization, with grad-P and the reductions fused.
 template <typename T>
-int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance) {
+// next_dt: finalize_step also computes the next step's CFL dt.
+int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance, int next_dt = 0) {
   int rc;
   if ((rc = do_advect_diffuse<T>(H, dt))) return rc;
   if (H->has_sphere && H->fp32) {
@@ -1279,7 +1296,8 @@ int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance) {
     int rc_ = launch_named(H, "finalize_step", [&]() -> int {
       k_finalize_step<<<1, 256, 0, H->stream>>>(partial(H, P_GRAD), H->n_grad_partials, H->grad_stride,
                                             H->grad_max_off, H->grad_ke_off, partial(H, P_PEN), H->n_pen_partials,
-                                            H->dstate, H->h * H->h * H->h, advance);
+                                            H->dstate, H->h * H->h * H->h, advance,
+                                            next_dt, CflParams{H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM});
       CKL();
       return CUP_OK;
     });
@@ -2145,7 +2163,8 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
     if (rc_) return rc_;
   }
   for (int i = 0; i < nsteps; ++i) {
-    {
+    // the dt of step i > 0 comes from the end of step i - 1
+    if (i == 0) {
       int rc_ = launch_named(H, "calc_dt", [&]() -> int {
         k_calc_dt<<<1, 1, 0, H->stream>>>(H->dstate, H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM);
         CKL();
@@ -2153,7 +2172,8 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
       });
       if (rc_) return rc_;
     }
-    rc = DISPATCH_T(H, do_step, DtArg{0.0, &H->dstate->dt}, (const double*)&H->dstate->lambda, 1);
+    rc = DISPATCH_T(H, do_step, DtArg{0.0, &H->dstate->dt}, (const double*)&H->dstate->lambda, 1,
+                    i + 1 < nsteps ? 1 : 0);
     if (rc) return rc;
   }
   if ((rc = read_state(H))) return rc;
