@@ -55,20 +55,20 @@ def kernel_bytes(name: str, fp32: bool) -> float:
         "dht_y_f64": 16,                    # FP64 inverse y pass of the correction solve
         "grad_p": 8 + 6 * s,
         # FP32 defect-correction passes
-        "rhs_residual": 3 * s + 8 + 8 + 4,   # u*, p in; b (FP64), r (FP32) out
-        "dc_residual": 8 + 8 + 4,            # p, b in; r out
+        "rhs_residual": 3 * s + 8 + 4,       # u*, p in; r (FP32) out (b = div u* in registers)
+        "dc_residual": 8 + 3 * s + 4,        # p, u* in (b recomputed); r out
         "dht_x_update_p": 4 + 8 + 8,         # correction rows in, p read-modify-write
-        "grad_p_check": 8 + 8 + 6 * s + 8 + 8,  # p, b, u* in, u out; previous p in, warm start out
+        "grad_p_check": 8 + 6 * s + 8 + 8,  # p, u* in (b recomputed), u out; previous p in, warm start out
     }
     return float(table.get(name, 0.0))
 
 
 # DRAM traffic per cell of one launch (dram__bytes_read.sum + dram__bytes_write.sum
-# of an ncu capture of the 256^3 FP32-DC step, profiles/step_fp32dc_upwind3_256_kernels_full.md),
+# of an ncu capture of the 256^3 FP32-DC step, profiles/step_fp32dc_upwind3_256_kernels.md),
 # scaled by the cells of the run; traffic grows with the cells streamed.
 MEASURED_DRAM_BYTES_PER_CELL_FP32DC = {
-    "grad_p_check": 55.3, "upwind3_stage1": 23.4, "upwind3_stage2": 35.1, "rhs_residual": 30.8,
-    "dht_x_update_p": 21.4, "dht_z_solve_mixed": 8.5, "dht_y_f64": 12.8, "dht_x": 4.6, "dht_y": 4.6,
+    "grad_p_check": 47.2, "upwind3_stage1": 21.8, "upwind3_stage2": 35.0, "rhs_residual": 23.5,
+    "dht_x_update_p": 21.4, "dht_z_solve_mixed": 8.5, "dht_y_f64": 12.6, "dht_x": 4.6, "dht_y": 4.6,
 }
 
 
