@@ -1029,7 +1029,7 @@ int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partia
   for (int q = 0; q < 3 && !rc; ++q) rc = make_map(H, &maps.f_main[q], f[q], tma_dtype<T>(), sizeof(T), H->nx, TY, 1);
   if (!rc) rc = make_map(H, &maps.v_halo, H->v, tma_dtype<T>(), sizeof(T), H->nx, 1, 1);
   if (rc) return rc;
-  const int zc = std::min(16, H->nz);
+  const int zc = ZCC ? ZCC : std::min(16, H->nz);
   if ((NXC && NXC != H->nx) || (ZCC && ZCC != zc)) return fail(H, CUP_ERR_ARG, "pressure specialisation mismatch");
   StreamGeom geo{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
   const size_t smem = pzq_smem_bytes_host<T, MODE, TY, NS, BU>(H->nx) + 128;
@@ -1058,20 +1058,20 @@ int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partia
 // Grids of nx 64, 128 or 256 with nz >= 16 take the compile-time-size
 // kernels; other shapes the same kernel with runtime sizes. BU: b from u*
 // (not stored).
-template <typename T, int MODE, int TY, int NS, int CPT, bool BU = false>
+template <typename T, int MODE, int TY, int NS, int CPT, bool BU = false, int ZC = 16>
 int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
                int* grid_out, const int* skip, int pred_order = -1, double* pred_out = nullptr,
                void* const* out = nullptr) {
-  if (H->nz >= 16) {
+  if (H->nz >= ZC) {
     switch (H->nx) {
       case 64:
-        return launch_pzq_sized<T, MODE, TY, NS, CPT, 64, 16, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 64, ZC, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
                                                               pred_order, pred_out, out);
       case 128:
-        return launch_pzq_sized<T, MODE, TY, NS, CPT, 128, 16, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 128, ZC, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
                                                                pred_order, pred_out, out);
       case 256:
-        return launch_pzq_sized<T, MODE, TY, NS, CPT, 256, 16, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 256, ZC, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
                                                                pred_order, pred_out, out);
       default: break;
     }
@@ -1139,7 +1139,7 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt, bool rhs_given = false) {
       rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
                                                   &H->n_grad_partials, skip, pred, H->p_old, unew);
     else
-      rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2, true>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
+      rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2, true, 8>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
                                                         &H->n_grad_partials, skip, pred, H->p_old, unew);
     if (rc) return rc;
     if ((rc = launch_finalize_residual(H, partial(H, P_GRAD), kGradStride, H->n_grad_partials, k))) return rc;
