@@ -189,6 +189,28 @@ class PoissonSolverPeriodic : public PoissonSolver {
   void solve() override { cup_check(cup_poisson_solve(sim.handle, &last), sim.handle, "PoissonSolverPeriodic::solve"); }
 };
 
+// CreateObstacles (source/operators/ObstaclesCreate.cpp:444-540): moves a
+// sphere that is not at rest in the frame by dt (transVel + uinf) and rebuilds
+// its chi; nothing otherwise.
+class CreateObstacles : public Operator {
+ public:
+  using Operator::Operator;
+  void operator()(const double dt) override {
+    cup_check(cup_create_obstacles(sim.handle, dt), sim.handle, "CreateObstacles");
+  }
+  std::string getName() override { return "CreateObstacles"; }
+};
+
+// UpdateObstacles (source/operators/ObstaclesUpdate.cpp:202-236) for a sphere
+// with every dof forced: its velocities stay the imposed ones
+// (source/obstacles/Obstacle.cpp:153-264), so there is nothing to integrate.
+class UpdateObstacles : public Operator {
+ public:
+  using Operator::Operator;
+  void operator()(const double) override {}
+  std::string getName() override { return "UpdateObstacles"; }
+};
+
 class AdvectionDiffusion : public Operator {
  public:
   using Operator::Operator;
@@ -284,9 +306,11 @@ class Simulation {
   void setupOperators() {
     for (auto* op : sim.pipeline) delete op;
     sim.pipeline.clear();
+    sim.pipeline.push_back(new CreateObstacles(sim));
     sim.pipeline.push_back(new AdvectionDiffusion(sim));
     sim.pipeline.push_back(new PressureRHS(sim));
     sim.pipeline.push_back(new PressureProjection(sim));
+    sim.pipeline.push_back(new UpdateObstacles(sim));
     sim.pipeline.push_back(new Penalization(sim));
   }
 

@@ -206,6 +206,28 @@ __global__ void k_finalize_rhs_obstacle(const double* p, int np, DevState* st) {
   }
 }
 
+// Zeroes a field of es-byte elements (4: FP32, 8: FP64) on a box.
+__global__ void k_clear_box(void* f, size_t es, Box box, int nx, int ny, int nz) {
+  const long long n = box.count();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = wrapi(box.lo[0] + (int)(i % box.n[0]), nx);
+    const int y = wrapi(box.lo[1] + (int)((i / box.n[0]) % box.n[1]), ny);
+    const int z = wrapi(box.lo[2] + (int)(i / ((long long)box.n[0] * box.n[1])), nz);
+    const size_t o = gidx(x, y, z, nx, ny);
+    if (es == 4)
+      static_cast<float*>(f)[o] = 0.f;
+    else
+      static_cast<double*>(f)[o] = 0.0;
+  }
+}
+
+// The sphere's position in the device parameters (stream-ordered).
+__global__ void k_set_sphere_position(SphereParams* sp, double x, double y, double z) {
+  sp->position[0] = x;
+  sp->position[1] = y;
+  sp->position[2] = z;
+}
+
 // Grid centre of mass (source/operators/ObstaclesCreate.cpp:230-256) -> SphereParams.
 __global__ void k_finalize_com(const double* p, int np, DevState* st, SphereParams* sp) {
   __shared__ double scratch[4 * 32];
@@ -447,7 +469,9 @@ struct cup_handle {
   double norm_factor = 0;
   // obstacle
   bool has_sphere = false;
-  cup_sphere sphere{};
+  cup_sphere sphere{};  // host mirror; sphere.position follows Obstacle::update
+  double sphere_vel[3] = {0, 0, 0};  // transVel (the imposed velocity of the forced dofs)
+  bool sphere_moves = false;         // transVel + uinf != 0: chi is rebuilt every step
   SphereParams* sp_dev = nullptr;
   Box box{};
   // host mirrors
@@ -1269,10 +1293,94 @@ int do_max_u(cup_handle* H) {
 // periodic pipeline of Simulation::setupOperators, source/Simulation.cpp:307-401):
 // AdvectionDiffusion -> PressureRHS -> PressureProjection -> UpdateObstacles
 // (forced sphere: no-op) -> Penalization, with grad-P and the reductions fused.
-template <typename T>
+// Active box of the sphere at its current position: every cell within
+// radius + (2 + SURFDH) h + 1 cell of the centre (SphereObstacle::FillBlocks
+// safety margin, source/obstacles/Sphere.cpp:21-27, plus the surface-detection
+// neighbour), wrapped periodically; the whole axis when it does not fit.
+void sphere_box(cup_handle* H) {
+  const int N[3] = {H->nx, H->ny, H->nz};
+  for (int d = 0; d < 3; ++d) {
+    const double r = H->sphere.radius + 3 * H->h;
+    int lo = (int)std::floor((H->sphere.position[d] - r) / H->h - 0.5) - 1;
+    int hi = (int)std::ceil((H->sphere.position[d] + r) / H->h - 0.5) + 1;
+    int cnt = hi - lo + 1;
+    if (cnt >= N[d]) {
+      lo = 0;
+      cnt = N[d];
+    }
+    lo = ((lo % N[d]) + N[d]) % N[d];
+    H->box.lo[d] = lo;
+    H->box.n[d] = cnt;
+  }
+}
+
+// chi on the active box and the grid centre of mass (the chi and CoM parts
+// of CreateObstacles, source/operators/ObstaclesCreate.cpp:51-136, 230-256).
+int build_sphere_chi(cup_handle* H) {
+  const int gb = box_grid(H->box);
+  {
+    int rc_ = launch_named(H, "sphere_chi", [&]() -> int {
+      if (H->fp32)
+        k_sphere_chi<float><<<gb, kBoxThreads, 0, H->stream>>>((float*)H->chi, H->sp_dev, H->box, H->nx, H->ny, H->nz,
+                                                                H->h, partial(H, P_CHI));
+      else
+        k_sphere_chi<double><<<gb, kBoxThreads, 0, H->stream>>>((double*)H->chi, H->sp_dev, H->box, H->nx, H->ny,
+                                                                 H->nz, H->h, partial(H, P_CHI));
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  return launch_named(H, "finalize_com", [&]() -> int {
+    k_finalize_com<<<1, 256, 0, H->stream>>>(partial(H, P_CHI), gb, H->dstate, H->sp_dev);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+// CreateObstacles (source/operators/ObstaclesCreate.cpp:444-540) for a sphere
+// that moves in the frame (transVel + uinf != 0): updateUinf, then
+// Obstacle::update (source/obstacles/Obstacle.cpp:314-321) advances the
+// position by dt (transVel + uinf) on the host mirror; chi is cleared on the
+// old box and rebuilt with the centre of mass on the box of the new position.
+// A sphere at rest in the frame keeps its chi (the rebuild would reproduce it).
+int do_create_obstacles(cup_handle* H, double dt) {
+  if (!H->has_sphere || !H->sphere_moves) return CUP_OK;
+  for (int d = 0; d < 3; ++d) H->sphere.position[d] += dt * (H->sphere_vel[d] + H->uinf[d]);
+  const size_t es = H->fp32 ? sizeof(float) : sizeof(double);
+  {
+    const Box old = H->box;
+    const int gb = box_grid(old);
+    int rc_ = launch_named(H, "sphere_clear", [&]() -> int {
+      k_clear_box<<<gb, kBoxThreads, 0, H->stream>>>(H->chi, es, old, H->nx, H->ny, H->nz);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  sphere_box(H);
+  {
+    const double* pos = H->sphere.position;
+    int rc_ = launch_named(H, "sphere_position", [&]() -> int {
+      k_set_sphere_position<<<1, 1, 0, H->stream>>>(H->sp_dev, pos[0], pos[1], pos[2]);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  return build_sphere_chi(H);
+}
+
 // next_dt: finalize_step also computes the next step's CFL dt.
+template <typename T>
 int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance, int next_dt = 0) {
   int rc;
+  // CreateObstacles first (source/Simulation.cpp:307-401 pipeline order); a
+  // moving sphere needs this step's dt on the host for its new position
+  if (H->has_sphere && H->sphere_moves) {
+    if (dt.dev) return fail(H, CUP_ERR_STATE, "a moving obstacle needs the step's dt on the host");
+    if ((rc = do_create_obstacles(H, dt.host))) return rc;
+  }
   if ((rc = do_advect_diffuse<T>(H, dt))) return rc;
   if (H->has_sphere && H->fp32) {
     // the obstacle terms need global sums over the RHS first: RHS pass, then
@@ -1811,8 +1919,14 @@ int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
   CK(cudaMalloc(&H->chi, H->n * es));
   CK(cudaMemsetAsync(H->chi, 0, H->n * es, H->stream));
   CK(cudaMalloc(&H->sp_dev, sizeof(SphereParams)));
-  // updateUinf (source/obstacles/ObstacleVector.h:60-76) for one obstacle
-  for (int d = 0; d < 3; ++d) H->uinf[d] = s->bFixFrameOfRef[d] ? -s->enforcedVelocity[d] : H->cfg.uinf[d];
+  // updateUinf (source/obstacles/ObstacleVector.h:60-76) for one obstacle: the
+  // frame follows the obstacle on its fixed dofs and is at rest on the others
+  for (int d = 0; d < 3; ++d) {
+    H->sphere_vel[d] = s->bForcedInSimFrame[d] ? s->enforcedVelocity[d] : 0.0;
+    H->uinf[d] = s->bFixFrameOfRef[d] ? -H->sphere_vel[d] : 0.0;
+  }
+  H->sphere_moves = false;
+  for (int d = 0; d < 3; ++d) H->sphere_moves = H->sphere_moves || (H->sphere_vel[d] + H->uinf[d] != 0.0);
   SphereParams sp{};
   sp.radius = s->radius;
   for (int d = 0; d < 3; ++d) {
@@ -1821,51 +1935,21 @@ int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
     sp.angVel[d] = 0.0;  // rotation blocked when any dof is forced (Obstacle.cpp:131-137)
   }
   sp.lambda_factor = 1.0;
-  // Active box: every cell within radius + (2 + SURFDH) h + 1 cell of the centre
-  // (SphereObstacle::FillBlocks safety margin, Sphere.cpp:21-27, plus the
-  // surface-detection neighbour).
-  const int N[3] = {H->nx, H->ny, H->nz};
-  for (int d = 0; d < 3; ++d) {
-    const double r = s->radius + 3 * H->h;
-    int lo = (int)std::floor((s->position[d] - r) / H->h - 0.5) - 1;
-    int hi = (int)std::ceil((s->position[d] + r) / H->h - 0.5) + 1;
-    int cnt = hi - lo + 1;
-    if (cnt >= N[d]) {
-      lo = 0;
-      cnt = N[d];
-    }
-    lo = ((lo % N[d]) + N[d]) % N[d];
-    H->box.lo[d] = lo;
-    H->box.n[d] = cnt;
-  }
+  sphere_box(H);
   CK(cudaMemcpyAsync(H->sp_dev, &sp, sizeof(sp), cudaMemcpyHostToDevice, H->stream));
-  // CreateObstacles: chi and centre of mass (the position does not move for a
-  // forced sphere in a frame fixed to it: dt (transVel + uinf) = 0).
-  const int gb = box_grid(H->box);
-  {
-    int rc_ = launch_named(H, "sphere_chi", [&]() -> int {
-      if (H->fp32)
-        k_sphere_chi<float><<<gb, kBoxThreads, 0, H->stream>>>((float*)H->chi, H->sp_dev, H->box, H->nx, H->ny, H->nz,
-                                                                H->h, partial(H, P_CHI));
-      else
-        k_sphere_chi<double><<<gb, kBoxThreads, 0, H->stream>>>((double*)H->chi, H->sp_dev, H->box, H->nx, H->ny,
-                                                                 H->nz, H->h, partial(H, P_CHI));
-      CKL();
-      return CUP_OK;
-    });
-    if (rc_) return rc_;
-  }
-  {
-    int rc_ = launch_named(H, "finalize_com", [&]() -> int {
-      k_finalize_com<<<1, 256, 0, H->stream>>>(partial(H, P_CHI), gb, H->dstate, H->sp_dev);
-      CKL();
-      return CUP_OK;
-    });
-    if (rc_) return rc_;
-  }
+  int rc = build_sphere_chi(H);
+  if (rc) return rc;
   H->umax_fresh = false;
   CK(cudaStreamSynchronize(H->stream));
   return check_dev_error(H);
+}
+
+int cup_create_obstacles(cup_handle* H, double dt) {
+  REQUIRE_H(H);
+  if (!(dt >= 0)) return fail(H, CUP_ERR_ARG, "dt must be >= 0");
+  int rc = do_create_obstacles(H, dt);
+  if (rc) return rc;
+  return CUP_OK;
 }
 
 int cup_get_obstacle_state(cup_handle* H, double force[3], double torque[3], double com[3], double uinf[3]) {
@@ -2090,6 +2174,8 @@ int cup_adjoint_step_obstacle(cup_handle* H, const void* un, const void* vn, con
   REQUIRE_H(H);
   if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
   if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_adjoint_step_obstacle: the handle has no obstacle");
+  if (H->sphere_moves)
+    return fail(H, CUP_ERR_STATE, "cup_adjoint_step_obstacle: the adjoint of a moving obstacle is not supported");
   if (!w_force || !g_chi || !g_vel) return fail(H, CUP_ERR_ARG, "null w_force / g_chi / g_vel");
   int rc = check_adjoint_fields(H, un, vn, wn, lu, lv, lw);
   if (!rc) rc = alloc_adjoint(H);
@@ -2161,6 +2247,17 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
       return CUP_OK;
     });
     if (rc_) return rc_;
+  }
+  if (H->has_sphere && H->sphere_moves) {
+    // a moving sphere's box follows its position on the host: dt is read back
+    // every step (calcMaxTimestep + timestep, as the reference runs them)
+    for (int i = 0; i < nsteps; ++i) {
+      double dt = 0;
+      if ((rc = cup_calc_max_timestep(H, &dt))) return rc;
+      if ((rc = cup_step(H, dt, nullptr))) return rc;
+    }
+    if (stats) return fill_stats(H, stats);
+    return CUP_OK;
   }
   for (int i = 0; i < nsteps; ++i) {
     // the dt of step i > 0 comes from the end of step i - 1

@@ -177,6 +177,16 @@ class Operator:
         raise NotImplementedError
 
 
+class CreateObstacles(Operator):
+    """CreateObstacles (source/operators/ObstaclesCreate.cpp:444-540): moves a
+    sphere that is not at rest in the frame by dt (transVel + uinf) and
+    rebuilds its chi; nothing otherwise."""
+    name = "CreateObstacles"
+
+    def __call__(self, dt: float):
+        L.check(L.lib().cup_create_obstacles(self.sim._h, float(dt)), self.sim._h, self.name)
+
+
 class AdvectionDiffusion(Operator):
     name = "AdvectionDiffusion"
 
@@ -198,6 +208,17 @@ class PressureProjection(Operator):
         st = L.CupSolveStats()
         L.check(L.lib().cup_pressure_projection(self.sim._h, float(dt), C.byref(st)), self.sim._h, self.name)
         self.last_stats = st
+
+
+class UpdateObstacles(Operator):
+    """UpdateObstacles (source/operators/ObstaclesUpdate.cpp:202-236) for a sphere
+    with every dof forced: its velocities stay the imposed ones
+    (source/obstacles/Obstacle.cpp:153-264) and the frame velocity is set by
+    CreateObstacles, so there is nothing to integrate."""
+    name = "UpdateObstacles"
+
+    def __call__(self, dt: float):
+        return None
 
 
 class Penalization(Operator):
@@ -268,11 +289,10 @@ class Simulation:
         self.shape = (self.cells[2], self.cells[1], self.cells[0])
         self.obstacles: List[Sphere] = []
         self.pressureSolver = PoissonSolverPeriodic(self)
-        # pipeline of the periodic hot path (Simulation::setupOperators); the
-        # obstacle create/update operators are folded into add_obstacle and
-        # the forced-sphere no-op update.
-        self.pipeline: List[Operator] = [AdvectionDiffusion(self), PressureRHS(self), PressureProjection(self),
-                                         Penalization(self)]
+        # pipeline of the periodic hot path in the order of
+        # Simulation::setupOperators (source/Simulation.cpp:307-401)
+        self.pipeline: List[Operator] = [CreateObstacles(self), AdvectionDiffusion(self), PressureRHS(self),
+                                         PressureProjection(self), UpdateObstacles(self), Penalization(self)]
         self.step = 0
         self.time = 0.0
         self.dt = 0.0

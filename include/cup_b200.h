@@ -130,6 +130,14 @@ int cup_global_to_blocks(const double* global, double* blocks, int nx, int ny, i
  * then CreateObstacles (source/operators/ObstaclesCreate.cpp:444-540) and
  * updateUinf (source/obstacles/ObstacleVector.h:60-76). At most one sphere. */
 int cup_add_sphere(struct cup_handle* h, const cup_sphere* s);
+/* CreateObstacles (source/operators/ObstaclesCreate.cpp:444-540) for a sphere
+ * that moves in the frame (transVel + uinf != 0: a dof with a non-zero imposed
+ * velocity and bFixFrameOfRef off): Obstacle::update
+ * (source/obstacles/Obstacle.cpp:314-321) advances its position by
+ * dt (transVel + uinf), then chi and the centre of mass are rebuilt. No-op for
+ * a sphere at rest in the frame or without an obstacle. cup_step and cup_run
+ * run it first in every step (cup_run then reads dt back once per step). */
+int cup_create_obstacles(struct cup_handle* h, double dt);
 /* Force / torque from the last Penalization (Penalization.cpp:101-123), centre of mass. */
 int cup_get_obstacle_state(struct cup_handle* h, double force[3], double torque[3], double com[3],
                            double uinf[3]);

@@ -79,15 +79,15 @@ def test_operators_vs_oracle(oracle, scheme):
     sim.set_velocity(u, v, w)
     orc.set_velocity(u, v, w)
     dt = 1e-3
-    for op in sim.pipeline[:1]:
-        op(dt)
+    ops = {op.getName(): op for op in sim.pipeline}
+    ops["AdvectionDiffusion"](dt)
     orc.operator("AdvectionDiffusion", dt)
     for a, b in zip(sim.velocity(), orc.velocity()):
         assert rel_l2(a, b) < 1e-13
-    sim.pipeline[1](dt)
+    ops["PressureRHS"](dt)
     orc.operator("PressureRHS", dt)
     assert rel_l2(sim.rhs(), orc.get("rhs")) < 1e-13
-    sim.pipeline[2](dt)
+    ops["PressureProjection"](dt)
     orc.operator("PressureProjection", dt)
     assert rel_l2(sim.pressure(), orc.get("p")) < 1e-12
     for a, b in zip(sim.velocity(), orc.velocity()):
@@ -206,7 +206,8 @@ def test_sphere_operator_by_operator_vs_oracle(oracle):
     orc.set_velocity(u, v, w)
     dt = 2e-3
     names = [op.getName() for op in sim.pipeline]
-    assert names == ["AdvectionDiffusion", "PressureRHS", "PressureProjection", "Penalization"]
+    assert names == ["CreateObstacles", "AdvectionDiffusion", "PressureRHS", "PressureProjection",
+                     "UpdateObstacles", "Penalization"]
     for op in sim.pipeline:
         op(dt)
         orc.operator(op.getName(), dt)
@@ -216,6 +217,80 @@ def test_sphere_operator_by_operator_vs_oracle(oracle):
         assert rel_l2(a, b) < 1e-12
     ft = sim.pipeline[-1].force_torque
     assert np.allclose(ft[:3], orc.stats()["force"], rtol=1e-10, atol=1e-14)
+
+
+MOVING_SPHERE = dict(SPHERE, enforcedVelocity=(1.0, 0.2, 0.0), bFixFrameOfRef=(False, False, False))
+
+
+def moving_sphere_pair(oracle, cells, extent, nu, precision="fp64", **kw):
+    import cubismup_3d_b200 as cup
+    nx, ny, nz = cells
+    sim = make_sim(cells, extent, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6, bImplicitPenalization=True,
+                   precision=precision, **kw)
+    sim.add_obstacle(cup.Sphere(**MOVING_SPHERE))
+    orc = oracle.OracleSim(nx, ny, nz, extent, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6,
+                           implicit_penalization=True,
+                           sphere={"radius": MOVING_SPHERE["radius"], "position": MOVING_SPHERE["position"],
+                                   "velocity": MOVING_SPHERE["enforcedVelocity"], "forced": (1, 1, 1),
+                                   "fix_frame": (0, 0, 0)})
+    z = np.zeros(orc.shape)
+    sim.set_velocity(z, z, z)
+    orc.set_velocity(z, z, z)
+    return sim, orc
+
+
+def test_moving_sphere_steps_vs_oracle(oracle):
+    # A forced sphere moving through a frame at rest (bFixFrameOfRef off):
+    # uinf = 0 (updateUinf) and CreateObstacles advances the sphere by dt U and
+    # rebuilds chi at the start of every step.
+    sim, orc = moving_sphere_pair(oracle, (64, 32, 32), 2.0, nu=2 * 0.25 / 300)
+    assert np.allclose(sim.obstacle_state()["uinf"], 0.0)
+    for s in range(6):
+        dt = orc.calc_max_timestep()
+        assert sim.calcMaxTimestep() == pytest.approx(dt, rel=1e-12)
+        st = sim.timestep(dt)
+        orc.timestep(dt)
+        assert np.max(np.abs(sim.chi() - orc.get("chi"))) < 1e-13
+        for a, b in zip(sim.velocity(), orc.velocity()):
+            assert rel_l2(a, b) < TOL_STEP
+        ost = orc.stats()
+        assert np.allclose(sim.obstacle_state()["com"], ost["com"], rtol=0, atol=1e-12)
+        of = ost["force"]
+        assert np.allclose(st.force, of, rtol=1e-10, atol=1e-12 * np.abs(of).max())
+    # the sphere has left its starting box
+    assert ost["com"][0] > MOVING_SPHERE["position"][0] + 0.05
+
+
+def test_moving_sphere_run_and_operators_vs_oracle(oracle):
+    # run_steps (dt read back per step for a moving sphere) and the operator
+    # pipeline (CreateObstacles first) against the oracle's run / operators
+    sim, orc = moving_sphere_pair(oracle, (32, 32, 32), 1.0, nu=1e-3)
+    st = sim.run_steps(4)
+    dts = orc.run(4)
+    assert st.step == 4
+    assert st.time == pytest.approx(float(np.sum(dts)), rel=1e-12)
+    for a, b in zip(sim.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < TOL_STEP
+    dt = 2e-3
+    for op in sim.pipeline:
+        op(dt)
+        orc.operator(op.getName(), dt)
+    assert np.max(np.abs(sim.chi() - orc.get("chi"))) < 1e-13
+    for a, b in zip(sim.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < 1e-11
+
+
+def test_fp32_dc_moving_sphere_tracks_oracle(oracle):
+    sim, orc = moving_sphere_pair(oracle, (64, 32, 32), 2.0, nu=1e-3, precision="fp32_dc", dc_max_iter=8)
+    for s in range(5):
+        dt = orc.calc_max_timestep()
+        st = sim.timestep(dt)
+        orc.timestep(dt)
+    assert np.max(np.abs(sim.chi() - orc.get("chi"))) < 1e-6
+    for a, b in zip(sim.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < 1e-5
+    of = orc.stats()["force"]
+    assert abs(st.force[0] - of[0]) < 1e-3 * abs(of[0])
 
 
 def test_calc_max_timestep_rampup_and_dlm(oracle):
