@@ -112,6 +112,7 @@ SIGNATURES = {
     "cup_set_velocity_raw": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_void_p]),
     "cup_poisson_solve_field": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_int]),
     "cup_diagnostics": (C.c_int, [_H, _dp]),
+    "cup_compute_dissipation": (C.c_int, [_H, _dp]),
     "cup_debug_shift": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]),
     "cup_max_velocity_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong, _dp, C.c_void_p,
                                            C.c_void_p]),

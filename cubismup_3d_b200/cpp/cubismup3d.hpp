@@ -16,6 +16,7 @@
 
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -140,6 +141,7 @@ struct SimulationData {
   // status
   int step = 0, nsteps = 0;
   double time = 0, endTime = 0, dt = 0;
+  int freqDiagnostics = 0;  // ComputeDissipation every this many steps (0: off)
   // B200 form
   int precision = CUP_PREC_FP64;
   int scheme = CUP_SCHEME_REF;
@@ -247,6 +249,30 @@ class Penalization : public Operator {
   std::string getName() override { return "Penalization"; }
 };
 
+// ComputeDissipation (source/operators/ComputeDissipation.cpp:119-177): every
+// freqDiagnostics steps, the 20 sums of the current fields appended to
+// diagnostics.dat in the reference's format (header at step 0).
+class ComputeDissipation : public Operator {
+ public:
+  using Operator::Operator;
+  std::array<double, 20> last{};
+  void operator()(const double) override {
+    if (sim.freqDiagnostics == 0 || sim.step % sim.freqDiagnostics) return;
+    cup_check(cup_compute_dissipation(sim.handle, last.data()), sim.handle, "ComputeDissipation");
+    std::FILE* f = std::fopen("diagnostics.dat", "a");
+    if (!f) throw std::runtime_error("ComputeDissipation: cannot open diagnostics.dat");
+    if (sim.step == 0)
+      std::fprintf(f, "step_id time circ_x circ_y circ_y linImp_x linImp_y linImp_z linMom_x linMom_y linMom_z "
+                      "angImp_x angImp_y angImp_z angMom_x angMom_y angMom_z presPow viscPow helicity kineticEn "
+                      "enstrophy\n");
+    std::fprintf(f, "%d %g", sim.step, sim.time);
+    for (double x : last) std::fprintf(f, " %g", x);
+    std::fprintf(f, "\n");
+    std::fclose(f);
+  }
+  std::string getName() override { return "ComputeDissipation"; }
+};
+
 SimulationData::~SimulationData() {
   while (!pipeline.empty()) {
     delete pipeline.back();
@@ -312,6 +338,7 @@ class Simulation {
     sim.pipeline.push_back(new PressureProjection(sim));
     sim.pipeline.push_back(new UpdateObstacles(sim));
     sim.pipeline.push_back(new Penalization(sim));
+    sim.pipeline.push_back(new ComputeDissipation(sim));
   }
 
   void add_obstacle(const SphereArguments& a) {
@@ -364,6 +391,7 @@ class Simulation {
     sim.bImplicitPenalization = c.bImplicitPenalization;
     sim.nsteps = c.nsteps;
     sim.endTime = c.endTime;
+    sim.freqDiagnostics = c.freqDiagnostics;
     sim.precision = c.precision;
     sim.scheme = c.scheme;
     sim.dc_tol = c.dc_tol;

@@ -288,6 +288,78 @@ __global__ void k_finalize_residual(const double* p, int stride, int np, DevStat
   }
 }
 
+// ComputeDissipation (source/operators/ComputeDissipation.cpp:38-116): per
+// cell, vorticity, pressure power -(1-chi) h^3 grad p . u, viscous power
+// (1-chi) h^3 nu (u . lap u + 2 D:D), and the linear / angular invariants
+// about the domain centre; per-CTA FP64 partials of the 20 sums in the order
+// of the reference's reduction (:132-152). hCube = pow(h, 3), inv2h = 1/(2h),
+// invHh = 1/h^2 and the centre come from the host as the reference computes
+// them.
+template <typename T>
+__global__ void k_dissipation(const T* u, const T* v, const T* w, const double* p, const T* chi, int nx, int ny,
+                              int nz, double h, double nu, double hCube, double inv2h, double invHh, double cx,
+                              double cy, double cz, double* partials /* [gridDim.x][20] */) {
+  __shared__ double scratch[20 * 32];
+  double R[20];
+#pragma unroll
+  for (int k = 0; k < 20; ++k) R[k] = 0.0;
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+    const int xp = wrapi(x + 1, nx), xm = wrapi(x - 1, nx), yp = wrapi(y + 1, ny), ym = wrapi(y - 1, ny),
+              zp = wrapi(z + 1, nz), zm = wrapi(z - 1, nz);
+    const size_t o = i;
+    const size_t oE = gidx(xp, y, z, nx, ny), oW = gidx(xm, y, z, nx, ny), oN = gidx(x, yp, z, nx, ny),
+                 oS = gidx(x, ym, z, nx, ny), oB = gidx(x, y, zp, nx, ny), oF = gidx(x, y, zm, nx, ny);
+    const double X = chi ? (double)chi[o] : 0.0;
+    const double PX = (x + 0.5) * h - cx, PY = (y + 0.5) * h - cy, PZ = (z + 0.5) * h - cz;
+    const double uc = u[o], vc = v[o], wc = w[o];
+    const double uE = u[oE], uW = u[oW], uN = u[oN], uS = u[oS], uB = u[oB], uF = u[oF];
+    const double vE = v[oE], vW = v[oW], vN = v[oN], vS = v[oS], vB = v[oB], vF = v[oF];
+    const double wE = w[oE], wW = w[oW], wN = w[oN], wS = w[oS], wB = w[oB], wF = w[oF];
+    const double WX = inv2h * ((wN - wS) - (vB - vF));
+    const double WY = inv2h * ((uB - uF) - (wE - wW));
+    const double WZ = inv2h * ((vE - vW) - (uN - uS));
+    const double dPdx = inv2h * (p[oE] - p[oW]);
+    const double dPdy = inv2h * (p[oN] - p[oS]);
+    const double dPdz = inv2h * (p[oB] - p[oF]);
+    R[15] -= (1 - X) * hCube * (dPdx * uc + dPdy * vc + dPdz * wc);
+    const double lapU = invHh * (uE + uW + uN + uS + uB + uF - 6 * uc);
+    const double lapV = invHh * (vE + vW + vN + vS + vB + vF - 6 * vc);
+    const double lapW = invHh * (wE + wW + wN + wS + wB + wF - 6 * wc);
+    const double V1 = lapU * uc + lapV * vc + lapW * wc;
+    const double D11 = inv2h * (uE - uW);
+    const double D22 = inv2h * (vN - vS);
+    const double D33 = inv2h * (wB - wF);
+    const double D12 = inv2h * (uN - uS + vE - vW) / 2;
+    const double D13 = inv2h * (uB - uF + wE - wW) / 2;
+    const double D23 = inv2h * (wN - wS + vB - vF) / 2;
+    const double V2 = D11 * D11 + D22 * D22 + D33 * D33 + 2 * (D12 * D12 + D13 * D13 + D23 * D23);
+    R[16] += (1 - X) * hCube * nu * (V1 + 2 * V2);
+    R[0] += hCube * WX;
+    R[1] += hCube * WY;
+    R[2] += hCube * WZ;
+    R[3] += hCube / 2 * (PY * WZ - PZ * WY);
+    R[4] += hCube / 2 * (PZ * WX - PX * WZ);
+    R[5] += hCube / 2 * (PX * WY - PY * WX);
+    R[6] += hCube * uc;
+    R[7] += hCube * vc;
+    R[8] += hCube * wc;
+    R[9] += hCube / 3 * (PX * (PY * WY + PZ * WZ) - WX * (PY * PY + PZ * PZ));
+    R[10] += hCube / 3 * (PY * (PX * WX + PZ * WZ) - WY * (PX * PX + PZ * PZ));
+    R[11] += hCube / 3 * (PZ * (PX * WX + PY * WY) - WZ * (PX * PX + PY * PY));
+    R[12] += hCube * (PY * wc - PZ * vc);
+    R[13] += hCube * (PZ * uc - PX * wc);
+    R[14] += hCube * (PX * vc - PY * uc);
+    R[17] += hCube * (WX * uc + WY * vc + WZ * wc);
+    R[18] += hCube * (uc * uc + vc * vc + wc * wc) / 2;
+    R[19] += sqrt(WX * WX + WY * WY + WZ * WZ);
+  }
+  block_reduce<20, false>(R, scratch);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 20; ++k) partials[20 * blockIdx.x + k] = R[k];
+}
+
 // Diagnostics: kinetic energy and central-divergence norms (FP64).
 template <typename T>
 __global__ void k_diag(const T* u, const T* v, const T* w, int nx, int ny, int nz, double inv2h, double* partials) {
@@ -2328,6 +2400,40 @@ int cup_diagnostics(cup_handle* H, double out[3]) {
   out[0] = ke * h3;
   out[1] = std::sqrt(d2 * h3);
   out[2] = dm;
+  return check_dev_error(H);
+}
+
+int cup_compute_dissipation(cup_handle* H, double out[20]) {
+  REQUIRE_H(H);
+  if (!out) return fail(H, CUP_ERR_ARG, "null output");
+  const int grid = std::min<size_t>(H->num_sms * 4, (H->n + 255) / 256);
+  double* part = partial(H, P_DIAG);
+  const double h = H->h;
+  const double hCube = std::pow(h, 3), inv2h = .5 / h, invHh = 1 / (h * h);
+  const double cx = H->nx * h / 2, cy = H->ny * h / 2, cz = H->nz * h / 2;  // extent / 2
+  {
+    int rc_ = launch_named(H, "dissipation", [&]() -> int {
+      if (H->fp32)
+        k_dissipation<float><<<grid, 256, 0, H->stream>>>((const float*)H->u, (const float*)H->v, (const float*)H->w,
+                                                           H->p, H->has_sphere ? (const float*)H->chi : nullptr, H->nx,
+                                                           H->ny, H->nz, h, H->cfg.nu, hCube, inv2h, invHh, cx, cy, cz,
+                                                           part);
+      else
+        k_dissipation<double><<<grid, 256, 0, H->stream>>>(
+            (const double*)H->u, (const double*)H->v, (const double*)H->w, H->p,
+            H->has_sphere ? (const double*)H->chi : nullptr, H->nx, H->ny, H->nz, h, H->cfg.nu, hCube, inv2h, invHh,
+            cx, cy, cz, part);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  std::vector<double> hp(20 * (size_t)grid);
+  CK(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  for (int k = 0; k < 20; ++k) out[k] = 0.0;
+  for (int i = 0; i < grid; ++i)
+    for (int k = 0; k < 20; ++k) out[k] += hp[20 * (size_t)i + k];
   return check_dev_error(H);
 }
 

@@ -53,6 +53,7 @@ class SimulationData:
     dc_min_iter: int = 1
     device: int = 0
     verbose: bool = False
+    freqDiagnostics: int = 0  # ComputeDissipation every this many steps (0: off), to diagnostics.dat
 
     def __post_init__(self):
         self.setCells(*self.cells)
@@ -230,6 +231,26 @@ class Penalization(Operator):
         self.force_torque = np.array(ft[:])
 
 
+# diagnostics.dat columns of ComputeDissipation (source/operators/ComputeDissipation.cpp:162-176),
+# header spelled as the reference writes it
+DISSIPATION_NAMES = ("circ_x", "circ_y", "circ_z", "linImp_x", "linImp_y", "linImp_z", "linMom_x", "linMom_y",
+                     "linMom_z", "angImp_x", "angImp_y", "angImp_z", "angMom_x", "angMom_y", "angMom_z", "presPow",
+                     "viscPow", "helicity", "kineticEn", "enstrophy")
+DIAGNOSTICS_HEADER = ("step_id time circ_x circ_y circ_y linImp_x linImp_y linImp_z linMom_x linMom_y linMom_z "
+                      "angImp_x angImp_y angImp_z angMom_x angMom_y angMom_z presPow viscPow helicity kineticEn "
+                      "enstrophy")
+
+
+class ComputeDissipation(Operator):
+    """ComputeDissipation (source/operators/ComputeDissipation.cpp:119-177): every
+    ``freqDiagnostics`` steps, the 20 sums of the current fields appended to
+    ``diagnostics.dat`` (header at step 0)."""
+    name = "ComputeDissipation"
+
+    def __call__(self, dt: float):
+        self.sim._diagnostics_line(self.sim.step, self.sim.time)
+
+
 class PoissonSolverPeriodic:
     """PoissonSolverPeriodic (source/poisson/PoissonSolverPeriodic.cpp) bound
     to a simulation's device buffers: ``solve()`` runs the FFT chain."""
@@ -292,7 +313,8 @@ class Simulation:
         # pipeline of the periodic hot path in the order of
         # Simulation::setupOperators (source/Simulation.cpp:307-401)
         self.pipeline: List[Operator] = [CreateObstacles(self), AdvectionDiffusion(self), PressureRHS(self),
-                                         PressureProjection(self), UpdateObstacles(self), Penalization(self)]
+                                         PressureProjection(self), UpdateObstacles(self), Penalization(self),
+                                         ComputeDissipation(self)]
         self.step = 0
         self.time = 0.0
         self.dt = 0.0
@@ -478,6 +500,7 @@ class Simulation:
         """Simulation::timestep (source/Simulation.cpp:593-623); returns True when finished."""
         st = L.CupStepStats()
         L.check(L.lib().cup_step(self._h, float(dt), C.byref(st) if stats else None), self._h, "timestep")
+        self._diagnostics_line(self.step, self.time)
         self.step += 1
         self.time += dt
         self.dt = dt
@@ -495,7 +518,7 @@ class Simulation:
         if self.sd.nsteps <= 0 and self.sd.endTime <= 0:
             raise ValueError("set nsteps or endTime before run()")
         last = None
-        if self.sd.endTime <= 0:
+        if self.sd.endTime <= 0 and self.sd.freqDiagnostics == 0:
             return self.run_steps(self.sd.nsteps - self.step)
         while True:
             dt = self.calcMaxTimestep()
@@ -503,6 +526,22 @@ class Simulation:
             if (self.sd.endTime > 0 and self.time > self.sd.endTime) or (
                     self.sd.nsteps != 0 and self.step >= self.sd.nsteps):
                 return last
+
+    def compute_dissipation(self) -> dict:
+        """ComputeDissipation's 20 FP64 sums of the current fields, by diagnostics.dat column name."""
+        out = (C.c_double * 20)()
+        L.check(L.lib().cup_compute_dissipation(self._h, out), self._h, "compute_dissipation")
+        return dict(zip(DISSIPATION_NAMES, out[:]))
+
+    def _diagnostics_line(self, step: int, time: float, path: str = "diagnostics.dat"):
+        f = int(self.sd.freqDiagnostics)
+        if f == 0 or step % f:
+            return
+        d = self.compute_dissipation()
+        with open(path, "a") as fh:
+            if step == 0:
+                fh.write(DIAGNOSTICS_HEADER + "\n")
+            fh.write(" ".join([str(step), f"{time:g}"] + [f"{d[k]:g}" for k in DISSIPATION_NAMES]) + "\n")
 
     def diagnostics(self) -> dict:
         out = (C.c_double * 3)()

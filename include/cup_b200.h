@@ -213,6 +213,11 @@ int cup_poisson_solve_field(struct cup_handle* h, const double* rhs, double* p, 
  * out[1] L2 norm (sum h^3 div^2)^(1/2) of the central divergence, out[2] max |div|
  * (ComputeDissipation.cpp:47-116 pattern, PoissonSolver.cpp:35-52 pattern). */
 int cup_diagnostics(struct cup_handle* h, double out[3]);
+/* ComputeDissipation (source/operators/ComputeDissipation.cpp:38-177) on the
+ * current fields: out[20] = circulation[3], linImpulse[3], linMomentum[3],
+ * angImpulse[3], angMomentum[3], presPow, viscPow, helicity, kineticEn,
+ * enstrophy (the reference's RDX order and diagnostics.dat columns), FP64. */
+int cup_compute_dissipation(struct cup_handle* h, double out[20]);
 
 /* Test hook for the halo staging (restates tests/cubismup3d/TestBoundaries.cpp):
  * out(x) = f(x - d) through the same periodic plane-streaming TMA path the

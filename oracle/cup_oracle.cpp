@@ -832,6 +832,7 @@ int orc_operator(void* hdl, const char* name, double dt) {
   else if (n == "PressureProjection") op_pressure_projection(*S, dt);
   else if (n == "UpdateObstacles") op_update_obstacles(*S);
   else if (n == "Penalization") op_penalization(*S, dt);
+  else if (n == "ComputeDissipation") {}  // diagnostics only (orc_dissipation): no state change
   else return 1;
   return 0;
 }
@@ -936,6 +937,82 @@ void orc_diagnostics(void* hdl, double* out) {
         dmax = std::max(dmax, std::fabs(div));
       }
   out[0] = ke; out[1] = std::sqrt(d2); out[2] = dmax;
+}
+
+// ComputeDissipation (source/operators/ComputeDissipation.cpp:38-116, reduced
+// as :119-160): per block, with a one-cell lab of u, v, w, p and the cell's
+// chi, the 20 sums circulation[3], linImpulse[3], linMomentum[3],
+// angImpulse[3], angMomentum[3], presPow, viscPow, helicity, kineticEn,
+// enstrophy, in that order. Blocks are summed in block order.
+void orc_dissipation(void* hdl, double* out) {
+  OState* S = static_cast<OState*>(hdl);
+  const Dims D = S->D;
+  const Real h = S->h, nu = S->cfg.nu;
+  const Real hCube = std::pow(h, 3), inv2h = .5 / h, invHh = 1 / (h * h);
+  const Real center[3] = {D.nx * h / 2, D.ny * h / 2, D.nz * h / 2};
+  const int nb = D.nblocks();
+  std::vector<double> per((size_t)nb * 20, 0.0);
+  for_each_block(D, [&](int bx, int by, int bz) {
+    Lab Lu, Lv, Lw, Lp;
+    Lu.load(S->u.data(), D, bx, by, bz, 1);
+    Lv.load(S->v.data(), D, bx, by, bz, 1);
+    Lw.load(S->w.data(), D, bx, by, bz, 1);
+    Lp.load(S->p.data(), D, bx, by, bz, 1);
+    double R[20] = {0};
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const int gx = bx * BS + ix, gy = by * BS + iy, gz = bz * BS + iz;
+      const Real X = S->has_sphere ? S->chi[D.idx(gx, gy, gz)] : 0.0;
+      const Real PX = (gx + 0.5) * h - center[0], PY = (gy + 0.5) * h - center[1], PZ = (gz + 0.5) * h - center[2];
+      const Real u = Lu(ix, iy, iz), v = Lv(ix, iy, iz), w = Lw(ix, iy, iz);
+      const Real WX = inv2h * ((Lw(ix, iy + 1, iz) - Lw(ix, iy - 1, iz)) - (Lv(ix, iy, iz + 1) - Lv(ix, iy, iz - 1)));
+      const Real WY = inv2h * ((Lu(ix, iy, iz + 1) - Lu(ix, iy, iz - 1)) - (Lw(ix + 1, iy, iz) - Lw(ix - 1, iy, iz)));
+      const Real WZ = inv2h * ((Lv(ix + 1, iy, iz) - Lv(ix - 1, iy, iz)) - (Lu(ix, iy + 1, iz) - Lu(ix, iy - 1, iz)));
+      const Real dPdx = inv2h * (Lp(ix + 1, iy, iz) - Lp(ix - 1, iy, iz));
+      const Real dPdy = inv2h * (Lp(ix, iy + 1, iz) - Lp(ix, iy - 1, iz));
+      const Real dPdz = inv2h * (Lp(ix, iy, iz + 1) - Lp(ix, iy, iz - 1));
+      R[15] -= (1 - X) * hCube * (dPdx * u + dPdy * v + dPdz * w);
+      const Real lapU = invHh * (Lu(ix + 1, iy, iz) + Lu(ix - 1, iy, iz) + Lu(ix, iy + 1, iz) + Lu(ix, iy - 1, iz) +
+                                 Lu(ix, iy, iz + 1) + Lu(ix, iy, iz - 1) - 6 * u);
+      const Real lapV = invHh * (Lv(ix + 1, iy, iz) + Lv(ix - 1, iy, iz) + Lv(ix, iy + 1, iz) + Lv(ix, iy - 1, iz) +
+                                 Lv(ix, iy, iz + 1) + Lv(ix, iy, iz - 1) - 6 * v);
+      const Real lapW = invHh * (Lw(ix + 1, iy, iz) + Lw(ix - 1, iy, iz) + Lw(ix, iy + 1, iz) + Lw(ix, iy - 1, iz) +
+                                 Lw(ix, iy, iz + 1) + Lw(ix, iy, iz - 1) - 6 * w);
+      const Real V1 = lapU * u + lapV * v + lapW * w;
+      const Real D11 = inv2h * (Lu(ix + 1, iy, iz) - Lu(ix - 1, iy, iz));
+      const Real D22 = inv2h * (Lv(ix, iy + 1, iz) - Lv(ix, iy - 1, iz));
+      const Real D33 = inv2h * (Lw(ix, iy, iz + 1) - Lw(ix, iy, iz - 1));
+      const Real D12 = inv2h * (Lu(ix, iy + 1, iz) - Lu(ix, iy - 1, iz) + Lv(ix + 1, iy, iz) - Lv(ix - 1, iy, iz)) / 2;
+      const Real D13 = inv2h * (Lu(ix, iy, iz + 1) - Lu(ix, iy, iz - 1) + Lw(ix + 1, iy, iz) - Lw(ix - 1, iy, iz)) / 2;
+      const Real D23 = inv2h * (Lw(ix, iy + 1, iz) - Lw(ix, iy - 1, iz) + Lv(ix, iy, iz + 1) - Lv(ix, iy, iz - 1)) / 2;
+      const Real V2 = D11 * D11 + D22 * D22 + D33 * D33 + 2 * (D12 * D12 + D13 * D13 + D23 * D23);
+      R[16] += (1 - X) * hCube * nu * (V1 + 2 * V2);
+      R[0] += hCube * WX;
+      R[1] += hCube * WY;
+      R[2] += hCube * WZ;
+      R[3] += hCube / 2 * (PY * WZ - PZ * WY);
+      R[4] += hCube / 2 * (PZ * WX - PX * WZ);
+      R[5] += hCube / 2 * (PX * WY - PY * WX);
+      R[6] += hCube * u;
+      R[7] += hCube * v;
+      R[8] += hCube * w;
+      R[9] += hCube / 3 * (PX * (PY * WY + PZ * WZ) - WX * (PY * PY + PZ * PZ));
+      R[10] += hCube / 3 * (PY * (PX * WX + PZ * WZ) - WY * (PX * PX + PZ * PZ));
+      R[11] += hCube / 3 * (PZ * (PX * WX + PY * WY) - WZ * (PX * PX + PY * PY));
+      R[12] += hCube * (PY * w - PZ * v);
+      R[13] += hCube * (PZ * u - PX * w);
+      R[14] += hCube * (PX * v - PY * u);
+      R[17] += hCube * (WX * u + WY * v + WZ * w);
+      R[18] += hCube * (u * u + v * v + w * w) / 2;
+      R[19] += std::sqrt(WX * WX + WY * WY + WZ * WZ);
+    }
+    const int b = bx + D.bpd(0) * (by + D.bpd(1) * bz);
+    for (int k = 0; k < 20; ++k) per[(size_t)b * 20 + k] = R[k];
+  });
+  for (int k = 0; k < 20; ++k) out[k] = 0.0;
+  for (int b = 0; b < nb; ++b)
+    for (int k = 0; k < 20; ++k) out[k] += per[(size_t)b * 20 + k];
 }
 
 // Tangent-linear rollout (no obstacle): advances the state nsteps with the

@@ -74,6 +74,7 @@ def lib():
         L.orc_lab_shift.argtypes = [dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_lab_shift.restype = C.c_int
         L.orc_diagnostics.argtypes = [C.c_void_p, dp]
+        L.orc_dissipation.argtypes = [C.c_void_p, dp]
         L.orc_tangent_run.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp]
         L.orc_tangent_run.restype = C.c_int
         L.orc_num_threads.restype = C.c_int
@@ -180,6 +181,12 @@ class OracleSim:
         out = np.zeros(3, dtype=np.float64)
         lib().orc_diagnostics(self._h, _p(out))
         return {"ke": out[0], "div_l2": out[1], "div_max": out[2]}
+
+    def dissipation(self) -> np.ndarray:
+        """ComputeDissipation's 20 sums (source/operators/ComputeDissipation.cpp:119-160 order)."""
+        out = np.zeros(20, dtype=np.float64)
+        lib().orc_dissipation(self._h, _p(out))
+        return out
 
 
 def poisson_solve(rhs: np.ndarray, h: float) -> np.ndarray:

@@ -207,7 +207,7 @@ def test_sphere_operator_by_operator_vs_oracle(oracle):
     dt = 2e-3
     names = [op.getName() for op in sim.pipeline]
     assert names == ["CreateObstacles", "AdvectionDiffusion", "PressureRHS", "PressureProjection",
-                     "UpdateObstacles", "Penalization"]
+                     "UpdateObstacles", "Penalization", "ComputeDissipation"]
     for op in sim.pipeline:
         op(dt)
         orc.operator(op.getName(), dt)
@@ -215,7 +215,7 @@ def test_sphere_operator_by_operator_vs_oracle(oracle):
             assert rel_l2(sim.rhs(), orc.get("rhs")) < 1e-13
     for a, b in zip(sim.velocity(), orc.velocity()):
         assert rel_l2(a, b) < 1e-12
-    ft = sim.pipeline[-1].force_torque
+    ft = next(op for op in sim.pipeline if op.getName() == "Penalization").force_torque
     assert np.allclose(ft[:3], orc.stats()["force"], rtol=1e-10, atol=1e-14)
 
 
@@ -291,6 +291,35 @@ def test_fp32_dc_moving_sphere_tracks_oracle(oracle):
         assert rel_l2(a, b) < 1e-5
     of = orc.stats()["force"]
     assert abs(st.force[0] - of[0]) < 1e-3 * abs(of[0])
+
+
+@pytest.mark.parametrize("with_sphere", [False, True])
+def test_compute_dissipation_vs_oracle(oracle, with_sphere, tmp_path, monkeypatch):
+    # ComputeDissipation's 20 sums after a few steps (with the sphere: chi
+    # masks the pressure and viscous power), and the diagnostics.dat lines
+    if with_sphere:
+        sim, orc = sphere_pair(oracle, (64, 32, 32), 2.0, nu=1e-3)
+    else:
+        cells = (64, 32, 32)
+        sim = make_sim(cells, 2.0, nu=1e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0)
+        orc = oracle.OracleSim(*cells, 2.0, nu=1e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0)
+    u, v, w = random_velocity((64, 32, 32), 17, 0.5)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    monkeypatch.chdir(tmp_path)
+    sim.sd.freqDiagnostics = 2
+    for s in range(3):
+        dt = orc.calc_max_timestep()
+        sim.timestep(dt)
+        orc.timestep(dt)
+    got = np.array(list(sim.compute_dissipation().values()))
+    ref = orc.dissipation()
+    scale = np.abs(ref).max()
+    assert np.all(np.abs(got - ref) <= 1e-10 * np.abs(ref) + 1e-13 * scale), (got, ref)
+    lines = open(tmp_path / "diagnostics.dat").read().splitlines()
+    assert lines[0].split()[:4] == ["step_id", "time", "circ_x", "circ_y"]
+    assert [int(l.split()[0]) for l in lines[1:]] == [0, 2]
+    assert all(len(l.split()) == 22 for l in lines[1:])
 
 
 def test_calc_max_timestep_rampup_and_dlm(oracle):
