@@ -1416,9 +1416,17 @@ int build_sphere_chi(cup_handle* H) {
 // position by dt (transVel + uinf) on the host mirror; chi is cleared on the
 // old box and rebuilt with the centre of mass on the box of the new position.
 // A sphere at rest in the frame keeps its chi (the rebuild would reproduce it).
+int relocate_sphere(cup_handle* H);
+
 int do_create_obstacles(cup_handle* H, double dt) {
   if (!H->has_sphere || !H->sphere_moves) return CUP_OK;
   for (int d = 0; d < 3; ++d) H->sphere.position[d] += dt * (H->sphere_vel[d] + H->uinf[d]);
+  return relocate_sphere(H);
+}
+
+// chi of the sphere at H->sphere.position: cleared on the old box, rebuilt
+// with the centre of mass on the box of the new position.
+int relocate_sphere(cup_handle* H) {
   const size_t es = H->fp32 ? sizeof(float) : sizeof(double);
   {
     const Box old = H->box;
@@ -2014,6 +2022,35 @@ int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
   H->umax_fresh = false;
   CK(cudaStreamSynchronize(H->stream));
   return check_dev_error(H);
+}
+
+int cup_set_sphere_position(cup_handle* H, const double position[3]) {
+  REQUIRE_H(H);
+  if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_set_sphere_position: the handle has no obstacle");
+  if (!position) return fail(H, CUP_ERR_ARG, "null position");
+  for (int d = 0; d < 3; ++d) H->sphere.position[d] = position[d];
+  int rc = relocate_sphere(H);
+  if (rc) return rc;
+  H->umax_fresh = false;
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+int cup_get_sphere_position(cup_handle* H, double position[3]) {
+  REQUIRE_H(H);
+  if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_get_sphere_position: the handle has no obstacle");
+  if (!position) return fail(H, CUP_ERR_ARG, "null position");
+  for (int d = 0; d < 3; ++d) position[d] = H->sphere.position[d];
+  return CUP_OK;
+}
+
+int cup_set_uinf(cup_handle* H, const double uinf[3]) {
+  REQUIRE_H(H);
+  if (!uinf) return fail(H, CUP_ERR_ARG, "null uinf");
+  if (H->has_sphere) return fail(H, CUP_ERR_STATE, "cup_set_uinf: with an obstacle the frame velocity follows it");
+  for (int d = 0; d < 3; ++d) H->uinf[d] = uinf[d];
+  H->umax_fresh = false;
+  return CUP_OK;
 }
 
 int cup_create_obstacles(cup_handle* H, double dt) {

@@ -11,6 +11,7 @@ with ``std::invalid_argument`` raise ``ValueError`` here as pybind11 would.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 from typing import List, Optional, Sequence, Tuple
 
@@ -54,6 +55,9 @@ class SimulationData:
     device: int = 0
     verbose: bool = False
     freqDiagnostics: int = 0  # ComputeDissipation every this many steps (0: off), to diagnostics.dat
+    saveFreq: int = 0         # restart dumps every this many steps (0: off)
+    saveTime: float = 0.0     # ... or every this much simulated time (0: off)
+    path4serialization: str = "./"
 
     def __post_init__(self):
         self.setCells(*self.cells)
@@ -499,11 +503,14 @@ class Simulation:
     def timestep(self, dt: float, stats: bool = True) -> Optional[StepStats]:
         """Simulation::timestep (source/Simulation.cpp:593-623); returns True when finished."""
         st = L.CupStepStats()
+        dump = self._maybe_serialize(dt)
         L.check(L.lib().cup_step(self._h, float(dt), C.byref(st) if stats else None), self._h, "timestep")
         self._diagnostics_line(self.step, self.time)
         self.step += 1
         self.time += dt
         self.dt = dt
+        if dump:
+            self.serialize()
         return StepStats.from_c(st) if stats else None
 
     def run_steps(self, nsteps: int) -> StepStats:
@@ -518,7 +525,7 @@ class Simulation:
         if self.sd.nsteps <= 0 and self.sd.endTime <= 0:
             raise ValueError("set nsteps or endTime before run()")
         last = None
-        if self.sd.endTime <= 0 and self.sd.freqDiagnostics == 0:
+        if self.sd.endTime <= 0 and self.sd.freqDiagnostics == 0 and self.sd.saveFreq == 0 and self.sd.saveTime == 0:
             return self.run_steps(self.sd.nsteps - self.step)
         while True:
             dt = self.calcMaxTimestep()
@@ -542,6 +549,120 @@ class Simulation:
             if step == 0:
                 fh.write(DIAGNOSTICS_HEADER + "\n")
             fh.write(" ".join([str(step), f"{time:g}"] + [f"{d[k]:g}" for k in DISSIPATION_NAMES]) + "\n")
+
+    # -- restart files -----------------------------------------------------------
+    def serialize(self, append: str = "") -> str:
+        """Simulation::_serialize (source/Simulation.cpp:426-524): ``restart.status`` and
+        ``<name>.status`` (time, stepid, uinf as the reference prints them), the
+        obstacle's ``<name>_0.txt`` (Obstacle::save, source/obstacles/Obstacle.cpp:402-423)
+        and the velocity, pressure and chi fields. HDF5 is not used: each field is a
+        raw little-endian FP64 array ``vel_/pres_/chi_<name>.raw`` ([z][y][x], velocity
+        with its 3 components innermost) with an XDMF descriptor ``.xmf`` beside it.
+        Returns the path prefix ``<path4serialization>/<name>``."""
+        name = (append if append else "restart_") + f"{self.step:09d}"
+        base = self.sd.path4serialization
+        os.makedirs(base, exist_ok=True)
+        fpath = os.path.join(base, name)
+        uinf = self.obstacle_state()["uinf"] if self.obstacles else np.array(self.sd.uinf, dtype=np.float64)
+        status = (f"time: {self.time:20.20e}\nstepid: {int(self.step)}\nuinfx: {uinf[0]:20.20e}\n"
+                  f"uinfy: {uinf[1]:20.20e}\nuinfz: {uinf[2]:20.20e}\n")
+        if self.obstacles:
+            pos = (C.c_double * 3)()
+            L.check(L.lib().cup_get_sphere_position(self._h, pos), self._h, "serialize")
+            sph = self.obstacles[0]
+            vel = [float(x) if f else 0.0 for x, f in zip(sph.enforcedVelocity, sph.bForcedInSimFrame)]
+            q = list(sph.quaternion) if getattr(sph, "quaternion", None) is not None else [1.0, 0.0, 0.0, 0.0]
+            # absPos (the position in the lab frame, advanced by transVel alone)
+            abspos = [p0 + self.time * vi for p0, vi in zip(sph.position, vel)]
+            lines = [f"{self.time:.16e}", "\t".join(f"{x:.16e}" for x in pos[:]),
+                     "\t".join(f"{x:.16e}" for x in abspos), "\t".join(f"{x:.16e}" for x in q),
+                     "\t".join(f"{x:.16e}" for x in vel), "\t".join(f"{0.0:.16e}" for _ in range(3)), f"{0.0:.16e}"]
+            with open(fpath + "_0.txt", "w") as f:
+                f.write("\n".join(lines) + "\n")
+        with open(fpath + ".status", "w") as f:
+            f.write(status)
+        u, v, w = self.velocity()
+        fields = {"vel_": (np.stack([u, v, w], axis=-1), "Vector"), "pres_": (self.pressure(), "Scalar"),
+                  "chi_": (self.chi() if self.obstacles else np.zeros(self.shape), "Scalar")}
+        for prefix, (arr, kind) in fields.items():
+            stem = prefix + name
+            np.ascontiguousarray(arr, dtype="<f8").tofile(os.path.join(base, stem + ".raw"))
+            self._write_xmf(os.path.join(base, stem + ".xmf"), stem + ".raw", kind)
+        with open(os.path.join(base, "restart.status"), "w") as f:
+            f.write(status)
+        return fpath
+
+    def _write_xmf(self, path: str, raw: str, kind: str):
+        nx, ny, nz = self.cells
+        dims = f"{nz} {ny} {nx}" + (" 3" if kind == "Vector" else "")
+        with open(path, "w") as f:
+            f.write('<?xml version="1.0" ?>\n<!DOCTYPE Xdmf SYSTEM "Xdmf.dtd" []>\n<Xdmf Version="2.0">\n <Domain>\n'
+                    '  <Grid GridType="Uniform">\n'
+                    f'   <Time Value="{self.time:.16e}"/>\n'
+                    f'   <Topology TopologyType="3DCORECTMesh" Dimensions="{nz + 1} {ny + 1} {nx + 1}"/>\n'
+                    '   <Geometry GeometryType="ORIGIN_DXDYDZ">\n'
+                    '    <DataItem Dimensions="3" NumberType="Double" Precision="8" Format="XML">0 0 0</DataItem>\n'
+                    f'    <DataItem Dimensions="3" NumberType="Double" Precision="8" Format="XML">'
+                    f'{self.h:.16e} {self.h:.16e} {self.h:.16e}</DataItem>\n'
+                    '   </Geometry>\n'
+                    f'   <Attribute Name="data" AttributeType="{kind}" Center="Cell">\n'
+                    f'    <DataItem Dimensions="{dims}" NumberType="Float" Precision="8" Endian="Little" '
+                    f'Format="Binary">{raw}</DataItem>\n'
+                    '   </Attribute>\n  </Grid>\n </Domain>\n</Xdmf>\n')
+
+    def deserialize(self) -> bool:
+        """Simulation::_deserialize (source/Simulation.cpp:526-580): reads
+        ``restart.status`` in path4serialization, then the velocity dump of that step
+        and the obstacle's position (Obstacle::restart, source/obstacles/Obstacle.cpp:425-447;
+        add the obstacle first, as the reference builds it from its arguments).
+        Returns False (a new run) when there is no restart.status."""
+        base = self.sd.path4serialization
+        st = os.path.join(base, "restart.status")
+        if not os.path.exists(st):
+            return False
+        vals = {}
+        with open(st) as f:
+            for line in f:
+                k, _, val = line.partition(":")
+                vals[k.strip()] = val.strip()
+        try:
+            time, step = float(vals["time"]), int(vals["stepid"])
+            uinf = [float(vals["uinfx"]), float(vals["uinfy"]), float(vals["uinfz"])]
+        except (KeyError, ValueError) as e:
+            raise ValueError(f"Error reading restart file {st}: {e}") from None
+        if step < 0 or time < 0:
+            raise ValueError(f"Error reading restart file {st}")
+        name = f"restart_{step:09d}"
+        nx, ny, nz = self.cells
+        vel = np.fromfile(os.path.join(base, "vel_" + name + ".raw"), dtype="<f8")
+        if vel.size != 3 * nx * ny * nz:
+            raise ValueError(f"restart velocity dump has {vel.size} values, the grid needs {3 * nx * ny * nz}")
+        vel = vel.reshape(nz, ny, nx, 3)
+        self.set_velocity(vel[..., 0], vel[..., 1], vel[..., 2])
+        if self.obstacles:
+            txt = os.path.join(base, name + "_0.txt")
+            if os.path.exists(txt):
+                with open(txt) as f:
+                    rows = f.read().split("\n")
+                pos = (C.c_double * 3)(*[float(x) for x in rows[1].split()[:3]])
+                L.check(L.lib().cup_set_sphere_position(self._h, pos), self._h, "deserialize")
+        else:
+            L.check(L.lib().cup_set_uinf(self._h, (C.c_double * 3)(*uinf)), self._h, "deserialize")
+            self.sd.uinf = tuple(uinf)
+        self.step, self.time = step, time
+        L.check(L.lib().cup_set_clock(self._h, step, time), self._h, "deserialize")
+        self._next_save_time = time + self.sd.saveTime
+        return True
+
+    def _maybe_serialize(self, dt: float):
+        """The dump decision of Simulation::timestep (source/Simulation.cpp:595-598, 611-613)."""
+        f, tsave = int(self.sd.saveFreq), float(self.sd.saveTime)
+        nxt = getattr(self, "_next_save_time", tsave)
+        dump_freq = f > 0 and (self.step + 1) % f == 0
+        dump_time = tsave > 0 and (self.time + dt) > nxt
+        if dump_time:
+            self._next_save_time = nxt + tsave
+        return dump_freq or dump_time
 
     def diagnostics(self) -> dict:
         out = (C.c_double * 3)()

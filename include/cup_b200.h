@@ -138,6 +138,15 @@ int cup_add_sphere(struct cup_handle* h, const cup_sphere* s);
  * a sphere at rest in the frame or without an obstacle. cup_step and cup_run
  * run it first in every step (cup_run then reads dt back once per step). */
 int cup_create_obstacles(struct cup_handle* h, double dt);
+/* Obstacle::restart's position (source/obstacles/Obstacle.cpp:425-447): moves
+ * the sphere to `position` and rebuilds chi and the centre of mass there. */
+int cup_set_sphere_position(struct cup_handle* h, const double position[3]);
+/* The sphere's position (Obstacle::position; it follows Obstacle::update). */
+int cup_get_sphere_position(struct cup_handle* h, double position[3]);
+/* The frame velocity sim.uinf as restored by Simulation::_deserialize
+ * (source/Simulation.cpp:526-580); only without an obstacle (updateUinf sets
+ * it from the obstacle otherwise). */
+int cup_set_uinf(struct cup_handle* h, const double uinf[3]);
 /* Force / torque from the last Penalization (Penalization.cpp:101-123), centre of mass. */
 int cup_get_obstacle_state(struct cup_handle* h, double force[3], double torque[3], double com[3],
                            double uinf[3]);

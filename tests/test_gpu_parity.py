@@ -322,6 +322,48 @@ def test_compute_dissipation_vs_oracle(oracle, with_sphere, tmp_path, monkeypatc
     assert all(len(l.split()) == 22 for l in lines[1:])
 
 
+@pytest.mark.parametrize("moving", [False, True])
+def test_serialize_deserialize_resumes_the_run(tmp_path, moving):
+    # Simulation::_serialize / _deserialize: 3 steps, a dump, a new simulation
+    # restarts from it and runs 3 more; it ends where the uninterrupted 6-step
+    # run does (FP64: the pressure is recomputed every step, so nothing but the
+    # velocity, the clock and the obstacle's position is state).
+    import cubismup_3d_b200 as cup
+    cells = (32, 32, 32)
+
+    def new_sim():
+        sim = make_sim(cells, 1.0, nu=1e-3, CFL=0.2, rampup=0, DLM=0.0, lambda_=1e6, bImplicitPenalization=True,
+                       uinf=(0.0, 0.0, 0.0) if moving else (0.1, -0.05, 0.0))
+        if moving:
+            sim.add_obstacle(cup.Sphere(**MOVING_SPHERE))
+        sim.sd.path4serialization = str(tmp_path)
+        return sim
+
+    u, v, w = random_velocity(cells, 23, 0.3)
+    a = new_sim()
+    a.set_velocity(u, v, w)
+    for _ in range(6):
+        a.timestep(a.calcMaxTimestep())
+    b = new_sim()
+    b.set_velocity(u, v, w)
+    for _ in range(3):
+        b.timestep(b.calcMaxTimestep())
+    b.serialize()
+    status = open(tmp_path / "restart.status").read().splitlines()
+    assert status[0].startswith("time: ") and status[1] == "stepid: 3"
+    assert (tmp_path / "vel_restart_000000003.xmf").exists()
+    c = new_sim()
+    assert c.deserialize()
+    assert c.step == 3 and c.time == b.time
+    if moving:
+        assert np.array_equal(c.chi(), b.chi())
+    for _ in range(3):
+        c.timestep(c.calcMaxTimestep())
+    assert c.time == pytest.approx(a.time, rel=1e-15)
+    for x, y in zip(c.velocity(), a.velocity()):
+        assert rel_l2(x, y) < 1e-13
+
+
 def test_calc_max_timestep_rampup_and_dlm(oracle):
     n = 32
     sim = make_sim((n, n, n), 1.0, nu=0.01, CFL=0.5, rampup=10, DLM=1.0, lambda_=1.0)
