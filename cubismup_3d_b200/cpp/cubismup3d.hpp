@@ -142,6 +142,7 @@ struct SimulationData {
   int step = 0, nsteps = 0;
   double time = 0, endTime = 0, dt = 0;
   int freqDiagnostics = 0;  // ComputeDissipation every this many steps (0: off)
+  double turbKinEn_target = 0, enInjectionRate = 0;  // SpectralForcing (SimulationData.cpp:60-66)
   // B200 form
   int precision = CUP_PREC_FP64;
   int scheme = CUP_SCHEME_REF;
@@ -220,6 +221,18 @@ class AdvectionDiffusion : public Operator {
     cup_check(cup_advect_diffuse(sim.handle, dt), sim.handle, "AdvectionDiffusion");
   }
   std::string getName() override { return "AdvectionDiffusion"; }
+};
+
+// SpectralForcing (source/spectralOperators/SpectralForcing.cpp:23-86): raises the
+// energy of the band 0 < k^2 <= 4 to meet turbKinEn_target or enInjectionRate.
+class SpectralForcing : public Operator {
+ public:
+  using Operator::Operator;
+  std::array<double, 6> stats{};  // totalKinEn, largeModesKinEn, viscousDissip, totalDissipRate, injectionRate, lIntegral
+  void operator()(const double dt) override {
+    cup_check(cup_spectral_forcing(sim.handle, dt, stats.data()), sim.handle, "SpectralForcing");
+  }
+  std::string getName() override { return "SpectralForcing"; }
 };
 
 class PressureRHS : public Operator {
@@ -334,6 +347,13 @@ class Simulation {
     sim.pipeline.clear();
     sim.pipeline.push_back(new CreateObstacles(sim));
     sim.pipeline.push_back(new AdvectionDiffusion(sim));
+    if (sim.turbKinEn_target > 0 || sim.enInjectionRate > 0) {
+      if (sim.turbKinEn_target > 0 && sim.enInjectionRate > 0)
+        throw std::invalid_argument("give either turbKinEn_target or enInjectionRate, not both");
+      cup_check(cup_set_spectral_forcing(sim.handle, sim.turbKinEn_target, sim.enInjectionRate), sim.handle,
+                "SpectralForcing");
+      sim.pipeline.push_back(new SpectralForcing(sim));
+    }
     sim.pipeline.push_back(new PressureRHS(sim));
     sim.pipeline.push_back(new PressureProjection(sim));
     sim.pipeline.push_back(new UpdateObstacles(sim));
@@ -392,6 +412,8 @@ class Simulation {
     sim.nsteps = c.nsteps;
     sim.endTime = c.endTime;
     sim.freqDiagnostics = c.freqDiagnostics;
+    sim.turbKinEn_target = c.turbKinEn_target;
+    sim.enInjectionRate = c.enInjectionRate;
     sim.precision = c.precision;
     sim.scheme = c.scheme;
     sim.dc_tol = c.dc_tol;

@@ -360,6 +360,98 @@ __global__ void k_dissipation(const T* u, const T* v, const T* w, const double* 
     for (int k = 0; k < 20; ++k) partials[20 * blockIdx.x + k] = R[k];
 }
 
+// Spectral analysis and forcing (source/spectralOperators/SpectralManipFFTW.cpp:25-193,
+// SpectralForcing.cpp:23-86) on the separable Hartley coefficients of the
+// Poisson passes instead of FFTW's r2c spectrum. The separable transform
+// mixes the DFT coefficients of the 8 modes (+-kx, +-ky, +-kz) orthogonally,
+// and every quantity the reference takes per mode is a function of |k| (the
+// shell of the spectrum, 1/|k|, the 0 < k^2 <= 4 forcing band), so sums over
+// modes are the same: E = 1/2 (Hu^2 + Hv^2 + Hw^2) per separable mode is the
+// reference's mult/2 |U|^2 summed over the conjugate-symmetric full spectrum.
+// The vorticity sum is taken in physical space, where Parseval puts it: the
+// reference's eps is nu times the mean of |curl_c u|^2 (central differences).
+template <typename T>
+__global__ void k_widen(const T* __restrict__ src, double* __restrict__ dst, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = (double)src[i];
+}
+
+// Per separable mode: E, E / |k| (the integral length), the binned spectrum
+// (bin floor(sqrt(kind) (nyquist - 1) / nyquist) for kind = ii^2 + jj^2 + kk^2
+// < nyquist^2) and, when filtering, the energy of the forcing band with every
+// other mode zeroed in place. Per-CTA partials: [tke, lIntegral, tkeFiltered,
+// nbin spectrum values]; the bins are summed with shared-memory atomics.
+__global__ void k_spectral_modes(double* hu, double* hv, double* hw, int nx, int ny, int nz, double wfx, double wfy,
+                                 double wfz, int nyquist, double nyq_scaling, int nbin, int filter,
+                                 double* partials) {
+  extern __shared__ double sbins[];
+  __shared__ double scratch[3 * 32];
+  for (int b = threadIdx.x; b < nbin; b += blockDim.x) sbins[b] = 0.0;
+  __syncthreads();
+  double acc[3] = {0, 0, 0};
+  const size_t n = (size_t)nx * ny * nz;
+  const long long nyq2 = (long long)nyquist * nyquist;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+    const long ii = x <= nx / 2 ? x : -(long)(nx - x);
+    const long jj = y <= ny / 2 ? y : -(long)(ny - y);
+    const long kk = z <= nz / 2 ? z : -(long)(nz - z);
+    const double kx = ii * wfx, ky = jj * wfy, kz = kk * wfz;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    const double U = hu[i], V = hv[i], W = hw[i];
+    const double E = 0.5 * (U * U + V * V + W * W);
+    acc[0] += E;
+    acc[1] += k2 > 0 ? E / sqrt(k2) : 0.0;
+    const long long kind = (long long)ii * ii + (long long)jj * jj + (long long)kk * kk;
+    if (kind < nyq2) {
+      const int b = (int)floor(sqrt((double)kind) * nyq_scaling);
+      if (b < nbin) atomicAdd(&sbins[b], E);
+    }
+    if (filter) {
+      if (k2 > 0 && k2 <= 4) {
+        acc[2] += E;
+      } else {
+        hu[i] = 0.0;
+        hv[i] = 0.0;
+        hw[i] = 0.0;
+      }
+    }
+  }
+  block_reduce<3, false>(acc, scratch);
+  const int stride = 3 + nbin;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) partials[(size_t)stride * blockIdx.x + k] = acc[k];
+  for (int b = threadIdx.x; b < nbin; b += blockDim.x) partials[(size_t)stride * blockIdx.x + 3 + b] = sbins[b];
+}
+
+// Per-CTA partial sums of |curl_c u|^2 (central differences / 2h).
+template <typename T>
+__global__ void k_vorticity2(const T* u, const T* v, const T* w, int nx, int ny, int nz, double inv2h,
+                             double* partials) {
+  __shared__ double scratch[32];
+  double acc[1] = {0.0};
+  const size_t n = (size_t)nx * ny * nz;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx), y = (int)((i / nx) % ny), z = (int)(i / ((size_t)nx * ny));
+    const size_t oE = gidx(wrapi(x + 1, nx), y, z, nx, ny), oW = gidx(wrapi(x - 1, nx), y, z, nx, ny);
+    const size_t oN = gidx(x, wrapi(y + 1, ny), z, nx, ny), oS = gidx(x, wrapi(y - 1, ny), z, nx, ny);
+    const size_t oB = gidx(x, y, wrapi(z + 1, nz), nx, ny), oF = gidx(x, y, wrapi(z - 1, nz), nx, ny);
+    const double WX = inv2h * (((double)w[oN] - (double)w[oS]) - ((double)v[oB] - (double)v[oF]));
+    const double WY = inv2h * (((double)u[oB] - (double)u[oF]) - ((double)w[oE] - (double)w[oW]));
+    const double WZ = inv2h * (((double)v[oE] - (double)v[oW]) - ((double)u[oN] - (double)u[oS]));
+    acc[0] += WX * WX + WY * WY + WZ * WZ;
+  }
+  block_reduce<1, false>(acc, scratch);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+}
+
+// f += factor * g (g FP64), rounded once to the storage type.
+template <typename T>
+__global__ void k_add_scaled(T* f, const double* g, double factor, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    f[i] = (T)((double)f[i] + factor * g[i]);
+}
+
 // Diagnostics: kinetic energy and central-divergence norms (FP64).
 template <typename T>
 __global__ void k_diag(const T* u, const T* v, const T* w, int nx, int ny, int nz, double inv2h, double* partials) {
@@ -560,6 +652,11 @@ struct cup_handle {
   // discrete adjoint scratch (allocated on the first adjoint call)
   void *au = nullptr, *av = nullptr, *aw = nullptr;
   double* p_adj = nullptr;
+  // spectral analysis / forcing: FP64 Hartley coefficients of u, v, w (allocated on first use)
+  double* spec[3] = {nullptr, nullptr, nullptr};
+  bool forcing = false;                 // SpectralForcing inside cup_step / cup_run
+  double forcing_target = 0, forcing_rate = 0, forcing_prev_tke = 0;
+  double forcing_stats[6] = {0, 0, 0, 0, 0, 0};
   // obstacle adjoint scratch: the velocity before penalization u** (T) and the
   // RHS before its obstacle terms b0 (FP64), recomputed per adjoint step
   void *aus = nullptr, *avs = nullptr, *aws = nullptr;
@@ -1451,6 +1548,121 @@ int relocate_sphere(cup_handle* H) {
   return build_sphere_chi(H);
 }
 
+// The spectral sums of the current velocity (see k_spectral_modes): raw[0..2]
+// = tke, lIntegral, tkeFiltered over the separable modes (unnormalised), raw[3]
+// = sum of |curl_c u|^2 over the cells; bins = the unnormalised spectrum
+// (nBin = max(N)/2 - 1 values, HITstatistics). filter: the coefficients in
+// spec[] keep only the forcing band afterwards.
+int do_spectral(cup_handle* H, bool filter, double raw[4], std::vector<double>& bins) {
+  if (!H->spec[0])
+    for (int c = 0; c < 3; ++c) CK(cudaMalloc(&H->spec[c], H->n * sizeof(double)));
+  const int grid = std::min<size_t>(H->num_sms * 4, (H->n + 255) / 256);
+  const void* f[3] = {H->u, H->v, H->w};
+  for (int c = 0; c < 3; ++c) {
+    int rc_ = launch_named(H, "spectral_widen", [&]() -> int {
+      if (H->fp32)
+        k_widen<float><<<grid, 256, 0, H->stream>>>((const float*)f[c], H->spec[c], H->n);
+      else
+        k_widen<double><<<grid, 256, 0, H->stream>>>((const double*)f[c], H->spec[c], H->n);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+    if ((rc_ = launch_rows_pipe<double>(H, "spectral_dht_x", H->spec[c], H->spec[c], nullptr))) return rc_;
+    if ((rc_ = launch_cols<double, 1, false>(H, H->spec[c], H->spec[c], nullptr))) return rc_;
+    if ((rc_ = launch_cols<double, 2, false>(H, H->spec[c], H->spec[c], nullptr))) return rc_;
+  }
+  const int N = std::max(H->nx, std::max(H->ny, H->nz));
+  const int nyquist = N / 2, nbin = nyquist - 1;
+  const double wf[3] = {2.0 * M_PI / (H->nx * H->h), 2.0 * M_PI / (H->ny * H->h), 2.0 * M_PI / (H->nz * H->h)};
+  const double nyq_scaling = (nyquist - 1) / (double)nyquist;
+  const int stride = 3 + nbin;
+  if ((size_t)stride * grid > (size_t)kPartialCap) return fail(H, CUP_ERR_ARG, "spectrum too large for the partials");
+  double* part = partial(H, P_DIAG);
+  double* pv = partial(H, P_RES);
+  {
+    int rc_ = launch_named(H, "spectral_modes", [&]() -> int {
+      k_spectral_modes<<<grid, 256, nbin * sizeof(double), H->stream>>>(H->spec[0], H->spec[1], H->spec[2], H->nx, H->ny,
+                                                                        H->nz, wf[0], wf[1], wf[2], nyquist,
+                                                                        nyq_scaling, nbin, filter ? 1 : 0, part);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  {
+    int rc_ = launch_named(H, "spectral_vorticity", [&]() -> int {
+      if (H->fp32)
+        k_vorticity2<float><<<grid, 256, 0, H->stream>>>((const float*)H->u, (const float*)H->v, (const float*)H->w,
+                                                          H->nx, H->ny, H->nz, 0.5 / H->h, pv);
+      else
+        k_vorticity2<double><<<grid, 256, 0, H->stream>>>((const double*)H->u, (const double*)H->v,
+                                                           (const double*)H->w, H->nx, H->ny, H->nz, 0.5 / H->h, pv);
+      CKL();
+      return CUP_OK;
+    });
+    if (rc_) return rc_;
+  }
+  std::vector<double> hp((size_t)stride * grid), hv(grid);
+  CK(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaMemcpyAsync(hv.data(), pv, hv.size() * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  for (int k = 0; k < 4; ++k) raw[k] = 0.0;
+  bins.assign(nbin, 0.0);
+  for (int i = 0; i < grid; ++i) {
+    for (int k = 0; k < 3; ++k) raw[k] += hp[(size_t)stride * i + k];
+    for (int b = 0; b < nbin; ++b) bins[b] += hp[(size_t)stride * i + 3 + b];
+    raw[3] += hv[i];
+  }
+  return check_dev_error(H);
+}
+
+// SpectralForcing::operator() (source/spectralOperators/SpectralForcing.cpp:23-86):
+// the energy of the band 0 < k^2 <= 4 is raised so that the total kinetic
+// energy meets turbKinEn_target (or grows at enInjectionRate): u += fac/N H(H(u)
+// restricted to the band), fac = dt rate / (2 tke_band). out: totalKinEn,
+// largeModesKinEn, viscousDissip, dissipationRate, injectionRate, lIntegral.
+template <typename T>
+int do_spectral_forcing(cup_handle* H, double dt) {
+  double raw[4];
+  std::vector<double> bins;
+  int rc = do_spectral(H, true, raw, bins);
+  if (rc) return rc;
+  const double NF = (double)H->n;  // normalizeFFT
+  const double tke = raw[0] / (NF * NF), tkeF = raw[2] / (NF * NF);
+  const double eps = H->cfg.nu * raw[3] / NF;
+  const double dissipationRate = (H->forcing_prev_tke - tke) / dt;
+  double rate = 0;
+  if (H->forcing_target > 0) rate = (H->forcing_target - tke) / dt;
+  else if (H->forcing_rate > 0) rate = H->forcing_rate;
+  const double fac = dt * rate / (2 * tkeF);
+  H->forcing_stats[0] = tke;
+  H->forcing_stats[1] = tkeF;
+  H->forcing_stats[2] = eps;
+  H->forcing_stats[3] = dissipationRate;
+  H->forcing_stats[4] = rate;
+  H->forcing_stats[5] = raw[0] > 0 ? raw[1] / raw[0] : 0.0;
+  if (fac > 0) {
+    H->forcing_prev_tke = tke + dt * rate;
+    void* f[3] = {H->u, H->v, H->w};
+    const int grid = std::min<size_t>(H->num_sms * 4, (H->n + 255) / 256);
+    for (int c = 0; c < 3; ++c) {
+      if ((rc = launch_rows_pipe<double>(H, "spectral_dht_x", H->spec[c], H->spec[c], nullptr))) return rc;
+      if ((rc = launch_cols<double, 1, false>(H, H->spec[c], H->spec[c], nullptr))) return rc;
+      if ((rc = launch_cols<double, 2, false>(H, H->spec[c], H->spec[c], nullptr))) return rc;
+      int rc_ = launch_named(H, "spectral_force", [&]() -> int {
+        k_add_scaled<T><<<grid, 256, 0, H->stream>>>((T*)f[c], H->spec[c], fac / NF, H->n);
+        CKL();
+        return CUP_OK;
+      });
+      if (rc_) return rc_;
+    }
+  } else {
+    H->forcing_prev_tke = tke;
+  }
+  return CUP_OK;
+}
+
 // next_dt: finalize_step also computes the next step's CFL dt.
 template <typename T>
 int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance, int next_dt = 0) {
@@ -1462,6 +1674,11 @@ int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance, int 
     if ((rc = do_create_obstacles(H, dt.host))) return rc;
   }
   if ((rc = do_advect_diffuse<T>(H, dt))) return rc;
+  // SpectralForcing follows AdvectionDiffusion (source/Simulation.cpp:330-340)
+  if (H->forcing) {
+    if (dt.dev) return fail(H, CUP_ERR_STATE, "spectral forcing needs the step's dt on the host");
+    if ((rc = do_spectral_forcing<T>(H, dt.host))) return rc;
+  }
   if (H->has_sphere && H->fp32) {
     // the obstacle terms need global sums over the RHS first: RHS pass, then
     // the z-queue defect correction on the given RHS
@@ -1848,7 +2065,7 @@ int cup_destroy(cup_handle* H) {
   if (!H) return CUP_OK;
   cudaSetDevice(H->dev);
   if (H->stream) cudaStreamSynchronize(H->stream);
-  for (void* f : {H->aus, H->avs, H->aws, (void*)H->ab0})
+  for (void* f : {H->aus, H->avs, H->aws, (void*)H->ab0, (void*)H->spec[0], (void*)H->spec[1], (void*)H->spec[2]})
     if (f) cudaFree(f);
   for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->au, H->av, H->aw, (void*)H->p_adj,
                   H->chi, (void*)H->p, (void*)H->p_old, (void*)H->p_pred, (void*)H->rhs,
@@ -2357,9 +2574,10 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
     });
     if (rc_) return rc_;
   }
-  if (H->has_sphere && H->sphere_moves) {
-    // a moving sphere's box follows its position on the host: dt is read back
-    // every step (calcMaxTimestep + timestep, as the reference runs them)
+  if ((H->has_sphere && H->sphere_moves) || H->forcing) {
+    // a moving sphere's box follows its position on the host, and the
+    // forcing's injection needs dt there: dt is read back every step
+    // (calcMaxTimestep + timestep, as the reference runs them)
     for (int i = 0; i < nsteps; ++i) {
       double dt = 0;
       if ((rc = cup_calc_max_timestep(H, &dt))) return rc;
@@ -2438,6 +2656,62 @@ int cup_diagnostics(cup_handle* H, double out[3]) {
   out[1] = std::sqrt(d2 * h3);
   out[2] = dm;
   return check_dev_error(H);
+}
+
+int cup_spectral_analysis(cup_handle* H, double stats[7], double* spectrum, int nbin) {
+  REQUIRE_H(H);
+  if (!stats) return fail(H, CUP_ERR_ARG, "null stats");
+  const int N = std::max(H->nx, std::max(H->ny, H->nz));
+  if (spectrum && nbin != N / 2 - 1) return fail(H, CUP_ERR_ARG, "spectrum needs max(N)/2 - 1 = %d bins", N / 2 - 1);
+  double raw[4];
+  std::vector<double> bins;
+  int rc = do_spectral(H, false, raw, bins);
+  if (rc) return rc;
+  const double NF = (double)H->n, nu = H->cfg.nu;
+  const double tke = raw[0] / (NF * NF), eps = nu * raw[3] / NF;
+  const double uprime = std::sqrt(2 * tke / 3);
+  const double lambda = std::sqrt(15 * nu / eps) * uprime;
+  const double l_integral = raw[0] > 0 ? raw[1] / raw[0] : 0.0;
+  stats[0] = tke;
+  stats[1] = eps;
+  stats[2] = uprime;
+  stats[3] = lambda;
+  stats[4] = uprime * lambda / nu;
+  stats[5] = l_integral;
+  stats[6] = l_integral / uprime;
+  if (spectrum)
+    for (int b = 0; b < nbin; ++b) spectrum[b] = bins[b] / (NF * NF);
+  return CUP_OK;
+}
+
+int cup_set_spectral_forcing(cup_handle* H, double turbKinEn_target, double enInjectionRate) {
+  REQUIRE_H(H);
+  if (turbKinEn_target > 0 && enInjectionRate > 0)
+    return fail(H, CUP_ERR_ARG, "give either turbKinEn_target or energyInjectionRate, not both");
+  H->forcing = turbKinEn_target > 0 || enInjectionRate > 0;
+  H->forcing_target = turbKinEn_target > 0 ? turbKinEn_target : 0.0;
+  H->forcing_rate = enInjectionRate > 0 ? enInjectionRate : 0.0;
+  return CUP_OK;
+}
+
+int cup_spectral_forcing(cup_handle* H, double dt, double stats[6]) {
+  REQUIRE_H(H);
+  if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
+  reset_pressure_history(H);
+  H->umax_fresh = false;
+  int rc = DISPATCH_T(H, do_spectral_forcing, dt);
+  if (rc) return rc;
+  if (stats)
+    for (int k = 0; k < 6; ++k) stats[k] = H->forcing_stats[k];
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+int cup_get_forcing_stats(cup_handle* H, double stats[6]) {
+  REQUIRE_H(H);
+  if (!stats) return fail(H, CUP_ERR_ARG, "null stats");
+  for (int k = 0; k < 6; ++k) stats[k] = H->forcing_stats[k];
+  return CUP_OK;
 }
 
 int cup_compute_dissipation(cup_handle* H, double out[20]) {

@@ -55,6 +55,8 @@ class SimulationData:
     device: int = 0
     verbose: bool = False
     freqDiagnostics: int = 0  # ComputeDissipation every this many steps (0: off), to diagnostics.dat
+    turbKinEn_target: float = 0.0   # SpectralForcing: hold the kinetic energy at this value ...
+    enInjectionRate: float = 0.0    # ... or inject energy at this rate (SimulationData.cpp:60-66)
     saveFreq: int = 0         # restart dumps every this many steps (0: off)
     saveTime: float = 0.0     # ... or every this much simulated time (0: off)
     path4serialization: str = "./"
@@ -255,6 +257,21 @@ class ComputeDissipation(Operator):
         self.sim._diagnostics_line(self.sim.step, self.sim.time)
 
 
+class SpectralForcing(Operator):
+    """SpectralForcing (source/spectralOperators/SpectralForcing.cpp:23-86): raises the
+    energy of the band 0 < k^2 <= 4 to meet turbKinEn_target or enInjectionRate."""
+    name = "SpectralForcing"
+
+    def __call__(self, dt: float):
+        st = (C.c_double * 6)()
+        L.check(L.lib().cup_spectral_forcing(self.sim._h, float(dt), st), self.sim._h, self.name)
+        self.stats = dict(zip(FORCING_NAMES, st[:]))
+
+
+FORCING_NAMES = ("totalKinEn", "largeModesKinEn", "viscousDissip", "totalDissipRate", "injectionRate", "lIntegral")
+SPECTRAL_NAMES = ("tke", "eps", "uprime", "lambda", "Re_lambda", "l_integral", "tau_integral")
+
+
 class PoissonSolverPeriodic:
     """PoissonSolverPeriodic (source/poisson/PoissonSolverPeriodic.cpp) bound
     to a simulation's device buffers: ``solve()`` runs the FFT chain."""
@@ -319,6 +336,13 @@ class Simulation:
         self.pipeline: List[Operator] = [CreateObstacles(self), AdvectionDiffusion(self), PressureRHS(self),
                                          PressureProjection(self), UpdateObstacles(self), Penalization(self),
                                          ComputeDissipation(self)]
+        if sd.turbKinEn_target > 0 and sd.enInjectionRate > 0:
+            raise ValueError("give either turbKinEn_target or enInjectionRate, not both (SimulationData.cpp:64-66)")
+        self.forcing = sd.turbKinEn_target > 0 or sd.enInjectionRate > 0
+        if self.forcing:
+            L.check(L.lib().cup_set_spectral_forcing(h, float(sd.turbKinEn_target), float(sd.enInjectionRate)), h,
+                    "spectral forcing")
+            self.pipeline.insert(2, SpectralForcing(self))
         self.step = 0
         self.time = 0.0
         self.dt = 0.0
@@ -505,6 +529,8 @@ class Simulation:
         st = L.CupStepStats()
         dump = self._maybe_serialize(dt)
         L.check(L.lib().cup_step(self._h, float(dt), C.byref(st) if stats else None), self._h, "timestep")
+        if self.forcing:
+            self._forcing_line(self.step, self.time, dt)
         self._diagnostics_line(self.step, self.time)
         self.step += 1
         self.time += dt
@@ -525,7 +551,8 @@ class Simulation:
         if self.sd.nsteps <= 0 and self.sd.endTime <= 0:
             raise ValueError("set nsteps or endTime before run()")
         last = None
-        if self.sd.endTime <= 0 and self.sd.freqDiagnostics == 0 and self.sd.saveFreq == 0 and self.sd.saveTime == 0:
+        if (self.sd.endTime <= 0 and self.sd.freqDiagnostics == 0 and self.sd.saveFreq == 0 and self.sd.saveTime == 0
+                and not self.forcing):
             return self.run_steps(self.sd.nsteps - self.step)
         while True:
             dt = self.calcMaxTimestep()
@@ -549,6 +576,30 @@ class Simulation:
             if step == 0:
                 fh.write(DIAGNOSTICS_HEADER + "\n")
             fh.write(" ".join([str(step), f"{time:g}"] + [f"{d[k]:g}" for k in DISSIPATION_NAMES]) + "\n")
+
+    # -- spectral analysis -------------------------------------------------------
+    def spectral_analysis(self) -> dict:
+        """SpectralAnalysis (source/spectralOperators/SpectralManipFFTW.cpp:110-193): HIT
+        statistics of the current velocity and its shell spectrum E_msr (key
+        ``spectrum``; shell i at wavenumber (i + 1) 2 pi / L, L the largest extent)."""
+        n = max(self.cells)
+        nbin = n // 2 - 1
+        st, spec = (C.c_double * 7)(), (C.c_double * nbin)()
+        L.check(L.lib().cup_spectral_analysis(self._h, st, spec, nbin), self._h, "spectral_analysis")
+        out = dict(zip(SPECTRAL_NAMES, st[:]))
+        out["spectrum"] = np.array(spec[:])
+        out["k"] = (np.arange(nbin) + 1) * 2 * np.pi / (n * self.h)
+        return out
+
+    def _forcing_line(self, step: int, time: float, dt: float, path: str = "forcingData.dat"):
+        """The forcingData.dat line of SpectralForcing (SpectralForcing.cpp:56-69)."""
+        st = (C.c_double * 6)()
+        L.check(L.lib().cup_get_forcing_stats(self._h, st), self._h, "forcing stats")
+        with open(path, "a") as fh:
+            if step == 0:
+                fh.write("step \t time \t dt \t totalKinEn \t largeModesKinEn \t viscousDissip \t "
+                         "totalDissipRate \t injectionRate \t lIntegral\n")
+            fh.write("\t".join([str(step)] + [f"{x:.7e}" for x in (time, dt) + tuple(st[:])]) + "\n")
 
     # -- restart files -----------------------------------------------------------
     def serialize(self, append: str = "") -> str:

@@ -227,6 +227,23 @@ int cup_diagnostics(struct cup_handle* h, double out[3]);
  * angImpulse[3], angMomentum[3], presPow, viscPow, helicity, kineticEn,
  * enstrophy (the reference's RDX order and diagnostics.dat columns), FP64. */
 int cup_compute_dissipation(struct cup_handle* h, double out[20]);
+/* SpectralAnalysis (source/spectralOperators/SpectralManipFFTW.cpp:110-193) of the
+ * current velocity: stats = tke, eps, uprime, lambda, Re_lambda, l_integral,
+ * tau_integral; spectrum (may be NULL) = E_msr, nbin = max(N)/2 - 1 shells
+ * (HITstatistics, source/spectralOperators/SpectralManip.h:50-100). Computed on
+ * the separable Hartley transform of the Poisson passes; the shell sums equal
+ * the r2c ones. */
+int cup_spectral_analysis(struct cup_handle* h, double stats[7], double* spectrum, int nbin);
+/* SpectralForcing (source/spectralOperators/SpectralForcing.cpp:23-86) in every
+ * cup_step / cup_run step after AdvectionDiffusion, to meet turbKinEn_target or
+ * inject enInjectionRate (one of them > 0; both <= 0 turns it off). */
+int cup_set_spectral_forcing(struct cup_handle* h, double turbKinEn_target, double enInjectionRate);
+/* One SpectralForcing application to the current velocity (operator by
+ * operator); stats = totalKinEn, largeModesKinEn, viscousDissip,
+ * totalDissipRate, injectionRate, lIntegral (forcingData.dat columns). */
+int cup_spectral_forcing(struct cup_handle* h, double dt, double stats[6]);
+/* The stats of the last forcing application. */
+int cup_get_forcing_stats(struct cup_handle* h, double stats[6]);
 
 /* Test hook for the halo staging (restates tests/cubismup3d/TestBoundaries.cpp):
  * out(x) = f(x - d) through the same periodic plane-streaming TMA path the

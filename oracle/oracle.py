@@ -214,3 +214,78 @@ def set_num_threads(n: int):
 
 def num_threads() -> int:
     return lib().orc_num_threads()
+
+
+def spectral(u: np.ndarray, v: np.ndarray, w: np.ndarray, h: float, nu: float, band: bool = False):
+    """SpectralManipFFTW::_compute_analysis and _compute_largeModesForcing
+    (source/spectralOperators/SpectralManipFFTW.cpp:25-193) restated with numpy's r2c
+    DFT (the transform FFTW computes; FFTW 3.3.7 is not vendored) on [z][y][x]
+    arrays. The reference halves its fastest axis (z in its x-slowest buffer);
+    here the halved axis is x (the last): the sums run over the same
+    conjugate-symmetric spectrum with the same multiplicities.
+    Returns (stats, E_msr, band-filtered c2r fields or None): stats as
+    HITstatistics (tke, eps, uprime, lambda, Re_lambda, l_integral,
+    tau_integral, tke_filtered)."""
+    nz, ny, nx = u.shape
+    N = nx * ny * nz  # normalizeFFT
+    U, V, W = (np.fft.rfftn(f) for f in (u, v, w))
+    ii = np.arange(nx // 2 + 1)[None, None, :]
+    jj = np.where(np.arange(ny) <= ny // 2, np.arange(ny), np.arange(ny) - ny)[None, :, None]
+    kk = np.where(np.arange(nz) <= nz // 2, np.arange(nz), np.arange(nz) - nz)[:, None, None]
+    wfx, wfy, wfz = (2 * np.pi / (n * h) for n in (nx, ny, nz))
+    mult = np.where((ii == 0) | (ii == nx // 2), 1.0, 2.0)
+    kx, ky, kz = ii * wfx, jj * wfy, kk * wfz
+    k2 = kx * kx + ky * ky + kz * kz
+    dX = 2 * np.sin(2 * np.pi / nx * ii)
+    dY = 2 * np.sin(2 * np.pi / ny * jj)
+    dZ = 2 * np.sin(2 * np.pi / nz * kk)
+    OX = 1j * (dY * W - dZ * V)
+    OY = 1j * (dZ * U - dX * W)
+    OZ = 1j * (dX * V - dY * U)
+    E = mult / 2 * (np.abs(U) ** 2 + np.abs(V) ** 2 + np.abs(W) ** 2)
+    tke = E.sum()
+    eps = (mult / 2 * (np.abs(OX) ** 2 + np.abs(OY) ** 2 + np.abs(OZ) ** 2)).sum()
+    with np.errstate(divide="ignore", invalid="ignore"):
+        lint = np.where(k2 > 0, E / np.sqrt(np.where(k2 > 0, k2, 1.0)), 0.0).sum()
+    nmax = max(nx, ny, nz)
+    nyq = nmax // 2
+    nbin = nyq - 1
+    kind = ii * ii + jj * jj + kk * kk
+    sel = np.broadcast_to(kind < nyq * nyq, E.shape)
+    bins = np.floor(np.sqrt(np.broadcast_to(kind, E.shape)[sel]) * ((nyq - 1) / nyq)).astype(np.int64)
+    E_msr = np.bincount(bins, weights=E[sel], minlength=nbin)[:nbin] / N ** 2
+    st = {"tke": tke / N ** 2, "eps": eps * 2 * nu / (N * 2 * h) ** 2}
+    st["uprime"] = np.sqrt(2 * st["tke"] / 3)
+    st["lambda"] = np.sqrt(15 * nu / st["eps"]) * st["uprime"]
+    st["Re_lambda"] = st["uprime"] * st["lambda"] / nu
+    st["l_integral"] = lint / tke
+    st["tau_integral"] = st["l_integral"] / st["uprime"]
+    filtered = None
+    if band:
+        keep = np.broadcast_to((k2 > 0) & (k2 <= 4), E.shape)
+        st["tke_filtered"] = E[keep].sum() / N ** 2
+        # FFTW's c2r is unnormalised: N times numpy's irfftn
+        filtered = tuple(N * np.fft.irfftn(np.where(keep, F, 0), s=u.shape, axes=(0, 1, 2)) for F in (U, V, W))
+    return st, E_msr, filtered
+
+
+def spectral_forcing(u, v, w, h, nu, dt, target_tke=0.0, injection_rate=0.0, prev_tke=0.0):
+    """SpectralForcing::operator() (source/spectralOperators/SpectralForcing.cpp:23-86)
+    on FP64 arrays: returns the forced (u, v, w) and (totalKinEn, largeModesKinEn,
+    viscousDissip, totalDissipRate, injectionRate, next totalKinEnPrev)."""
+    st, _, filt = spectral(u, v, w, h, nu, band=True)
+    N = u.size
+    tke, tkeF = st["tke"], st["tke_filtered"]
+    rate = 0.0
+    if target_tke > 0:
+        rate = (target_tke - tke) / dt
+    elif injection_rate > 0:
+        rate = injection_rate
+    fac = dt * rate / (2 * tkeF)
+    out = (u, v, w)
+    prev = tke
+    if fac > 0:
+        prev = tke + dt * rate
+        out = tuple(f + fac / N * g for f, g in zip((u, v, w), filt))
+    return out, (tke, tkeF, st["eps"], (prev_tke - tke) / dt, rate, prev)
+

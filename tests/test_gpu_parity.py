@@ -364,6 +364,61 @@ def test_serialize_deserialize_resumes_the_run(tmp_path, moving):
         assert rel_l2(x, y) < 1e-13
 
 
+SPECTRAL_KEYS = ("tke", "eps", "uprime", "lambda", "Re_lambda", "l_integral", "tau_integral")
+
+
+@pytest.mark.parametrize("cells", [(32, 32, 32), (64, 32, 32)])
+def test_spectral_analysis_vs_numpy(oracle, cells):
+    # HIT statistics and the shell spectrum from the separable Hartley passes
+    # against the r2c restatement (numpy's DFT)
+    sim = make_sim(cells, 2 * np.pi, nu=1e-2, rampup=0, DLM=0.0, lambda_=1.0)
+    u, v, w = random_velocity(cells, 31)
+    sim.set_velocity(u, v, w)
+    got = sim.spectral_analysis()
+    ref, E, _ = oracle.spectral(u, v, w, sim.h, 1e-2)
+    for k in SPECTRAL_KEYS:
+        assert got[k] == pytest.approx(ref[k], rel=1e-10), k
+    assert np.allclose(got["spectrum"], E, rtol=1e-9, atol=1e-13 * E.max())
+
+
+def test_spectral_forcing_vs_numpy(oracle):
+    cells = (32, 32, 32)
+    nu, dt = 1e-2, 1e-2
+    u, v, w = random_velocity(cells, 37)
+    tke0 = 0.5 * np.mean(u * u + v * v + w * w)
+    sim = make_sim(cells, 2 * np.pi, nu=nu, rampup=0, DLM=0.0, lambda_=1.0, turbKinEn_target=1.3 * tke0)
+    assert [op.getName() for op in sim.pipeline][:3] == ["CreateObstacles", "AdvectionDiffusion", "SpectralForcing"]
+    sim.set_velocity(u, v, w)
+    op = sim.pipeline[2]
+    op(dt)
+    (fu, fv, fw), st = oracle.spectral_forcing(u, v, w, sim.h, nu, dt, target_tke=1.3 * tke0)
+    for a, b in zip(sim.velocity(), (fu, fv, fw)):
+        assert rel_l2(a, b) < 1e-12
+    for k, x in zip(("totalKinEn", "largeModesKinEn", "viscousDissip", "totalDissipRate", "injectionRate"), st):
+        assert op.stats[k] == pytest.approx(x, rel=1e-10), k
+    # u += fac u_band with fac = (target - tke) / (2 tke_band): the energy grows by
+    # 2 fac tke_band (the missing energy, to first order) + fac^2 tke_band
+    tkeF = op.stats["largeModesKinEn"]
+    fac = (1.3 * tke0 - op.stats["totalKinEn"]) / (2 * tkeF)
+    tke1 = 0.5 * np.mean(sum(f * f for f in sim.velocity()))
+    assert tke1 == pytest.approx(op.stats["totalKinEn"] + 2 * fac * tkeF + fac * fac * tkeF, rel=1e-9)
+
+
+def test_forced_steps_log_and_hold_energy(tmp_path, monkeypatch):
+    import cubismup_3d_b200.initial_conditions as ic
+    cells = (32, 32, 32)
+    monkeypatch.chdir(tmp_path)
+    sim = make_sim(cells, 2 * np.pi, nu=1e-2, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0, turbKinEn_target=0.2)
+    sim.set_velocity(*ic.taylor_green(cells, 2 * np.pi / 32))
+    for _ in range(4):
+        sim.timestep(sim.calcMaxTimestep())
+    lines = open(tmp_path / "forcingData.dat").read().splitlines()
+    assert lines[0].startswith("step") and len(lines) == 5
+    assert [int(l.split()[0]) for l in lines[1:]] == [0, 1, 2, 3]
+    st = sim.spectral_analysis()
+    assert st["tke"] == pytest.approx(0.2, rel=0.05)
+
+
 def test_calc_max_timestep_rampup_and_dlm(oracle):
     n = 32
     sim = make_sim((n, n, n), 1.0, nu=0.01, CFL=0.5, rampup=10, DLM=1.0, lambda_=1.0)
