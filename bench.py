@@ -313,7 +313,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
 
     # ---- end-to-end through the public API with pinned host buffers ----
     out = [torch.empty_like(p).pin_memory() for p in pinned]
-    sim_e2e_steps = min(args.steps, 50)
+    sim_e2e_steps = args.steps  # the same run length as the device-timed steps
     barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
