@@ -67,8 +67,8 @@ def kernel_bytes(name: str, fp32: bool) -> float:
 # of an ncu capture of the 256^3 FP32-DC step, profiles/step_fp32dc_upwind3_256_kernels.md),
 # scaled by the cells of the run; traffic grows with the cells streamed.
 MEASURED_DRAM_BYTES_PER_CELL_FP32DC = {
-    "grad_p_check": 47.2, "upwind3_stage1": 21.8, "upwind3_stage2": 35.0, "rhs_residual": 23.5,
-    "dht_x_update_p": 21.4, "dht_z_solve_mixed": 8.5, "dht_y_f64": 12.6, "dht_x": 4.6, "dht_y": 4.6,
+    "grad_p_check": 46.1, "upwind3_stage1": 21.7, "upwind3_stage2": 35.1, "rhs_residual": 23.5,
+    "dht_x_update_p": 21.5, "dht_z_solve_mixed": 8.6, "dht_y_f64": 12.7, "dht_x": 4.7, "dht_y": 4.6,
 }
 
 
