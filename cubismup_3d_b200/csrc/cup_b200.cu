@@ -661,6 +661,15 @@ struct cup_handle {
   // RHS before its obstacle terms b0 (FP64), recomputed per adjoint step
   void *aus = nullptr, *avs = nullptr, *aws = nullptr;
   double* ab0 = nullptr;
+  // cup_run in steady state: kGraphSteps steps captured once as a CUDA graph
+  // and replayed (the field pointers rotate with period 6: u/tmp swap every
+  // step, the three FP32-DC pressure levels every step); the graph is tied to
+  // the pointer tuple it was captured with
+  bool use_graphs = true;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  void* graph_key[9] = {};
+  long long graph_launches = 0;
   // launch accounting and optional per-kernel CUDA-event profiling
   long long launches = 0;
   bool prof_on = false;
@@ -1935,9 +1944,97 @@ int get_field(cup_handle* H, const void* src, double* dst, int where) {
 
 int valid_where(int where) { return where == CUP_WHERE_HOST || where == CUP_WHERE_DEVICE; }
 
+#define DISPATCH_T(H, fn, ...) ((H)->fp32 ? fn<float>(H, ##__VA_ARGS__) : fn<double>(H, ##__VA_ARGS__))
+
+constexpr int kGraphSteps = 6;
+
+void graph_key_of(const cup_handle* H, void* key[9]) {
+  void* k[9] = {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->p, H->p_old, H->p_pred};
+  for (int i = 0; i < 9; ++i) key[i] = k[i];
+}
+
+void drop_graph(cup_handle* H) {
+  if (H->graph_exec) cudaGraphExecDestroy(H->graph_exec);
+  if (H->graph) cudaGraphDestroy(H->graph);
+  H->graph_exec = nullptr;
+  H->graph = nullptr;
+}
+
+// A run of steps may replay a captured graph: no per-kernel profiling, a
+// stream that can be captured, nothing that needs the host between steps
+// (a moving obstacle, spectral forcing), and the FP32-DC pressure history in
+// its steady state (warm start ready), so that every step issues the same
+// launches.
+bool graph_ok(const cup_handle* H) {
+  if (!H->use_graphs || H->prof_on || !H->stream || H->forcing) return false;
+  if (H->has_sphere && H->sphere_moves) return false;
+  if (H->fp32 && !(H->pred_ready && H->p_valid >= 1)) return false;
+  return true;
+}
+
+// Runs floor(maxsteps / kGraphSteps) * kGraphSteps steps of a cup_run through
+// the graph (captured here when the pointer tuple differs from the graph's),
+// each step computing the next step's dt on the device; *done = steps run
+// (0: the capture failed and nothing ran; the host state is as before).
+int run_graph_steps(cup_handle* H, int maxsteps, int* done) {
+  *done = 0;
+  const int reps = maxsteps / kGraphSteps;
+  if (reps == 0) return CUP_OK;
+  void* key[9];
+  graph_key_of(H, key);
+  bool same = H->graph_exec != nullptr;
+  for (int i = 0; i < 9 && same; ++i) same = key[i] == H->graph_key[i];
+  if (!same) {
+    drop_graph(H);
+    // host state a failed capture must restore (the launches advance it)
+    void* k0[9];
+    graph_key_of(H, k0);
+    const int p_valid0 = H->p_valid, ngp0 = H->n_grad_partials, gs0 = H->grad_stride, gm0 = H->grad_max_off,
+              gk0 = H->grad_ke_off;
+    const bool pr0 = H->pred_ready;
+    const long long l0 = H->launches;
+    if (cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+      cudaGetLastError();
+      H->use_graphs = false;
+      return CUP_OK;
+    }
+    int rc = CUP_OK;
+    for (int s = 0; s < kGraphSteps && rc == CUP_OK; ++s)
+      rc = DISPATCH_T(H, do_step, DtArg{0.0, &H->dstate->dt}, (const double*)&H->dstate->lambda, 1, 1);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(H->stream, &g);
+    void* k1[9];
+    graph_key_of(H, k1);
+    bool cycled = true;
+    for (int i = 0; i < 9; ++i) cycled = cycled && k1[i] == k0[i];
+    cudaGraphExec_t ex = nullptr;
+    if (rc == CUP_OK && e == cudaSuccess && g && cycled && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
+      H->graph = g;
+      H->graph_exec = ex;
+      for (int i = 0; i < 9; ++i) H->graph_key[i] = k0[i];
+      H->graph_launches = H->launches - l0;
+      H->launches = l0;
+    } else {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      H->u = k0[0], H->v = k0[1], H->w = k0[2], H->tu = k0[3], H->tv = k0[4], H->tw = k0[5];
+      H->p = (double*)k0[6], H->p_old = (double*)k0[7], H->p_pred = (double*)k0[8];
+      H->p_valid = p_valid0, H->pred_ready = pr0, H->n_grad_partials = ngp0, H->grad_stride = gs0;
+      H->grad_max_off = gm0, H->grad_ke_off = gk0, H->launches = l0;
+      H->use_graphs = false;
+      return CUP_OK;
+    }
+  }
+  for (int r = 0; r < reps; ++r) {
+    CK(cudaGraphLaunch(H->graph_exec, H->stream));
+    H->launches += H->graph_launches;
+  }
+  *done = reps * kGraphSteps;
+  return CUP_OK;
+}
+
 }  // namespace
 
-#define DISPATCH_T(H, fn, ...) ((H)->fp32 ? fn<float>(H, ##__VA_ARGS__) : fn<double>(H, ##__VA_ARGS__))
 
 #define REQUIRE_H(H)                        \
   do {                                      \
@@ -2065,6 +2162,7 @@ int cup_destroy(cup_handle* H) {
   if (!H) return CUP_OK;
   cudaSetDevice(H->dev);
   if (H->stream) cudaStreamSynchronize(H->stream);
+  drop_graph(H);
   for (void* f : {H->aus, H->avs, H->aws, (void*)H->ab0, (void*)H->spec[0], (void*)H->spec[1], (void*)H->spec[2]})
     if (f) cudaFree(f);
   for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->au, H->av, H->aw, (void*)H->p_adj,
@@ -2267,6 +2365,13 @@ int cup_set_uinf(cup_handle* H, const double uinf[3]) {
   if (H->has_sphere) return fail(H, CUP_ERR_STATE, "cup_set_uinf: with an obstacle the frame velocity follows it");
   for (int d = 0; d < 3; ++d) H->uinf[d] = uinf[d];
   H->umax_fresh = false;
+  return CUP_OK;
+}
+
+int cup_set_graphs(cup_handle* H, int on) {
+  REQUIRE_H(H);
+  H->use_graphs = on != 0;
+  if (!H->use_graphs) drop_graph(H);
   return CUP_OK;
 }
 
@@ -2586,7 +2691,7 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
     if (stats) return fill_stats(H, stats);
     return CUP_OK;
   }
-  for (int i = 0; i < nsteps; ++i) {
+  for (int i = 0; i < nsteps;) {
     // the dt of step i > 0 comes from the end of step i - 1
     if (i == 0) {
       int rc_ = launch_named(H, "calc_dt", [&]() -> int {
@@ -2596,9 +2701,20 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
       });
       if (rc_) return rc_;
     }
+    // steady state: whole graphs of steps, keeping the last step (which does
+    // not compute a next dt) out of them
+    if (nsteps - i > kGraphSteps && graph_ok(H)) {
+      int done = 0;
+      if ((rc = run_graph_steps(H, nsteps - i - 1, &done))) return rc;
+      if (done > 0) {
+        i += done;
+        continue;
+      }
+    }
     rc = DISPATCH_T(H, do_step, DtArg{0.0, &H->dstate->dt}, (const double*)&H->dstate->lambda, 1,
                     i + 1 < nsteps ? 1 : 0);
     if (rc) return rc;
+    ++i;
   }
   if ((rc = read_state(H))) return rc;
   H->step = H->hstate->step;

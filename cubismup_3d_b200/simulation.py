@@ -539,6 +539,10 @@ class Simulation:
             self.serialize()
         return StepStats.from_c(st) if stats else None
 
+    def use_graphs(self, on: bool = True):
+        """run_steps replays its steady-state steps as a captured CUDA graph (default on)."""
+        L.check(L.lib().cup_set_graphs(self._h, int(bool(on))), self._h, "use_graphs")
+
     def run_steps(self, nsteps: int) -> StepStats:
         """nsteps of calcMaxTimestep + timestep with dt chained on the device."""
         st = L.CupStepStats()

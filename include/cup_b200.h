@@ -178,6 +178,9 @@ int cup_step(struct cup_handle* h, double dt, cup_step_stats* stats);
 /* Simulation::run (source/Simulation.cpp:582-591) for nsteps: calcMaxTimestep + timestep,
  * with dt computed on the device (no host round trip per step). */
 int cup_run(struct cup_handle* h, int nsteps, cup_step_stats* stats);
+/* cup_run replays its steady-state steps as a CUDA graph of 6 steps (captured
+ * on first use; same kernels, same results); off: every step is launched. */
+int cup_set_graphs(struct cup_handle* h, int on);
 
 /* Discrete adjoint of one cup_step with the given dt (no counterpart in the
  * reference, which has no adjoint). un, vn, wn: the velocity at the start of the

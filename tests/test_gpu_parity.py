@@ -419,6 +419,34 @@ def test_forced_steps_log_and_hold_energy(tmp_path, monkeypatch):
     assert st["tke"] == pytest.approx(0.2, rel=0.05)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32_dc"])
+def test_run_steps_graph_replay_matches_launches(precision):
+    # run_steps replays steady-state steps from a captured CUDA graph: the same
+    # kernels in the same order, so the results are bitwise those of launching
+    # every step
+    cells = (64, 64, 64)
+    u, v, w = random_velocity(cells, 41, 0.5)
+    out = []
+    for graphs in (True, False):
+        sim = make_sim(cells, 2 * np.pi, nu=1e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0, precision=precision,
+                       scheme="upwind3_rk2")
+        sim.use_graphs(graphs)
+        sim.set_velocity(u, v, w)
+        n0 = sim.launch_count()
+        st = sim.run_steps(20)
+        out.append((st, sim.velocity(), sim.launch_count() - n0))
+        st2 = sim.run_steps(9)  # the captured graph again (same pointer tuple after a multiple of 6 steps)
+        out[-1] += (st2, sim.velocity())
+    (a_st, a_v, a_n, a_st2, a_v2), (b_st, b_v, b_n, b_st2, b_v2) = out
+    assert a_st.step == b_st.step == 20 and a_st.time == b_st.time and a_st.dt == b_st.dt
+    assert a_n == b_n  # replayed launches are counted
+    for x, y in zip(a_v, b_v):
+        assert np.array_equal(x, y)
+    assert a_st2.step == b_st2.step == 29 and a_st2.time == b_st2.time
+    for x, y in zip(a_v2, b_v2):
+        assert np.array_equal(x, y)
+
+
 def test_calc_max_timestep_rampup_and_dlm(oracle):
     n = 32
     sim = make_sim((n, n, n), 1.0, nu=0.01, CFL=0.5, rampup=10, DLM=1.0, lambda_=1.0)
