@@ -666,10 +666,20 @@ struct cup_handle {
   // step, the three FP32-DC pressure levels every step); the graph is tied to
   // the pointer tuple it was captured with
   bool use_graphs = true;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t graph_exec = nullptr;
-  void* graph_key[9] = {};
-  long long graph_launches = 0;
+  // host state a step reads and advances (the graph replays the device part)
+  struct StepState {
+    void* f[9];  // u, v, w, tu, tv, tw, p, p_old, p_pred
+    int p_valid, n_grad_partials, grad_stride, grad_max_off, grad_ke_off;
+    bool pred_ready;
+  };
+  struct StepGraph {
+    StepState in, out;
+    int nsteps, next_dt;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    long long launches;
+  };
+  std::vector<StepGraph> graphs;
   // launch accounting and optional per-kernel CUDA-event profiling
   long long launches = 0;
   bool prof_on = false;
@@ -1948,23 +1958,39 @@ int valid_where(int where) { return where == CUP_WHERE_HOST || where == CUP_WHER
 
 constexpr int kGraphSteps = 6;
 
-void graph_key_of(const cup_handle* H, void* key[9]) {
-  void* k[9] = {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->p, H->p_old, H->p_pred};
-  for (int i = 0; i < 9; ++i) key[i] = k[i];
+cup_handle::StepState step_state(const cup_handle* H) {
+  cup_handle::StepState s{{H->u, H->v, H->w, H->tu, H->tv, H->tw, H->p, H->p_old, H->p_pred},
+                          H->p_valid, H->n_grad_partials, H->grad_stride, H->grad_max_off, H->grad_ke_off,
+                          H->pred_ready};
+  return s;
+}
+
+void set_step_state(cup_handle* H, const cup_handle::StepState& s) {
+  H->u = s.f[0], H->v = s.f[1], H->w = s.f[2], H->tu = s.f[3], H->tv = s.f[4], H->tw = s.f[5];
+  H->p = (double*)s.f[6], H->p_old = (double*)s.f[7], H->p_pred = (double*)s.f[8];
+  H->p_valid = s.p_valid, H->n_grad_partials = s.n_grad_partials, H->grad_stride = s.grad_stride;
+  H->grad_max_off = s.grad_max_off, H->grad_ke_off = s.grad_ke_off, H->pred_ready = s.pred_ready;
+}
+
+bool same_state(const cup_handle::StepState& a, const cup_handle::StepState& b) {
+  for (int i = 0; i < 9; ++i)
+    if (a.f[i] != b.f[i]) return false;
+  return a.p_valid == b.p_valid && a.n_grad_partials == b.n_grad_partials && a.grad_stride == b.grad_stride &&
+         a.grad_max_off == b.grad_max_off && a.grad_ke_off == b.grad_ke_off && a.pred_ready == b.pred_ready;
 }
 
 void drop_graph(cup_handle* H) {
-  if (H->graph_exec) cudaGraphExecDestroy(H->graph_exec);
-  if (H->graph) cudaGraphDestroy(H->graph);
-  H->graph_exec = nullptr;
-  H->graph = nullptr;
+  for (auto& g : H->graphs) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+  }
+  H->graphs.clear();
 }
 
-// A run of steps may replay a captured graph: no per-kernel profiling, a
-// stream that can be captured, nothing that needs the host between steps
-// (a moving obstacle, spectral forcing), and the FP32-DC pressure history in
-// its steady state (warm start ready), so that every step issues the same
-// launches.
+// Steps may replay a captured graph: no per-kernel profiling, a stream that
+// can be captured, nothing that needs the host between steps (a moving
+// obstacle, spectral forcing), and the FP32-DC pressure history in its steady
+// state (warm start ready), so that every step issues the same launches.
 bool graph_ok(const cup_handle* H) {
   if (!H->use_graphs || H->prof_on || !H->stream || H->forcing) return false;
   if (H->has_sphere && H->sphere_moves) return false;
@@ -1972,26 +1998,20 @@ bool graph_ok(const cup_handle* H) {
   return true;
 }
 
-// Runs floor(maxsteps / kGraphSteps) * kGraphSteps steps of a cup_run through
-// the graph (captured here when the pointer tuple differs from the graph's),
-// each step computing the next step's dt on the device; *done = steps run
-// (0: the capture failed and nothing ran; the host state is as before).
-int run_graph_steps(cup_handle* H, int maxsteps, int* done) {
-  *done = 0;
-  const int reps = maxsteps / kGraphSteps;
-  if (reps == 0) return CUP_OK;
-  void* key[9];
-  graph_key_of(H, key);
-  bool same = H->graph_exec != nullptr;
-  for (int i = 0; i < 9 && same; ++i) same = key[i] == H->graph_key[i];
-  if (!same) {
-    drop_graph(H);
-    // host state a failed capture must restore (the launches advance it)
-    void* k0[9];
-    graph_key_of(H, k0);
-    const int p_valid0 = H->p_valid, ngp0 = H->n_grad_partials, gs0 = H->grad_stride, gm0 = H->grad_max_off,
-              gk0 = H->grad_ke_off;
-    const bool pr0 = H->pred_ready;
+// Runs nsteps steps (dt from the device state; next_dt: each computes the
+// next step's dt) from a CUDA graph captured once per host state (the field
+// pointers rotate with period 6: the u/tmp swap and the three FP32-DC
+// pressure levels) and replayed with the host state set to what the captured
+// steps left. *ran = false: the capture failed, nothing ran, the host state
+// is as before and graphs are off for the handle.
+int run_graph(cup_handle* H, int nsteps, int next_dt, bool* ran) {
+  *ran = false;
+  const cup_handle::StepState in = step_state(H);
+  cup_handle::StepGraph* hit = nullptr;
+  for (auto& g : H->graphs)
+    if (g.nsteps == nsteps && g.next_dt == next_dt && same_state(g.in, in)) hit = &g;
+  if (!hit) {
+    if (H->graphs.size() >= 16) drop_graph(H);
     const long long l0 = H->launches;
     if (cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
       cudaGetLastError();
@@ -1999,37 +2019,28 @@ int run_graph_steps(cup_handle* H, int maxsteps, int* done) {
       return CUP_OK;
     }
     int rc = CUP_OK;
-    for (int s = 0; s < kGraphSteps && rc == CUP_OK; ++s)
-      rc = DISPATCH_T(H, do_step, DtArg{0.0, &H->dstate->dt}, (const double*)&H->dstate->lambda, 1, 1);
+    for (int s = 0; s < nsteps && rc == CUP_OK; ++s)
+      rc = DISPATCH_T(H, do_step, DtArg{0.0, &H->dstate->dt}, (const double*)&H->dstate->lambda, 1, next_dt);
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(H->stream, &g);
-    void* k1[9];
-    graph_key_of(H, k1);
-    bool cycled = true;
-    for (int i = 0; i < 9; ++i) cycled = cycled && k1[i] == k0[i];
     cudaGraphExec_t ex = nullptr;
-    if (rc == CUP_OK && e == cudaSuccess && g && cycled && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
-      H->graph = g;
-      H->graph_exec = ex;
-      for (int i = 0; i < 9; ++i) H->graph_key[i] = k0[i];
-      H->graph_launches = H->launches - l0;
+    if (rc == CUP_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
+      H->graphs.push_back({in, step_state(H), nsteps, next_dt, g, ex, H->launches - l0});
+      hit = &H->graphs.back();
       H->launches = l0;
     } else {
       if (g) cudaGraphDestroy(g);
       cudaGetLastError();
-      H->u = k0[0], H->v = k0[1], H->w = k0[2], H->tu = k0[3], H->tv = k0[4], H->tw = k0[5];
-      H->p = (double*)k0[6], H->p_old = (double*)k0[7], H->p_pred = (double*)k0[8];
-      H->p_valid = p_valid0, H->pred_ready = pr0, H->n_grad_partials = ngp0, H->grad_stride = gs0;
-      H->grad_max_off = gm0, H->grad_ke_off = gk0, H->launches = l0;
+      set_step_state(H, in);
+      H->launches = l0;
       H->use_graphs = false;
       return CUP_OK;
     }
   }
-  for (int r = 0; r < reps; ++r) {
-    CK(cudaGraphLaunch(H->graph_exec, H->stream));
-    H->launches += H->graph_launches;
-  }
-  *done = reps * kGraphSteps;
+  CK(cudaGraphLaunch(hit->exec, H->stream));
+  H->launches += hit->launches;
+  set_step_state(H, hit->out);
+  *ran = true;
   return CUP_OK;
 }
 
@@ -2310,6 +2321,7 @@ int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
   (void)anyForced;
   H->has_sphere = true;
   H->sphere = *s;
+  drop_graph(H);  // captured steps hold no obstacle
   const size_t es = H->fp32 ? sizeof(float) : sizeof(double);
   CK(cudaMalloc(&H->chi, H->n * es));
   CK(cudaMemsetAsync(H->chi, 0, H->n * es, H->stream));
@@ -2344,6 +2356,7 @@ int cup_set_sphere_position(cup_handle* H, const double position[3]) {
   if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_set_sphere_position: the handle has no obstacle");
   if (!position) return fail(H, CUP_ERR_ARG, "null position");
   for (int d = 0; d < 3; ++d) H->sphere.position[d] = position[d];
+  drop_graph(H);  // captured steps hold the obstacle's box
   int rc = relocate_sphere(H);
   if (rc) return rc;
   H->umax_fresh = false;
@@ -2364,6 +2377,7 @@ int cup_set_uinf(cup_handle* H, const double uinf[3]) {
   if (!uinf) return fail(H, CUP_ERR_ARG, "null uinf");
   if (H->has_sphere) return fail(H, CUP_ERR_STATE, "cup_set_uinf: with an obstacle the frame velocity follows it");
   for (int d = 0; d < 3; ++d) H->uinf[d] = uinf[d];
+  drop_graph(H);  // captured steps hold uinf
   H->umax_fresh = false;
   return CUP_OK;
 }
@@ -2557,7 +2571,12 @@ int cup_step(cup_handle* H, double dt, cup_step_stats* stats) {
     });
     if (rc_) return rc_;
   }
-  int rc = DISPATCH_T(H, do_step, DtArg{dt, nullptr}, (const double*)&H->dstate->lambda, 1);
+  // one step from a captured graph in the steady state (it reads dt from the
+  // device state set above), else launched
+  bool ran = false;
+  int rc = graph_ok(H) ? run_graph(H, 1, 0, &ran) : CUP_OK;
+  if (rc) return rc;
+  if (!ran) rc = DISPATCH_T(H, do_step, DtArg{dt, nullptr}, (const double*)&H->dstate->lambda, 1);
   if (rc) return rc;
   H->step += 1;
   H->time += dt;
@@ -2704,10 +2723,10 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
     // steady state: whole graphs of steps, keeping the last step (which does
     // not compute a next dt) out of them
     if (nsteps - i > kGraphSteps && graph_ok(H)) {
-      int done = 0;
-      if ((rc = run_graph_steps(H, nsteps - i - 1, &done))) return rc;
-      if (done > 0) {
-        i += done;
+      bool ran = false;
+      if ((rc = run_graph(H, kGraphSteps, 1, &ran))) return rc;
+      if (ran) {
+        i += kGraphSteps;
         continue;
       }
     }

@@ -437,13 +437,19 @@ def test_run_steps_graph_replay_matches_launches(precision):
         out.append((st, sim.velocity(), sim.launch_count() - n0))
         st2 = sim.run_steps(9)  # the captured graph again (same pointer tuple after a multiple of 6 steps)
         out[-1] += (st2, sim.velocity())
-    (a_st, a_v, a_n, a_st2, a_v2), (b_st, b_v, b_n, b_st2, b_v2) = out
+        for _ in range(8):  # timestep: one-step graphs, one per phase of the pointer rotation
+            st3 = sim.timestep(sim.calcMaxTimestep())
+        out[-1] += (st3, sim.velocity())
+    (a_st, a_v, a_n, a_st2, a_v2, a_st3, a_v3), (b_st, b_v, b_n, b_st2, b_v2, b_st3, b_v3) = out
     assert a_st.step == b_st.step == 20 and a_st.time == b_st.time and a_st.dt == b_st.dt
     assert a_n == b_n  # replayed launches are counted
     for x, y in zip(a_v, b_v):
         assert np.array_equal(x, y)
     assert a_st2.step == b_st2.step == 29 and a_st2.time == b_st2.time
     for x, y in zip(a_v2, b_v2):
+        assert np.array_equal(x, y)
+    assert a_st3.time == b_st3.time and a_st3.kinetic_energy == b_st3.kinetic_energy
+    for x, y in zip(a_v3, b_v3):
         assert np.array_equal(x, y)
 
 
