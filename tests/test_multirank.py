@@ -1,7 +1,7 @@
 """The multi-process plumbing of ``bench.py`` on CPU (world_size 2, gloo).
 
-On GPUs each rank is an independent replica of the simulation (the path has
-no exchange step in this build): the only collectives are the barrier around
+On GPUs each rank is an independent replica of the simulation (the ranks
+exchange no data): the only collectives are the barrier around
 the timed region and the max over ranks of the device time. These tests run
 the same helpers over gloo on the host, and the reference arm under two
 ranks: rank 0 alone runs the CPU baseline and prints the JSON line.
