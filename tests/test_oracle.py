@@ -191,3 +191,69 @@ def test_tangent_linear_matches_central_differences(oracle, scheme):
     fd = [(a - b) / (2 * eps) for a, b in zip(*out)]
     for a, b in zip(tang, fd):
         assert rel_l2(a, b) < 1e-6
+
+
+def test_moving_sphere_advances_with_its_velocity(oracle):
+    # bFixFrameOfRef off: uinf = 0 (updateUinf) and every step moves the sphere
+    # by dt U (Obstacle::update) before chi is rebuilt; the grid CoM follows
+    n = 32
+    sphere = {"radius": 0.15, "position": (0.4, 0.5, 0.5), "velocity": (1.0, 0.5, 0.0), "forced": (1, 1, 1),
+              "fix_frame": (0, 0, 0)}
+    sim = oracle.OracleSim(n, n, n, 1.0, nu=0.01, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6,
+                           implicit_penalization=True, sphere=sphere)
+    com0 = sim.stats()["com"].copy()
+    assert np.allclose(sim.stats()["uinf"], 0.0)
+    dts = sim.run(4)
+    shift = sim.stats()["com"] - com0
+    travelled = np.sum(dts) * np.array([1.0, 0.5, 0.0])
+    # the CoM of the discrete chi tracks the position to a fraction of a cell
+    assert np.allclose(shift, travelled, atol=0.1 / n)
+
+
+def test_dissipation_sums_vs_numpy(oracle):
+    # ComputeDissipation's linear and quadratic sums restated in numpy on the
+    # oracle's own fields (periodic central differences)
+    n, L = 32, 2 * np.pi
+    sim = oracle.OracleSim(n, n, n, L, nu=0.01, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0)
+    rng = np.random.default_rng(3)
+    u, v, w = (rng.standard_normal((n, n, n)) for _ in range(3))
+    sim.set_velocity(u, v, w)
+    sim.run(2)
+    d = sim.dissipation()
+    u, v, w, p = (sim.get(k) for k in ("u", "v", "w", "p"))
+    h = L / n
+    h3 = h ** 3
+
+    def dd(f, ax):
+        return (np.roll(f, -1, ax) - np.roll(f, 1, ax)) / (2 * h)
+
+    wx, wy, wz = dd(w, 1) - dd(v, 0), dd(u, 0) - dd(w, 2), dd(v, 2) - dd(u, 1)
+    assert d[18] == pytest.approx(h3 * 0.5 * np.sum(u * u + v * v + w * w), rel=1e-12)  # kineticEn
+    assert np.allclose(d[6:9], [h3 * u.sum(), h3 * v.sum(), h3 * w.sum()], rtol=1e-10, atol=1e-12)  # linMom
+    assert np.allclose(d[0:3], [h3 * wx.sum(), h3 * wy.sum(), h3 * wz.sum()], atol=1e-10)  # circulation ~ 0
+    assert d[17] == pytest.approx(h3 * np.sum(wx * u + wy * v + wz * w), rel=1e-9, abs=1e-9)  # helicity
+    assert d[19] == pytest.approx(np.sum(np.sqrt(wx * wx + wy * wy + wz * wz)), rel=1e-12)  # enstrophy
+    pres = -h3 * np.sum(dd(p, 2) * u + dd(p, 1) * v + dd(p, 0) * w)
+    assert d[15] == pytest.approx(pres, rel=1e-9, abs=1e-12)  # presPow
+
+
+def test_spectral_restatement_parseval(oracle):
+    # the r2c restatement of the HIT statistics against physical-space
+    # identities: tke = <|u|^2> / 2, eps = nu <|curl_c u|^2>; the forcing band
+    # field carries exactly tke_filtered
+    rng = np.random.default_rng(5)
+    shape = (16, 32, 32)
+    u, v, w = (rng.standard_normal(shape) for _ in range(3))
+    h, nu = 0.1, 0.02
+    st, E, filt = oracle.spectral(u, v, w, h, nu, band=True)
+    assert st["tke"] == pytest.approx(0.5 * np.mean(u * u + v * v + w * w), rel=1e-12)
+
+    def dd(f, ax):
+        return (np.roll(f, -1, ax) - np.roll(f, 1, ax)) / (2 * h)
+
+    wx, wy, wz = dd(w, 1) - dd(v, 0), dd(u, 0) - dd(w, 2), dd(v, 2) - dd(u, 1)
+    assert st["eps"] == pytest.approx(nu * np.mean(wx * wx + wy * wy + wz * wz), rel=1e-12)
+    N = u.size
+    fu, fv, fw = (f / N for f in filt)
+    assert st["tke_filtered"] == pytest.approx(0.5 * np.mean(fu * fu + fv * fv + fw * fw), rel=1e-10)
+    assert len(E) == max(shape) // 2 - 1 and np.all(E >= 0) and E.sum() <= st["tke"]
