@@ -834,7 +834,7 @@ int launch_rows_M(cup_handle* H, const char* name, const Prod& prod, const Cons&
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
   // the read-modify-write of p runs on half tiles (128 threads): more CTAs per
   // SM overlap one CTA's bulk copies with another's transform
-  const int lpc = (Cons::kAddBulk && TPL <= 16 ? 128 : 256) / TPL;
+  const int lpc = 256 / TPL;
   const int nrows = H->ny * H->nz;
   // reduction scratch only for producers that compute rows (and may reduce)
   const size_t scratch = Prod::kBulk ? 0 : 32 * 20 * sizeof(double);
