@@ -7,6 +7,8 @@ reference's Python bindings (``cubismup3d.SimulationData``, ``Simulation``,
 """
 from .simulation import (  # noqa: F401
     AdvectionDiffusion,
+    ComputeDissipation,
+    CreateObstacles,
     ObstacleArguments,
     Operator,
     Penalization,
@@ -15,15 +17,17 @@ from .simulation import (  # noqa: F401
     PressureRHS,
     Simulation,
     SimulationData,
+    SpectralForcing,
     Sphere,
     StepStats,
+    UpdateObstacles,
     blocks_to_global,
     global_to_blocks,
 )
 from . import _lib  # noqa: F401
 
 __all__ = [
-    "AdvectionDiffusion", "ObstacleArguments", "Operator", "Penalization", "PoissonSolverPeriodic",
-    "PressureProjection", "PressureRHS", "Simulation", "SimulationData", "Sphere", "StepStats",
-    "blocks_to_global", "global_to_blocks",
+    "AdvectionDiffusion", "ComputeDissipation", "CreateObstacles", "ObstacleArguments", "Operator", "Penalization",
+    "PoissonSolverPeriodic", "PressureProjection", "PressureRHS", "Simulation", "SimulationData", "SpectralForcing",
+    "Sphere", "StepStats", "UpdateObstacles", "blocks_to_global", "global_to_blocks",
 ]
