@@ -95,6 +95,7 @@ SIGNATURES = {
     "cup_add_sphere": (C.c_int, [_H, C.POINTER(CupSphere)]),
     "cup_create_obstacles": (C.c_int, [_H, C.c_double]),
     "cup_set_graphs": (C.c_int, [_H, C.c_int]),
+    "cup_prepare_run": (C.c_int, [_H, C.POINTER(C.c_int)]),
     "cup_set_sphere_position": (C.c_int, [_H, _dp]),
     "cup_get_sphere_position": (C.c_int, [_H, _dp]),
     "cup_set_uinf": (C.c_int, [_H, _dp]),
@@ -106,6 +107,9 @@ SIGNATURES = {
     "cup_pressure_rhs": (C.c_int, [_H, C.c_double]),
     "cup_poisson_solve": (C.c_int, [_H, C.POINTER(CupSolveStats)]),
     "cup_grad_correct": (C.c_int, [_H, C.c_double]),
+    "cup_poisson_buffer": (C.c_int, [_H, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "cup_poisson_reset": (C.c_int, [_H]),
+    "cup_set_rhs": (C.c_int, [_H, C.c_void_p, C.c_int]),
     "cup_pressure_projection": (C.c_int, [_H, C.c_double, C.POINTER(CupSolveStats)]),
     "cup_penalize": (C.c_int, [_H, C.c_double, _dp]),
     "cup_step": (C.c_int, [_H, C.c_double, C.POINTER(CupStepStats)]),

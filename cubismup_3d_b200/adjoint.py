@@ -13,6 +13,13 @@ the segment's checkpoint, recomputes the segment's states forward and applies
 the adjoint steps in reverse. Peak extra memory is (n/K + K) velocity fields
 for n steps and checkpoint interval K, so long rollouts fit in HBM.
 
+The forward and the recomputation advance the handle with ``Simulation._advance``
+(the step and the clock only), so a rollout writes no restart dump and no
+diagnostics.dat / forcingData.dat line. In FP32-DC form the recomputed states
+match the forward ones to within the defect-correction tolerance, not bitwise:
+restoring a checkpoint restarts the pressure warm start, so the recomputed
+steps start their correction solves from another initial pressure.
+
 The fixed-dt convention makes the rollout a smooth function of u0 except where
 an upwind switch flips sign; the adjoint freezes the switch at the forward
 state (the derivative from either side at a kink is the one-sided one).
@@ -40,6 +47,8 @@ class Rollout(torch.autograd.Function):
     def forward(ctx, u0: torch.Tensor, sim: Simulation, dts: Sequence[float], checkpoint_every: int):
         if sim.obstacles:
             raise ValueError("rollout: the discrete adjoint does not support obstacles")
+        if sim.forcing:
+            raise ValueError("rollout: spectral forcing has no discrete adjoint")
         K = int(checkpoint_every)
         if K < 1:
             raise ValueError("checkpoint_every must be >= 1")
@@ -51,7 +60,7 @@ class Rollout(torch.autograd.Function):
         for s, dt in enumerate(dts):
             if s % K == 0:
                 ckpts.append(sim.velocity_raw())
-            sim.timestep(dt, stats=False)
+            sim._advance(dt)
         uT = sim.velocity_raw()
         ctx.sim, ctx.dts, ctx.K, ctx.ckpts, ctx.clock = sim, dts, K, ckpts, clock
         ctx.in_dtype = u0.dtype
@@ -70,7 +79,7 @@ class Rollout(torch.autograd.Function):
             sim.set_velocity_raw(ctx.ckpts[seg])
             states = [ctx.ckpts[seg]]
             for s in range(s0, s1 - 1):
-                sim.timestep(dts[s], stats=False)
+                sim._advance(dts[s])
                 states.append(sim.velocity_raw())
             for s in reversed(range(s0, s1)):
                 sim.adjoint_step(states[s - s0], dts[s], lam)
@@ -87,6 +96,8 @@ def obstacle_gradients(sim: Simulation, u0: torch.Tensor, dts: Sequence[float], 
     grid's shape, FP64 of 3), plus the list of forces F_n of the forward."""
     if not sim.obstacles:
         raise ValueError("obstacle_gradients: the simulation has no obstacle")
+    if sim.forcing:
+        raise ValueError("obstacle_gradients: spectral forcing has no discrete adjoint")
     K = int(checkpoint_every)
     if K < 1:
         raise ValueError("checkpoint_every must be >= 1")
@@ -99,7 +110,7 @@ def obstacle_gradients(sim: Simulation, u0: torch.Tensor, dts: Sequence[float], 
     for s, dt in enumerate(dts):
         if s % K == 0:
             ckpts.append(sim.velocity_raw())
-        forces.append(sim.timestep(dt).force.copy())
+        forces.append(sim._advance(dt, stats=True).force.copy())
     end_clock = (sim.step, sim.time)
     dev = u0.device
     lam = (torch.zeros((3,) + sim.shape, dtype=sim.storage_dtype, device=dev) if grad_uT is None
@@ -112,7 +123,7 @@ def obstacle_gradients(sim: Simulation, u0: torch.Tensor, dts: Sequence[float], 
         sim.set_velocity_raw(ckpts[seg])
         states = [ckpts[seg]]
         for s in range(s0, s1 - 1):
-            sim.timestep(dts[s], stats=False)
+            sim._advance(dts[s])
             states.append(sim.velocity_raw())
         for s in reversed(range(s0, s1)):
             sim.adjoint_step_obstacle(states[s - s0], dts[s], lam, w_force, g_chi, g_vel)

@@ -177,19 +177,40 @@ class Operator {
   virtual std::string getName() = 0;
 };
 
+// PoissonSolver (source/poisson/PoissonSolver.h:22-122): the public buffer
+// contract `data`, stridex/y/z, data_size, _offset / _offset_ext / _dest,
+// reset() and _fftw2cub(). `data` is the handle's FP64 device array: device
+// code (or cudaMemcpy, or cup_set_rhs for a host array) writes the
+// h^3-premultiplied RHS at data[_dest(_offset_ext(info), iz, iy, ix)] before
+// solve(), as the reference's kernels write solver->data.
 class PoissonSolver {
  public:
+  size_t stridez = 0, stridey = 0, stridex = 0, data_size = 0;
+  Real* data = nullptr;
   virtual ~PoissonSolver() = default;
   virtual void solve() = 0;
+  virtual void reset() const = 0;
+  // The solve writes the solution into the pressure itself (the last inverse
+  // transform pass), so the copy back into the blocks has nothing left to do.
+  void _fftw2cub() const {}
+  size_t _offset(const BlockInfo& info) const {
+    return stridez * (size_t)info.index[2] * FluidBlock::sizeZ + stridey * (size_t)info.index[1] * FluidBlock::sizeY +
+           stridex * (size_t)info.index[0] * FluidBlock::sizeX;
+  }
+  size_t _offset_ext(const BlockInfo& info) const { return _offset(info); }
+  size_t _dest(const size_t offset, const int z, const int y, const int x) const {
+    return offset + stridez * z + stridey * y + stridex * x;
+  }
 };
 
 class PoissonSolverPeriodic : public PoissonSolver {
   SimulationData& sim;
 
  public:
-  explicit PoissonSolverPeriodic(SimulationData& s) : sim(s) {}
+  inline explicit PoissonSolverPeriodic(SimulationData& s);
   cup_solve_stats last{};
   void solve() override { cup_check(cup_poisson_solve(sim.handle, &last), sim.handle, "PoissonSolverPeriodic::solve"); }
+  void reset() const override { cup_check(cup_poisson_reset(sim.handle), sim.handle, "PoissonSolver::reset"); }
 };
 
 // CreateObstacles (source/operators/ObstaclesCreate.cpp:444-540): moves a
@@ -247,6 +268,7 @@ class PressureProjection : public Operator {
   using Operator::Operator;
   void operator()(const double dt) override {
     sim.pressureSolver->solve();
+    sim.pressureSolver->_fftw2cub();
     cup_check(cup_grad_correct(sim.handle, dt), sim.handle, "PressureProjection");
   }
   std::string getName() override { return "PressureProjection"; }
@@ -285,6 +307,14 @@ class ComputeDissipation : public Operator {
   }
   std::string getName() override { return "ComputeDissipation"; }
 };
+
+PoissonSolverPeriodic::PoissonSolverPeriodic(SimulationData& s) : sim(s) {
+  size_t st[3] = {0, 0, 0};
+  cup_check(cup_poisson_buffer(sim.handle, &data, st, &data_size), sim.handle, "PoissonSolverPeriodic");
+  stridex = st[0];
+  stridey = st[1];
+  stridez = st[2];
+}
 
 SimulationData::~SimulationData() {
   while (!pipeline.empty()) {

@@ -495,33 +495,62 @@ struct OpShift {
 // Allocation-free max |u + uinf| (cup_max_velocity_noalloc). Its per-CTA
 // partial maxima live in this fixed device array instead of handle-owned
 // memory: every GPU that loads the library holds the array until exit, and all
-// calls share it. Each CTA reduces one chunk of kNoAllocChunk cells, so one
-// call handles at most kNoAllocMaxCtas * kNoAllocChunk cells.
+// calls share it. A call splits the n cells into at most kNoAllocMaxCtas
+// contiguous chunks (a multiple of 1024 cells each), one per CTA; the host
+// caps n at kNoAllocMaxCtas * kNoAllocChunk cells. The maximum propagates NaN
+// (fmax would drop it), so a non-finite field gives a NaN result.
 constexpr int kNoAllocMaxCtas = 4096;
 constexpr long long kNoAllocChunk = 65536;
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocMaxCtas];
 
-__global__ void k_noalloc_max_partial(const double* __restrict__ u, const double* __restrict__ v,
-                                      const double* __restrict__ w, long long n, double ux, double uy, double uz,
-                                      double* partials) {
-  __shared__ double scratch[32];
-  double m[1] = {0.0};
-  const long long lo = blockIdx.x * kNoAllocChunk;
-  const long long hi = lo + kNoAllocChunk < n ? lo + kNoAllocChunk : n;
-  for (long long i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-    const double a = fabs(u[i] + ux), b = fabs(v[i] + uy), c = fabs(w[i] + uz);
-    m[0] = fmax(m[0], fmax(fmax(a, b), c));
+__device__ __forceinline__ double nan_max(double a, double b) { return (a > b || a != a) ? a : b; }
+
+__device__ __forceinline__ double noalloc_block_max(double m, double* scratch) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) m = nan_max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) scratch[wid] = m;
+  __syncthreads();
+  if (wid == 0) {
+    m = lane < nw ? scratch[lane] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = nan_max(m, __shfl_xor_sync(0xffffffffu, m, o));
   }
-  block_reduce<1, true>(m, scratch);
-  if (threadIdx.x == 0) partials[blockIdx.x] = m[0];  // every used slot is written before it is read
+  return m;
 }
 
-__global__ void k_noalloc_max_final(const double* partials, int np, double* out) {
+// One CTA of 256 threads per chunk of `chunk` cells; four independent loads in
+// flight per thread and field.
+__global__ void __launch_bounds__(256) k_noalloc_max_partial(const double* __restrict__ u,
+                                                             const double* __restrict__ v,
+                                                             const double* __restrict__ w, long long n,
+                                                             long long chunk, double ux, double uy, double uz,
+                                                             double* partials) {
   __shared__ double scratch[32];
-  double m[1] = {0.0};
-  for (int i = threadIdx.x; i < np; i += blockDim.x) m[0] = fmax(m[0], partials[i]);
-  block_reduce<1, true>(m, scratch);
-  if (threadIdx.x == 0) *out = m[0];
+  double m0 = 0.0, m1 = 0.0, m2 = 0.0, m3 = 0.0;
+  const long long lo = blockIdx.x * chunk;
+  const long long hi = lo + chunk < n ? lo + chunk : n;
+  auto cell = [&](long long i) {
+    return nan_max(nan_max(fabs(u[i] + ux), fabs(v[i] + uy)), fabs(w[i] + uz));
+  };
+  long long i = lo + threadIdx.x;
+  for (; i + 768 < hi; i += 1024) {
+    m0 = nan_max(m0, cell(i));
+    m1 = nan_max(m1, cell(i + 256));
+    m2 = nan_max(m2, cell(i + 512));
+    m3 = nan_max(m3, cell(i + 768));
+  }
+  for (; i < hi; i += 256) m0 = nan_max(m0, cell(i));
+  const double m = noalloc_block_max(nan_max(nan_max(m0, m1), nan_max(m2, m3)), scratch);
+  if (threadIdx.x == 0) partials[blockIdx.x] = m;  // every used slot is written before it is read
+}
+
+__global__ void __launch_bounds__(256) k_noalloc_max_final(const double* partials, int np, double* out) {
+  __shared__ double scratch[32];
+  double m = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) m = nan_max(m, partials[i]);
+  m = noalloc_block_max(m, scratch);
+  if (threadIdx.x == 0) *out = m;
 }
 
 // ---------------------------------------------------------------------------
@@ -1998,45 +2027,58 @@ bool graph_ok(const cup_handle* H) {
   return true;
 }
 
-// Runs nsteps steps (dt from the device state; next_dt: each computes the
-// next step's dt) from a CUDA graph captured once per host state (the field
-// pointers rotate with period 6: the u/tmp swap and the three FP32-DC
-// pressure levels) and replayed with the host state set to what the captured
-// steps left. *ran = false: the capture failed, nothing ran, the host state
-// is as before and graphs are off for the handle.
+// Captures (without running) the nsteps-step graph of the current host state
+// (dt from the device state; next_dt: each step computes the next step's dt)
+// unless it is cached; *out = the cached graph, or nullptr when the capture
+// failed (graphs are then off for the handle). The host state is left as it
+// was: the captured steps only move it forward when the graph is replayed.
+int capture_graph(cup_handle* H, int nsteps, int next_dt, cup_handle::StepGraph** out) {
+  *out = nullptr;
+  const cup_handle::StepState in = step_state(H);
+  for (auto& g : H->graphs)
+    if (g.nsteps == nsteps && g.next_dt == next_dt && same_state(g.in, in)) {
+      *out = &g;
+      return CUP_OK;
+    }
+  if (H->graphs.size() >= 16) drop_graph(H);
+  const long long l0 = H->launches;
+  if (cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    cudaGetLastError();
+    H->use_graphs = false;
+    return CUP_OK;
+  }
+  int rc = CUP_OK;
+  for (int s = 0; s < nsteps && rc == CUP_OK; ++s)
+    rc = DISPATCH_T(H, do_step, DtArg{0.0, &H->dstate->dt}, (const double*)&H->dstate->lambda, 1, next_dt);
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(H->stream, &g);
+  cudaGraphExec_t ex = nullptr;
+  const cup_handle::StepState after = step_state(H);
+  set_step_state(H, in);
+  const long long nl = H->launches - l0;
+  H->launches = l0;
+  if (rc == CUP_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
+    H->graphs.push_back({in, after, nsteps, next_dt, g, ex, nl});
+    *out = &H->graphs.back();
+    return CUP_OK;
+  }
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  H->use_graphs = false;
+  return CUP_OK;
+}
+
+// Runs nsteps steps from the CUDA graph of the current host state, captured
+// once per host state (the field pointers rotate with period 6: the u/tmp
+// swap and the three FP32-DC pressure levels) and replayed with the host
+// state set to what the captured steps left. *ran = false: the capture
+// failed, nothing ran, the host state is as before and graphs are off for
+// the handle.
 int run_graph(cup_handle* H, int nsteps, int next_dt, bool* ran) {
   *ran = false;
-  const cup_handle::StepState in = step_state(H);
   cup_handle::StepGraph* hit = nullptr;
-  for (auto& g : H->graphs)
-    if (g.nsteps == nsteps && g.next_dt == next_dt && same_state(g.in, in)) hit = &g;
-  if (!hit) {
-    if (H->graphs.size() >= 16) drop_graph(H);
-    const long long l0 = H->launches;
-    if (cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
-      cudaGetLastError();
-      H->use_graphs = false;
-      return CUP_OK;
-    }
-    int rc = CUP_OK;
-    for (int s = 0; s < nsteps && rc == CUP_OK; ++s)
-      rc = DISPATCH_T(H, do_step, DtArg{0.0, &H->dstate->dt}, (const double*)&H->dstate->lambda, 1, next_dt);
-    cudaGraph_t g = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(H->stream, &g);
-    cudaGraphExec_t ex = nullptr;
-    if (rc == CUP_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
-      H->graphs.push_back({in, step_state(H), nsteps, next_dt, g, ex, H->launches - l0});
-      hit = &H->graphs.back();
-      H->launches = l0;
-    } else {
-      if (g) cudaGraphDestroy(g);
-      cudaGetLastError();
-      set_step_state(H, in);
-      H->launches = l0;
-      H->use_graphs = false;
-      return CUP_OK;
-    }
-  }
+  int rc = capture_graph(H, nsteps, next_dt, &hit);
+  if (rc || !hit) return rc;
   CK(cudaGraphLaunch(hit->exec, H->stream));
   H->launches += hit->launches;
   set_step_state(H, hit->out);
@@ -2389,6 +2431,17 @@ int cup_set_graphs(cup_handle* H, int on) {
   return CUP_OK;
 }
 
+int cup_prepare_run(cup_handle* H, int* captured) {
+  REQUIRE_H(H);
+  if (captured) *captured = 0;
+  if (!graph_ok(H)) return CUP_OK;
+  cup_handle::StepGraph* g = nullptr;
+  const int rc = capture_graph(H, kGraphSteps, 1, &g);
+  if (rc) return rc;
+  if (captured) *captured = g ? 1 : 0;
+  return CUP_OK;
+}
+
 int cup_create_obstacles(cup_handle* H, double dt) {
   REQUIRE_H(H);
   if (!(dt >= 0)) return fail(H, CUP_ERR_ARG, "dt must be >= 0");
@@ -2462,6 +2515,32 @@ int cup_pressure_rhs(cup_handle* H, double dt) {
   REQUIRE_H(H);
   reset_pressure_history(H);
   return DISPATCH_T(H, do_pressure_rhs, DtArg{dt, nullptr});
+}
+
+int cup_set_rhs(cup_handle* H, const double* r, int where) {
+  REQUIRE_H(H);
+  if (!r || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad rhs arguments");
+  CK(cudaMemcpyAsync(H->rhs, r, H->n * sizeof(double),
+                     where == CUP_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  return check_dev_error(H);
+}
+
+int cup_poisson_buffer(cup_handle* H, double** data, size_t strides[3], size_t* data_size) {
+  REQUIRE_H(H);
+  if (!data || !strides || !data_size) return fail(H, CUP_ERR_ARG, "null output");
+  *data = H->rhs;
+  strides[0] = 1;
+  strides[1] = (size_t)H->nx;
+  strides[2] = (size_t)H->nx * H->ny;
+  *data_size = H->n;
+  return CUP_OK;
+}
+
+int cup_poisson_reset(cup_handle* H) {
+  REQUIRE_H(H);
+  CK(cudaMemsetAsync(H->rhs, 0, H->n * sizeof(double), H->stream));
+  return CUP_OK;
 }
 
 int cup_poisson_solve(cup_handle* H, cup_solve_stats* stats) {
@@ -2611,6 +2690,8 @@ int cup_adjoint_step(cup_handle* H, const void* un, const void* vn, const void* 
   REQUIRE_H(H);
   if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
   if (H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_adjoint_step: the handle has an obstacle (use cup_adjoint_step_obstacle)");
+  if (H->forcing)
+    return fail(H, CUP_ERR_STATE, "cup_adjoint_step: spectral forcing is on and has no adjoint (turn it off first)");
   int rc = check_adjoint_fields(H, un, vn, wn, lu, lv, lw);
   if (!rc) rc = alloc_adjoint(H);
   if (rc) return rc;
@@ -2626,6 +2707,9 @@ int cup_adjoint_step_obstacle(cup_handle* H, const void* un, const void* vn, con
   if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_adjoint_step_obstacle: the handle has no obstacle");
   if (H->sphere_moves)
     return fail(H, CUP_ERR_STATE, "cup_adjoint_step_obstacle: the adjoint of a moving obstacle is not supported");
+  if (H->forcing)
+    return fail(H, CUP_ERR_STATE,
+                "cup_adjoint_step_obstacle: spectral forcing is on and has no adjoint (turn it off first)");
   if (!w_force || !g_chi || !g_vel) return fail(H, CUP_ERR_ARG, "null w_force / g_chi / g_vel");
   int rc = check_adjoint_fields(H, un, vn, wn, lu, lv, lw);
   if (!rc) rc = alloc_adjoint(H);
@@ -2902,51 +2986,97 @@ int cup_debug_shift(cup_handle* H, const double* f, double* out, int g, int dx, 
   return check_dev_error(H);
 }
 
-// Device address of g_noalloc_partials per device, looked up once with that
-// device current (host code must not use the symbol itself as an address).
+// Device address of g_noalloc_partials in the current context, looked up once
+// per (device, context) with that device current: host code must not use the
+// symbol itself as an address. Keying on the context as well as the ordinal
+// makes a new primary context (after cudaDeviceReset) or a context the caller
+// made current look the address up again.
+using PFN_ctxGetCurrent = CUresult (*)(CUcontext*);
+static void* current_context() {
+  static PFN_ctxGetCurrent fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_ctxGetCurrent>(f);
+  });
+  CUcontext c = nullptr;
+  if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+  return c;
+}
+
 static double* noalloc_partials_ptr(int dev, int* err_out) {
+  struct Entry {
+    int dev;
+    void* ctx;
+    double* ptr;
+  };
   static std::mutex mu;
-  static double* ptrs[64] = {nullptr};
-  if (dev < 0 || dev >= 64) {
-    *err_out = CUP_ERR_ARG;
+  static std::vector<Entry> cache;
+  void* ctx = current_context();
+  std::lock_guard<std::mutex> lk(mu);
+  for (const Entry& e : cache)
+    if (e.dev == dev && e.ctx == ctx) return e.ptr;
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+  if (e != cudaSuccess || !p) {
+    fprintf(stderr, "cup_max_velocity_noalloc: cudaGetSymbolAddress failed on device %d: %s\n", dev,
+            cudaGetErrorString(e));
+    *err_out = CUP_ERR_CUDA;
     return nullptr;
   }
-  std::lock_guard<std::mutex> lk(mu);
-  if (!ptrs[dev]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
-    if (e != cudaSuccess || !p) {
-      fprintf(stderr, "cup_max_velocity_noalloc: cudaGetSymbolAddress failed: %s\n", cudaGetErrorString(e));
-      *err_out = CUP_ERR_CUDA;
-      return nullptr;
+  ctx = current_context();  // the lookup may have created the primary context
+  for (Entry& en : cache)
+    if (en.dev == dev) {
+      en.ctx = ctx;
+      en.ptr = static_cast<double*>(p);
+      return en.ptr;
     }
-    ptrs[dev] = static_cast<double*>(p);
-  }
-  return ptrs[dev];
+  cache.push_back({dev, ctx, static_cast<double*>(p)});
+  return cache.back().ptr;
 }
 
 int cup_max_velocity_noalloc(const double* u, const double* v, const double* w, long long n, const double uinf[3],
                              double* umax_dev, void* stream) {
-  if (!u || !v || !w || !uinf || !umax_dev || n <= 0) return CUP_ERR_ARG;
+  if (!u || !v || !w || !uinf || !umax_dev || n <= 0) {
+    fprintf(stderr, "cup_max_velocity_noalloc: null pointer or n <= 0\n");
+    return CUP_ERR_ARG;
+  }
   const long long max_cells = (long long)kNoAllocMaxCtas * kNoAllocChunk;
   if (n > max_cells) {
     fprintf(stderr,
             "cup_max_velocity_noalloc: %lld cells exceed the fixed scratch limit of %lld cells per call "
-            "(%d partials of %lld cells); split the field or use cup_max_velocity\n",
+            "(%d partials of at most %lld cells); split the field or use cup_max_velocity\n",
             n, max_cells, kNoAllocMaxCtas, kNoAllocChunk);
     return CUP_ERR_ARG;
   }
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return CUP_ERR_CUDA;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    fprintf(stderr, "cup_max_velocity_noalloc: cudaGetDevice: %s\n", cudaGetErrorString(e));
+    return CUP_ERR_CUDA;
+  }
   int rc = CUP_OK;
   double* partials = noalloc_partials_ptr(dev, &rc);
   if (!partials) return rc;
-  const int nblocks = (int)((n + kNoAllocChunk - 1) / kNoAllocChunk);
+  // chunks of a multiple of 1024 cells, at most kNoAllocMaxCtas of them
+  long long chunk = (n + kNoAllocMaxCtas - 1) / kNoAllocMaxCtas;
+  chunk = std::max(4096LL, (chunk + 1023) / 1024 * 1024);
+  const int nblocks = (int)((n + chunk - 1) / chunk);
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  k_noalloc_max_partial<<<nblocks, 256, 0, st>>>(u, v, w, n, uinf[0], uinf[1], uinf[2], partials);
-  if (cudaGetLastError() != cudaSuccess) return CUP_ERR_CUDA;
-  k_noalloc_max_final<<<1, 256, 0, st>>>(partials, nblocks, umax_dev);
-  if (cudaGetLastError() != cudaSuccess) return CUP_ERR_CUDA;
+  cudaGetLastError();  // an earlier launch's error is not this call's
+  k_noalloc_max_partial<<<nblocks, 256, 0, st>>>(u, v, w, n, chunk, uinf[0], uinf[1], uinf[2], partials);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    k_noalloc_max_final<<<1, 256, 0, st>>>(partials, nblocks, umax_dev);
+    e = cudaGetLastError();
+  }
+  if (e != cudaSuccess) {
+    fprintf(stderr, "cup_max_velocity_noalloc: kernel launch failed: %s\n", cudaGetErrorString(e));
+    return CUP_ERR_CUDA;
+  }
   return CUP_OK;
 }
 

@@ -272,12 +272,63 @@ FORCING_NAMES = ("totalKinEn", "largeModesKinEn", "viscousDissip", "totalDissipR
 SPECTRAL_NAMES = ("tke", "eps", "uprime", "lambda", "Re_lambda", "l_integral", "tau_integral")
 
 
+class _DeviceArray:
+    """A raw FP64 device allocation described by the CUDA array interface, so
+    that torch.as_tensor can view it without a copy."""
+
+    def __init__(self, ptr: int, shape, device: int):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": "<f8", "data": (ptr, False),
+                                         "version": 3, "strides": None}
+        self.device = device
+
+
 class PoissonSolverPeriodic:
     """PoissonSolverPeriodic (source/poisson/PoissonSolverPeriodic.cpp) bound
-    to a simulation's device buffers: ``solve()`` runs the FFT chain."""
+    to a simulation's device buffers: ``solve()`` runs the FFT chain.
+
+    The buffer contract of PoissonSolver (source/poisson/PoissonSolver.h:51-122):
+    ``data`` is the FP64 device array the RHS is written into (a torch CUDA
+    tensor of shape (nz, ny, nx) viewing it without a copy), with ``stridex``,
+    ``stridey``, ``stridez`` (elements) and ``data_size``; ``_offset(info)`` /
+    ``_offset_ext(info)`` give a block's first cell, ``_dest`` a cell of it.
+    ``reset()`` zeroes the buffer. ``solve()`` includes ``_fftw2cub`` (the
+    solution goes to the pressure), so ``_fftw2cub()`` itself has nothing left
+    to do."""
 
     def __init__(self, sim: "Simulation"):
         self.sim = sim
+        ptr = C.c_void_p()
+        strides = (C.c_size_t * 3)()
+        size = C.c_size_t()
+        L.check(L.lib().cup_poisson_buffer(sim._h, C.byref(ptr), strides, C.byref(size)), sim._h, "poisson buffer")
+        self._ptr = ptr.value
+        self.stridex, self.stridey, self.stridez = (int(x) for x in strides)
+        self.data_size = int(size.value)
+
+    @property
+    def data(self):
+        import torch
+        return torch.as_tensor(_DeviceArray(self._ptr, self.sim.shape, self.sim.sd.device),
+                               device=f"cuda:{self.sim.sd.device}")
+
+    def _offset(self, info) -> int:
+        """First cell of a block: ``info`` has ``index`` (bx, by, bz) or is that triple."""
+        bx, by, bz = getattr(info, "index", info)
+        return BLOCK_SIZE * (self.stridez * bz + self.stridey * by + self.stridex * bx)
+
+    _offset_ext = _offset
+
+    def _dest(self, offset: int, z: int, y: int, x: int) -> int:
+        return offset + self.stridez * z + self.stridey * y + self.stridex * x
+
+    def reset(self):
+        L.check(L.lib().cup_poisson_reset(self.sim._h), self.sim._h, "PoissonSolver::reset")
+
+    def _cub2fftw(self):
+        """Nothing to do: the RHS is written into ``data`` directly."""
+
+    def _fftw2cub(self):
+        """Nothing to do: ``solve()`` writes the solution into the pressure."""
 
     def solve(self):
         st = L.CupSolveStats()
@@ -539,9 +590,28 @@ class Simulation:
             self.serialize()
         return StepStats.from_c(st) if stats else None
 
+    def _advance(self, dt: float, stats: bool = False) -> Optional[StepStats]:
+        """One cup_step with the clock update and nothing else: no restart dump,
+        no diagnostics.dat or forcingData.dat line. For the adjoint rollouts,
+        whose forward and checkpoint recomputation must leave the run's output
+        files and restart point as they were."""
+        st = L.CupStepStats()
+        L.check(L.lib().cup_step(self._h, float(dt), C.byref(st) if stats else None), self._h, "timestep")
+        self.step += 1
+        self.time += dt
+        self.dt = dt
+        return StepStats.from_c(st) if stats else None
+
     def use_graphs(self, on: bool = True):
         """run_steps replays its steady-state steps as a captured CUDA graph (default on)."""
         L.check(L.lib().cup_set_graphs(self._h, int(bool(on))), self._h, "use_graphs")
+
+    def prepare_run(self) -> bool:
+        """Captures (without running) the CUDA graph that run_steps replays from
+        the current state; True when it is cached (see cup_prepare_run)."""
+        c = C.c_int()
+        L.check(L.lib().cup_prepare_run(self._h, C.byref(c)), self._h, "prepare_run")
+        return bool(c.value)
 
     def run_steps(self, nsteps: int) -> StepStats:
         """nsteps of calcMaxTimestep + timestep with dt chained on the device."""

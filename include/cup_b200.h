@@ -166,6 +166,23 @@ int cup_advect_diffuse(struct cup_handle* h, double dt);
 int cup_pressure_rhs(struct cup_handle* h, double dt);
 /* PoissonSolverPeriodic::solve (source/poisson/PoissonSolverPeriodic.cpp:129-146) + _fftw2cub */
 int cup_poisson_solve(struct cup_handle* h, cup_solve_stats* stats);
+/* PoissonSolver's buffer contract (public data, stridex/y/z, data_size,
+ * source/poisson/PoissonSolver.h:51-56; _offset/_dest, :72-101): *data = the
+ * handle's FP64 device array that PressureRHS writes the h^3-premultiplied RHS
+ * into and cup_poisson_solve reads; strides = {stridex, stridey, stridez} in
+ * elements, so the cell (ix, iy, iz) of the block at index (bx, by, bz) is
+ * data[16 (stridez bz + stridey by + stridex bx) + stridez iz + stridey iy +
+ * stridex ix]; *data_size = its length. Valid for the handle's lifetime. A
+ * caller may write its own RHS there (its kernels, cudaMemcpy, cup_set_rhs)
+ * before cup_poisson_solve, as the reference's kernels write solver->data. In
+ * the FP64 form the solve uses the array as its transform work space (as FFTW's
+ * in-place buffer), so it does not hold the RHS afterwards; the solution is in
+ * the pressure (cup_get_pressure: the solve includes _fftw2cub). */
+int cup_poisson_buffer(struct cup_handle* h, double** data, size_t strides[3], size_t* data_size);
+/* PoissonSolver::reset (source/poisson/PoissonSolver.cpp:132-135): zeroes the buffer. */
+int cup_poisson_reset(struct cup_handle* h);
+/* Writes the Poisson buffer (the mirror of cup_get_rhs); FP64, nx*ny*nz values. */
+int cup_set_rhs(struct cup_handle* h, const double* rhs, int where);
 /* KernelGradP (source/operators/PressureProjection.cpp:38-50) */
 int cup_grad_correct(struct cup_handle* h, double dt);
 /* PressureProjection::operator() (source/operators/PressureProjection.cpp:107-129) */
@@ -181,6 +198,13 @@ int cup_run(struct cup_handle* h, int nsteps, cup_step_stats* stats);
 /* cup_run replays its steady-state steps as a CUDA graph of 6 steps (captured
  * on first use; same kernels, same results); off: every step is launched. */
 int cup_set_graphs(struct cup_handle* h, int on);
+/* Captures, without running anything, the 6-step graph that cup_run replays
+ * from the handle's current state, so that the capture and instantiation cost
+ * of a later cup_run from this state is paid here (no counterpart in the
+ * reference). *captured (may be NULL) = 1 when the graph is cached; 0 when the
+ * state cannot replay graphs yet (the FP32-DC warm start is not ready, a moving
+ * obstacle, spectral forcing, profiling on, graphs off). Nothing is launched. */
+int cup_prepare_run(struct cup_handle* h, int* captured);
 
 /* Discrete adjoint of one cup_step with the given dt (no counterpart in the
  * reference, which has no adjoint). un, vn, wn: the velocity at the start of the
@@ -190,7 +214,8 @@ int cup_set_graphs(struct cup_handle* h, int on);
  * must not alias the state. Upwind signs are frozen at the state; the projection
  * is applied as the exact (FP64 FFT) symmetric projector. The handle's own
  * velocity and pressure are untouched; its stage and RHS scratch are overwritten.
- * Handles with an obstacle return CUP_ERR_ARG. Stream-ordered, no host sync. */
+ * Handles with an obstacle return CUP_ERR_ARG; handles with spectral forcing on
+ * return CUP_ERR_STATE (the forcing has no adjoint). Stream-ordered, no host sync. */
 int cup_adjoint_step(struct cup_handle* h, const void* un, const void* vn, const void* wn, double dt, void* lu,
                      void* lv, void* lw);
 /* Discrete adjoint of one cup_step of a handle with the sphere (no counterpart
@@ -203,7 +228,8 @@ int cup_adjoint_step(struct cup_handle* h, const void* un, const void* vn, const
  * box (the derivative from the chi >= 0 side); g_vel (device, 3 doubles) +=
  * dJ/dU for the sphere's penalization target velocity U with uinf held fixed.
  * The step is recomputed from un (projection by the FP64 FFT solve); the surface
- * set and the sign of the RHS correction are frozen at it. Stream-ordered. */
+ * set and the sign of the RHS correction are frozen at it. CUP_ERR_STATE for a
+ * moving sphere or with spectral forcing on. Stream-ordered. */
 int cup_adjoint_step_obstacle(struct cup_handle* h, const void* un, const void* vn, const void* wn, double dt,
                               void* lu, void* lv, void* lw, const double w_force[3], double* g_chi, double* g_vel);
 /* Replaces the obstacle's characteristic function (FP64, nx*ny*nz; only cells in
@@ -262,13 +288,17 @@ int cup_debug_shift(struct cup_handle* h, const double* f, double* out, int g, i
  * long-running service), and loops that must not allocate once running, since
  * cudaMalloc can synchronise the device and can fail late. It allocates
  * nothing: its per-block partial maxima live in a fixed 32 KiB array inside the
- * library (4096 partials of 65536 cells), which every GPU that loads the library
- * keeps until exit; n above 2^28 cells is rejected with CUP_ERR_ARG and a message
- * on stderr. The first call on a device looks up that array's device address
- * with the device current; make that first call before any stream capture. All
- * calls share the array, so calls that overlap on the GPU (other streams, other
- * host threads) race; every slot a call reads is written by the same call first,
- * so nothing needs clearing between calls. */
+ * library (4096 partials, each over at most 65536 cells), which every GPU that
+ * loads the library keeps until exit; n above 2^28 cells is rejected with
+ * CUP_ERR_ARG. A NaN anywhere in the field makes the result NaN (the handle
+ * path reports the same field as CUP_ERR_NONFINITE). Failures return
+ * CUP_ERR_ARG or CUP_ERR_CUDA with the reason on stderr (there is no handle for
+ * cup_last_error). The first call on a device (and in each new context on it,
+ * e.g. after cudaDeviceReset) looks up that array's device address with the
+ * device current; make that first call before any stream capture. All calls
+ * share the array, so calls that overlap on the GPU (other streams, other host
+ * threads) race; every slot a call reads is written by the same call first, so
+ * nothing needs clearing between calls. */
 int cup_max_velocity_noalloc(const double* u, const double* v, const double* w, long long n,
                              const double uinf[3], double* umax_dev, void* stream);
 

@@ -355,3 +355,52 @@ def test_obstacle_adjoint_argument_checks():
     with pytest.raises(ValueError):
         sim.adjoint_step_obstacle(z, 0.01, lam, (1, 0, 0), torch.zeros(3, device="cuda"),
                                   torch.zeros(3, dtype=torch.float64, device="cuda"))
+
+
+def test_adjoint_refuses_spectral_forcing():
+    # the forcing has no transpose: the rollout and the C entry point refuse it
+    import ctypes as C
+
+    import torch
+
+    import cubismup_3d_b200 as cup
+    from cubismup_3d_b200 import _lib
+    from cubismup_3d_b200.adjoint import rollout
+    sd = cup.SimulationData(CFL=0.5, cells=(32, 32, 32))
+    sd.extent, sd.nu, sd.rampup, sd.turbKinEn_target = 2 * np.pi, 5e-3, 0, 0.5
+    sim = cup.Simulation(sd)
+    u0 = torch.zeros((3,) + sim.shape, dtype=torch.float64, device="cuda")
+    with pytest.raises(ValueError, match="forcing"):
+        rollout(sim, u0, [1e-3])
+    lam = torch.zeros_like(u0)
+    rc = _lib.lib().cup_adjoint_step(sim._h, *[C.c_void_p(u0[i].data_ptr()) for i in range(3)], 1e-3,
+                                     *[C.c_void_p(lam[i].data_ptr()) for i in range(3)])
+    assert rc == _lib.CUP_ERR_STATE
+    assert b"forcing" in _lib.lib().cup_last_error(sim._h)
+    sim.close()
+
+
+def test_rollout_backward_leaves_output_files(tmp_path, monkeypatch):
+    # the rollout's forward and recomputation write no diagnostics line and no
+    # restart dump: the run's files and its restart point stay as they were
+    import torch
+
+    from cubismup_3d_b200.adjoint import rollout
+    monkeypatch.chdir(tmp_path)
+    cells = (32, 32, 16)
+    sim = make_sim(cells, 1.0)
+    sim.sd.freqDiagnostics = 1
+    sim.sd.saveFreq = 2
+    sim.sd.path4serialization = str(tmp_path)
+    u = initial_state(cells, sim.h, seed=3)
+    sim.set_velocity(*u)
+    for _ in range(2):
+        sim.timestep(sim.calcMaxTimestep())
+    files = {p.name: p.read_bytes() for p in tmp_path.iterdir() if p.is_file()}
+    assert "diagnostics.dat" in files and "restart.status" in files
+    u0 = to_dev(u, torch.float64).requires_grad_(True)
+    uT = rollout(sim, u0, [2e-3] * 6, checkpoint_every=2)
+    (0.5 * (uT ** 2).sum()).backward()
+    assert u0.grad is not None and torch.isfinite(u0.grad).all()
+    after = {p.name: p.read_bytes() for p in tmp_path.iterdir() if p.is_file()}
+    assert after == files

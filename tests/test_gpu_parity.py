@@ -585,3 +585,33 @@ def test_wide_grid_steps_vs_oracle(oracle, scheme, precision):
         orc.timestep(dt)
         for a, b in zip(sim.velocity(), orc.velocity()):
             assert rel_l2(a, b) < tol
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32_dc", 1e-9)])
+def test_poisson_buffer_contract_vs_oracle(oracle, precision, tol):
+    # PoissonSolver's public buffer (source/poisson/PoissonSolver.h:51-122): the
+    # RHS is written block by block at data[_dest(_offset_ext(info), iz, iy, ix)]
+    # as KernelPressureRHS writes solver->data, then solve() + _fftw2cub()
+    import torch
+    nx, ny, nz = 64, 32, 32
+    sim = make_sim((nx, ny, nz), 1.3, precision=precision)
+    ps = sim.pressureSolver
+    assert (ps.stridex, ps.stridey, ps.stridez, ps.data_size) == (1, nx, nx * ny, nx * ny * nz)
+    buf = ps.data.view(-1)
+    buf.fill_(1.0)
+    ps.reset()
+    torch.cuda.synchronize()
+    assert float(buf.abs().max()) == 0.0
+    rhs = np.random.default_rng(21).standard_normal((nz, ny, nx))
+    iz, iy, ix = np.meshgrid(np.arange(16), np.arange(16), np.arange(16), indexing="ij")
+    for bz in range(nz // 16):
+        for by in range(ny // 16):
+            for bx in range(nx // 16):
+                off = ps._offset_ext((bx, by, bz))
+                idx = ps._dest(off, iz, iy, ix).ravel()
+                vals = rhs[16 * bz:16 * bz + 16, 16 * by:16 * by + 16, 16 * bx:16 * bx + 16].ravel()
+                buf[torch.from_numpy(idx).cuda()] = torch.from_numpy(vals).cuda()
+    torch.cuda.synchronize()
+    ps.solve()
+    ps._fftw2cub()
+    assert rel_l2(sim.pressure(), oracle.poisson_solve(rhs, sim.h)) < tol

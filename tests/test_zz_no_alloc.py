@@ -54,6 +54,19 @@ def test_noalloc_max_velocity_matches_handle_twice():
         assert got == pytest.approx(ref, rel=1e-15, abs=0)
 
 
+def test_noalloc_propagates_nan():
+    # one NaN cell makes the result NaN (a finite maximum would hide it and
+    # give a plausible CFL time step)
+    rng = np.random.default_rng(3)
+    nx, ny, nz = 64, 32, 32
+    u, v, w = (rng.standard_normal((nz, ny, nx)) for _ in range(3))
+    v[17, 5, 40] = np.nan
+    assert np.isnan(noalloc_max(u, v, w, (0.0, 0.0, 0.0)))
+    v[17, 5, 40] = 0.0
+    assert noalloc_max(u, v, w, (0.0, 0.0, 0.0)) == pytest.approx(
+        max(np.abs(a).max() for a in (u, v, w)), rel=1e-15, abs=0)
+
+
 def test_noalloc_rejects_oversized_fields():
     from cubismup_3d_b200 import _lib
     ui = (C.c_double * 3)(0.0, 0.0, 0.0)
