@@ -121,6 +121,7 @@ SIGNATURES = {
     "cup_poisson_solve_field": (C.c_int, [_H, C.c_void_p, C.c_void_p, C.c_int]),
     "cup_diagnostics": (C.c_int, [_H, _dp]),
     "cup_compute_dissipation": (C.c_int, [_H, _dp]),
+    "cup_compute_forces": (C.c_int, [_H, _dp]),
     "cup_spectral_analysis": (C.c_int, [_H, _dp, _dp, C.c_int]),
     "cup_set_spectral_forcing": (C.c_int, [_H, C.c_double, C.c_double]),
     "cup_spectral_forcing": (C.c_int, [_H, C.c_double, _dp]),

@@ -151,6 +151,7 @@ struct SimulationData {
   int device = 0;
   // owned state
   cup_handle* handle = nullptr;
+  bool has_obstacle = false;  // obstacle_vector->nObstacles() > 0
   std::unique_ptr<FluidGrid> grid;
   std::vector<Operator*> pipeline;
   PoissonSolver* pressureSolver = nullptr;
@@ -284,6 +285,42 @@ class Penalization : public Operator {
   std::string getName() override { return "Penalization"; }
 };
 
+// ComputeForces (source/operators/FluidSolidForces.cpp:200-222) after
+// Penalization: the surface forces of the sphere on the final velocity and
+// pressure (cup_compute_forces), appended every step to
+// forceValues_surface_0.dat and powerValues_surface_0.dat in the format of
+// Obstacle::_writeSurfForcesToFile (source/obstacles/Obstacle.cpp:518-556).
+// Nothing without an obstacle.
+class ComputeForces : public Operator {
+ public:
+  using Operator::Operator;
+  // surfForce[3], presForce[3], viscForce[3], surfTorque[3], gamma[3], drag, thrust, Pout, PoutBnd,
+  // defPower, defPowerBnd, pLocom, Pthrust, Pdrag, EffPDef, EffPDefBnd, mass
+  std::array<double, 27> last{};
+  void operator()(const double) override {
+    if (!sim.has_obstacle) return;
+    cup_check(cup_compute_forces(sim.handle, last.data()), sim.handle, "ComputeForces");
+    const double* q = last.data();
+    std::FILE* f = std::fopen("forceValues_surface_0.dat", "a");
+    if (!f) throw std::runtime_error("ComputeForces: cannot open forceValues_surface_0.dat");
+    if (sim.step == 0)
+      std::fprintf(f, "step\ttime\tmass\tforce_x\tforce_y\tforce_z\ttorque_x\ttorque_y\ttorque_z\tpresF_x\t"
+                      "presF_y\tpresF_z\tviscF_x\tviscF_y\tviscF_z\tgamma_x\tgamma_y\tgamma_z\tdrag\tthrust\n");
+    std::fprintf(f, "%d\t%.7e\t%.7e", sim.step, sim.time, q[26]);
+    for (int k : {0, 1, 2, 9, 10, 11, 3, 4, 5, 6, 7, 8, 12, 13, 14, 15, 16}) std::fprintf(f, "\t%.7e", q[k]);
+    std::fprintf(f, "\n");
+    std::fclose(f);
+    f = std::fopen("powerValues_surface_0.dat", "a");
+    if (!f) throw std::runtime_error("ComputeForces: cannot open powerValues_surface_0.dat");
+    if (sim.step == 0)
+      std::fprintf(f, "step\ttime\tPthrust\tPdrag\tPout\tpDef\tetaPDef\tpLocom\tPoutBnd\tdefPowerBnd\tetaPDefBnd\n");
+    std::fprintf(f, "%d\t%.7e\t%.7e\t%.7e\t%.7e\t%.7e\t%.7e\t%.7e\t%.7e\t%.7e\t%.7e\n", sim.step, sim.time, q[22],
+                 q[23], q[17], -q[19], q[24], q[21], q[18], -q[20], q[25]);
+    std::fclose(f);
+  }
+  std::string getName() override { return "ComputeForces"; }
+};
+
 // ComputeDissipation (source/operators/ComputeDissipation.cpp:119-177): every
 // freqDiagnostics steps, the 20 sums of the current fields appended to
 // diagnostics.dat in the reference's format (header at step 0).
@@ -388,6 +425,7 @@ class Simulation {
     sim.pipeline.push_back(new PressureProjection(sim));
     sim.pipeline.push_back(new UpdateObstacles(sim));
     sim.pipeline.push_back(new Penalization(sim));
+    sim.pipeline.push_back(new ComputeForces(sim));
     sim.pipeline.push_back(new ComputeDissipation(sim));
   }
 
@@ -401,6 +439,7 @@ class Simulation {
       s.bFixFrameOfRef[d] = a.bFixFrameOfRef[d];
     }
     cup_check(cup_add_sphere(sim.handle, &s), sim.handle, "add_obstacle");
+    sim.has_obstacle = true;
   }
 
   double calcMaxTimestep() {

@@ -54,6 +54,7 @@ __global__ void __launch_bounds__(512) k_adjoint_zq(const __grid_constant__ Adjo
                                                    T* __restrict__ ou, T* __restrict__ ov, T* __restrict__ ow,
                                                    T alpha, T beta, DtArg dt, double h, double nu, double ux,
                                                    double uy, double uz, int* err) {
+  pdl_entry();
   constexpr int G = SCHEME == 0 ? 1 : 2;
   constexpr int ROWS = TY + 2 * G;
   constexpr int Q = 2 * G + 1;

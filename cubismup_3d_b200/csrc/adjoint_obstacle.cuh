@@ -65,6 +65,7 @@ __global__ void k_adj_penalize(T* lu, T* lv, T* lw, const T* su, const T* sv, co
                                const SphereParams* sp, Box box, int nx, int ny, int nz, double h, double dt,
                                double Lfac, int implicit_pen, double wF0, double wF1, double wF2, double* g_chi,
                                double* partials /* [gridDim.x][3] */) {
+  pdl_entry();
   __shared__ double scratch[3 * 32];
   const SphereParams s = *sp;
   const double dv = h * h * h;
@@ -109,6 +110,7 @@ __global__ void k_adj_penalize(T* lu, T* lv, T* lw, const T* su, const T* sv, co
 template <typename T>
 __global__ void k_adj_rhs_sum(const double* q, const double* b0, const T* chi, Box box, int nx, int ny, int nz,
                               const double* rhs_sums, const double* corr, double* partials /* [gridDim.x] */) {
+  pdl_entry();
   __shared__ double scratch[32];
   const ObstacleRhsState rs = obstacle_rhs_state(rhs_sums, *corr);
   double acc[1] = {0};
@@ -132,6 +134,7 @@ template <typename T>
 __global__ void k_adj_rhs_apply(double* q, const double* b0, const T* chi, Box box, int nx, int ny, int nz,
                                 const double* rhs_sums, const double* corr, const double* sq_dev, double kappa,
                                 double* g_chi) {
+  pdl_entry();
   const ObstacleRhsState rs = obstacle_rhs_state(rhs_sums, *corr);
   const double sq = rs.sigma != 0 ? *sq_dev : 0.0;
   const double invD = 1.0 / rs.D, SD2 = rs.S / (rs.D * rs.D);
@@ -155,6 +158,7 @@ __global__ void k_adj_rhs_apply(double* q, const double* b0, const T* chi, Box b
 
 // Adds the sum of n partials (stride `stride`, k values each) to out[0..k) (k <= 3).
 __global__ void k_adj_accumulate(const double* partials, int n, int stride, int k, double* out) {
+  pdl_entry();
   __shared__ double scratch[3 * 32];
   double s[3] = {0, 0, 0};
   for (int i = threadIdx.x; i < n; i += blockDim.x)

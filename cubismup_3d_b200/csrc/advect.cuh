@@ -54,6 +54,7 @@ template <typename T, int SCHEME, int TY, int NS, int CPT, int NXC = 0, int ZCC 
 __global__ void __launch_bounds__(512) k_advect_zq(const __grid_constant__ AdvectMaps maps, const StreamGeom g,
                                                   T* __restrict__ ou, T* __restrict__ ov, T* __restrict__ ow, DtArg dt,
                                                   double h, double nu, double ux, double uy, double uz, int* err) {
+  pdl_entry();
   constexpr int G = AdvectTraits<SCHEME>::G;
   constexpr bool BASE = AdvectTraits<SCHEME>::BASE;
   constexpr int ROWS = TY + 2 * G;

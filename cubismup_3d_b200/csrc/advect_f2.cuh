@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(512) k_advect_zq_f2(const __grid_constant__ Ad
                                                      float* __restrict__ ou, float* __restrict__ ov,
                                                      float* __restrict__ ow, DtArg dt, double h, double nu, double ux,
                                                      double uy, double uz, int* err) {
+  pdl_entry();
   constexpr int G = 2;
   constexpr int ROWS = TY + 2 * G;
   constexpr int Q = 2 * G + 1;

@@ -130,6 +130,23 @@ __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
+// ---- programmatic dependent launch ----------------------------------------
+// The step's kernels are launched with programmatic stream serialization: a
+// kernel's CTAs may be scheduled while the previous kernel of the stream is
+// still finishing (its launch and set-up overlap that kernel's tail). Each
+// such kernel calls pdl_wait() before its first access to global memory that
+// an earlier kernel writes or reads (everything except the tables written
+// once at creation): it returns once the previous kernel has completed and
+// its writes are visible. pdl_launch_dependents() then lets the next kernel
+// of the stream launch early in turn. Both are no-ops for a kernel launched
+// without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_launch_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_entry() {
+  pdl_wait();
+  pdl_launch_dependents();
+}
+
 // ---- reductions -----------------------------------------------------------
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

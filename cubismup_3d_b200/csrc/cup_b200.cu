@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
 #include <map>
 #include <mutex>
 #include <string>
@@ -61,11 +62,13 @@ constexpr int kBoxBlocksMax = 296;
 
 template <typename T>
 __global__ void k_convert_from_f64(T* dst, const double* src, size_t n) {
+  pdl_entry();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     dst[i] = (T)src[i];
 }
 template <typename T>
 __global__ void k_convert_to_f64(double* dst, const T* src, size_t n) {
+  pdl_entry();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     dst[i] = (double)src[i];
 }
@@ -74,6 +77,7 @@ __global__ void k_convert_to_f64(double* dst, const T* src, size_t n) {
 template <typename T>
 __global__ void k_max_u(const T* u, const T* v, const T* w, size_t n, double ux, double uy, double uz,
                         double* partials) {
+  pdl_entry();
   __shared__ double scratch[32];
   double m[1] = {0.0};
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -85,6 +89,7 @@ __global__ void k_max_u(const T* u, const T* v, const T* w, size_t n, double ux,
 }
 
 __global__ void k_finalize_max(const double* partials, int np, DevState* st) {
+  pdl_entry();
   __shared__ double scratch[32];
   double m[1] = {0.0};
   for (int i = threadIdx.x; i < np; i += blockDim.x) m[0] = fmax(m[0], partials[i]);
@@ -117,6 +122,7 @@ __device__ __forceinline__ void calc_dt_device(DevState* st, const CflParams& c)
 
 // step >= 0: the host's step counter, stored first (the ramp-up reads it).
 __global__ void k_calc_dt(DevState* st, double h, double nu, double CFL, int rampup, double DLM, int step = -1) {
+  pdl_entry();
   if (step >= 0) st->step = step;
   calc_dt_device(st, CflParams{h, nu, CFL, rampup, DLM});
 }
@@ -126,6 +132,7 @@ __global__ void k_calc_dt(DevState* st, double h, double nu, double CFL, int ram
 // when DLM > 0), bit 2 lambda (when DLM <= 0), bit 4 step and time.
 enum { SET_DT = 1, SET_LAMBDA = 2, SET_CLOCK = 4 };
 __global__ void k_set_state(DevState* st, int what, double dt, double DLM, double lambda, int step, double time) {
+  pdl_entry();
   if (what & SET_DT) {
     st->dt = dt;
     if (DLM > 0) st->lambda = DLM / dt;
@@ -144,6 +151,7 @@ __global__ void k_set_state(DevState* st, int what, double dt, double DLM, doubl
 __global__ void k_finalize_step(const double* pgrad, int ngrad, int gstride, int max_off, int ke_off,
                                 const double* ppen, int npen, DevState* st, double h3, int advance, int next_dt,
                                 CflParams cfl) {
+  pdl_entry();
   __shared__ double scratch[8 * 32];
   double mx[1] = {0.0};
   double s[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -176,6 +184,7 @@ __global__ void k_finalize_step(const double* pgrad, int ngrad, int gstride, int
 
 // Penalization-only finalize (operator-by-operator path).
 __global__ void k_finalize_pen(const double* ppen, int npen, DevState* st) {
+  pdl_entry();
   __shared__ double scratch[6 * 32];
   double s[6] = {0, 0, 0, 0, 0, 0};
   for (int i = threadIdx.x; i < npen; i += blockDim.x)
@@ -190,6 +199,7 @@ __global__ void k_finalize_pen(const double* ppen, int npen, DevState* st) {
 
 // PressureRHS correction factor (source/operators/PressureRHS.cpp:328-334).
 __global__ void k_finalize_rhs_obstacle(const double* p, int np, DevState* st) {
+  pdl_entry();
   __shared__ double scratch[3 * 32];
   double s[3] = {0, 0, 0};
   for (int i = threadIdx.x; i < np; i += blockDim.x)
@@ -208,6 +218,7 @@ __global__ void k_finalize_rhs_obstacle(const double* p, int np, DevState* st) {
 
 // Zeroes a field of es-byte elements (4: FP32, 8: FP64) on a box.
 __global__ void k_clear_box(void* f, size_t es, Box box, int nx, int ny, int nz) {
+  pdl_entry();
   const long long n = box.count();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     const int x = wrapi(box.lo[0] + (int)(i % box.n[0]), nx);
@@ -223,6 +234,7 @@ __global__ void k_clear_box(void* f, size_t es, Box box, int nx, int ny, int nz)
 
 // The sphere's position in the device parameters (stream-ordered).
 __global__ void k_set_sphere_position(SphereParams* sp, double x, double y, double z) {
+  pdl_entry();
   sp->position[0] = x;
   sp->position[1] = y;
   sp->position[2] = z;
@@ -230,6 +242,7 @@ __global__ void k_set_sphere_position(SphereParams* sp, double x, double y, doub
 
 // Grid centre of mass (source/operators/ObstaclesCreate.cpp:230-256) -> SphereParams.
 __global__ void k_finalize_com(const double* p, int np, DevState* st, SphereParams* sp) {
+  pdl_entry();
   __shared__ double scratch[4 * 32];
   double s[4] = {0, 0, 0, 0};
   for (int i = threadIdx.x; i < np; i += blockDim.x)
@@ -251,6 +264,7 @@ __global__ void k_finalize_com(const double* p, int np, DevState* st, SpherePara
 // min_iter on; check max_iter is final).
 __global__ void k_finalize_residual(const double* p, int stride, int np, DevState* st, double tol, int k,
                                     int min_iter, int max_iter, double inv_class_cells) {
+  pdl_entry();
   __shared__ double scratch[18 * 32];
   if (k > 0 && st->converged) return;
   double s[18];
@@ -299,6 +313,7 @@ template <typename T>
 __global__ void k_dissipation(const T* u, const T* v, const T* w, const double* p, const T* chi, int nx, int ny,
                               int nz, double h, double nu, double hCube, double inv2h, double invHh, double cx,
                               double cy, double cz, double* partials /* [gridDim.x][20] */) {
+  pdl_entry();
   __shared__ double scratch[20 * 32];
   double R[20];
 #pragma unroll
@@ -372,6 +387,7 @@ __global__ void k_dissipation(const T* u, const T* v, const T* w, const double* 
 // reference's eps is nu times the mean of |curl_c u|^2 (central differences).
 template <typename T>
 __global__ void k_widen(const T* __restrict__ src, double* __restrict__ dst, size_t n) {
+  pdl_entry();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     dst[i] = (double)src[i];
 }
@@ -384,6 +400,7 @@ __global__ void k_widen(const T* __restrict__ src, double* __restrict__ dst, siz
 __global__ void k_spectral_modes(double* hu, double* hv, double* hw, int nx, int ny, int nz, double wfx, double wfy,
                                  double wfz, int nyquist, double nyq_scaling, int nbin, int filter,
                                  double* partials) {
+  pdl_entry();
   extern __shared__ double sbins[];
   __shared__ double scratch[3 * 32];
   for (int b = threadIdx.x; b < nbin; b += blockDim.x) sbins[b] = 0.0;
@@ -428,6 +445,7 @@ __global__ void k_spectral_modes(double* hu, double* hv, double* hw, int nx, int
 template <typename T>
 __global__ void k_vorticity2(const T* u, const T* v, const T* w, int nx, int ny, int nz, double inv2h,
                              double* partials) {
+  pdl_entry();
   __shared__ double scratch[32];
   double acc[1] = {0.0};
   const size_t n = (size_t)nx * ny * nz;
@@ -448,6 +466,7 @@ __global__ void k_vorticity2(const T* u, const T* v, const T* w, int nx, int ny,
 // f += factor * g (g FP64), rounded once to the storage type.
 template <typename T>
 __global__ void k_add_scaled(T* f, const double* g, double factor, size_t n) {
+  pdl_entry();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
     f[i] = (T)((double)f[i] + factor * g[i]);
 }
@@ -455,6 +474,7 @@ __global__ void k_add_scaled(T* f, const double* g, double factor, size_t n) {
 // Diagnostics: kinetic energy and central-divergence norms (FP64).
 template <typename T>
 __global__ void k_diag(const T* u, const T* v, const T* w, int nx, int ny, int nz, double inv2h, double* partials) {
+  pdl_entry();
   __shared__ double scratch[3 * 32];
   double s[2] = {0, 0};
   double m[1] = {0};
@@ -695,6 +715,10 @@ struct cup_handle {
   // step, the three FP32-DC pressure levels every step); the graph is tied to
   // the pointer tuple it was captured with
   bool use_graphs = true;
+  // kernels launched as programmatic dependent launches: off by default (the
+  // captured 6-step graphs measured 34 us per step slower at 256^3 with it);
+  // CUP_PDL=1 in the environment at cup_create turns it on
+  bool pdl = false;
   // host state a step reads and advances (the graph replays the device part)
   struct StepState {
     void* f[9];  // u, v, w, tu, tv, tw, p, p_old, p_pred
@@ -815,6 +839,27 @@ int prepare_kernel(cup_handle* H, K kern, size_t smem, int threads, int* blocks_
   return CUP_OK;
 }
 
+// Launches a kernel on the handle's stream; with H->pdl (the default) as a
+// programmatic dependent launch: its CTAs may be scheduled while the previous
+// kernel of the stream finishes, and wait in pdl_entry() for that kernel's
+// completion before touching its data. A failure is left for CKL() to report.
+template <typename... KArgs, typename... Args>
+void klaunch(cup_handle* H, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = H->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  // (the default streams keep plain stream order)
+  const bool named = H->stream && H->stream != cudaStreamLegacy && H->stream != cudaStreamPerThread;
+  cfg.numAttrs = H->pdl && named ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 // Launches k_stencil_stream over `fields` (device arrays of T). Returns the
 // grid size through *grid_out (the number of per-CTA partials written).
 template <typename T, int NF, int G, int TY, int NS, class Op>
@@ -827,17 +872,26 @@ int launch_stream(cup_handle* H, const char* name, const void* const* fields, co
     rc = make_map(H, &maps.halo[f], fields[f], tma_dtype<T>(), sizeof(T), H->nx, G, 1);
     if (rc) return rc;
   }
-  const int zc = std::min(16, H->nz);
-  StreamGeom g{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
   const size_t smem = stream_smem_bytes<T, NF, G, TY, NS>(H->nx) + 128;
   auto kern = k_stencil_stream<T, NF, G, TY, NS, Op>;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, 256, &bpsm);
   if (rc) return rc;
+  // planes per work item (16, 8 or 4): the fewest plane loads on the busiest
+  // CTA, waves of items times the planes an item loads (its 2G halo planes too)
+  int zc = std::min(16, H->nz);
+  long long best = -1;
+  for (int c = std::min(16, H->nz); c >= 4; c /= 2) {
+    const long long items = (long long)(H->ny / TY) * (H->nz / c);
+    const long long resident = std::min<long long>(items, (long long)bpsm * H->num_sms);
+    const long long cost = (items + resident - 1) / resident * (c + 2 * G);
+    if (best < 0 || cost < best) best = cost, zc = c;
+  }
+  StreamGeom g{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
   const int grid = std::min(g.n_items, bpsm * H->num_sms);
   if (grid > kPartialCap / 16) return fail(H, CUP_ERR_ARG, "too many CTAs for the partial buffers");
   rc = launch_named(H, name, [&]() -> int {
-    kern<<<grid, 256, smem, H->stream>>>(maps, g, op, H->derr, skip);
+    klaunch(H, kern, grid, 256, smem, maps, g, op, H->derr, skip);
     CKL();
     return CUP_OK;
   });
@@ -878,7 +932,7 @@ int launch_rows_M(cup_handle* H, const char* name, const Prod& prod, const Cons&
   const int grid = (nrows + lpc - 1) / lpc;
   if (!Prod::kBulk && grid > kPartialCap / 20) return fail(H, CUP_ERR_ARG, "too many row tiles for the partial buffers");
   return launch_named(H, name, [&]() -> int {
-    kern<<<grid, lpc * TPL, smem, H->stream>>>(prod, cons, nrows, lpc, table<R>(H, 0), H->derr, skip);
+    klaunch(H, kern, grid, lpc * TPL, smem, prod, cons, nrows, lpc, table<R>(H, 0), H->derr, skip);
     CKL();
     return CUP_OK;
   });
@@ -916,7 +970,7 @@ int launch_rows_pipe_M(cup_handle* H, const char* name, const R* in, R* out, con
   const int ntiles = (nrows + lpc - 1) / lpc;
   const int grid = std::min(ntiles, bpsm * H->num_sms);
   return launch_named(H, name, [&]() -> int {
-    kern<<<grid, threads, smem, H->stream>>>(in, out, nrows, lpc, table<R>(H, 0), H->derr, skip);
+    klaunch(H, kern, grid, threads, smem, in, out, nrows, lpc, table<R>(H, 0), H->derr, skip);
     CKL();
     return CUP_OK;
   });
@@ -935,12 +989,15 @@ int launch_rows_pipe(cup_handle* H, const char* name, const R* in, R* out, const
   return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
 }
 
-template <int M, typename R, int AXIS, bool DIVIDE, typename RIN = R>
+template <int M, typename R, int AXIS, bool DIVIDE, typename RIN = R, bool T8X = true>
 int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   // W x-columns per tile (FP32: 128-B rows of a tile, FP64: 128 B), NB = 3 tile buffers
   // 256-long FP32 lines: the 8-thread plan (radix 16, then radix 8 fused with the
   // split); measured slower than the 16-thread plan for FP64 tiles (fewer CTAs fit)
-  constexpr bool T8 = M == 128;
+  if constexpr (M == 128 && sizeof(RIN) < sizeof(R) && T8X) {
+    if (getenv("CUP_ZMIX16")) return launch_cols_M<M, R, AXIS, DIVIDE, RIN, false>(H, in, out, skip);
+  }
+  constexpr bool T8 = M == 128 && T8X;
   constexpr int N = 2 * M, TPL = T8 ? 8 : M / 8, NB = T8 ? 2 : 3;
   constexpr int W = sizeof(R) == 4 ? 32 : 16;
   if (H->nx % W) return fail(H, CUP_ERR_ARG, "nx must be a multiple of %d for this precision", W);
@@ -965,7 +1022,7 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   const char* name = AXIS == 1 ? (inv64 ? "dht_y_f64" : "dht_y")
                                : (sizeof(RIN) < sizeof(R) ? "dht_z_solve_mixed" : "dht_z_solve");
   return launch_named(H, name, [&]() -> int {
-    kern<<<grid, threads, smem, H->stream>>>(map_in, map_out, ntx, ntiles, table<R>(H, AXIS), table<RIN>(H, AXIS),
+    klaunch(H, kern, grid, threads, smem, map_in, map_out, ntx, ntiles, table<R>(H, AXIS), table<RIN>(H, AXIS),
                                              sp, H->derr, skip);
     CKL();
     return CUP_OK;
@@ -1086,7 +1143,7 @@ int launch_advect_sized(cup_handle* H, const char* name, void* const* in, void* 
   if (rc) return rc;
   const int grid = std::min(g.n_items, bpsm * H->num_sms);
   return launch_named(H, name, [&]() -> int {
-    kern<<<grid, threads, smem, H->stream>>>(maps, g, (T*)out[0], (T*)out[1], (T*)out[2], dt, H->h, H->cfg.nu,
+    klaunch(H, kern, grid, threads, smem, maps, g, (T*)out[0], (T*)out[1], (T*)out[2], dt, H->h, H->cfg.nu,
                                              H->uinf[0], H->uinf[1], H->uinf[2], H->derr);
     CKL();
     return CUP_OK;
@@ -1139,7 +1196,7 @@ int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* con
   if (rc) return rc;
   const int grid = std::min(g.n_items, bpsm * H->num_sms);
   return launch_named(H, name, [&]() -> int {
-    kern<<<grid, threads, smem, H->stream>>>(maps, g, (float*)out[0], (float*)out[1], (float*)out[2], dt, H->h,
+    klaunch(H, kern, grid, threads, smem, maps, g, (float*)out[0], (float*)out[1], (float*)out[2], dt, H->h,
                                              H->cfg.nu, H->uinf[0], H->uinf[1], H->uinf[2], H->derr);
     CKL();
     return CUP_OK;
@@ -1210,8 +1267,7 @@ int do_pressure_rhs(cup_handle* H, DtArg dt, void* const* fields = nullptr, doub
   if (fields)
     for (int q = 0; q < 3; ++q) uvw[q] = fields[q];
   OpPressureRHS<T> op{H->rhs, dt, H->h, H->nx, H->ny};
-  if (H->fp32) rc = launch_stream<T, 3, 1, 8, 4>(H, "pressure_rhs", uvw, op);
-  else rc = launch_stream<T, 3, 1, 4, 4>(H, "pressure_rhs", uvw, op);
+  rc = launch_stream<T, 3, 1, 4, 4>(H, "pressure_rhs", uvw, op);
   if (rc) return rc;
   // the RHS before its obstacle terms (the obstacle adjoint linearises them there)
   if (save_b0) CK(cudaMemcpyAsync(save_b0, H->rhs, H->n * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
@@ -1219,7 +1275,7 @@ int do_pressure_rhs(cup_handle* H, DtArg dt, void* const* fields = nullptr, doub
     const int gb = box_grid(H->box);
     {
       int rc_ = launch_named(H, "rhs_obstacle", [&]() -> int {
-        k_rhs_obstacle<T><<<gb, kBoxThreads, 0, H->stream>>>(H->rhs, (const T*)H->chi, H->box, H->nx, H->ny, H->nz,
+        klaunch(H, k_rhs_obstacle<T>, gb, kBoxThreads, 0, H->rhs, (const T*)H->chi, H->box, H->nx, H->ny, H->nz,
                                                          partial(H, P_RHSOB));
         CKL();
         return CUP_OK;
@@ -1228,7 +1284,7 @@ int do_pressure_rhs(cup_handle* H, DtArg dt, void* const* fields = nullptr, doub
     }
     {
       int rc_ = launch_named(H, "finalize_rhs_obstacle", [&]() -> int {
-        k_finalize_rhs_obstacle<<<1, 256, 0, H->stream>>>(partial(H, P_RHSOB), gb, H->dstate);
+        klaunch(H, k_finalize_rhs_obstacle, 1, 256, 0, partial(H, P_RHSOB), gb, H->dstate);
         CKL();
         return CUP_OK;
       });
@@ -1236,7 +1292,7 @@ int do_pressure_rhs(cup_handle* H, DtArg dt, void* const* fields = nullptr, doub
     }
     {
       int rc_ = launch_named(H, "rhs_obstacle_correct", [&]() -> int {
-        k_rhs_obstacle_correct<T><<<gb, kBoxThreads, 0, H->stream>>>(H->rhs, (const T*)H->chi, H->box, H->nx, H->ny,
+        klaunch(H, k_rhs_obstacle_correct<T>, gb, kBoxThreads, 0, H->rhs, (const T*)H->chi, H->box, H->nx, H->ny,
                                                                  H->nz, &H->dstate->corr);
         CKL();
         return CUP_OK;
@@ -1286,7 +1342,7 @@ int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partia
   if (out)
     for (int q = 0; q < 3; ++q) o[q] = (T*)out[q];
   rc = launch_named(H, name, [&]() -> int {
-    kern<<<grid, threads, smem, H->stream>>>(maps, geo, o[0], o[1], o[2], H->rhs, H->work32, partials, rmean, prm,
+    klaunch(H, kern, grid, threads, smem, maps, geo, o[0], o[1], o[2], H->rhs, H->work32, partials, rmean, prm,
                                              H->derr, skip);
     CKL();
     return CUP_OK;
@@ -1324,7 +1380,7 @@ int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, co
 int launch_finalize_residual(cup_handle* H, const double* partials, int stride, int grid, int k) {
   const double inv_class = 8.0 / (double)H->n;
   return launch_named(H, "finalize_residual", [&]() -> int {
-    k_finalize_residual<<<1, 256, 0, H->stream>>>(partials, stride, grid, H->dstate, dc_tol(H), k, dc_min_iter(H),
+    klaunch(H, k_finalize_residual, 1, 256, 0, partials, stride, grid, H->dstate, dc_tol(H), k, dc_min_iter(H),
                                                   dc_max_iter(H), inv_class);
     CKL();
     return CUP_OK;
@@ -1420,7 +1476,7 @@ int do_poisson_dc(cup_handle* H) {
     if ((rc = launch_stream<double, 1, 2, 4, 6>(H, "dc_residual", pf, op, &grid, k > 0 ? conv : nullptr))) return rc;
     {
       int rc_ = launch_named(H, "finalize_residual", [&]() -> int {
-        k_finalize_residual<<<1, 256, 0, H->stream>>>(partial(H, P_RES), 18, grid, H->dstate, tol, k, min_iter, max_iter,
+        klaunch(H, k_finalize_residual, 1, 256, 0, partial(H, P_RES), 18, grid, H->dstate, tol, k, min_iter, max_iter,
                                                       inv_class);
         CKL();
         return CUP_OK;
@@ -1470,7 +1526,7 @@ int do_penalize(cup_handle* H, DtArg dt, const double* lambda_dev) {
   const int gb = box_grid(H->box);
   {
     int rc_ = launch_named(H, "penalize", [&]() -> int {
-      k_penalize<T><<<gb, kBoxThreads, 0, H->stream>>>((T*)H->u, (T*)H->v, (T*)H->w, (const T*)H->chi, H->sp_dev, H->box,
+      klaunch(H, k_penalize<T>, gb, kBoxThreads, 0, (T*)H->u, (T*)H->v, (T*)H->w, (const T*)H->chi, H->sp_dev, H->box,
                                                    H->nx, H->ny, H->nz, H->h, dt, lambda_dev, H->lambda,
                                                    H->cfg.bImplicitPenalization, H->uinf[0], H->uinf[1], H->uinf[2],
                                                    partial(H, P_PEN));
@@ -1484,11 +1540,21 @@ int do_penalize(cup_handle* H, DtArg dt, const double* lambda_dev) {
 }
 
 template <typename T>
+int do_surface_forces(cup_handle* H, double* part, int gb) {
+  return launch_named(H, "surface_forces", [&]() -> int {
+    klaunch(H, k_surface_forces<T>, gb, kBoxThreads, 0, (const T*)H->u, (const T*)H->v, (const T*)H->w,
+            (const double*)H->p, (const SphereParams*)H->sp_dev, H->box, H->nx, H->ny, H->nz, H->h, H->cfg.nu, part);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+template <typename T>
 int do_max_u(cup_handle* H) {
   const int grid = std::min<size_t>(H->num_sms * 4, (H->n + 255) / 256);
   {
     int rc_ = launch_named(H, "max_u", [&]() -> int {
-      k_max_u<T><<<grid, 256, 0, H->stream>>>((const T*)H->u, (const T*)H->v, (const T*)H->w, H->n, H->uinf[0], H->uinf[1],
+      klaunch(H, k_max_u<T>, grid, 256, 0, (const T*)H->u, (const T*)H->v, (const T*)H->w, H->n, H->uinf[0], H->uinf[1],
                                           H->uinf[2], partial(H, P_MAX));
       CKL();
       return CUP_OK;
@@ -1497,7 +1563,7 @@ int do_max_u(cup_handle* H) {
   }
   {
     int rc_ = launch_named(H, "finalize_max", [&]() -> int {
-      k_finalize_max<<<1, 256, 0, H->stream>>>(partial(H, P_MAX), grid, H->dstate);
+      klaunch(H, k_finalize_max, 1, 256, 0, partial(H, P_MAX), grid, H->dstate);
       CKL();
       return CUP_OK;
     });
@@ -1538,10 +1604,10 @@ int build_sphere_chi(cup_handle* H) {
   {
     int rc_ = launch_named(H, "sphere_chi", [&]() -> int {
       if (H->fp32)
-        k_sphere_chi<float><<<gb, kBoxThreads, 0, H->stream>>>((float*)H->chi, H->sp_dev, H->box, H->nx, H->ny, H->nz,
+        klaunch(H, k_sphere_chi<float>, gb, kBoxThreads, 0, (float*)H->chi, H->sp_dev, H->box, H->nx, H->ny, H->nz,
                                                                 H->h, partial(H, P_CHI));
       else
-        k_sphere_chi<double><<<gb, kBoxThreads, 0, H->stream>>>((double*)H->chi, H->sp_dev, H->box, H->nx, H->ny,
+        klaunch(H, k_sphere_chi<double>, gb, kBoxThreads, 0, (double*)H->chi, H->sp_dev, H->box, H->nx, H->ny,
                                                                  H->nz, H->h, partial(H, P_CHI));
       CKL();
       return CUP_OK;
@@ -1549,7 +1615,7 @@ int build_sphere_chi(cup_handle* H) {
     if (rc_) return rc_;
   }
   return launch_named(H, "finalize_com", [&]() -> int {
-    k_finalize_com<<<1, 256, 0, H->stream>>>(partial(H, P_CHI), gb, H->dstate, H->sp_dev);
+    klaunch(H, k_finalize_com, 1, 256, 0, partial(H, P_CHI), gb, H->dstate, H->sp_dev);
     CKL();
     return CUP_OK;
   });
@@ -1577,7 +1643,7 @@ int relocate_sphere(cup_handle* H) {
     const Box old = H->box;
     const int gb = box_grid(old);
     int rc_ = launch_named(H, "sphere_clear", [&]() -> int {
-      k_clear_box<<<gb, kBoxThreads, 0, H->stream>>>(H->chi, es, old, H->nx, H->ny, H->nz);
+      klaunch(H, k_clear_box, gb, kBoxThreads, 0, H->chi, es, old, H->nx, H->ny, H->nz);
       CKL();
       return CUP_OK;
     });
@@ -1587,7 +1653,7 @@ int relocate_sphere(cup_handle* H) {
   {
     const double* pos = H->sphere.position;
     int rc_ = launch_named(H, "sphere_position", [&]() -> int {
-      k_set_sphere_position<<<1, 1, 0, H->stream>>>(H->sp_dev, pos[0], pos[1], pos[2]);
+      klaunch(H, k_set_sphere_position, 1, 1, 0, H->sp_dev, pos[0], pos[1], pos[2]);
       CKL();
       return CUP_OK;
     });
@@ -1609,9 +1675,9 @@ int do_spectral(cup_handle* H, bool filter, double raw[4], std::vector<double>& 
   for (int c = 0; c < 3; ++c) {
     int rc_ = launch_named(H, "spectral_widen", [&]() -> int {
       if (H->fp32)
-        k_widen<float><<<grid, 256, 0, H->stream>>>((const float*)f[c], H->spec[c], H->n);
+        klaunch(H, k_widen<float>, grid, 256, 0, (const float*)f[c], H->spec[c], H->n);
       else
-        k_widen<double><<<grid, 256, 0, H->stream>>>((const double*)f[c], H->spec[c], H->n);
+        klaunch(H, k_widen<double>, grid, 256, 0, (const double*)f[c], H->spec[c], H->n);
       CKL();
       return CUP_OK;
     });
@@ -1630,7 +1696,7 @@ int do_spectral(cup_handle* H, bool filter, double raw[4], std::vector<double>& 
   double* pv = partial(H, P_RES);
   {
     int rc_ = launch_named(H, "spectral_modes", [&]() -> int {
-      k_spectral_modes<<<grid, 256, nbin * sizeof(double), H->stream>>>(H->spec[0], H->spec[1], H->spec[2], H->nx, H->ny,
+      klaunch(H, k_spectral_modes, grid, 256, nbin * sizeof(double), H->spec[0], H->spec[1], H->spec[2], H->nx, H->ny,
                                                                         H->nz, wf[0], wf[1], wf[2], nyquist,
                                                                         nyq_scaling, nbin, filter ? 1 : 0, part);
       CKL();
@@ -1641,10 +1707,10 @@ int do_spectral(cup_handle* H, bool filter, double raw[4], std::vector<double>& 
   {
     int rc_ = launch_named(H, "spectral_vorticity", [&]() -> int {
       if (H->fp32)
-        k_vorticity2<float><<<grid, 256, 0, H->stream>>>((const float*)H->u, (const float*)H->v, (const float*)H->w,
+        klaunch(H, k_vorticity2<float>, grid, 256, 0, (const float*)H->u, (const float*)H->v, (const float*)H->w,
                                                           H->nx, H->ny, H->nz, 0.5 / H->h, pv);
       else
-        k_vorticity2<double><<<grid, 256, 0, H->stream>>>((const double*)H->u, (const double*)H->v,
+        klaunch(H, k_vorticity2<double>, grid, 256, 0, (const double*)H->u, (const double*)H->v,
                                                            (const double*)H->w, H->nx, H->ny, H->nz, 0.5 / H->h, pv);
       CKL();
       return CUP_OK;
@@ -1699,7 +1765,7 @@ int do_spectral_forcing(cup_handle* H, double dt) {
       if ((rc = launch_cols<double, 1, false>(H, H->spec[c], H->spec[c], nullptr))) return rc;
       if ((rc = launch_cols<double, 2, false>(H, H->spec[c], H->spec[c], nullptr))) return rc;
       int rc_ = launch_named(H, "spectral_force", [&]() -> int {
-        k_add_scaled<T><<<grid, 256, 0, H->stream>>>((T*)f[c], H->spec[c], fac / NF, H->n);
+        klaunch(H, k_add_scaled<T>, grid, 256, 0, (T*)f[c], H->spec[c], fac / NF, H->n);
         CKL();
         return CUP_OK;
       });
@@ -1747,7 +1813,7 @@ int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance, int 
   if ((rc = do_penalize<T>(H, dt, lambda_dev))) return rc;
   {
     int rc_ = launch_named(H, "finalize_step", [&]() -> int {
-      k_finalize_step<<<1, 256, 0, H->stream>>>(partial(H, P_GRAD), H->n_grad_partials, H->grad_stride,
+      klaunch(H, k_finalize_step, 1, 256, 0, partial(H, P_GRAD), H->n_grad_partials, H->grad_stride,
                                             H->grad_max_off, H->grad_ke_off, partial(H, P_PEN), H->n_pen_partials,
                                             H->dstate, H->h * H->h * H->h, advance,
                                             next_dt, CflParams{H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM});
@@ -1787,7 +1853,7 @@ int launch_adjoint(cup_handle* H, const char* name, const void* const* f, const 
   if (rc) return rc;
   const int grid = std::min(geo.n_items, bpsm * H->num_sms);
   return launch_named(H, name, [&]() -> int {
-    kern<<<grid, threads, smem, H->stream>>>(maps, geo, (T*)out[0], (T*)out[1], (T*)out[2], (T)alpha, (T)beta, dt, H->h,
+    klaunch(H, kern, grid, threads, smem, maps, geo, (T*)out[0], (T*)out[1], (T*)out[2], (T)alpha, (T)beta, dt, H->h,
                                              H->cfg.nu, H->uinf[0], H->uinf[1], H->uinf[2], H->derr);
     CKL();
     return CUP_OK;
@@ -1890,12 +1956,12 @@ int do_adjoint_step_obstacle(cup_handle* H, void* const* un, void* const* lam, D
   const double lambda = H->cfg.DLM > 0 ? H->cfg.DLM / dtv : H->lambda;
   {
     int rc_ = launch_named(H, "adjoint_penalize", [&]() -> int {
-      k_adj_penalize<T><<<gb, kBoxThreads, 0, H->stream>>>(
+      klaunch(H, k_adj_penalize<T>, gb, kBoxThreads, 0, 
           (T*)lam[0], (T*)lam[1], (T*)lam[2], (const T*)us[0], (const T*)us[1], (const T*)us[2], (const T*)H->chi,
           H->sp_dev, H->box, H->nx, H->ny, H->nz, H->h, dtv, lambda, H->cfg.bImplicitPenalization, wF[0], wF[1],
           wF[2], g_chi, partial(H, P_PEN));
       CKL();
-      k_adj_accumulate<<<1, 256, 0, H->stream>>>(partial(H, P_PEN), gb, 3, 3, g_vel);
+      klaunch(H, k_adj_accumulate, 1, 256, 0, partial(H, P_PEN), gb, 3, 3, g_vel);
       CKL();
       return CUP_OK;
     });
@@ -1907,13 +1973,13 @@ int do_adjoint_step_obstacle(cup_handle* H, void* const* un, void* const* lam, D
   {
     int rc_ = launch_named(H, "adjoint_rhs_obstacle", [&]() -> int {
       CK(cudaMemsetAsync(&H->dstate->adj_sq, 0, sizeof(double), H->stream));
-      k_adj_rhs_sum<T><<<gb, kBoxThreads, 0, H->stream>>>(H->p_adj, H->ab0, (const T*)H->chi, H->box, H->nx, H->ny,
+      klaunch(H, k_adj_rhs_sum<T>, gb, kBoxThreads, 0, H->p_adj, H->ab0, (const T*)H->chi, H->box, H->nx, H->ny,
                                                          H->nz, H->dstate->rhs_sums, &H->dstate->corr,
                                                          partial(H, P_RHSOB));
       CKL();
-      k_adj_accumulate<<<1, 256, 0, H->stream>>>(partial(H, P_RHSOB), gb, 1, 1, &H->dstate->adj_sq);
+      klaunch(H, k_adj_accumulate, 1, 256, 0, partial(H, P_RHSOB), gb, 1, 1, &H->dstate->adj_sq);
       CKL();
-      k_adj_rhs_apply<T><<<gb, kBoxThreads, 0, H->stream>>>(H->p_adj, H->ab0, (const T*)H->chi, H->box, H->nx,
+      klaunch(H, k_adj_rhs_apply<T>, gb, kBoxThreads, 0, H->p_adj, H->ab0, (const T*)H->chi, H->box, H->nx,
                                                            H->ny, H->nz, H->dstate->rhs_sums, &H->dstate->corr,
                                                            &H->dstate->adj_sq, kappa, g_chi);
       CKL();
@@ -1951,7 +2017,7 @@ int set_field(cup_handle* H, void* dst, const double* src, int where) {
   }
   {
     int rc_ = launch_named(H, "convert_from_f64", [&]() -> int {
-      k_convert_from_f64<T><<<H->num_sms * 4, 256, 0, H->stream>>>((T*)dst, s, H->n);
+      klaunch(H, k_convert_from_f64<T>, H->num_sms * 4, 256, 0, (T*)dst, s, H->n);
       CKL();
       return CUP_OK;
     });
@@ -1970,7 +2036,7 @@ int get_field(cup_handle* H, const void* src, double* dst, int where) {
   double* d = where == CUP_WHERE_HOST ? H->rhs : dst;
   {
     int rc_ = launch_named(H, "convert_to_f64", [&]() -> int {
-      k_convert_to_f64<T><<<H->num_sms * 4, 256, 0, H->stream>>>(d, (const T*)src, H->n);
+      klaunch(H, k_convert_to_f64<T>, H->num_sms * 4, 256, 0, d, (const T*)src, H->n);
       CKL();
       return CUP_OK;
     });
@@ -2145,6 +2211,7 @@ int cup_create(const cup_config* cfg, cup_handle** out) {
   H->lambda = cfg->lambda;
   for (int d = 0; d < 3; ++d) H->uinf[d] = cfg->uinf[d];
   H->dev = cfg->device;
+  if (const char* pdl = getenv("CUP_PDL")) H->pdl = atoi(pdl) != 0;
   cudaError_t e = cudaSetDevice(H->dev);
   if (e != cudaSuccess) {
     fail(H, CUP_ERR_CUDA, "cudaSetDevice(%d): %s", H->dev, cudaGetErrorString(e));
@@ -2491,7 +2558,7 @@ int cup_calc_max_timestep(cup_handle* H, double* dt) {
   {
     // the device keeps its own step counter in sync with the host mirror
     int rc_ = launch_named(H, "calc_dt", [&]() -> int {
-      k_calc_dt<<<1, 1, 0, H->stream>>>(H->dstate, H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM, H->step);
+      klaunch(H, k_calc_dt, 1, 1, 0, H->dstate, H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM, H->step);
       CKL();
       return CUP_OK;
     });
@@ -2586,7 +2653,7 @@ int cup_penalize(cup_handle* H, double dt, double force_torque[6]) {
   }
   {
     int rc_ = launch_named(H, "set_state", [&]() -> int {
-      k_set_state<<<1, 1, 0, H->stream>>>(H->dstate, SET_LAMBDA, 0.0, H->cfg.DLM, H->lambda, 0, 0.0);
+      klaunch(H, k_set_state, 1, 1, 0, H->dstate, SET_LAMBDA, 0.0, H->cfg.DLM, H->lambda, 0, 0.0);
       CKL();
       return CUP_OK;
     });
@@ -2596,7 +2663,7 @@ int cup_penalize(cup_handle* H, double dt, double force_torque[6]) {
   if (rc) return rc;
   {
     int rc_ = launch_named(H, "finalize_pen", [&]() -> int {
-      k_finalize_pen<<<1, 256, 0, H->stream>>>(partial(H, P_PEN), H->n_pen_partials, H->dstate);
+      klaunch(H, k_finalize_pen, 1, 256, 0, partial(H, P_PEN), H->n_pen_partials, H->dstate);
       CKL();
       return CUP_OK;
     });
@@ -2644,7 +2711,7 @@ int cup_step(cup_handle* H, double dt, cup_step_stats* stats) {
   // device dt/lambda follow the host values for this step
   {
     int rc_ = launch_named(H, "set_dt", [&]() -> int {
-      k_set_state<<<1, 1, 0, H->stream>>>(H->dstate, SET_DT | SET_LAMBDA, dt, H->cfg.DLM, H->lambda, 0, 0.0);
+      klaunch(H, k_set_state, 1, 1, 0, H->dstate, SET_DT | SET_LAMBDA, dt, H->cfg.DLM, H->lambda, 0, 0.0);
       CKL();
       return CUP_OK;
     });
@@ -2775,7 +2842,7 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
   }
   {
     int rc_ = launch_named(H, "set_state", [&]() -> int {
-      k_set_state<<<1, 1, 0, H->stream>>>(H->dstate, SET_LAMBDA | SET_CLOCK, 0.0, H->cfg.DLM, H->lambda, H->step,
+      klaunch(H, k_set_state, 1, 1, 0, H->dstate, SET_LAMBDA | SET_CLOCK, 0.0, H->cfg.DLM, H->lambda, H->step,
                                           H->time);
       CKL();
       return CUP_OK;
@@ -2798,7 +2865,7 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
     // the dt of step i > 0 comes from the end of step i - 1
     if (i == 0) {
       int rc_ = launch_named(H, "calc_dt", [&]() -> int {
-        k_calc_dt<<<1, 1, 0, H->stream>>>(H->dstate, H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM);
+        klaunch(H, k_calc_dt, 1, 1, 0, H->dstate, H->h, H->cfg.nu, H->cfg.CFL, H->cfg.rampup, H->cfg.DLM, -1);
         CKL();
         return CUP_OK;
       });
@@ -2851,10 +2918,10 @@ int cup_diagnostics(cup_handle* H, double out[3]) {
   {
     int rc_ = launch_named(H, "diag", [&]() -> int {
       if (H->fp32)
-        k_diag<float><<<grid, 256, 0, H->stream>>>((const float*)H->u, (const float*)H->v, (const float*)H->w, H->nx,
+        klaunch(H, k_diag<float>, grid, 256, 0, (const float*)H->u, (const float*)H->v, (const float*)H->w, H->nx,
                                                     H->ny, H->nz, 0.5 / H->h, part);
       else
-        k_diag<double><<<grid, 256, 0, H->stream>>>((const double*)H->u, (const double*)H->v, (const double*)H->w,
+        klaunch(H, k_diag<double>, grid, 256, 0, (const double*)H->u, (const double*)H->v, (const double*)H->w,
                                                      H->nx, H->ny, H->nz, 0.5 / H->h, part);
       CKL();
       return CUP_OK;
@@ -2933,6 +3000,36 @@ int cup_get_forcing_stats(cup_handle* H, double stats[6]) {
   return CUP_OK;
 }
 
+int cup_compute_forces(cup_handle* H, double out[27]) {
+  REQUIRE_H(H);
+  if (!out) return fail(H, CUP_ERR_ARG, "null output");
+  for (int k = 0; k < 27; ++k) out[k] = 0.0;
+  if (!H->has_sphere) return CUP_OK;  // ComputeForces: nothing without obstacles
+  const int gb = box_grid(H->box);
+  double* part = partial(H, P_DIAG);
+  int rc = H->fp32 ? do_surface_forces<float>(H, part, gb) : do_surface_forces<double>(H, part, gb);
+  if (rc) return rc;
+  std::vector<double> hp((size_t)kSurfQoI * gb);
+  SphereParams sp;
+  CK(cudaMemcpyAsync(hp.data(), part, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaMemcpyAsync(&sp, H->sp_dev, sizeof(SphereParams), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  for (int b = 0; b < gb; ++b)
+    for (int k = 0; k < kSurfQoI; ++k) out[k] += hp[(size_t)kSurfQoI * b + k];
+  // derived quantities of Obstacle::computeForces (source/obstacles/Obstacle.cpp:283-294)
+  const double EPS = 2.220446049250313080847e-16;
+  const double vel_norm = std::sqrt(sp.transVel[0] * sp.transVel[0] + sp.transVel[1] * sp.transVel[1] +
+                                    sp.transVel[2] * sp.transVel[2]);
+  const double drag = out[15], thrust = out[16], defPower = out[19], defPowerBnd = out[20];
+  out[22] = thrust * vel_norm;                                            // Pthrust
+  out[23] = drag * vel_norm;                                              // Pdrag
+  out[24] = out[22] / (out[22] - std::min(defPower, 0.0) + EPS);          // EffPDef
+  out[25] = out[22] / (out[22] - defPowerBnd + EPS);                      // EffPDefBnd
+  if ((rc = read_state(H))) return rc;
+  out[26] = H->hstate->mass;  // the grid mass of chi (ObstaclesCreate.cpp:230-256)
+  return check_dev_error(H);
+}
+
 int cup_compute_dissipation(cup_handle* H, double out[20]) {
   REQUIRE_H(H);
   if (!out) return fail(H, CUP_ERR_ARG, "null output");
@@ -2944,12 +3041,12 @@ int cup_compute_dissipation(cup_handle* H, double out[20]) {
   {
     int rc_ = launch_named(H, "dissipation", [&]() -> int {
       if (H->fp32)
-        k_dissipation<float><<<grid, 256, 0, H->stream>>>((const float*)H->u, (const float*)H->v, (const float*)H->w,
+        klaunch(H, k_dissipation<float>, grid, 256, 0, (const float*)H->u, (const float*)H->v, (const float*)H->w,
                                                            H->p, H->has_sphere ? (const float*)H->chi : nullptr, H->nx,
                                                            H->ny, H->nz, h, H->cfg.nu, hCube, inv2h, invHh, cx, cy, cz,
                                                            part);
       else
-        k_dissipation<double><<<grid, 256, 0, H->stream>>>(
+        klaunch(H, k_dissipation<double>, grid, 256, 0, 
             (const double*)H->u, (const double*)H->v, (const double*)H->w, H->p,
             H->has_sphere ? (const double*)H->chi : nullptr, H->nx, H->ny, H->nz, h, H->cfg.nu, hCube, inv2h, invHh,
             cx, cy, cz, part);

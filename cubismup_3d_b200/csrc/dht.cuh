@@ -587,6 +587,7 @@ struct AddToPRows {
 template <int M, typename R, class Prod, class Cons>
 __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons cons, int nrows, int lpc,
                                                   const typename Cplx<R>::T* tw_g, int* err, const int* skip) {
+  pdl_entry();
   using R2 = typename Cplx<R>::T;
   if (skip && *skip) return;
   constexpr int N = 2 * M, TPL = M / 8;
@@ -679,6 +680,7 @@ template <int M, typename R, int NB>
 __global__ void __launch_bounds__(256, 2) k_dht_rows_pipe(const R* __restrict__ in, R* __restrict__ out, int nrows,
                                                           int lpc, const typename Cplx<R>::T* tw_g, int* err,
                                                           const int* skip) {
+  pdl_entry();
   using R2 = typename Cplx<R>::T;
   static_assert(NB >= 2, "need at least two tile buffers");
   if (skip && *skip) return;
@@ -806,6 +808,7 @@ __global__ void __launch_bounds__(W * (T8 ? 8 : M / 8)) k_dht_cols_pipe(const __
                                                        int ntiles, const typename Cplx<R>::T* tw_g,
                                                        const typename Cplx<RIN>::T* tw_in_g, SpectralParams sp,
                                                        int* err, const int* skip) {
+  pdl_entry();
   using R2 = typename Cplx<R>::T;
   using RI2 = typename Cplx<RIN>::T;
   static_assert(NB >= 2, "need at least two tile buffers");

@@ -299,6 +299,7 @@ __device__ __forceinline__ double sphere_sdf(const SphereParams& s, double x, do
 template <typename T>
 __global__ void k_sphere_chi(T* chi, const SphereParams* sp, Box box, int nx, int ny, int nz, double h,
                              double* partials /* [gridDim.x][4] */) {
+  pdl_entry();
   __shared__ double scratch[4 * 32];
   const SphereParams s = *sp;
   double acc[4] = {0, 0, 0, 0};
@@ -355,6 +356,7 @@ __global__ void k_sphere_chi(T* chi, const SphereParams* sp, Box box, int nx, in
 template <typename T>
 __global__ void k_rhs_obstacle(double* rhs, const T* chi, Box box, int nx, int ny, int nz,
                                double* partials /* [gridDim.x][3] */) {
+  pdl_entry();
   __shared__ double scratch[3 * 32];
   double acc[3] = {0, 0, 0};
   const long long n = box.count();
@@ -386,6 +388,7 @@ __global__ void k_rhs_obstacle(double* rhs, const T* chi, Box box, int nx, int n
 template <typename T>
 __global__ void k_rhs_obstacle_correct(double* rhs, const T* chi, Box box, int nx, int ny, int nz,
                                        const double* corr_dev) {
+  pdl_entry();
   const double corr = *corr_dev;
   const long long n = box.count();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -404,6 +407,110 @@ __global__ void k_rhs_obstacle_correct(double* rhs, const T* chi, Box box, int n
   }
 }
 
+// Surface forces of the sphere: the surface points of KernelCharacteristicFunction
+// (source/operators/ObstaclesCreate.cpp:106-131: the SDF shifted outward by
+// SURFDH cells, Heaviside differences of the neighbours, Delta = h^2/2 gradH .
+// gradU / |gradU|^2 = h^3 delta, dchi = -Delta gradU) and, at each, the
+// pressure and viscous stress integrands of KernelComputeForces
+// (source/operators/FluidSolidForces.cpp:43-158) with the current u, v, w
+// (central differences) and p; no rotation and no deformation velocity for the
+// forced sphere. Per-CTA partials of the 22 quantities in ObstacleBlock::sumQoI
+// order (source/ObstacleBlock.h:81-93): surface force, pressure force, viscous
+// force, torque about the centre of mass, gamma, drag, thrust, Pout, PoutBnd,
+// defPower, defPowerBnd, pLocom.
+constexpr int kSurfQoI = 22;
+template <typename T>
+__global__ void k_surface_forces(const T* u, const T* v, const T* w, const double* p, const SphereParams* sp, Box box,
+                                 int nx, int ny, int nz, double h, double nu, double* partials /* [gridDim.x][22] */) {
+  pdl_entry();
+  __shared__ double scratch[kSurfQoI * 32];
+  const SphereParams s = *sp;
+  double acc[kSurfQoI];
+#pragma unroll
+  for (int k = 0; k < kSurfQoI; ++k) acc[k] = 0.0;
+  const double EPS = 2.220446049250313080847e-16;  // std::numeric_limits<double>::epsilon()
+  const double inv2h = .5 / h, fac1 = .5 * h * h, shift = h * 1.0;  // SURFDH = 1
+  const double _1oH = nu / h;
+  const double* CM = s.centerOfMass;
+  const double* uT = s.transVel;
+  double velUnit[3] = {0., 0., 0.};
+  const double vel_norm = sqrt(uT[0] * uT[0] + uT[1] * uT[1] + uT[2] * uT[2]);
+  if (vel_norm > 1e-9) {
+    velUnit[0] = uT[0] / vel_norm;
+    velUnit[1] = uT[1] / vel_norm;
+    velUnit[2] = uT[2] / vel_norm;
+  }
+  const long long n = box.count();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = wrapi(box.lo[0] + (int)(i % box.n[0]), nx);
+    const int y = wrapi(box.lo[1] + (int)((i / box.n[0]) % box.n[1]), ny);
+    const int z = wrapi(box.lo[2] + (int)(i / ((long long)box.n[0] * box.n[1])), nz);
+    const double sdf = sphere_sdf(s, (x + 0.5) * h, (y + 0.5) * h, (z + 0.5) * h) + shift;
+    if (sdf > +2 * h || sdf < -2 * h) continue;
+    const int xp = wrapi(x + 1, nx), xm = wrapi(x - 1, nx), yp = wrapi(y + 1, ny), ym = wrapi(y - 1, ny),
+              zp = wrapi(z + 1, nz), zm = wrapi(z - 1, nz);
+    const double distPx = sphere_sdf(s, (xp + 0.5) * h, (y + 0.5) * h, (z + 0.5) * h) + shift;
+    const double distMx = sphere_sdf(s, (xm + 0.5) * h, (y + 0.5) * h, (z + 0.5) * h) + shift;
+    const double distPy = sphere_sdf(s, (x + 0.5) * h, (yp + 0.5) * h, (z + 0.5) * h) + shift;
+    const double distMy = sphere_sdf(s, (x + 0.5) * h, (ym + 0.5) * h, (z + 0.5) * h) + shift;
+    const double distPz = sphere_sdf(s, (x + 0.5) * h, (y + 0.5) * h, (zp + 0.5) * h) + shift;
+    const double distMz = sphere_sdf(s, (x + 0.5) * h, (y + 0.5) * h, (zm + 0.5) * h) + shift;
+    const double gradUX = inv2h * (distPx - distMx);
+    const double gradUY = inv2h * (distPy - distMy);
+    const double gradUZ = inv2h * (distPz - distMz);
+    const double gradUSq = gradUX * gradUX + gradUY * gradUY + gradUZ * gradUZ + EPS;
+    auto H = [&](double d) { return fabs(d) < EPS ? 0.5 : (d < 0 ? 0.0 : 1.0); };
+    const double gradHX = H(distPx) - H(distMx);
+    const double gradHY = H(distPy) - H(distMy);
+    const double gradHZ = H(distPz) - H(distMz);
+    const double numD = gradHX * gradUX + gradHY * gradUY + gradHZ * gradUZ;
+    const double Delta = fac1 * numD / gradUSq;
+    if (!(Delta > EPS)) continue;
+    const double normX = -Delta * gradUX, normY = -Delta * gradUY, normZ = -Delta * gradUZ;
+    auto U = [&](const T* f, int a, int b, int c) { return (double)f[gidx(a, b, c, nx, ny)]; };
+    const double D11 = _1oH * (U(u, xp, y, z) - U(u, xm, y, z));
+    const double D22 = _1oH * (U(v, x, yp, z) - U(v, x, ym, z));
+    const double D33 = _1oH * (U(w, x, y, zp) - U(w, x, y, zm));
+    const double D12 = .5 * _1oH * (U(u, x, yp, z) - U(u, x, ym, z) + U(v, xp, y, z) - U(v, xm, y, z));
+    const double D13 = .5 * _1oH * (U(u, x, y, zp) - U(u, x, y, zm) + U(w, xp, y, z) - U(w, xm, y, z));
+    const double D23 = .5 * _1oH * (U(w, x, yp, z) - U(w, x, ym, z) + U(v, x, y, zp) - U(v, x, y, zm));
+    const double P = p[gidx(x, y, z, nx, ny)];
+    const double fXV = D11 * normX + D12 * normY + D13 * normZ;
+    const double fYV = D12 * normX + D22 * normY + D23 * normZ;
+    const double fZV = D13 * normX + D23 * normY + D33 * normZ;
+    const double fXP = -P * normX, fYP = -P * normY, fZP = -P * normZ;
+    const double fXT = fXV + fXP, fYT = fYV + fYP, fZT = fZV + fZP;
+    const double px = (x + 0.5) * h, py = (y + 0.5) * h, pz = (z + 0.5) * h;
+    const double vX = U(u, x, y, z), vY = U(v, x, y, z), vZ = U(w, x, y, z);
+    acc[0] += fXT;
+    acc[1] += fYT;
+    acc[2] += fZT;
+    acc[3] += fXP;
+    acc[4] += fYP;
+    acc[5] += fZP;
+    acc[6] += fXV;
+    acc[7] += fYV;
+    acc[8] += fZV;
+    acc[9] += (py - CM[1]) * fZT - (pz - CM[2]) * fYT;
+    acc[10] += (pz - CM[2]) * fXT - (px - CM[0]) * fZT;
+    acc[11] += (px - CM[0]) * fYT - (py - CM[1]) * fXT;
+    acc[12] += normY * vZ - normZ * vY;
+    acc[13] += normZ * vX - normX * vZ;
+    acc[14] += normX * vY - normY * vX;
+    const double forcePar = fXT * velUnit[0] + fYT * velUnit[1] + fZT * velUnit[2];
+    acc[15] -= .5 * (forcePar - fabs(forcePar));  // drag
+    acc[16] += .5 * (forcePar + fabs(forcePar));  // thrust
+    const double powOut = fXT * vX + fYT * vY + fZT * vZ;
+    acc[17] += powOut;
+    acc[18] += fmin(0.0, powOut);
+    // defPower, defPowerBnd: the sphere has no deformation velocity (acc[19], acc[20] stay 0)
+    acc[21] += fXT * uT[0] + fYT * uT[1] + fZT * uT[2];  // pLocom with angVel = 0
+  }
+  block_reduce<kSurfQoI, false>(acc, scratch);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kSurfQoI; ++k) partials[kSurfQoI * blockIdx.x + k] = acc[k];
+}
+
 // KernelPenalization<implicit> (source/operators/Penalization.cpp:40-98) over
 // the box, FP64 force/torque partials (KernelFinalizePenalizationForce,
 // :101-123) and the max |u + uinf| of every box cell after penalization.
@@ -411,6 +518,7 @@ template <typename T>
 __global__ void k_penalize(T* u, T* v, T* w, const T* chi, const SphereParams* sp, Box box, int nx, int ny, int nz,
                            double h, DtArg dt, const double* lambda_dev, double lambda_host, int implicit_pen,
                            double uinf0, double uinf1, double uinf2, double* partials /* [gridDim.x][8] */) {
+  pdl_entry();
   __shared__ double scratch[8 * 32];
   const SphereParams s = *sp;
   const double dtv = dt.get();

@@ -129,6 +129,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
                                                 double* __restrict__ bout, float* __restrict__ rout,
                                                 double* __restrict__ partials, const double* __restrict__ rmean,
                                                 const PzqParams prm, int* err, const int* skip) {
+  pdl_entry();
   constexpr int G = 2;
   constexpr int Q = 2 * G + 1;
   constexpr int U = ZCC ? ZCC + 2 * G : 10;  // planes per unrolled chunk: a whole item, or lcm(Q, G)

@@ -56,6 +56,7 @@ constexpr size_t stream_smem_bytes(int nx) {
 template <typename T, int NF, int G, int TY, int NS, class Op>
 __global__ void __launch_bounds__(256) k_stencil_stream(const __grid_constant__ FieldMaps<NF> maps,
                                                        const StreamGeom g, Op op, int* err, const int* skip) {
+  pdl_entry();
   static_assert(NS >= 2 * G + 1, "ring must hold the stencil planes");
   // a G-row halo box starting at y0 - G (wrapped) stays inside [0, ny) only if y0 is a multiple of TY >= G
   static_assert(TY >= G, "tile height must cover the halo depth");

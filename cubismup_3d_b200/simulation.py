@@ -257,6 +257,30 @@ class ComputeDissipation(Operator):
         self.sim._diagnostics_line(self.sim.step, self.sim.time)
 
 
+# ComputeForces outputs (source/obstacles/Obstacle.cpp:266-295): the 22 sums in
+# ObstacleBlock::sumQoI order (source/ObstacleBlock.h:81-93), the derived
+# powers and efficiencies, the grid mass of chi
+FORCE_NAMES = ("surfForce_x", "surfForce_y", "surfForce_z", "presForce_x", "presForce_y", "presForce_z",
+               "viscForce_x", "viscForce_y", "viscForce_z", "surfTorque_x", "surfTorque_y", "surfTorque_z",
+               "gamma_x", "gamma_y", "gamma_z", "drag", "thrust", "Pout", "PoutBnd", "defPower", "defPowerBnd",
+               "pLocom", "Pthrust", "Pdrag", "EffPDef", "EffPDefBnd", "mass")
+
+
+class ComputeForces(Operator):
+    """ComputeForces (source/operators/FluidSolidForces.cpp:200-222) after
+    Penalization: the surface forces of the sphere on the final velocity and
+    pressure, appended to forceValues_surface_<id>.dat and
+    powerValues_surface_<id>.dat in the reference's format
+    (source/obstacles/Obstacle.cpp:518-556); nothing without obstacles."""
+    name = "ComputeForces"
+
+    def __call__(self, dt: float):
+        if not self.sim.obstacles:
+            return
+        self.forces = self.sim.compute_forces()
+        self.sim._forces_lines(self.sim.step, self.sim.time, self.forces)
+
+
 class SpectralForcing(Operator):
     """SpectralForcing (source/spectralOperators/SpectralForcing.cpp:23-86): raises the
     energy of the band 0 < k^2 <= 4 to meet turbKinEn_target or enInjectionRate."""
@@ -313,7 +337,7 @@ class PoissonSolverPeriodic:
 
     def _offset(self, info) -> int:
         """First cell of a block: ``info`` has ``index`` (bx, by, bz) or is that triple."""
-        bx, by, bz = getattr(info, "index", info)
+        bx, by, bz = info if isinstance(info, (tuple, list)) else info.index
         return BLOCK_SIZE * (self.stridez * bz + self.stridey * by + self.stridex * bx)
 
     _offset_ext = _offset
@@ -386,7 +410,7 @@ class Simulation:
         # Simulation::setupOperators (source/Simulation.cpp:307-401)
         self.pipeline: List[Operator] = [CreateObstacles(self), AdvectionDiffusion(self), PressureRHS(self),
                                          PressureProjection(self), UpdateObstacles(self), Penalization(self),
-                                         ComputeDissipation(self)]
+                                         ComputeForces(self), ComputeDissipation(self)]
         if sd.turbKinEn_target > 0 and sd.enInjectionRate > 0:
             raise ValueError("give either turbKinEn_target or enInjectionRate, not both (SimulationData.cpp:64-66)")
         self.forcing = sd.turbKinEn_target > 0 or sd.enInjectionRate > 0
@@ -634,6 +658,36 @@ class Simulation:
             if (self.sd.endTime > 0 and self.time > self.sd.endTime) or (
                     self.sd.nsteps != 0 and self.step >= self.sd.nsteps):
                 return last
+
+    def compute_forces(self) -> dict:
+        """ComputeForces' surface forces of the current fields (cup_compute_forces),
+        by name (FORCE_NAMES); all zero without an obstacle."""
+        out = (C.c_double * 27)()
+        L.check(L.lib().cup_compute_forces(self._h, out), self._h, "compute_forces")
+        return dict(zip(FORCE_NAMES, out[:]))
+
+    def _forces_lines(self, step: int, time: float, f: dict, oid: int = 0):
+        """Obstacle::_writeSurfForcesToFile (source/obstacles/Obstacle.cpp:518-556):
+        tab-separated, header at step 0, values in scientific notation with 8
+        significant digits."""
+        tab = "\t"
+        e = lambda x: f"{x:.7e}"  # noqa: E731  (std::scientific, precision digits10 + 1)
+        with open(f"forceValues_surface_{oid}.dat", "a") as fh:
+            if step == 0:
+                fh.write(tab.join(["step", "time", "mass", "force_x", "force_y", "force_z", "torque_x", "torque_y",
+                                   "torque_z", "presF_x", "presF_y", "presF_z", "viscF_x", "viscF_y", "viscF_z",
+                                   "gamma_x", "gamma_y", "gamma_z", "drag", "thrust"]) + "\n")
+            keys = ("mass", "surfForce_x", "surfForce_y", "surfForce_z", "surfTorque_x", "surfTorque_y", "surfTorque_z",
+                    "presForce_x", "presForce_y", "presForce_z", "viscForce_x", "viscForce_y", "viscForce_z",
+                    "gamma_x", "gamma_y", "gamma_z", "drag", "thrust")
+            fh.write(f"{step}{tab}" + tab.join([e(time)] + [e(f[k]) for k in keys]) + "\n")
+        with open(f"powerValues_surface_{oid}.dat", "a") as fh:
+            if step == 0:
+                fh.write(tab.join(["step", "time", "Pthrust", "Pdrag", "Pout", "pDef", "etaPDef", "pLocom", "PoutBnd",
+                                   "defPowerBnd", "etaPDefBnd"]) + "\n")
+            vals = [time, f["Pthrust"], f["Pdrag"], f["Pout"], -f["defPower"], f["EffPDef"], f["pLocom"], f["PoutBnd"],
+                    -f["defPowerBnd"], f["EffPDefBnd"]]
+            fh.write(f"{step}{tab}" + tab.join(e(x) for x in vals) + "\n")
 
     def compute_dissipation(self) -> dict:
         """ComputeDissipation's 20 FP64 sums of the current fields, by diagnostics.dat column name."""

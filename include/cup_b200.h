@@ -251,6 +251,18 @@ int cup_poisson_solve_field(struct cup_handle* h, const double* rhs, double* p, 
  * out[1] L2 norm (sum h^3 div^2)^(1/2) of the central divergence, out[2] max |div|
  * (ComputeDissipation.cpp:47-116 pattern, PoissonSolver.cpp:35-52 pattern). */
 int cup_diagnostics(struct cup_handle* h, double out[3]);
+/* ComputeForces (source/operators/FluidSolidForces.cpp:17-222) and
+ * Obstacle::computeForces (source/obstacles/Obstacle.cpp:266-295) for the
+ * sphere on the current fields: the surface points of CreateObstacles
+ * (ObstaclesCreate.cpp:106-131) and the pressure and viscous stress on them.
+ * out[27] = the 22 sums in ObstacleBlock::sumQoI order (surfForce[3],
+ * presForce[3], viscForce[3], surfTorque[3], gamma[3], drag, thrust, Pout,
+ * PoutBnd, defPower, defPowerBnd, pLocom), then Pthrust, Pdrag, EffPDef,
+ * EffPDefBnd and the grid mass of chi. All zero without an obstacle. The reference runs it after
+ * Penalization every step; cup_step / cup_run leave it out (they report the
+ * penalization force), so call it after a step when the surface forces are
+ * wanted. Synchronises the stream. */
+int cup_compute_forces(struct cup_handle* h, double out[27]);
 /* ComputeDissipation (source/operators/ComputeDissipation.cpp:38-177) on the
  * current fields: out[20] = circulation[3], linImpulse[3], linMomentum[3],
  * angImpulse[3], angMomentum[3], presPow, viscPow, helicity, kineticEn,

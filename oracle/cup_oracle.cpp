@@ -256,6 +256,14 @@ struct Sphere {
   double force[3] = {0, 0, 0}, torque[3] = {0, 0, 0};
   std::vector<char> touched;         // obstacle block present (ObstacleBlock* != nullptr)
   std::vector<Real> SDF, CHI;        // per cell, meaningful on touched blocks
+  // surface points of ObstacleBlock::write (source/ObstacleBlock.h:157-166), in
+  // block order and, per block, in the (iz, iy, ix) order they were found
+  struct SurfacePoint {
+    int gx, gy, gz;
+    double dchidx, dchidy, dchidz, delta;
+  };
+  std::vector<int> surf_begin;       // per block: first surface point (nblocks + 1 entries)
+  std::vector<SurfacePoint> surface;
 };
 
 }  // namespace
@@ -470,6 +478,8 @@ void op_create_obstacles(OState& S) {
   }
   const Real inv2h = .5 / h, vol = h * h * h;
   double com[4] = {0, 0, 0, 0};
+  s.surface.clear();
+  s.surf_begin.assign(nb + 1, 0);
   for (int b = 0; b < nb; ++b) {
     if (!s.touched[b]) continue;
     const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
@@ -507,9 +517,25 @@ void op_create_obstacles(OState& S) {
       const Real p[3] = {(gx + 0.5) * h, (gy + 0.5) * h, (gz + 0.5) * h};
       cx += chi * vol * p[0]; cy += chi * vol * p[1]; cz += chi * vol * p[2];
       m += chi * vol;
+      // surface delta and normal with the SDF shifted outward by SURFDH cells
+      // (ObstaclesCreate.cpp:106-131)
+      const Real sdfs = sdf + h * SURFDH;
+      if (sdfs > +2 * h || sdfs < -2 * h) continue;
+      const Real dPx = L(ix+1,iy,iz) + h * SURFDH, dMx = L(ix-1,iy,iz) + h * SURFDH;
+      const Real dPy = L(ix,iy+1,iz) + h * SURFDH, dMy = L(ix,iy-1,iz) + h * SURFDH;
+      const Real dPz = L(ix,iy,iz+1) + h * SURFDH, dMz = L(ix,iy,iz-1) + h * SURFDH;
+      const Real gUX = inv2h * (dPx - dMx), gUY = inv2h * (dPy - dMy), gUZ = inv2h * (dPz - dMz);
+      const Real gUSq = gUX * gUX + gUY * gUY + gUZ * gUZ + EPS;
+      auto Hs = [](Real d) -> Real { return std::fabs(d) < EPS ? 0.5 : (d < 0 ? 0 : 1); };
+      const Real gHX = Hs(dPx) - Hs(dMx), gHY = Hs(dPy) - Hs(dMy), gHZ = Hs(dPz) - Hs(dMz);
+      const Real numD = gHX * gUX + gHY * gUY + gHZ * gUZ;
+      const Real Delta = .5 * h * h * numD / gUSq;  // h^3 * Delta
+      if (Delta > EPS) s.surface.push_back({gx, gy, gz, -Delta * gUX, -Delta * gUY, -Delta * gUZ, Delta});
     }
     com[0] += m; com[1] += cx; com[2] += cy; com[3] += cz;
+    s.surf_begin[b + 1] = (int)s.surface.size();
   }
+  for (int b = 1; b <= nb; ++b) s.surf_begin[b] = std::max(s.surf_begin[b], s.surf_begin[b - 1]);
   s.centerOfMass[0] = com[1] / com[0];
   s.centerOfMass[1] = com[2] / com[0];
   s.centerOfMass[2] = com[3] / com[0];
@@ -821,6 +847,99 @@ double orc_calc_max_timestep(void* hdl) {
 
 double orc_max_u(void* hdl) { return find_max_u(*static_cast<OState*>(hdl)); }
 
+// ComputeForces (source/operators/FluidSolidForces.cpp:17-158, 200-222) on the
+// surface points of the last CreateObstacles: per block, the stress integrands
+// of KernelComputeForces at each point (lab of u, v, w, p with a one-cell
+// halo), summed per block in ObstacleBlock::sumQoI order
+// (source/ObstacleBlock.h:81-93), then over blocks; then the derived powers of
+// Obstacle::computeForces (source/obstacles/Obstacle.cpp:266-295) and the
+// grid mass. out[27]; all zero without an obstacle.
+void orc_compute_forces(void* hdl, double* out) {
+  OState* S = static_cast<OState*>(hdl);
+  for (int k = 0; k < 27; ++k) out[k] = 0;
+  if (!S->has_sphere) return;
+  const Dims D = S->D;
+  const Sphere& s = S->sph;
+  const Real h = S->h, _1oH = S->cfg.nu / h;
+  const double* CM = s.centerOfMass;
+  const double* uTrans = s.transVel;
+  const double* omega = s.angVel;
+  double velUnit[3] = {0., 0., 0.};
+  const double vel_norm = std::sqrt(uTrans[0] * uTrans[0] + uTrans[1] * uTrans[1] + uTrans[2] * uTrans[2]);
+  if (vel_norm > 1e-9)
+    for (int d = 0; d < 3; ++d) velUnit[d] = uTrans[d] / vel_norm;
+  const int nb = D.nblocks();
+  std::vector<double> sum(22, 0.0);
+  for (int b = 0; b < nb; ++b) {
+    if (!s.touched[b] || s.surf_begin[b + 1] == s.surf_begin[b]) continue;
+    const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
+    Lab LU, LV, LW;
+    LU.load(S->u.data(), D, bx, by, bz, 1);
+    LV.load(S->v.data(), D, bx, by, bz, 1);
+    LW.load(S->w.data(), D, bx, by, bz, 1);
+    double q[22] = {0};
+    for (int i = s.surf_begin[b]; i < s.surf_begin[b + 1]; ++i) {
+      const Sphere::SurfacePoint& sp = s.surface[i];
+      const int ix = sp.gx - bx * BS, iy = sp.gy - by * BS, iz = sp.gz - bz * BS;
+      const Real p[3] = {(sp.gx + 0.5) * h, (sp.gy + 0.5) * h, (sp.gz + 0.5) * h};
+      const double D11 = _1oH * (LU(ix+1,iy,iz) - LU(ix-1,iy,iz));
+      const double D22 = _1oH * (LV(ix,iy+1,iz) - LV(ix,iy-1,iz));
+      const double D33 = _1oH * (LW(ix,iy,iz+1) - LW(ix,iy,iz-1));
+      const double D12 = .5 * _1oH * (LU(ix,iy+1,iz) - LU(ix,iy-1,iz) + LV(ix+1,iy,iz) - LV(ix-1,iy,iz));
+      const double D13 = .5 * _1oH * (LU(ix,iy,iz+1) - LU(ix,iy,iz-1) + LW(ix+1,iy,iz) - LW(ix-1,iy,iz));
+      const double D23 = .5 * _1oH * (LW(ix,iy+1,iz) - LW(ix,iy-1,iz) + LV(ix,iy,iz+1) - LV(ix,iy,iz-1));
+      const double P = S->p[D.idx(sp.gx, sp.gy, sp.gz)];
+      const double normX = sp.dchidx, normY = sp.dchidy, normZ = sp.dchidz;
+      const double fXV = D11 * normX + D12 * normY + D13 * normZ;
+      const double fYV = D12 * normX + D22 * normY + D23 * normZ;
+      const double fZV = D13 * normX + D23 * normY + D33 * normZ;
+      const double fXP = -P * normX, fYP = -P * normY, fZP = -P * normZ;
+      const double fXT = fXV + fXP, fYT = fYV + fYP, fZT = fZV + fZP;
+      const double vX = LU(ix,iy,iz), vY = LV(ix,iy,iz), vZ = LW(ix,iy,iz);
+      q[12] += normY * vZ - normZ * vY;
+      q[13] += normZ * vX - normX * vZ;
+      q[14] += normX * vY - normY * vX;
+      q[0] += fXT; q[1] += fYT; q[2] += fZT;
+      q[6] += fXV; q[7] += fYV; q[8] += fZV;
+      q[3] += fXP; q[4] += fYP; q[5] += fZP;
+      q[9] += (p[1] - CM[1]) * fZT - (p[2] - CM[2]) * fYT;
+      q[10] += (p[2] - CM[2]) * fXT - (p[0] - CM[0]) * fZT;
+      q[11] += (p[0] - CM[0]) * fYT - (p[1] - CM[1]) * fXT;
+      const double forcePar = fXT * velUnit[0] + fYT * velUnit[1] + fZT * velUnit[2];
+      q[16] += .5 * (forcePar + std::fabs(forcePar));
+      q[15] -= .5 * (forcePar - std::fabs(forcePar));
+      const double powOut = fXT * vX + fYT * vY + fZT * vZ;
+      const double powDef = 0;  // the sphere has no deformation velocity
+      q[17] += powOut; q[18] += std::min(0.0, powOut);
+      q[19] += powDef; q[20] += std::min(0.0, powDef);
+      const double rVec[3] = {p[0] - CM[0], p[1] - CM[1], p[2] - CM[2]};
+      const double uSolid[3] = {uTrans[0] + omega[1] * rVec[2] - rVec[1] * omega[2],
+                                uTrans[1] + omega[2] * rVec[0] - rVec[2] * omega[0],
+                                uTrans[2] + omega[0] * rVec[1] - rVec[0] * omega[1]};
+      q[21] += fXT * uSolid[0] + fYT * uSolid[1] + fZT * uSolid[2];
+    }
+    for (int k = 0; k < 22; ++k) sum[k] += q[k];
+  }
+  for (int k = 0; k < 22; ++k) out[k] = sum[k];
+  const double drag = sum[15], thrust = sum[16], defPower = sum[19], defPowerBnd = sum[20];
+  out[22] = thrust * vel_norm;
+  out[23] = drag * vel_norm;
+  out[24] = out[22] / (out[22] - std::min(defPower, 0.0) + EPS);
+  out[25] = out[22] / (out[22] - defPowerBnd + EPS);
+  double mass = 0;
+  const Real vol = h * h * h;
+  for (int b = 0; b < nb; ++b) {
+    if (!s.touched[b]) continue;
+    const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
+    double m = 0;
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) m += s.CHI[D.idx(bx * BS + ix, by * BS + iy, bz * BS + iz)] * vol;
+    mass += m;
+  }
+  out[26] = mass;
+}
+
 // Pipeline operators by reference name (source/Simulation.cpp:307-401).
 int orc_operator(void* hdl, const char* name, double dt) {
   OState* S = static_cast<OState*>(hdl);
@@ -832,6 +951,7 @@ int orc_operator(void* hdl, const char* name, double dt) {
   else if (n == "PressureProjection") op_pressure_projection(*S, dt);
   else if (n == "UpdateObstacles") op_update_obstacles(*S);
   else if (n == "Penalization") op_penalization(*S, dt);
+  else if (n == "ComputeForces") {}  // diagnostics only (orc_compute_forces): no state change
   else if (n == "ComputeDissipation") {}  // diagnostics only (orc_dissipation): no state change
   else return 1;
   return 0;

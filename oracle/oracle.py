@@ -75,6 +75,7 @@ def lib():
         L.orc_lab_shift.restype = C.c_int
         L.orc_diagnostics.argtypes = [C.c_void_p, dp]
         L.orc_dissipation.argtypes = [C.c_void_p, dp]
+        L.orc_compute_forces.argtypes = [C.c_void_p, dp]
         L.orc_tangent_run.argtypes = [C.c_void_p, C.c_int, dp, dp, dp, dp]
         L.orc_tangent_run.restype = C.c_int
         L.orc_num_threads.restype = C.c_int
@@ -181,6 +182,13 @@ class OracleSim:
         out = np.zeros(3, dtype=np.float64)
         lib().orc_diagnostics(self._h, _p(out))
         return {"ke": out[0], "div_l2": out[1], "div_max": out[2]}
+
+    def compute_forces(self) -> np.ndarray:
+        """ComputeForces' 22 sums, Pthrust, Pdrag, EffPDef, EffPDefBnd and the grid mass
+        (source/operators/FluidSolidForces.cpp:17-222, source/obstacles/Obstacle.cpp:266-295)."""
+        out = np.zeros(27, dtype=np.float64)
+        lib().orc_compute_forces(self._h, _p(out))
+        return out
 
     def dissipation(self) -> np.ndarray:
         """ComputeDissipation's 20 sums (source/operators/ComputeDissipation.cpp:119-160 order)."""

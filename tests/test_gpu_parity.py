@@ -199,7 +199,8 @@ def test_sphere_steps_vs_oracle(oracle):
         assert np.allclose(st.force, of, rtol=1e-10, atol=1e-12 * np.abs(of).max())
 
 
-def test_sphere_operator_by_operator_vs_oracle(oracle):
+def test_sphere_operator_by_operator_vs_oracle(oracle, tmp_path, monkeypatch):
+    monkeypatch.chdir(tmp_path)  # ComputeForces appends its forceValues / powerValues lines here
     sim, orc = sphere_pair(oracle, (32, 32, 32), 1.0, nu=1e-3)
     u, v, w = random_velocity((32, 32, 32), 9, 0.1)
     sim.set_velocity(u, v, w)
@@ -207,7 +208,7 @@ def test_sphere_operator_by_operator_vs_oracle(oracle):
     dt = 2e-3
     names = [op.getName() for op in sim.pipeline]
     assert names == ["CreateObstacles", "AdvectionDiffusion", "PressureRHS", "PressureProjection",
-                     "UpdateObstacles", "Penalization", "ComputeDissipation"]
+                     "UpdateObstacles", "Penalization", "ComputeForces", "ComputeDissipation"]
     for op in sim.pipeline:
         op(dt)
         orc.operator(op.getName(), dt)
@@ -217,6 +218,64 @@ def test_sphere_operator_by_operator_vs_oracle(oracle):
         assert rel_l2(a, b) < 1e-12
     ft = next(op for op in sim.pipeline if op.getName() == "Penalization").force_torque
     assert np.allclose(ft[:3], orc.stats()["force"], rtol=1e-10, atol=1e-14)
+    lines = open(tmp_path / "forceValues_surface_0.dat").read().splitlines()
+    assert lines[0].split("\t")[:5] == ["step", "time", "mass", "force_x", "force_y"] and len(lines) == 2
+    assert len(lines[1].split("\t")) == 20
+    assert len(open(tmp_path / "powerValues_surface_0.dat").read().splitlines()[1].split("\t")) == 11
+
+
+def check_surface_forces(sim, orc, tol):
+    from cubismup_3d_b200.simulation import FORCE_NAMES
+    got = sim.compute_forces()
+    ref = orc.compute_forces()
+    scale = np.abs(ref[:3]).max()
+    for k, name in enumerate(FORCE_NAMES):
+        s = scale if k < 22 else abs(ref[k])
+        if name.startswith("surfTorque") or name.startswith("gamma"):
+            s = max(s, np.abs(ref[9:15]).max())
+        if name in ("Pout", "PoutBnd", "pLocom", "Pthrust", "Pdrag"):
+            s = max(abs(ref[k]), scale)
+        assert abs(got[name] - ref[k]) <= tol * max(s, 1e-300), (name, got[name], ref[k])
+
+
+def test_sphere_surface_forces_vs_oracle(oracle):
+    # ComputeForces (FluidSolidForces.cpp:17-222): the surface points of the
+    # shifted SDF and the pressure and viscous stress on them, after steps of
+    # the fixed-frame sphere (flow from rest) and of one moving through the frame
+    for pair in (lambda: sphere_pair(oracle, (64, 32, 32), 2.0, nu=2 * 0.25 / 300),
+                 lambda: moving_sphere_pair(oracle, (64, 32, 32), 2.0, nu=2 * 0.25 / 300)):
+        sim, orc = pair()
+        z = np.zeros(orc.shape)
+        sim.set_velocity(z, z, z)
+        orc.set_velocity(z, z, z)
+        for s in range(4):
+            dt = orc.calc_max_timestep()
+            sim.timestep(dt)
+            orc.timestep(dt)
+        check_surface_forces(sim, orc, 1e-10)
+        f = sim.compute_forces()
+        # the flow pushes the sphere along its motion relative to the fluid:
+        # drag > 0 and the surface force points against the imposed velocity
+        assert f["drag"] > 0 and f["surfForce_x"] < 0
+        assert f["mass"] == pytest.approx(4 / 3 * np.pi * sim.obstacles[0].radius ** 3, rel=0.05)
+        sim.close()
+
+
+def test_sphere_surface_forces_fp32_dc_vs_oracle(oracle):
+    sim, orc = sphere_pair(oracle, (64, 32, 32), 2.0, nu=2 * 0.25 / 300)
+    sim.close()
+    import cubismup_3d_b200 as cup
+    sim = make_sim((64, 32, 32), 2.0, nu=2 * 0.25 / 300, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6,
+                   bImplicitPenalization=True, precision="fp32_dc", dc_max_iter=8)
+    sim.add_obstacle(cup.Sphere(**SPHERE))
+    z = np.zeros(orc.shape)
+    sim.set_velocity(z, z, z)
+    orc.set_velocity(z, z, z)
+    for s in range(4):
+        dt = orc.calc_max_timestep()
+        sim.timestep(dt)
+        orc.timestep(dt)
+    check_surface_forces(sim, orc, 1e-5)
 
 
 MOVING_SPHERE = dict(SPHERE, enforcedVelocity=(1.0, 0.2, 0.0), bFixFrameOfRef=(False, False, False))
