@@ -129,6 +129,14 @@ class GridMPI : public TGrid {
  public:
   typedef typename TGrid::BlockType BlockType;
   using TGrid::TGrid;
+  GridMPI() = default;
+  // (processes per dimension, blocks per process and dimension, the longest
+  // side): one process, so the grid is the processes' blocks, with
+  // h = maxextent / (cells along the longest dimension)
+  GridMPI(int npx, int npy, int npz, int bx, int by, int bz, double maxextent, MPI_Comm) {
+    const int mx = std::max({bx * npx, by * npy, bz * npz});
+    this->setup(bx * npx, by * npy, bz * npz, maxextent / (mx * TGrid::BlockType::sizeX));
+  }
   SynchronizerMPI<double> synch;
   MPI_Comm getCartComm() const { return MPI_COMM_WORLD; }
   MPI_Comm getWorldComm() const { return MPI_COMM_WORLD; }

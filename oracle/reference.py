@@ -1,0 +1,99 @@
+"""ORACLE CHECKER — test infrastructure only.
+
+ctypes binding of ``oracle/_ref/libref.so``: the reference's own operator
+sources (source/operators/AdvectionDiffusion.cpp, PressureRHS.cpp,
+PressureProjection.cpp, source/poisson/PoissonSolverPeriodic.cpp,
+PoissonSolver.cpp) compiled unmodified against the stand-ins in
+``oracle/ref_shim`` (``make -C oracle ref``; needs the reference tree, which
+only the build machine has). It runs the reference's operator() objects on a
+one-process grid of FluidBlocks, so the oracle's restatement can be checked
+against the reference's arithmetic. The FFT inside PoissonSolverPeriodic is
+the stand-in's direct DFT (FFTW is not in the reference snapshot); everything
+else on the path is the reference's code. Only tests import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libref.so")
+REFERENCE_SOURCE = os.environ.get("CUP_REFERENCE_SOURCE", "/root/reference/source")
+FIELDS = {"u": 0, "v": 1, "w": 2, "p": 3, "chi": 4, "tmpU": 5, "tmpV": 6, "tmpW": 7}
+_lib = None
+
+
+def available() -> bool:
+    """The library is built, or can be (the reference tree is present)."""
+    return os.path.exists(LIB_PATH) or os.path.isdir(REFERENCE_SOURCE)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REFERENCE={REFERENCE_SOURCE}"], check=True)
+        L = C.CDLL(LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        L.ref_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, dp]
+        L.ref_create.restype = C.c_void_p
+        L.ref_destroy.argtypes = [C.c_void_p]
+        L.ref_set_field.argtypes = [C.c_void_p, C.c_int, dp]
+        L.ref_get_field.argtypes = [C.c_void_p, C.c_int, dp]
+        L.ref_get_rhs.argtypes = [C.c_void_p, dp]
+        L.ref_operator.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
+        L.ref_operator.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class ReferenceSim:
+    """The reference's periodic pipeline objects (SimulationData, FluidGridMPI,
+    AdvectionDiffusion, PressureRHS, PressureProjection) on an nx x ny x nz grid."""
+
+    def __init__(self, nx, ny, nz, maxextent, nu, uinf=(0.0, 0.0, 0.0)):
+        ui = np.ascontiguousarray(uinf, dtype=np.float64)
+        self.shape = (nz, ny, nx)
+        self._h = lib().ref_create(nx, ny, nz, maxextent, nu, _p(ui))
+        if not self._h:
+            raise RuntimeError("reference: construction failed (see stderr)")
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().ref_destroy(self._h)
+            self._h = None
+
+    def set(self, name: str, f):
+        a = np.ascontiguousarray(f, dtype=np.float64)
+        assert a.shape == self.shape
+        lib().ref_set_field(self._h, FIELDS[name], _p(a))
+
+    def get(self, name: str) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        lib().ref_get_field(self._h, FIELDS[name], _p(out))
+        return out
+
+    def set_velocity(self, u, v, w):
+        for n, f in zip("uvw", (u, v, w)):
+            self.set(n, f)
+
+    def velocity(self):
+        return self.get("u"), self.get("v"), self.get("w")
+
+    def rhs(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=np.float64)
+        lib().ref_get_rhs(self._h, _p(out))
+        return out
+
+    def operator(self, name: str, dt: float):
+        rc = lib().ref_operator(self._h, name.encode(), dt)
+        if rc:
+            raise RuntimeError(f"reference operator {name} failed ({rc})")

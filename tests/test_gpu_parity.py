@@ -674,3 +674,31 @@ def test_poisson_buffer_contract_vs_oracle(oracle, precision, tol):
     ps.solve()
     ps._fftw2cub()
     assert rel_l2(sim.pressure(), oracle.poisson_solve(rhs, sim.h)) < tol
+
+
+def test_gpu_operators_vs_reference_code():
+    # The FP64 operators (reference scheme) against the reference's own
+    # operator sources (oracle/_ref/libref.so, built where the reference tree
+    # is present and carried with the repository) on the same inputs
+    import os
+
+    from oracle import reference as R
+    if not os.path.exists(R.LIB_PATH):
+        pytest.skip("the reference's sources were not built (oracle/_ref/libref.so is absent)")
+    cells, uinf = (64, 32, 32), (0.3, -0.2, 0.1)
+    sim = make_sim(cells, 2 * np.pi, nu=0.01, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0, uinf=uinf)
+    ref = R.ReferenceSim(*cells, 2 * np.pi, 0.01, uinf)
+    u, v, w = random_velocity(cells, 41, 0.5)
+    sim.set_velocity(u, v, w)
+    ref.set_velocity(u, v, w)
+    ops = {op.getName(): op for op in sim.pipeline}
+    dt = 1e-3
+    for name in ("AdvectionDiffusion", "PressureRHS", "PressureProjection"):
+        ops[name](dt)
+        ref.operator(name, dt)
+        if name == "PressureRHS":
+            assert rel_l2(sim.rhs(), ref.rhs()) < 1e-14
+        else:
+            for a, b in zip(sim.velocity(), ref.velocity()):
+                assert rel_l2(a, b) < 1e-14
+    assert rel_l2(sim.pressure(), ref.get("p")) < 1e-12

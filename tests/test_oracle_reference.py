@@ -1,0 +1,61 @@
+"""The oracle against the reference's own code (CPU): the reference's operator
+sources compiled unmodified against oracle/ref_shim (oracle/_ref/libref.so,
+built by ``make -C oracle ref`` where the reference tree is present) run on a
+one-process grid of FluidBlocks beside the oracle on the same inputs.
+
+AdvectionDiffusion (KernelAdvectDiffuse + the tmp -> u copy) and PressureRHS
+(KernelPressureRHS) match bitwise. PressureProjection (PoissonSolverPeriodic:
+_cub2fftw, r2c, _solve, c2r, _fftw2cub; KernelGradP) matches to rounding: its
+FFT is the stand-in's direct DFT, not FFTW or the oracle's radix-2 FFT.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+
+ref_mod = pytest.importorskip("oracle.reference")
+pytestmark = pytest.mark.skipif(not ref_mod.available(), reason="reference tree and its build are absent")
+
+
+def pair(oracle, cells, extent, nu, uinf):
+    nx, ny, nz = cells
+    orc = oracle.OracleSim(nx, ny, nz, extent, nu=nu, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0, uinf=uinf)
+    ref = ref_mod.ReferenceSim(nx, ny, nz, extent, nu, uinf)
+    return orc, ref
+
+
+@pytest.mark.parametrize("cells,uinf", [((32, 32, 32), (0.3, -0.2, 0.1)), ((64, 32, 16), (0.0, 0.0, 0.0))])
+def test_advection_and_rhs_bitwise_vs_reference(oracle, cells, uinf):
+    nx, ny, nz = cells
+    orc, ref = pair(oracle, cells, 2 * np.pi, 0.01, uinf)
+    rng = np.random.default_rng(3)
+    u, v, w = (0.5 * rng.standard_normal((nz, ny, nx)) for _ in range(3))
+    orc.set_velocity(u, v, w)
+    ref.set_velocity(u, v, w)
+    dt = 1e-3
+    orc.operator("AdvectionDiffusion", dt)
+    ref.operator("AdvectionDiffusion", dt)
+    for a, b in zip(orc.velocity(), ref.velocity()):
+        assert np.array_equal(a, b)
+    orc.operator("PressureRHS", dt)
+    ref.operator("PressureRHS", dt)
+    assert np.array_equal(orc.get("rhs"), ref.rhs())
+
+
+def test_projection_and_steps_vs_reference(oracle):
+    from cubismup_3d_b200 import initial_conditions as ic
+    cells = (32, 32, 32)
+    orc, ref = pair(oracle, cells, 2 * np.pi, 0.01, (0.0, 0.0, 0.0))
+    u, v, w = ic.taylor_green(cells, 2 * np.pi / 32)
+    rng = np.random.default_rng(5)
+    u, v, w = (a + 0.05 * rng.standard_normal(a.shape) for a in (u, v, w))
+    orc.set_velocity(u, v, w)
+    ref.set_velocity(u, v, w)
+    for step in range(3):
+        dt = orc.calc_max_timestep()
+        for name in ("AdvectionDiffusion", "PressureRHS", "PressureProjection"):
+            orc.operator(name, dt)
+            ref.operator(name, dt)
+        assert rel_l2(orc.get("p"), ref.get("p")) < 1e-13
+        for a, b in zip(orc.velocity(), ref.velocity()):
+            assert rel_l2(a, b) < 1e-14
