@@ -328,7 +328,7 @@ def sphere_leg(torch, cup, stream, args, local_rank: int, barrier) -> dict:
         z = np.zeros(s.shape)
         s.set_velocity(z, z, z)
         st0 = s.run_steps(n_warm)
-        s.prepare_run()
+        s.prepare_run(n_steps)
         ms, st = timed_run(torch, s, stream, n_steps, barrier)
         res[prec] = {"ms_per_step": ms / n_steps, "cell_steps_per_s": float(np.prod(SPHERE_CELLS)) * n_steps / (ms * 1e-3),
                      "drag": float(st.force[0]), "diagnostics": s.diagnostics(), "time": st.time}
@@ -395,7 +395,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     st_w = None
     for _ in range(args.warmup):
         st_w = sim.run_steps(1)
-    graph_ready = sim.prepare_run()
+    graph_ready = sim.prepare_run(args.steps)
     sim.sync()
 
     # ---- device-timed region: K steps chained on the device ----
@@ -458,7 +458,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         s64.set_velocity(*[p.numpy() for p in pinned])
         for _ in range(args.warmup):
             s64.run_steps(1)
-        s64.prepare_run()
+        s64.prepare_run(args.steps)
         ms64, st64 = timed_run(torch, s64, stream, args.steps, barrier)
         ms64 = max_over_ranks(torch, world, dev, ms64)
         v64 = world * n ** 3 * args.steps / (ms64 * 1e-3)
@@ -512,7 +512,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                 "note": "one FP64 velocity upload and download per run (3 x %d MB each way) and per step the dt "
                         "and the step stats read back; the transfers weigh less in longer runs"
                         % (n ** 3 * 8 // 2 ** 20)},
-        "graph_captured_before_timing": graph_ready,
+        "graphs_captured_before_timing": graph_ready,
         "gpu_launches": launches,
         "clocks": clk,
         "final_state": {"time": st.time, "kinetic_energy": st.kinetic_energy, "umax": st.umax},

@@ -95,7 +95,7 @@ SIGNATURES = {
     "cup_add_sphere": (C.c_int, [_H, C.POINTER(CupSphere)]),
     "cup_create_obstacles": (C.c_int, [_H, C.c_double]),
     "cup_set_graphs": (C.c_int, [_H, C.c_int]),
-    "cup_prepare_run": (C.c_int, [_H, C.POINTER(C.c_int)]),
+    "cup_prepare_run": (C.c_int, [_H, C.c_int, C.POINTER(C.c_int)]),
     "cup_set_sphere_position": (C.c_int, [_H, _dp]),
     "cup_get_sphere_position": (C.c_int, [_H, _dp]),
     "cup_set_uinf": (C.c_int, [_H, _dp]),

@@ -989,15 +989,13 @@ int launch_rows_pipe(cup_handle* H, const char* name, const R* in, R* out, const
   return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
 }
 
-template <int M, typename R, int AXIS, bool DIVIDE, typename RIN = R, bool T8X = true>
+template <int M, typename R, int AXIS, bool DIVIDE, typename RIN = R>
 int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   // W x-columns per tile (FP32: 128-B rows of a tile, FP64: 128 B), NB = 3 tile buffers
-  // 256-long FP32 lines: the 8-thread plan (radix 16, then radix 8 fused with the
-  // split); measured slower than the 16-thread plan for FP64 tiles (fewer CTAs fit)
-  if constexpr (M == 128 && sizeof(RIN) < sizeof(R) && T8X) {
-    if (getenv("CUP_ZMIX16")) return launch_cols_M<M, R, AXIS, DIVIDE, RIN, false>(H, in, out, skip);
-  }
-  constexpr bool T8 = M == 128 && T8X;
+  // 256-long lines: the 8-thread plan (radix 16, then radix 8 fused with the
+  // split), also for the mixed-precision z pass (the 16-thread plan measured
+  // 89 against 75 us there at 256^3)
+  constexpr bool T8 = M == 128;
   constexpr int N = 2 * M, TPL = T8 ? 8 : M / 8, NB = T8 ? 2 : 3;
   constexpr int W = sizeof(R) == 4 ? 32 : 16;
   if (H->nx % W) return fail(H, CUP_ERR_ARG, "nx must be a multiple of %d for this precision", W);
@@ -2106,7 +2104,7 @@ int capture_graph(cup_handle* H, int nsteps, int next_dt, cup_handle::StepGraph*
       *out = &g;
       return CUP_OK;
     }
-  if (H->graphs.size() >= 16) drop_graph(H);
+  if (H->graphs.size() >= 32) drop_graph(H);
   const long long l0 = H->launches;
   if (cudaStreamBeginCapture(H->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
     cudaGetLastError();
@@ -2124,6 +2122,7 @@ int capture_graph(cup_handle* H, int nsteps, int next_dt, cup_handle::StepGraph*
   const long long nl = H->launches - l0;
   H->launches = l0;
   if (rc == CUP_OK && e == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess) {
+    cudaGraphUpload(ex, H->stream);  // the first replay then starts at once
     H->graphs.push_back({in, after, nsteps, next_dt, g, ex, nl});
     *out = &H->graphs.back();
     return CUP_OK;
@@ -2498,15 +2497,28 @@ int cup_set_graphs(cup_handle* H, int on) {
   return CUP_OK;
 }
 
-int cup_prepare_run(cup_handle* H, int* captured) {
+int cup_prepare_run(cup_handle* H, int nsteps, int* captured) {
   REQUIRE_H(H);
   if (captured) *captured = 0;
+  if (nsteps < 0) return fail(H, CUP_ERR_ARG, "nsteps must be >= 0");
   if (!graph_ok(H)) return CUP_OK;
-  cup_handle::StepGraph* g = nullptr;
-  const int rc = capture_graph(H, kGraphSteps, 1, &g);
-  if (rc) return rc;
-  if (captured) *captured = g ? 1 : 0;
-  return CUP_OK;
+  // walk the graphs cup_run(nsteps) would replay from here, capturing the
+  // missing ones; the host state is put back afterwards
+  const cup_handle::StepState start = step_state(H);
+  int n = 0, rc = CUP_OK;
+  for (int i = 0; i < nsteps && rc == CUP_OK;) {
+    const bool whole = nsteps - i > kGraphSteps;
+    cup_handle::StepGraph* g = nullptr;
+    rc = capture_graph(H, whole ? kGraphSteps : 1, whole || i + 1 < nsteps ? 1 : 0, &g);
+    if (rc || !g) break;
+    set_step_state(H, g->out);
+    ++n;
+    i += whole ? kGraphSteps : 1;
+    if (whole && nsteps - i > kGraphSteps) i += (nsteps - i - 1) / kGraphSteps * kGraphSteps;  // same state again
+  }
+  set_step_state(H, start);
+  if (captured) *captured = n;
+  return rc;
 }
 
 int cup_create_obstacles(cup_handle* H, double dt) {
@@ -2871,13 +2883,15 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
       });
       if (rc_) return rc_;
     }
-    // steady state: whole graphs of steps, keeping the last step (which does
-    // not compute a next dt) out of them
-    if (nsteps - i > kGraphSteps && graph_ok(H)) {
+    // steady state: whole graphs of kGraphSteps steps, each computing the
+    // next step's dt; the steps of the run's tail from one-step graphs (the
+    // last one computes no next dt)
+    if (graph_ok(H)) {
+      const bool whole = nsteps - i > kGraphSteps;
       bool ran = false;
-      if ((rc = run_graph(H, kGraphSteps, 1, &ran))) return rc;
+      if ((rc = run_graph(H, whole ? kGraphSteps : 1, whole || i + 1 < nsteps ? 1 : 0, &ran))) return rc;
       if (ran) {
-        i += kGraphSteps;
+        i += whole ? kGraphSteps : 1;
         continue;
       }
     }

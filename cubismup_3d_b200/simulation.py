@@ -630,12 +630,12 @@ class Simulation:
         """run_steps replays its steady-state steps as a captured CUDA graph (default on)."""
         L.check(L.lib().cup_set_graphs(self._h, int(bool(on))), self._h, "use_graphs")
 
-    def prepare_run(self) -> bool:
-        """Captures (without running) the CUDA graph that run_steps replays from
-        the current state; True when it is cached (see cup_prepare_run)."""
+    def prepare_run(self, nsteps: int) -> int:
+        """Captures (without running) the CUDA graphs that run_steps(nsteps)
+        replays from the current state; returns how many (cup_prepare_run)."""
         c = C.c_int()
-        L.check(L.lib().cup_prepare_run(self._h, C.byref(c)), self._h, "prepare_run")
-        return bool(c.value)
+        L.check(L.lib().cup_prepare_run(self._h, int(nsteps), C.byref(c)), self._h, "prepare_run")
+        return c.value
 
     def run_steps(self, nsteps: int) -> StepStats:
         """nsteps of calcMaxTimestep + timestep with dt chained on the device."""

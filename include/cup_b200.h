@@ -195,16 +195,19 @@ int cup_step(struct cup_handle* h, double dt, cup_step_stats* stats);
 /* Simulation::run (source/Simulation.cpp:582-591) for nsteps: calcMaxTimestep + timestep,
  * with dt computed on the device (no host round trip per step). */
 int cup_run(struct cup_handle* h, int nsteps, cup_step_stats* stats);
-/* cup_run replays its steady-state steps as a CUDA graph of 6 steps (captured
- * on first use; same kernels, same results); off: every step is launched. */
+/* cup_run replays its steady-state steps from CUDA graphs of 6 steps and its
+ * tail from one-step graphs (captured on first use; same kernels, same
+ * results); off: every step is launched. */
 int cup_set_graphs(struct cup_handle* h, int on);
-/* Captures, without running anything, the 6-step graph that cup_run replays
- * from the handle's current state, so that the capture and instantiation cost
- * of a later cup_run from this state is paid here (no counterpart in the
- * reference). *captured (may be NULL) = 1 when the graph is cached; 0 when the
- * state cannot replay graphs yet (the FP32-DC warm start is not ready, a moving
- * obstacle, spectral forcing, profiling on, graphs off). Nothing is launched. */
-int cup_prepare_run(struct cup_handle* h, int* captured);
+/* Captures, without running anything, the CUDA graphs that cup_run(nsteps)
+ * replays from the handle's current state (6-step graphs, then one-step graphs
+ * for the run's tail), so that their capture, instantiation and upload are
+ * paid here rather than in the run (no counterpart in the reference).
+ * *captured (may be NULL) = the number of graphs the run will replay, all
+ * cached now; 0 when the state cannot replay graphs yet (the FP32-DC warm
+ * start is not ready, a moving obstacle, spectral forcing, profiling on,
+ * graphs off). Nothing is launched on the stream. */
+int cup_prepare_run(struct cup_handle* h, int nsteps, int* captured);
 
 /* Discrete adjoint of one cup_step with the given dt (no counterpart in the
  * reference, which has no adjoint). un, vn, wn: the velocity at the start of the

@@ -15,7 +15,13 @@
 #include <cassert>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
+#include <functional>
+#include <map>
 #include <memory>
+#include <new>
+#include <set>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -80,6 +86,7 @@ class Grid {
  public:
   typedef TBlock BlockType;
   typedef typename TBlock::ElementType ElementType;
+  static constexpr size_t kAlign = 64;  // CUBISM_ALIGNMENT: blocks hold 32-byte aligned members
   std::vector<TBlock*> blocks;
   std::vector<BlockInfo> infos;
   int bpd[3] = {1, 1, 1};
@@ -87,7 +94,7 @@ class Grid {
   Grid() = default;
   Grid(int bx, int by, int bz, double hh) { setup(bx, by, bz, hh); }
   ~Grid() {
-    for (TBlock* b : blocks) ::operator delete(static_cast<void*>(b));
+    for (TBlock* b : blocks) ::operator delete(static_cast<void*>(b), std::align_val_t(kAlign));
   }
   void setup(int bx, int by, int bz, double hh) {
     bpd[0] = bx, bpd[1] = by, bpd[2] = bz, h = hh;
@@ -95,7 +102,7 @@ class Grid {
     blocks.resize(nb);
     infos.resize(nb);
     for (int i = 0; i < nb; ++i) {
-      void* mem = ::operator new(sizeof(TBlock));
+      void* mem = ::operator new(sizeof(TBlock), std::align_val_t(kAlign));
       std::memset(mem, 0, sizeof(TBlock));
       blocks[i] = static_cast<TBlock*>(mem);
       BlockInfo& I = infos[i];

@@ -38,7 +38,7 @@ def lib():
             subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REFERENCE={REFERENCE_SOURCE}"], check=True)
         L = C.CDLL(LIB_PATH)
         dp = C.POINTER(C.c_double)
-        L.ref_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, dp]
+        L.ref_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, dp, C.c_double, C.c_int]
         L.ref_create.restype = C.c_void_p
         L.ref_destroy.argtypes = [C.c_void_p]
         L.ref_set_field.argtypes = [C.c_void_p, C.c_int, dp]
@@ -46,6 +46,12 @@ def lib():
         L.ref_get_rhs.argtypes = [C.c_void_p, dp]
         L.ref_operator.argtypes = [C.c_void_p, C.c_char_p, C.c_double]
         L.ref_operator.restype = C.c_int
+        ip = C.POINTER(C.c_int)
+        L.ref_add_sphere.argtypes = [C.c_void_p, C.c_double, dp, dp, ip, ip]
+        L.ref_add_sphere.restype = C.c_int
+        L.ref_obstacle.argtypes = [C.c_void_p, dp]
+        L.ref_obstacle.restype = C.c_int
+        L.ref_set_clock.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
         _lib = L
     return _lib
 
@@ -57,12 +63,18 @@ def _p(a: np.ndarray):
 
 class ReferenceSim:
     """The reference's periodic pipeline objects (SimulationData, FluidGridMPI,
-    AdvectionDiffusion, PressureRHS, PressureProjection) on an nx x ny x nz grid."""
+    ObstacleVector, CreateObstacles, AdvectionDiffusion, PressureRHS,
+    PressureProjection, UpdateObstacles, Penalization, ComputeForces) on an
+    nx x ny x nz grid."""
 
-    def __init__(self, nx, ny, nz, maxextent, nu, uinf=(0.0, 0.0, 0.0)):
+    PIPELINE = ("CreateObstacles", "AdvectionDiffusion", "PressureRHS", "PressureProjection", "UpdateObstacles",
+                "Penalization", "ComputeForces")
+
+    def __init__(self, nx, ny, nz, maxextent, nu, uinf=(0.0, 0.0, 0.0), lambda_=1e6, implicit=True):
         ui = np.ascontiguousarray(uinf, dtype=np.float64)
         self.shape = (nz, ny, nx)
-        self._h = lib().ref_create(nx, ny, nz, maxextent, nu, _p(ui))
+        self.step, self.time = 0, 0.0
+        self._h = lib().ref_create(nx, ny, nz, maxextent, nu, _p(ui), lambda_, int(bool(implicit)))
         if not self._h:
             raise RuntimeError("reference: construction failed (see stderr)")
 
@@ -92,6 +104,30 @@ class ReferenceSim:
         out = np.empty(self.shape, dtype=np.float64)
         lib().ref_get_rhs(self._h, _p(out))
         return out
+
+    def add_sphere(self, radius, position, velocity, forced=(1, 1, 1), fix_frame=(0, 0, 0)):
+        pos = np.ascontiguousarray(position, dtype=np.float64)
+        vel = np.ascontiguousarray(velocity, dtype=np.float64)
+        f = (C.c_int * 3)(*[int(bool(x)) for x in forced])
+        ff = (C.c_int * 3)(*[int(bool(x)) for x in fix_frame])
+        if lib().ref_add_sphere(self._h, radius, _p(pos), _p(vel), f, ff):
+            raise RuntimeError("reference: adding the sphere failed (see stderr)")
+
+    def obstacle(self) -> dict:
+        out = np.zeros(48, dtype=np.float64)
+        if lib().ref_obstacle(self._h, _p(out)):
+            raise RuntimeError("reference: no obstacle")
+        return {"force": out[0:3], "torque": out[3:6], "com": out[6:9], "transVel": out[9:12],
+                "angVel": out[12:15], "position": out[15:18], "uinf": out[18:21], "mass": out[21],
+                "forces": out[22:48]}
+
+    def timestep(self, dt: float):
+        """Simulation::timestep (source/Simulation.cpp:593-623) over the pipeline."""
+        lib().ref_set_clock(self._h, self.step, self.time, dt)
+        for name in self.PIPELINE:
+            self.operator(name, dt)
+        self.step += 1
+        self.time += dt
 
     def operator(self, name: str, dt: float):
         rc = lib().ref_operator(self._h, name.encode(), dt)

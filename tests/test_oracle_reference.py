@@ -59,3 +59,37 @@ def test_projection_and_steps_vs_reference(oracle):
         assert rel_l2(orc.get("p"), ref.get("p")) < 1e-13
         for a, b in zip(orc.velocity(), ref.velocity()):
             assert rel_l2(a, b) < 1e-14
+
+
+@pytest.mark.parametrize("fix_frame", [(1, 1, 1), (0, 0, 0)])
+def test_sphere_pipeline_vs_reference(oracle, fix_frame):
+    # The whole pipeline with a forced sphere, in a frame fixed to it or moving
+    # through the frame: the reference's own Sphere, ObstacleVector,
+    # CreateObstacles (SDF, chi, centre of mass, surface points), UpdateObstacles,
+    # Penalization and ComputeForces against the oracle's restatements.
+    cells, L, nu = (64, 32, 32), 2.0, 2 * 0.25 / 300
+    nx, ny, nz = cells
+    orc = oracle.OracleSim(nx, ny, nz, L, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6, implicit_penalization=True,
+                           scheme="ref", sphere={"radius": 0.25, "position": (0.5, 0.5, 0.5),
+                                                 "velocity": (1.0, 0.0, 0.0), "forced": (1, 1, 1),
+                                                 "fix_frame": fix_frame})
+    ref = ref_mod.ReferenceSim(nx, ny, nz, L, nu, (0.0, 0.0, 0.0), 1e6, True)
+    ref.add_sphere(0.25, (0.5, 0.5, 0.5), (1.0, 0.0, 0.0), (1, 1, 1), fix_frame)
+    z = np.zeros(orc.shape)
+    orc.set_velocity(z, z, z)
+    ref.set_velocity(z, z, z)
+    assert np.array_equal(orc.get("chi"), ref.get("chi"))
+    for step in range(3):
+        dt = orc.calc_max_timestep()
+        orc.timestep(dt)
+        ref.timestep(dt)
+        ob, st = ref.obstacle(), orc.stats()
+        assert np.array_equal(orc.get("chi"), ref.get("chi"))
+        assert np.allclose(st["com"], ob["com"], rtol=0, atol=1e-15)
+        assert np.allclose(st["uinf"], ob["uinf"], rtol=0, atol=0)
+        assert np.allclose(st["force"], ob["force"], rtol=1e-12, atol=1e-12 * abs(ob["force"][0]))
+        for a, b in zip(orc.velocity(), ref.velocity()):
+            assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(np.stack(ref.velocity()))
+    f, rf = orc.compute_forces(), ob["forces"]
+    assert np.abs(f[:26] - rf).max() <= 1e-13 * np.abs(rf[:3]).max()
+    assert f[26] == pytest.approx(ob["mass"], rel=1e-14)
