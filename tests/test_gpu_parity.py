@@ -702,3 +702,37 @@ def test_gpu_operators_vs_reference_code():
             for a, b in zip(sim.velocity(), ref.velocity()):
                 assert rel_l2(a, b) < 1e-14
     assert rel_l2(sim.pressure(), ref.get("p")) < 1e-12
+
+
+@pytest.mark.parametrize("fix_frame", [(True, True, True), (False, False, False)])
+def test_gpu_sphere_steps_vs_reference_code(fix_frame):
+    # The FP64 sphere step against the reference's own obstacle pipeline
+    # (Sphere, CreateObstacles, Penalization, ComputeForces sources in
+    # oracle/_ref/libref.so): chi, velocity, penalization and surface forces
+    import os
+
+    import cubismup_3d_b200 as cup
+    from cubismup_3d_b200.simulation import FORCE_NAMES
+    from oracle import reference as R
+    if not os.path.exists(R.LIB_PATH):
+        pytest.skip("the reference's sources were not built (oracle/_ref/libref.so is absent)")
+    cells, L, nu = (64, 32, 32), 2.0, 2 * 0.25 / 300
+    sim = make_sim(cells, L, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6, bImplicitPenalization=True)
+    sim.add_obstacle(cup.Sphere(**dict(SPHERE, bFixFrameOfRef=fix_frame)))
+    ref = R.ReferenceSim(*cells, L, nu, (0.0, 0.0, 0.0), 1e6, True)
+    ref.add_sphere(SPHERE["radius"], SPHERE["position"], SPHERE["enforcedVelocity"], (1, 1, 1), fix_frame)
+    z = np.zeros(sim.shape)
+    sim.set_velocity(z, z, z)
+    ref.set_velocity(z, z, z)
+    assert np.max(np.abs(sim.chi() - ref.get("chi"))) < 1e-14
+    for s in range(3):
+        dt = sim.calcMaxTimestep()
+        st = sim.timestep(dt)
+        ref.timestep(dt)
+        for a, b in zip(sim.velocity(), ref.velocity()):
+            assert np.linalg.norm(a - b) <= 1e-12 * np.linalg.norm(np.stack(ref.velocity()))
+        ob = ref.obstacle()
+        assert np.allclose(st.force, ob["force"], rtol=1e-10, atol=1e-12 * abs(ob["force"][0]))
+    f = sim.compute_forces()
+    got = np.array([f[k] for k in FORCE_NAMES[:26]])
+    assert np.abs(got - ob["forces"]).max() <= 1e-10 * np.abs(ob["forces"][:3]).max()
