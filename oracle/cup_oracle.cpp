@@ -254,6 +254,14 @@ struct Sphere {
   bool bFixFrameOfRef[3] = {false, false, false};
   double lambda_factor = 1.0;        // source/obstacles/Obstacle.h:106
   double force[3] = {0, 0, 0}, torque[3] = {0, 0, 0};
+  // rigid-body state of source/obstacles/Obstacle.h:94-130 for free dofs
+  double transVel_imposed[3] = {0, 0, 0};
+  bool bBlockRotation[3] = {false, false, false};
+  double quaternion[4] = {1, 0, 0, 0};
+  double mass = 0, J[6] = {0, 0, 0, 0, 0, 0};
+  double transVel_computed[3] = {0, 0, 0}, angVel_computed[3] = {0, 0, 0};
+  double penalM = 0, penalCM[3] = {0, 0, 0}, penalJ[6] = {0, 0, 0, 0, 0, 0};
+  double penalLmom[3] = {0, 0, 0}, penalAmom[3] = {0, 0, 0};
   std::vector<char> touched;         // obstacle block present (ObstacleBlock* != nullptr)
   std::vector<Real> SDF, CHI;        // per cell, meaningful on touched blocks
   // surface points of ObstacleBlock::write (source/ObstacleBlock.h:157-166), in
@@ -446,6 +454,20 @@ void op_create_obstacles(OState& S) {
   // position advection (source/obstacles/Obstacle.cpp:314-321).
   for (int d = 0; d < 3; ++d) S.uinf[d] = s.bFixFrameOfRef[d] ? -s.transVel[d] : 0.0;
   for (int d = 0; d < 3; ++d) s.position[d] += S.dt * (s.transVel[d] + S.uinf[d]);
+  {  // orientation (source/obstacles/Obstacle.cpp:323-346; the sphere's shape does not depend on it)
+    const double* w = s.angVel;
+    const double* Q = s.quaternion;
+    const double dqdt[4] = {.5 * (-w[0] * Q[1] - w[1] * Q[2] - w[2] * Q[3]), .5 * (+w[0] * Q[0] + w[1] * Q[3] - w[2] * Q[2]),
+                            .5 * (-w[0] * Q[3] + w[1] * Q[0] + w[2] * Q[1]), .5 * (+w[0] * Q[2] - w[1] * Q[1] + w[2] * Q[0])};
+    const double DQ[4] = {dqdt[0] * S.dt, dqdt[1] * S.dt, dqdt[2] * S.dt, dqdt[3] * S.dt};
+    const double DQn = std::sqrt(DQ[0] * DQ[0] + DQ[1] * DQ[1] + DQ[2] * DQ[2] + DQ[3] * DQ[3]);
+    if (DQn > std::numeric_limits<double>::epsilon()) {
+      const double tanF = std::tan(DQn) / DQn;
+      const double Dq[4] = {Q[0] + tanF * DQ[0], Q[1] + tanF * DQ[1], Q[2] + tanF * DQ[2], Q[3] + tanF * DQ[3]};
+      const double invD = 1 / std::sqrt(Dq[0] * Dq[0] + Dq[1] * Dq[1] + Dq[2] * Dq[2] + Dq[3] * Dq[3]);
+      for (int k = 0; k < 4; ++k) s.quaternion[k] = Dq[k] * invD;
+    }
+  }
   const Real safety = (2 + SURFDH) * h;
   const Real box[3][2] = {
     {(Real)s.position[0] - (s.radius + safety), (Real)s.position[0] + (s.radius + safety)},
@@ -638,11 +660,142 @@ void op_pressure_projection(OState& S, double dt) {
   });
 }
 
-// UpdateObstacles for a sphere with every translational dof forced: all rotation
-// blocked (source/obstacles/Obstacle.cpp:131-137), translational velocity kept
-// at the imposed value and angular velocity zero (:153-264). Free dofs are out
-// of scope for this oracle.
-void op_update_obstacles(OState&) {}
+// Dense solve A x = b by LU with partial pivoting (the GSL LU routines that
+// Obstacle::computeVelocities calls, source/obstacles/Obstacle.cpp:200-207).
+void lu_solve6(double A[6][6], double b[6], double x[6]) {
+  int perm[6] = {0, 1, 2, 3, 4, 5};
+  for (int j = 0; j < 5; ++j) {
+    int piv = j;
+    double mx = std::fabs(A[j][j]);
+    for (int i = j + 1; i < 6; ++i)
+      if (std::fabs(A[i][j]) > mx) mx = std::fabs(A[i][j]), piv = i;
+    if (piv != j) {
+      for (int k = 0; k < 6; ++k) std::swap(A[j][k], A[piv][k]);
+      std::swap(perm[j], perm[piv]);
+    }
+    if (A[j][j] == 0) continue;
+    for (int i = j + 1; i < 6; ++i) {
+      const double l = A[i][j] / A[j][j];
+      A[i][j] = l;
+      for (int k = j + 1; k < 6; ++k) A[i][k] -= l * A[j][k];
+    }
+  }
+  double y[6];
+  for (int i = 0; i < 6; ++i) y[i] = b[perm[i]];
+  for (int i = 0; i < 6; ++i)
+    for (int k = 0; k < i; ++k) y[i] -= A[i][k] * y[k];
+  for (int i = 5; i >= 0; --i) {
+    for (int k = i + 1; k < 6; ++k) y[i] -= A[i][k] * y[k];
+    y[i] /= A[i][i];
+  }
+  for (int i = 0; i < 6; ++i) x[i] = y[i];
+}
+
+// UpdateObstacles (source/operators/ObstaclesUpdate.cpp:202-236):
+// KernelIntegrateFluidMomenta (:24-134) over the obstacle blocks (cells with
+// chi > 0, moments about the centre of mass; the sphere has no deformation
+// velocity), KernelFinalizeObstacleVel (:136-200) and
+// Obstacle::computeVelocities (source/obstacles/Obstacle.cpp:153-264): the
+// 6x6 momentum balance, forced dofs and blocked rotations replaced by their
+// imposed values; the computed velocities become the free dofs' velocities.
+void op_update_obstacles(OState& S) {
+  if (!S.has_sphere) return;
+  const Dims D = S.D;
+  const Real h = S.h;
+  Sphere& s = S.sph;
+  const bool implicitPen = S.cfg.implicit_penalization != 0;
+  const double lambdt = S.lambda * S.dt;
+  const double* CM = s.centerOfMass;
+  const int nb = D.nblocks();
+  double M[29] = {0};
+  for (int b = 0; b < nb; ++b) {
+    if (!s.touched[b]) continue;
+    const int bx = b % D.bpd(0), by = (b / D.bpd(0)) % D.bpd(1), bz = b / (D.bpd(0) * D.bpd(1));
+    double q[29] = {0};
+    for (int iz = 0; iz < BS; ++iz)
+    for (int iy = 0; iy < BS; ++iy)
+    for (int ix = 0; ix < BS; ++ix) {
+      const int gx = bx * BS + ix, gy = by * BS + iy, gz = bz * BS + iz;
+      const size_t o = D.idx(gx, gy, gz);
+      if (s.CHI[o] <= 0) continue;
+      double p[3] = {(gx + 0.5) * h, (gy + 0.5) * h, (gz + 0.5) * h};
+      const double dv = h * h * h, X = s.CHI[o];
+      p[0] -= CM[0]; p[1] -= CM[1]; p[2] -= CM[2];
+      const double u = S.u[o], v = S.v[o], w = S.w[o];
+      q[0] += X * dv;
+      q[7] += X * dv * (p[1] * p[1] + p[2] * p[2]);
+      q[8] += X * dv * (p[0] * p[0] + p[2] * p[2]);
+      q[9] += X * dv * (p[0] * p[0] + p[1] * p[1]);
+      q[10] -= X * dv * p[0] * p[1];
+      q[11] -= X * dv * p[0] * p[2];
+      q[12] -= X * dv * p[1] * p[2];
+      q[1] += X * dv * u; q[2] += X * dv * v; q[3] += X * dv * w;
+      q[4] += X * dv * (p[1] * w - p[2] * v);
+      q[5] += X * dv * (p[2] * u - p[0] * w);
+      q[6] += X * dv * (p[0] * v - p[1] * u);
+      if (implicitPen) {
+        const double penalFac = dv * lambdt * X / (1 + X * lambdt);
+        q[13] += penalFac;
+        q[14] += penalFac * p[0]; q[15] += penalFac * p[1]; q[16] += penalFac * p[2];
+        q[17] += penalFac * (p[1] * p[1] + p[2] * p[2]);
+        q[18] += penalFac * (p[0] * p[0] + p[2] * p[2]);
+        q[19] += penalFac * (p[0] * p[0] + p[1] * p[1]);
+        q[20] -= penalFac * p[0] * p[1];
+        q[21] -= penalFac * p[0] * p[2];
+        q[22] -= penalFac * p[1] * p[2];
+        q[23] += penalFac * u; q[24] += penalFac * v; q[25] += penalFac * w;
+        q[26] += penalFac * (p[1] * w - p[2] * v);
+        q[27] += penalFac * (p[2] * u - p[0] * w);
+        q[28] += penalFac * (p[0] * v - p[1] * u);
+      }
+    }
+    for (int k = 0; k < 29; ++k) M[k] += q[k];
+  }
+  s.mass = M[0];
+  for (int k = 0; k < 6; ++k) s.J[k] = M[7 + k];
+  if (implicitPen) {
+    s.penalM = M[13];
+    for (int d = 0; d < 3; ++d) s.penalCM[d] = M[14 + d], s.penalLmom[d] = M[23 + d], s.penalAmom[d] = M[26 + d];
+    for (int k = 0; k < 6; ++k) s.penalJ[k] = M[17 + k];
+  } else {
+    s.penalM = M[0];
+    for (int d = 0; d < 3; ++d) s.penalCM[d] = 0, s.penalLmom[d] = M[1 + d], s.penalAmom[d] = M[4 + d];
+    for (int k = 0; k < 6; ++k) s.penalJ[k] = M[7 + k];
+  }
+  const double pM = s.penalM, *pC = s.penalCM, *pJ = s.penalJ;
+  double A[6][6] = {{pM, 0, 0, 0, +pC[2], -pC[1]},
+                    {0, pM, 0, -pC[2], 0, +pC[0]},
+                    {0, 0, pM, +pC[1], -pC[0], 0},
+                    {0, -pC[2], +pC[1], pJ[0], pJ[3], pJ[4]},
+                    {+pC[2], 0, -pC[0], pJ[3], pJ[1], pJ[5]},
+                    {-pC[1], +pC[0], 0, pJ[4], pJ[5], pJ[2]}};
+  double b[6] = {s.penalLmom[0], s.penalLmom[1], s.penalLmom[2], s.penalAmom[0], s.penalAmom[1], s.penalAmom[2]};
+  for (int d = 0; d < 3; ++d) {
+    if (s.bForcedInSimFrame[d]) {
+      for (int k = 0; k < 6; ++k)
+        if (k != d) A[d][k] = 0;
+      b[d] = pM * s.transVel_imposed[d];
+    }
+    if (s.bBlockRotation[d]) {
+      for (int k = 0; k < 6; ++k)
+        if (k != 3 + d) A[3 + d][k] = 0;
+      b[3 + d] = 0;
+    }
+  }
+  double x[6];
+  lu_solve6(A, b, x);
+  for (int d = 0; d < 3; ++d) s.transVel_computed[d] = x[d], s.angVel_computed[d] = x[3 + d];
+  for (int d = 0; d < 3; ++d) s.force[d] = s.mass * (s.transVel_computed[d] - s.transVel[d]) / S.dt;
+  const double dAv[3] = {(s.angVel_computed[0] - s.angVel[0]) / S.dt, (s.angVel_computed[1] - s.angVel[1]) / S.dt,
+                         (s.angVel_computed[2] - s.angVel[2]) / S.dt};
+  s.torque[0] = s.J[0] * dAv[0] + s.J[3] * dAv[1] + s.J[4] * dAv[2];
+  s.torque[1] = s.J[3] * dAv[0] + s.J[1] * dAv[1] + s.J[5] * dAv[2];
+  s.torque[2] = s.J[4] * dAv[0] + s.J[5] * dAv[1] + s.J[2] * dAv[2];
+  for (int d = 0; d < 3; ++d) {
+    s.transVel[d] = s.bForcedInSimFrame[d] ? s.transVel_imposed[d] : s.transVel_computed[d];
+    s.angVel[d] = s.bBlockRotation[d] ? 0.0 : s.angVel_computed[d];
+  }
+}
 
 // Penalization::operator() (source/operators/Penalization.cpp:129-156):
 // KernelPenalization<implicit> (:40-98) + KernelFinalizePenalizationForce (:101-123).
@@ -789,8 +942,11 @@ void* orc_create(const orc_config* cfg) {
       s.position[d] = cfg->sphere_position[d];
       s.bForcedInSimFrame[d] = cfg->sphere_forced[d] != 0;
       s.bFixFrameOfRef[d] = cfg->sphere_fix_frame[d] != 0;
-      if (s.bForcedInSimFrame[d]) s.transVel[d] = cfg->sphere_velocity[d];
+      if (s.bForcedInSimFrame[d]) s.transVel_imposed[d] = s.transVel[d] = cfg->sphere_velocity[d];
     }
+    // any forced dof blocks rotation (source/obstacles/Obstacle.cpp:131-137)
+    const bool anyForced = s.bForcedInSimFrame[0] || s.bForcedInSimFrame[1] || s.bForcedInSimFrame[2];
+    for (int d = 0; d < 3; ++d) s.bBlockRotation[d] = anyForced;
     // Initial CreateObstacles call with dt = 0 (source/Simulation.cpp:399-400).
     S->dt = 0;
     op_create_obstacles(*S);
@@ -1001,6 +1157,12 @@ void orc_get_stats(void* hdl, double* out) {
   for (int d = 0; d < 3; ++d) out[13 + d] = S->sph.centerOfMass[d];
   for (int d = 0; d < 3; ++d) out[16 + d] = S->rhs_sums[d];
   out[19] = S->corr; out[20] = S->uMax_measured;
+  for (int d = 0; d < 3; ++d) {
+    out[21 + d] = S->sph.transVel[d];
+    out[24 + d] = S->sph.angVel[d];
+    out[27 + d] = S->sph.position[d];
+  }
+  for (int k = 0; k < 4; ++k) out[30 + k] = S->sph.quaternion[k];
 }
 
 // Stand-alone periodic Poisson solve of rhs (premultiplied by h^3, as the

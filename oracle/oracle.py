@@ -170,12 +170,13 @@ class OracleSim:
         return tuple(t)
 
     def stats(self) -> dict:
-        out = np.zeros(21, dtype=np.float64)
+        out = np.zeros(34, dtype=np.float64)
         lib().orc_get_stats(self._h, _p(out))
         return {
             "force": out[0:3].copy(), "torque": out[3:6].copy(), "time": out[6], "step": int(out[7]),
             "uinf": out[8:11].copy(), "dt": out[11], "lambda": out[12], "com": out[13:16].copy(),
-            "rhs_sums": out[16:19].copy(), "corr": out[19], "umax": out[20],
+            "rhs_sums": out[16:19].copy(), "corr": out[19], "umax": out[20], "transVel": out[21:24].copy(),
+            "angVel": out[24:27].copy(), "position": out[27:30].copy(), "quaternion": out[30:34].copy(),
         }
 
     def diagnostics(self) -> dict:

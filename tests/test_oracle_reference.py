@@ -93,3 +93,39 @@ def test_sphere_pipeline_vs_reference(oracle, fix_frame):
     f, rf = orc.compute_forces(), ob["forces"]
     assert np.abs(f[:26] - rf).max() <= 1e-13 * np.abs(rf[:3]).max()
     assert f[26] == pytest.approx(ob["mass"], rel=1e-14)
+
+
+@pytest.mark.parametrize("forced,fix_frame", [((0, 1, 1), (0, 0, 0)), ((0, 0, 0), (0, 0, 0)), ((0, 0, 0), (1, 0, 0))])
+def test_free_sphere_rigid_update_vs_reference(oracle, forced, fix_frame):
+    # UpdateObstacles with free dofs: the momentum integrals of
+    # KernelIntegrateFluidMomenta and the 6x6 balance of
+    # Obstacle::computeVelocities (free translation, and rotation when no dof
+    # is forced), position and orientation advanced by CreateObstacles, the
+    # frame following a free dof (updateUinf), against the reference's code
+    cells, L, nu = (64, 32, 32), 2.0, 1e-3
+    nx, ny, nz = cells
+    pos = (0.6, 0.5, 0.45)
+    orc = oracle.OracleSim(nx, ny, nz, L, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6, implicit_penalization=True,
+                           scheme="ref", sphere={"radius": 0.25, "position": pos, "velocity": (0.0, 0.0, 0.0),
+                                                 "forced": forced, "fix_frame": fix_frame})
+    ref = ref_mod.ReferenceSim(nx, ny, nz, L, nu, (0.0, 0.0, 0.0), 1e6, True)
+    ref.add_sphere(0.25, pos, (0.0, 0.0, 0.0), forced, fix_frame)
+    Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    u, v, w = 0.5 + 0.2 * np.sin(2 * np.pi * Y / ny), 0.3 * np.sin(2 * np.pi * X / nx), 0.1 * np.cos(2 * np.pi * Z / nz)
+    orc.set_velocity(u, v, w)
+    ref.set_velocity(u, v, w)
+    for step in range(4):
+        dt = orc.calc_max_timestep()
+        orc.timestep(dt)
+        ref.timestep(dt)
+        st, ob = orc.stats(), ref.obstacle()
+        scale = max(1.0, np.abs(ob["transVel"]).max())
+        assert np.allclose(st["transVel"], ob["transVel"], rtol=0, atol=1e-13 * scale)
+        assert np.allclose(st["angVel"], ob["angVel"], rtol=0, atol=1e-12)
+        assert np.allclose(st["position"], ob["position"], rtol=0, atol=1e-15)
+        assert np.allclose(st["uinf"], ob["uinf"], rtol=0, atol=1e-13 * scale)
+        assert np.array_equal(orc.get("chi"), ref.get("chi"))
+        for a, b in zip(orc.velocity(), ref.velocity()):
+            assert np.linalg.norm(a - b) <= 1e-13 * np.linalg.norm(np.stack(ref.velocity()))
+    if not any(forced):
+        assert abs(st["angVel"][2]) > 0.1  # the shear spins a free sphere
