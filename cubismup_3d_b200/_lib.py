@@ -94,6 +94,9 @@ SIGNATURES = {
     "cup_global_to_blocks": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "cup_add_sphere": (C.c_int, [_H, C.POINTER(CupSphere)]),
     "cup_create_obstacles": (C.c_int, [_H, C.c_double]),
+    "cup_update_obstacles": (C.c_int, [_H, C.c_double]),
+    "cup_get_sphere_motion": (C.c_int, [_H, _dp, _dp, _dp]),
+    "cup_set_sphere_motion": (C.c_int, [_H, _dp, _dp, _dp]),
     "cup_set_graphs": (C.c_int, [_H, C.c_int]),
     "cup_prepare_run": (C.c_int, [_H, C.c_int, C.POINTER(C.c_int)]),
     "cup_set_sphere_position": (C.c_int, [_H, _dp]),

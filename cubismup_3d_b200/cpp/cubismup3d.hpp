@@ -226,13 +226,16 @@ class CreateObstacles : public Operator {
   std::string getName() override { return "CreateObstacles"; }
 };
 
-// UpdateObstacles (source/operators/ObstaclesUpdate.cpp:202-236) for a sphere
-// with every dof forced: its velocities stay the imposed ones
-// (source/obstacles/Obstacle.cpp:153-264), so there is nothing to integrate.
+// UpdateObstacles (source/operators/ObstaclesUpdate.cpp:202-236): the free
+// dofs' velocities from the fluid momentum balance of
+// Obstacle::computeVelocities (source/obstacles/Obstacle.cpp:153-264); forced
+// dofs keep their imposed velocity.
 class UpdateObstacles : public Operator {
  public:
   using Operator::Operator;
-  void operator()(const double) override {}
+  void operator()(const double dt) override {
+    cup_check(cup_update_obstacles(sim.handle, dt), sim.handle, "UpdateObstacles");
+  }
   std::string getName() override { return "UpdateObstacles"; }
 };
 

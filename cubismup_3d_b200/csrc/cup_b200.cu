@@ -51,7 +51,7 @@ struct DevState {
   long long solves_total;  // correction solves of all decided defect corrections (cumulative)
 };
 
-enum PartialRegion { P_GRAD = 0, P_PEN, P_RHSOB, P_CHI, P_MAX, P_RES, P_DIAG, P_COUNT };
+enum PartialRegion { P_GRAD = 0, P_PEN, P_RHSOB, P_CHI, P_MAX, P_RES, P_DIAG, P_RIGID, P_COUNT };
 constexpr int kPartialCap = 98304;  // doubles per region (>= 20 per CTA of a 4096-CTA pass)
 
 constexpr int kBoxThreads = 256;
@@ -254,6 +254,104 @@ __global__ void k_finalize_com(const double* p, int np, DevState* st, SpherePara
       st->com[k] = s[1 + k] / s[0];
       sp->centerOfMass[k] = st->com[k];
     }
+  }
+}
+
+// KernelFinalizeObstacleVel (source/operators/ObstaclesUpdate.cpp:136-200)
+// and Obstacle::computeVelocities (source/obstacles/Obstacle.cpp:153-264) for
+// the sphere: the 29 momentum sums, then the 6x6 momentum balance with the
+// rows of forced translations and blocked rotations replaced by their imposed
+// values, solved by LU with partial pivoting (the GSL routines the reference
+// calls); the free dofs take the computed velocities. force / torque are the
+// rigid-body ones of computeVelocities (Penalization overwrites them).
+__global__ void k_rigid_update(const double* partials, int np, SphereParams* sp, DevState* st, DtArg dt,
+                               int implicit_pen) {
+  pdl_entry();
+  __shared__ double scratch[kRigidQoI * 32];
+  double M[kRigidQoI];
+  for (int k = 0; k < kRigidQoI; ++k) M[k] = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x)
+    for (int k = 0; k < kRigidQoI; ++k) M[k] += partials[(size_t)kRigidQoI * i + k];
+  block_reduce<kRigidQoI, false>(M, scratch);
+  if (threadIdx.x != 0) return;
+  SphereParams& s = *sp;
+  const double dtv = dt.get();
+  s.mass = M[0];
+  for (int k = 0; k < 6; ++k) s.J[k] = M[7 + k];
+  double pM, pC[3], pJ[6], Lm[3], Am[3];
+  if (implicit_pen) {
+    pM = M[13];
+    for (int d = 0; d < 3; ++d) pC[d] = M[14 + d], Lm[d] = M[23 + d], Am[d] = M[26 + d];
+    for (int k = 0; k < 6; ++k) pJ[k] = M[17 + k];
+  } else {
+    pM = M[0];
+    for (int d = 0; d < 3; ++d) pC[d] = 0, Lm[d] = M[1 + d], Am[d] = M[4 + d];
+    for (int k = 0; k < 6; ++k) pJ[k] = M[7 + k];
+  }
+  double A[6][6] = {{pM, 0, 0, 0, +pC[2], -pC[1]},
+                    {0, pM, 0, -pC[2], 0, +pC[0]},
+                    {0, 0, pM, +pC[1], -pC[0], 0},
+                    {0, -pC[2], +pC[1], pJ[0], pJ[3], pJ[4]},
+                    {+pC[2], 0, -pC[0], pJ[3], pJ[1], pJ[5]},
+                    {-pC[1], +pC[0], 0, pJ[4], pJ[5], pJ[2]}};
+  double b[6] = {Lm[0], Lm[1], Lm[2], Am[0], Am[1], Am[2]};
+  for (int d = 0; d < 3; ++d) {
+    if (s.forced[d]) {
+      for (int k = 0; k < 6; ++k)
+        if (k != d) A[d][k] = 0;
+      b[d] = pM * s.transVel_imposed[d];
+    }
+    if (s.block_rot[d]) {
+      for (int k = 0; k < 6; ++k)
+        if (k != 3 + d) A[3 + d][k] = 0;
+      b[3 + d] = 0;
+    }
+  }
+  // LU with partial pivoting, then forward and back substitution
+  int perm[6] = {0, 1, 2, 3, 4, 5};
+  for (int j = 0; j < 5; ++j) {
+    int piv = j;
+    double mx = fabs(A[j][j]);
+    for (int i = j + 1; i < 6; ++i)
+      if (fabs(A[i][j]) > mx) mx = fabs(A[i][j]), piv = i;
+    if (piv != j) {
+      for (int k = 0; k < 6; ++k) {
+        const double t = A[j][k];
+        A[j][k] = A[piv][k];
+        A[piv][k] = t;
+      }
+      const int t = perm[j];
+      perm[j] = perm[piv];
+      perm[piv] = t;
+    }
+    if (A[j][j] == 0) continue;
+    for (int i = j + 1; i < 6; ++i) {
+      const double l = A[i][j] / A[j][j];
+      A[i][j] = l;
+      for (int k = j + 1; k < 6; ++k) A[i][k] -= l * A[j][k];
+    }
+  }
+  double x[6];
+  for (int i = 0; i < 6; ++i) x[i] = b[perm[i]];
+  for (int i = 0; i < 6; ++i)
+    for (int k = 0; k < i; ++k) x[i] -= A[i][k] * x[k];
+  for (int i = 5; i >= 0; --i) {
+    for (int k = i + 1; k < 6; ++k) x[i] -= A[i][k] * x[k];
+    x[i] /= A[i][i];
+  }
+  double dAv[3];
+  for (int d = 0; d < 3; ++d) {
+    s.transVel_computed[d] = x[d];
+    s.angVel_computed[d] = x[3 + d];
+    st->force[d] = s.mass * (x[d] - s.transVel[d]) / dtv;
+    dAv[d] = (x[3 + d] - s.angVel[d]) / dtv;
+  }
+  st->torque[0] = s.J[0] * dAv[0] + s.J[3] * dAv[1] + s.J[4] * dAv[2];
+  st->torque[1] = s.J[3] * dAv[0] + s.J[1] * dAv[1] + s.J[5] * dAv[2];
+  st->torque[2] = s.J[4] * dAv[0] + s.J[5] * dAv[1] + s.J[2] * dAv[2];
+  for (int d = 0; d < 3; ++d) {
+    s.transVel[d] = s.forced[d] ? s.transVel_imposed[d] : x[d];
+    s.angVel[d] = s.block_rot[d] ? 0.0 : x[3 + d];
   }
 }
 
@@ -685,6 +783,9 @@ struct cup_handle {
   cup_sphere sphere{};  // host mirror; sphere.position follows Obstacle::update
   double sphere_vel[3] = {0, 0, 0};  // transVel (the imposed velocity of the forced dofs)
   bool sphere_moves = false;         // transVel + uinf != 0: chi is rebuilt every step
+  bool sphere_free = false;          // a translation is not forced: UpdateObstacles computes the velocities
+  double sphere_angvel[3] = {0, 0, 0};       // angVel (host mirror, read back after each step when free)
+  double sphere_quat[4] = {1, 0, 0, 0};      // Obstacle::quaternion
   SphereParams* sp_dev = nullptr;
   Box box{};
   // host mirrors
@@ -1629,8 +1730,62 @@ int relocate_sphere(cup_handle* H);
 
 int do_create_obstacles(cup_handle* H, double dt) {
   if (!H->has_sphere || !H->sphere_moves) return CUP_OK;
+  if (H->sphere_free) {
+    // updateUinf with the velocities of the last UpdateObstacles
+    for (int d = 0; d < 3; ++d) H->uinf[d] = H->sphere.bFixFrameOfRef[d] ? -H->sphere_vel[d] : 0.0;
+    // orientation (Obstacle::update, source/obstacles/Obstacle.cpp:323-346;
+    // the sphere's chi does not depend on it)
+    const double* w = H->sphere_angvel;
+    const double* Q = H->sphere_quat;
+    const double dqdt[4] = {.5 * (-w[0] * Q[1] - w[1] * Q[2] - w[2] * Q[3]), .5 * (+w[0] * Q[0] + w[1] * Q[3] - w[2] * Q[2]),
+                            .5 * (-w[0] * Q[3] + w[1] * Q[0] + w[2] * Q[1]), .5 * (+w[0] * Q[2] - w[1] * Q[1] + w[2] * Q[0])};
+    const double DQ[4] = {dqdt[0] * dt, dqdt[1] * dt, dqdt[2] * dt, dqdt[3] * dt};
+    const double DQn = std::sqrt(DQ[0] * DQ[0] + DQ[1] * DQ[1] + DQ[2] * DQ[2] + DQ[3] * DQ[3]);
+    if (DQn > 2.220446049250313080847e-16) {
+      const double tanF = std::tan(DQn) / DQn;
+      const double D[4] = {Q[0] + tanF * DQ[0], Q[1] + tanF * DQ[1], Q[2] + tanF * DQ[2], Q[3] + tanF * DQ[3]};
+      const double invD = 1 / std::sqrt(D[0] * D[0] + D[1] * D[1] + D[2] * D[2] + D[3] * D[3]);
+      for (int k = 0; k < 4; ++k) H->sphere_quat[k] = D[k] * invD;
+    }
+  }
   for (int d = 0; d < 3; ++d) H->sphere.position[d] += dt * (H->sphere_vel[d] + H->uinf[d]);
   return relocate_sphere(H);
+}
+
+// UpdateObstacles (source/operators/ObstaclesUpdate.cpp:202-236) for a sphere
+// with free dofs: the momentum integrals over its box, then the 6x6 balance
+// on the device (k_rigid_update), which sets the sphere's velocities for the
+// penalization that follows.
+template <typename T>
+int do_rigid_update(cup_handle* H, DtArg dt, const double* lambda_dev) {
+  const int gb = box_grid(H->box);
+  int rc = launch_named(H, "integrate_momenta", [&]() -> int {
+    klaunch(H, k_integrate_momenta<T>, gb, kBoxThreads, 0, (const T*)H->u, (const T*)H->v, (const T*)H->w,
+            (const T*)H->chi, (const SphereParams*)H->sp_dev, H->box, H->nx, H->ny, H->nz, H->h, dt, lambda_dev,
+            H->lambda, H->cfg.bImplicitPenalization, partial(H, P_RIGID));
+    CKL();
+    return CUP_OK;
+  });
+  if (rc) return rc;
+  return launch_named(H, "rigid_update", [&]() -> int {
+    klaunch(H, k_rigid_update, 1, 256, 0, (const double*)partial(H, P_RIGID), gb, H->sp_dev, H->dstate, dt,
+            H->cfg.bImplicitPenalization);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+// The velocities UpdateObstacles computed, into the host mirror (the next
+// CreateObstacles moves the sphere and the frame with them). Synchronises.
+int read_sphere_motion(cup_handle* H) {
+  SphereParams sp;
+  CK(cudaMemcpyAsync(&sp, H->sp_dev, sizeof(sp), cudaMemcpyDeviceToHost, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  for (int d = 0; d < 3; ++d) {
+    H->sphere_vel[d] = sp.transVel[d];
+    H->sphere_angvel[d] = sp.angVel[d];
+  }
+  return CUP_OK;
 }
 
 // chi of the sphere at H->sphere.position: cleared on the old box, rebuilt
@@ -1808,6 +1963,8 @@ int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance, int 
   if (!H->fp32) {
     if ((rc = do_grad<T>(H, dt))) return rc;
   }
+  // UpdateObstacles: the free dofs' velocities from the pre-penalization flow
+  if (H->has_sphere && H->sphere_free && (rc = do_rigid_update<T>(H, dt, lambda_dev))) return rc;
   if ((rc = do_penalize<T>(H, dt, lambda_dev))) return rc;
   {
     int rc_ = launch_named(H, "finalize_step", [&]() -> int {
@@ -2423,10 +2580,6 @@ int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
   if (H->has_sphere) return fail(H, CUP_ERR_STATE, "only one obstacle is supported");
   bool anyForced = false;
   for (int d = 0; d < 3; ++d) anyForced = anyForced || s->bForcedInSimFrame[d];
-  for (int d = 0; d < 3; ++d)
-    if (!s->bForcedInSimFrame[d])
-      return fail(H, CUP_ERR_ARG, "free (unforced) obstacle dofs are not supported; force all three");
-  (void)anyForced;
   H->has_sphere = true;
   H->sphere = *s;
   drop_graph(H);  // captured steps hold no obstacle
@@ -2440,14 +2593,20 @@ int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
     H->sphere_vel[d] = s->bForcedInSimFrame[d] ? s->enforcedVelocity[d] : 0.0;
     H->uinf[d] = s->bFixFrameOfRef[d] ? -H->sphere_vel[d] : 0.0;
   }
-  H->sphere_moves = false;
+  H->sphere_free = !(s->bForcedInSimFrame[0] && s->bForcedInSimFrame[1] && s->bForcedInSimFrame[2]);
+  H->sphere_moves = H->sphere_free;
   for (int d = 0; d < 3; ++d) H->sphere_moves = H->sphere_moves || (H->sphere_vel[d] + H->uinf[d] != 0.0);
+  for (int d = 0; d < 3; ++d) H->sphere_angvel[d] = 0.0;
+  H->sphere_quat[0] = 1, H->sphere_quat[1] = H->sphere_quat[2] = H->sphere_quat[3] = 0;
   SphereParams sp{};
   sp.radius = s->radius;
   for (int d = 0; d < 3; ++d) {
     sp.position[d] = s->position[d];
     sp.transVel[d] = s->bForcedInSimFrame[d] ? s->enforcedVelocity[d] : 0.0;
-    sp.angVel[d] = 0.0;  // rotation blocked when any dof is forced (Obstacle.cpp:131-137)
+    sp.angVel[d] = 0.0;
+    sp.transVel_imposed[d] = sp.transVel[d];
+    sp.forced[d] = s->bForcedInSimFrame[d] ? 1 : 0;
+    sp.block_rot[d] = anyForced ? 1 : 0;  // any forced dof blocks rotation (Obstacle.cpp:131-137)
   }
   sp.lambda_factor = 1.0;
   sphere_box(H);
@@ -2526,6 +2685,50 @@ int cup_create_obstacles(cup_handle* H, double dt) {
   if (!(dt >= 0)) return fail(H, CUP_ERR_ARG, "dt must be >= 0");
   int rc = do_create_obstacles(H, dt);
   if (rc) return rc;
+  return CUP_OK;
+}
+
+int cup_update_obstacles(cup_handle* H, double dt) {
+  REQUIRE_H(H);
+  if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
+  if (!H->has_sphere || !H->sphere_free) return CUP_OK;  // forced dofs keep their imposed velocity
+  // lambda from the host, as cup_penalize takes it
+  int rc = H->fp32 ? do_rigid_update<float>(H, DtArg{dt, nullptr}, nullptr)
+                   : do_rigid_update<double>(H, DtArg{dt, nullptr}, nullptr);
+  if (rc) return rc;
+  return read_sphere_motion(H);
+}
+
+int cup_get_sphere_motion(cup_handle* H, double transVel[3], double angVel[3], double quaternion[4]) {
+  REQUIRE_H(H);
+  if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "the handle has no obstacle");
+  if (!transVel || !angVel || !quaternion) return fail(H, CUP_ERR_ARG, "null output");
+  for (int d = 0; d < 3; ++d) {
+    transVel[d] = H->sphere_vel[d];
+    angVel[d] = H->sphere_angvel[d];
+  }
+  for (int k = 0; k < 4; ++k) quaternion[k] = H->sphere_quat[k];
+  return CUP_OK;
+}
+
+int cup_set_sphere_motion(cup_handle* H, const double transVel[3], const double angVel[3], const double quaternion[4]) {
+  REQUIRE_H(H);
+  if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "the handle has no obstacle");
+  if (!transVel || !angVel || !quaternion) return fail(H, CUP_ERR_ARG, "null input");
+  for (int d = 0; d < 3; ++d) {
+    H->sphere_vel[d] = transVel[d];
+    H->sphere_angvel[d] = angVel[d];
+  }
+  for (int k = 0; k < 4; ++k) H->sphere_quat[k] = quaternion[k];
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(H->sp_dev) + offsetof(SphereParams, transVel), transVel,
+                     3 * sizeof(double), cudaMemcpyHostToDevice, H->stream));
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(H->sp_dev) + offsetof(SphereParams, angVel), angVel, 3 * sizeof(double),
+                     cudaMemcpyHostToDevice, H->stream));
+  CK(cudaStreamSynchronize(H->stream));
+  if (H->sphere_free)
+    for (int d = 0; d < 3; ++d) H->uinf[d] = H->sphere.bFixFrameOfRef[d] ? -H->sphere_vel[d] : 0.0;
+  drop_graph(H);
+  H->umax_fresh = false;
   return CUP_OK;
 }
 
@@ -2736,6 +2939,7 @@ int cup_step(cup_handle* H, double dt, cup_step_stats* stats) {
   if (rc) return rc;
   if (!ran) rc = DISPATCH_T(H, do_step, DtArg{dt, nullptr}, (const double*)&H->dstate->lambda, 1);
   if (rc) return rc;
+  if (H->has_sphere && H->sphere_free && (rc = read_sphere_motion(H))) return rc;
   H->step += 1;
   H->time += dt;
   H->umax_fresh = true;

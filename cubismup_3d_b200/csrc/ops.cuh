@@ -283,6 +283,13 @@ struct SphereParams {
   double angVel[3];
   double centerOfMass[3];
   double lambda_factor;
+  // rigid-body update of the free dofs (Obstacle::computeVelocities,
+  // source/obstacles/Obstacle.cpp:153-264): forced translations keep
+  // transVel_imposed; rotation is blocked when any translation is forced
+  double transVel_imposed[3];
+  int forced[3], block_rot[3];
+  double mass, J[6];
+  double transVel_computed[3], angVel_computed[3];
 };
 
 __device__ __forceinline__ double sphere_sdf(const SphereParams& s, double x, double y, double z) {
@@ -509,6 +516,75 @@ __global__ void k_surface_forces(const T* u, const T* v, const T* w, const doubl
   block_reduce<kSurfQoI, false>(acc, scratch);
   if (threadIdx.x == 0)
     for (int k = 0; k < kSurfQoI; ++k) partials[kSurfQoI * blockIdx.x + k] = acc[k];
+}
+
+// KernelIntegrateFluidMomenta (source/operators/ObstaclesUpdate.cpp:24-134)
+// over the box: for every cell with chi > 0, the volume, linear and angular
+// momentum and inertia moments about the centre of mass and, for implicit
+// penalization, the same weighted by dv lambda dt chi / (1 + chi lambda dt);
+// the sphere has no deformation velocity. Per-CTA partials of the 29 sums in
+// the order of KernelFinalizeObstacleVel (:142-160).
+constexpr int kRigidQoI = 29;
+template <typename T>
+__global__ void k_integrate_momenta(const T* u, const T* v, const T* w, const T* chi, const SphereParams* sp, Box box,
+                                    int nx, int ny, int nz, double h, DtArg dt, const double* lambda_dev,
+                                    double lambda_host, int implicit_pen, double* partials /* [gridDim.x][29] */) {
+  pdl_entry();
+  __shared__ double scratch[kRigidQoI * 32];
+  const SphereParams s = *sp;
+  const double lambda = lambda_dev ? *lambda_dev : lambda_host;
+  const double lambdt = lambda * dt.get();
+  const double dv = h * h * h;
+  double q[kRigidQoI];
+#pragma unroll
+  for (int k = 0; k < kRigidQoI; ++k) q[k] = 0.0;
+  const long long n = box.count();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = wrapi(box.lo[0] + (int)(i % box.n[0]), nx);
+    const int y = wrapi(box.lo[1] + (int)((i / box.n[0]) % box.n[1]), ny);
+    const int z = wrapi(box.lo[2] + (int)(i / ((long long)box.n[0] * box.n[1])), nz);
+    const size_t o = gidx(x, y, z, nx, ny);
+    const double X = chi[o];
+    if (X <= 0) continue;
+    const double p0 = (x + 0.5) * h - s.centerOfMass[0], p1 = (y + 0.5) * h - s.centerOfMass[1],
+                 p2 = (z + 0.5) * h - s.centerOfMass[2];
+    const double uu = u[o], vv = v[o], ww = w[o];
+    q[0] += X * dv;
+    q[1] += X * dv * uu;
+    q[2] += X * dv * vv;
+    q[3] += X * dv * ww;
+    q[4] += X * dv * (p1 * ww - p2 * vv);
+    q[5] += X * dv * (p2 * uu - p0 * ww);
+    q[6] += X * dv * (p0 * vv - p1 * uu);
+    q[7] += X * dv * (p1 * p1 + p2 * p2);
+    q[8] += X * dv * (p0 * p0 + p2 * p2);
+    q[9] += X * dv * (p0 * p0 + p1 * p1);
+    q[10] -= X * dv * p0 * p1;
+    q[11] -= X * dv * p0 * p2;
+    q[12] -= X * dv * p1 * p2;
+    if (implicit_pen) {
+      const double f = dv * lambdt * X / (1 + X * lambdt);
+      q[13] += f;
+      q[14] += f * p0;
+      q[15] += f * p1;
+      q[16] += f * p2;
+      q[17] += f * (p1 * p1 + p2 * p2);
+      q[18] += f * (p0 * p0 + p2 * p2);
+      q[19] += f * (p0 * p0 + p1 * p1);
+      q[20] -= f * p0 * p1;
+      q[21] -= f * p0 * p2;
+      q[22] -= f * p1 * p2;
+      q[23] += f * uu;
+      q[24] += f * vv;
+      q[25] += f * ww;
+      q[26] += f * (p1 * ww - p2 * vv);
+      q[27] += f * (p2 * uu - p0 * ww);
+      q[28] += f * (p0 * vv - p1 * uu);
+    }
+  }
+  block_reduce<kRigidQoI, false>(q, scratch);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < kRigidQoI; ++k) partials[kRigidQoI * blockIdx.x + k] = q[k];
 }
 
 // KernelPenalization<implicit> (source/operators/Penalization.cpp:40-98) over

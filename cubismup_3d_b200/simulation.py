@@ -218,14 +218,15 @@ class PressureProjection(Operator):
 
 
 class UpdateObstacles(Operator):
-    """UpdateObstacles (source/operators/ObstaclesUpdate.cpp:202-236) for a sphere
-    with every dof forced: its velocities stay the imposed ones
-    (source/obstacles/Obstacle.cpp:153-264) and the frame velocity is set by
-    CreateObstacles, so there is nothing to integrate."""
+    """UpdateObstacles (source/operators/ObstaclesUpdate.cpp:202-236): for a
+    sphere with free dofs, the fluid momentum integrals and the 6x6 momentum
+    balance of Obstacle::computeVelocities (source/obstacles/Obstacle.cpp:153-264)
+    give the free dofs' velocities (cup_update_obstacles); forced dofs keep
+    their imposed velocity."""
     name = "UpdateObstacles"
 
     def __call__(self, dt: float):
-        return None
+        L.check(L.lib().cup_update_obstacles(self.sim._h, float(dt)), self.sim._h, self.name)
 
 
 class Penalization(Operator):
@@ -473,7 +474,16 @@ class Simulation:
     def obstacle_state(self) -> dict:
         f, t, c, u = (C.c_double * 3)(), (C.c_double * 3)(), (C.c_double * 3)(), (C.c_double * 3)()
         L.check(L.lib().cup_get_obstacle_state(self._h, f, t, c, u), self._h, "obstacle_state")
-        return {"force": np.array(f[:]), "torque": np.array(t[:]), "com": np.array(c[:]), "uinf": np.array(u[:])}
+        tv, av, q = (C.c_double * 3)(), (C.c_double * 3)(), (C.c_double * 4)()
+        L.check(L.lib().cup_get_sphere_motion(self._h, tv, av, q), self._h, "obstacle_state")
+        return {"force": np.array(f[:]), "torque": np.array(t[:]), "com": np.array(c[:]), "uinf": np.array(u[:]),
+                "transVel": np.array(tv[:]), "angVel": np.array(av[:]), "quaternion": np.array(q[:])}
+
+    def set_sphere_motion(self, transVel, angVel, quaternion=(1.0, 0.0, 0.0, 0.0)):
+        """Restores the sphere's velocities and orientation (Obstacle::restart)."""
+        tv, av = (C.c_double * 3)(*map(float, transVel)), (C.c_double * 3)(*map(float, angVel))
+        q = (C.c_double * 4)(*map(float, quaternion))
+        L.check(L.lib().cup_set_sphere_motion(self._h, tv, av, q), self._h, "set_sphere_motion")
 
     # -- fields ----------------------------------------------------------------
     def set_velocity(self, u, v, w):
@@ -749,13 +759,15 @@ class Simulation:
             pos = (C.c_double * 3)()
             L.check(L.lib().cup_get_sphere_position(self._h, pos), self._h, "serialize")
             sph = self.obstacles[0]
-            vel = [float(x) if f else 0.0 for x, f in zip(sph.enforcedVelocity, sph.bForcedInSimFrame)]
-            q = list(sph.quaternion) if getattr(sph, "quaternion", None) is not None else [1.0, 0.0, 0.0, 0.0]
-            # absPos (the position in the lab frame, advanced by transVel alone)
+            mot = self.obstacle_state()
+            vel, ang, q = list(mot["transVel"]), list(mot["angVel"]), list(mot["quaternion"])
+            # absPos (the position in the lab frame, advanced by transVel alone;
+            # exact for forced velocities, the latest velocity for free dofs)
             abspos = [p0 + self.time * vi for p0, vi in zip(sph.position, vel)]
+            angle2d = 2 * np.arctan2(q[3], q[0])  # _2Dangle from the quaternion (Obstacle.cpp:348-350)
             lines = [f"{self.time:.16e}", "\t".join(f"{x:.16e}" for x in pos[:]),
                      "\t".join(f"{x:.16e}" for x in abspos), "\t".join(f"{x:.16e}" for x in q),
-                     "\t".join(f"{x:.16e}" for x in vel), "\t".join(f"{0.0:.16e}" for _ in range(3)), f"{0.0:.16e}"]
+                     "\t".join(f"{x:.16e}" for x in vel), "\t".join(f"{x:.16e}" for x in ang), f"{angle2d:.16e}"]
             with open(fpath + "_0.txt", "w") as f:
                 f.write("\n".join(lines) + "\n")
         with open(fpath + ".status", "w") as f:
@@ -825,6 +837,10 @@ class Simulation:
                     rows = f.read().split("\n")
                 pos = (C.c_double * 3)(*[float(x) for x in rows[1].split()[:3]])
                 L.check(L.lib().cup_set_sphere_position(self._h, pos), self._h, "deserialize")
+                q = [float(x) for x in rows[3].split()[:4]]
+                vel = [float(x) for x in rows[4].split()[:3]]
+                ang = [float(x) for x in rows[5].split()[:3]]
+                self.set_sphere_motion(vel, ang, q)
         else:
             L.check(L.lib().cup_set_uinf(self._h, (C.c_double * 3)(*uinf)), self._h, "deserialize")
             self.sd.uinf = tuple(uinf)

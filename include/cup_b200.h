@@ -75,8 +75,10 @@ typedef struct cup_config {
 } cup_config;
 
 /* One sphere obstacle (source/obstacles/Sphere.cpp, ObstacleArguments in
- * source/obstacles/Obstacle.h:60-75). Any forced dof blocks rotation
- * (source/obstacles/Obstacle.cpp:131-137); free dofs are not supported. */
+ * source/obstacles/Obstacle.h:60-75). Forced translations move with
+ * enforcedVelocity; free ones take the velocity of the momentum balance of
+ * UpdateObstacles every step, and so does the rotation when no translation is
+ * forced (any forced dof blocks rotation, source/obstacles/Obstacle.cpp:131-137). */
 typedef struct cup_sphere {
   double radius;
   double position[3];
@@ -147,6 +149,23 @@ int cup_get_sphere_position(struct cup_handle* h, double position[3]);
  * (source/Simulation.cpp:526-580); only without an obstacle (updateUinf sets
  * it from the obstacle otherwise). */
 int cup_set_uinf(struct cup_handle* h, const double uinf[3]);
+/* UpdateObstacles (source/operators/ObstaclesUpdate.cpp:202-236) for a sphere
+ * with free dofs, on the current velocity (before Penalization): the fluid
+ * momentum integrals of KernelIntegrateFluidMomenta (:24-134) over chi > 0 and
+ * the 6x6 momentum balance of Obstacle::computeVelocities
+ * (source/obstacles/Obstacle.cpp:153-264), solved on the device; the free dofs
+ * take the computed velocities. No-op for a fully forced sphere. cup_step and
+ * cup_run run it between the projection and the penalization, and then read
+ * the velocities back (one synchronisation per step for a free sphere).
+ * Synchronises. */
+int cup_update_obstacles(struct cup_handle* h, double dt);
+/* The sphere's translational and angular velocity (Obstacle::transVel, angVel)
+ * and orientation (Obstacle::quaternion, advanced by CreateObstacles). */
+int cup_get_sphere_motion(struct cup_handle* h, double transVel[3], double angVel[3], double quaternion[4]);
+/* Restores them (Obstacle::restart, source/obstacles/Obstacle.cpp:425-447);
+ * for a frame fixed to a free dof, uinf follows (updateUinf). */
+int cup_set_sphere_motion(struct cup_handle* h, const double transVel[3], const double angVel[3],
+                          const double quaternion[4]);
 /* Force / torque from the last Penalization (Penalization.cpp:101-123), centre of mass. */
 int cup_get_obstacle_state(struct cup_handle* h, double force[3], double torque[3], double com[3],
                            double uinf[3]);

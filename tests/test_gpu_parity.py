@@ -381,7 +381,7 @@ def test_compute_dissipation_vs_oracle(oracle, with_sphere, tmp_path, monkeypatc
     assert all(len(l.split()) == 22 for l in lines[1:])
 
 
-@pytest.mark.parametrize("moving", [False, True])
+@pytest.mark.parametrize("moving", [False, True, "free"])
 def test_serialize_deserialize_resumes_the_run(tmp_path, moving):
     # Simulation::_serialize / _deserialize: 3 steps, a dump, a new simulation
     # restarts from it and runs 3 more; it ends where the uninterrupted 6-step
@@ -393,7 +393,9 @@ def test_serialize_deserialize_resumes_the_run(tmp_path, moving):
     def new_sim():
         sim = make_sim(cells, 1.0, nu=1e-3, CFL=0.2, rampup=0, DLM=0.0, lambda_=1e6, bImplicitPenalization=True,
                        uinf=(0.0, 0.0, 0.0) if moving else (0.1, -0.05, 0.0))
-        if moving:
+        if moving == "free":  # translation free along x: the restart restores its velocity
+            sim.add_obstacle(cup.Sphere(**dict(MOVING_SPHERE, bForcedInSimFrame=(False, True, True))))
+        elif moving:
             sim.add_obstacle(cup.Sphere(**MOVING_SPHERE))
         sim.sd.path4serialization = str(tmp_path)
         return sim
@@ -736,3 +738,71 @@ def test_gpu_sphere_steps_vs_reference_code(fix_frame):
     f = sim.compute_forces()
     got = np.array([f[k] for k in FORCE_NAMES[:26]])
     assert np.abs(got - ob["forces"]).max() <= 1e-10 * np.abs(ob["forces"][:3]).max()
+
+
+FREE_CASES = [((False, True, True), (False, False, False)), ((False, False, False), (False, False, False)),
+              ((False, False, False), (True, False, False))]
+
+
+def free_sphere_pair(oracle, forced, fix_frame, precision="fp64", **kw):
+    import cubismup_3d_b200 as cup
+    cells, L, nu, pos = (64, 32, 32), 2.0, 1e-3, (0.6, 0.5, 0.45)
+    nx, ny, nz = cells
+    sim = make_sim(cells, L, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6, bImplicitPenalization=True,
+                   precision=precision, **kw)
+    sim.add_obstacle(cup.Sphere(radius=0.25, position=pos, enforcedVelocity=(0.0, 0.0, 0.0),
+                                bForcedInSimFrame=forced, bFixFrameOfRef=fix_frame))
+    orc = oracle.OracleSim(nx, ny, nz, L, nu=nu, CFL=0.1, rampup=0, DLM=0.0, lambda_=1e6, implicit_penalization=True,
+                           sphere={"radius": 0.25, "position": pos, "velocity": (0.0, 0.0, 0.0),
+                                   "forced": [int(x) for x in forced], "fix_frame": [int(x) for x in fix_frame]})
+    Z, Y, X = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    u, v, w = 0.5 + 0.2 * np.sin(2 * np.pi * Y / ny), 0.3 * np.sin(2 * np.pi * X / nx), 0.1 * np.cos(2 * np.pi * Z / nz)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    return sim, orc
+
+
+@pytest.mark.parametrize("forced,fix_frame", FREE_CASES)
+def test_free_sphere_steps_vs_oracle(oracle, forced, fix_frame):
+    # UpdateObstacles with free dofs on the device (momentum integrals and the
+    # 6x6 balance of Obstacle::computeVelocities): velocities, position,
+    # frame velocity and the flow against the oracle, step by step
+    sim, orc = free_sphere_pair(oracle, forced, fix_frame)
+    for s in range(4):
+        dt = orc.calc_max_timestep()
+        assert sim.calcMaxTimestep() == pytest.approx(dt, rel=1e-12)
+        sim.timestep(dt)
+        orc.timestep(dt)
+        st, ob = sim.obstacle_state(), orc.stats()
+        assert np.allclose(st["transVel"], ob["transVel"], rtol=0, atol=1e-11)
+        assert np.allclose(st["angVel"], ob["angVel"], rtol=0, atol=1e-10)
+        assert np.allclose(st["uinf"], ob["uinf"], rtol=0, atol=1e-11)
+        assert np.allclose(st["quaternion"], ob["quaternion"], rtol=0, atol=1e-12)
+        for a, b in zip(sim.velocity(), orc.velocity()):
+            assert rel_l2(a, b) < TOL_STEP
+    assert np.allclose(sim.obstacle_state()["com"], orc.stats()["com"], rtol=0, atol=1e-12)
+
+
+def test_free_sphere_operators_and_fp32_dc(oracle):
+    # the operator pipeline (UpdateObstacles runs the rigid update) and the
+    # FP32-DC form of a fully free sphere
+    sim, orc = free_sphere_pair(oracle, (False, False, False), (False, False, False))
+    dt = 2e-3
+    for op in sim.pipeline:
+        if op.getName() != "ComputeForces":
+            op(dt)
+        orc.operator(op.getName(), dt)
+    assert np.allclose(sim.obstacle_state()["transVel"], orc.stats()["transVel"], rtol=0, atol=1e-11)
+    for a, b in zip(sim.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < 1e-11
+    sim32, orc = free_sphere_pair(oracle, (False, False, False), (False, False, False), precision="fp32_dc",
+                                  dc_max_iter=8)
+    for s in range(4):
+        dt = orc.calc_max_timestep()
+        sim32.timestep(dt)
+        orc.timestep(dt)
+    st, ob = sim32.obstacle_state(), orc.stats()
+    assert np.allclose(st["transVel"], ob["transVel"], rtol=0, atol=1e-5)
+    assert np.allclose(st["angVel"], ob["angVel"], rtol=0, atol=1e-4)
+    for a, b in zip(sim32.velocity(), orc.velocity()):
+        assert rel_l2(a, b) < 1e-5
