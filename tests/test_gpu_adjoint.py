@@ -220,16 +220,26 @@ def test_adjoint_rollout_taylor_green_128(oracle):
         x = u0.to(dtype).clone().requires_grad_(True)
         loss(sim, x).backward()
         grads[name] = x.grad.double()
-    worst = {"fp64": 0.0, "fp32": 0.0}
-    d0 = None
-    for seed in range(100, 116):
-        d = to_dev(random_solenoidal(cells, seed, lambda k: np.ones_like(k), kmax=8, amplitude=1.0), torch.float64)
-        if d0 is None:
-            d0 = d
+    # the 16 directions through the replica map (one process here: all local;
+    # under torch.distributed each GPU takes every world-th direction)
+    from cubismup_3d_b200 import replicas
+
+    def direction(i):
+        return to_dev(random_solenoidal(cells, 100 + i, lambda k: np.ones_like(k), kmax=8, amplitude=1.0),
+                      torch.float64)
+
+    def central(i):
+        d = direction(i)
         with torch.no_grad():
-            fd = (loss(s64, u0 + eps * d) - loss(s64, u0 - eps * d)).item() / (2 * eps)
+            return (loss(s64, u0 + eps * d) - loss(s64, u0 - eps * d)).item() / (2 * eps)
+
+    fds = replicas.distributed_map(central, 16)
+    worst = {"fp64": 0.0, "fp32": 0.0}
+    for i, fd in enumerate(fds):
+        d = direction(i)
         for name, g in grads.items():
             worst[name] = max(worst[name], abs(float((g * d).sum()) - fd) / abs(fd))
+    d0 = direction(0)
     assert worst["fp64"] <= 1e-4 and worst["fp32"] <= 1e-4, worst
     # FP64 tangent-linear rollout of the oracle along the first direction
     orc = make_oracle(oracle, cells, ext)
