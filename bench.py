@@ -294,9 +294,32 @@ def adjoint_cost(torch, sim, stream, reps: int = 10) -> dict:
     torch.cuda.synchronize()
     fwd = ev[0].elapsed_time(ev[1]) / reps
     adj = ev[2].elapsed_time(ev[3]) / reps
-    return {"forward_ms_per_step": fwd, "adjoint_ms_per_step": adj, "adjoint_over_forward": adj / fwd,
-            "note": "adjoint step = stage-1 recompute + adjoint projection + two transposed RK stages; "
-                    "a checkpointed rollout adds one forward recompute per step"}
+    out = {"forward_ms_per_step": fwd, "adjoint_ms_per_step": adj, "adjoint_over_forward": adj / fwd,
+           "note": "adjoint step = stage-1 recompute + adjoint projection + two transposed RK stages"}
+    # whole differentiable rollouts (torch.autograd through adjoint.rollout):
+    # forward and backward time per step, the checkpoint interval chosen by the
+    # memory budget (every state kept: no recomputation) and K = 8 (one
+    # forward recompute per step in the backward)
+    from cubismup_3d_b200.adjoint import _auto_interval, rollout
+    n = 16
+    u0 = sim.velocity_raw()
+    for label, K in (("auto", None), ("K8", 8)):
+        for rep in range(2):  # the first pass allocates and captures
+            x = u0.clone().requires_grad_(True)
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            torch.cuda.synchronize()
+            e[0].record(stream)
+            loss = (rollout(sim, x, [dt] * n, checkpoint_every=K).double() ** 2).sum()
+            e[1].record(stream)
+            loss.backward()
+            e[2].record(stream)
+            torch.cuda.synchronize()
+        f_ms, b_ms = e[0].elapsed_time(e[1]) / n, e[1].elapsed_time(e[2]) / n
+        out[f"rollout_{label}"] = {"steps": n, "checkpoint_every": K if K else _auto_interval(sim, n),
+                                   "forward_ms_per_step": f_ms, "backward_ms_per_step": b_ms,
+                                   "backward_over_forward": b_ms / f_ms,
+                                   "backward_over_forward_step": b_ms / fwd}
+    return out
 
 
 SPHERE_CELLS = (256, 128, 128)

@@ -11,7 +11,12 @@ Memory: the forward keeps one velocity checkpoint every ``checkpoint_every``
 steps; the backward walks the segments from the last to the first, restores
 the segment's checkpoint, recomputes the segment's states forward and applies
 the adjoint steps in reverse. Peak extra memory is (n/K + K) velocity fields
-for n steps and checkpoint interval K, so long rollouts fit in HBM.
+for n steps and checkpoint interval K, so long rollouts fit in HBM. By default
+(``checkpoint_every=None``) K is the smallest interval whose checkpoints fit
+in half of the device's free memory: K = 1 (every state kept, no
+recomputation, the backward is the adjoint steps alone) whenever the rollout
+fits, which on a 180 GB device covers the benchmark rollouts with room to
+spare.
 
 The forward and the recomputation advance the handle with ``Simulation._advance``
 (the step and the clock only), so a rollout writes no restart dump and no
@@ -32,12 +37,30 @@ velocity, the characteristic function chi and the sphere's target velocity
 from __future__ import annotations
 
 import ctypes as C
-from typing import Sequence
+from typing import Optional, Sequence
 
 import torch
 
 from . import _lib as L
 from .simulation import Simulation
+
+
+def checkpoint_interval(nsteps: int, state_bytes: int, budget_bytes: int) -> int:
+    """The smallest checkpoint interval K whose peak extra memory
+    (ceil(n / K) checkpoints plus K - 1 recomputed states) fits the budget."""
+    if nsteps <= 0:
+        return 1
+    for K in range(1, nsteps + 1):
+        need = (-(-nsteps // K) + (K - 1 if K > 1 else 0)) * state_bytes
+        if need <= budget_bytes:
+            return K
+    raise MemoryError(f"a {nsteps}-step rollout of {state_bytes}-byte states does not fit {budget_bytes} bytes")
+
+
+def _auto_interval(sim: Simulation, nsteps: int) -> int:
+    free, _ = torch.cuda.mem_get_info(sim.sd.device)
+    state = 3 * int(torch.tensor([], dtype=sim.storage_dtype).element_size()) * int(torch.Size(sim.shape).numel())
+    return checkpoint_interval(nsteps, state, free // 2)
 
 
 class Rollout(torch.autograd.Function):
@@ -49,7 +72,7 @@ class Rollout(torch.autograd.Function):
             raise ValueError("rollout: the discrete adjoint does not support obstacles")
         if sim.forcing:
             raise ValueError("rollout: spectral forcing has no discrete adjoint")
-        K = int(checkpoint_every)
+        K = _auto_interval(sim, len(dts)) if checkpoint_every is None else int(checkpoint_every)
         if K < 1:
             raise ValueError("checkpoint_every must be >= 1")
         dts = [float(d) for d in dts]
@@ -75,21 +98,23 @@ class Rollout(torch.autograd.Function):
         n = len(dts)
         for seg in reversed(range(len(ctx.ckpts))):
             s0, s1 = seg * K, min(n, seg * K + K)
-            _set_clock(sim, ctx.clock[0] + s0, ctx.clock[1] + sum(dts[:s0]))
-            sim.set_velocity_raw(ctx.ckpts[seg])
             states = [ctx.ckpts[seg]]
-            for s in range(s0, s1 - 1):
-                sim._advance(dts[s])
-                states.append(sim.velocity_raw())
+            if s1 - s0 > 1:  # recompute the segment's states from its checkpoint
+                _set_clock(sim, ctx.clock[0] + s0, ctx.clock[1] + sum(dts[:s0]))
+                sim.set_velocity_raw(ctx.ckpts[seg])
+                for s in range(s0, s1 - 1):
+                    sim._advance(dts[s])
+                    states.append(sim.velocity_raw())
             for s in reversed(range(s0, s1)):
                 sim.adjoint_step(states[s - s0], dts[s], lam)
+            ctx.ckpts[seg] = None  # its memory goes back as the backward proceeds
         _set_clock(sim, *ctx.end_clock)
         ctx.ckpts = None
         return lam.to(ctx.in_dtype), None, None, None
 
 
 def obstacle_gradients(sim: Simulation, u0: torch.Tensor, dts: Sequence[float], w_force, grad_uT=None,
-                       checkpoint_every: int = 8):
+                       checkpoint_every: Optional[int] = None):
     """Gradients of J = <grad_uT, u_T> + sum_n w_force . F_n over ``len(dts)``
     steps of ``sim`` (which has the sphere) from ``u0`` (3, nz, ny, nx):
     returns (dJ/du0, dJ/dchi, dJ/dU) as CUDA tensors (storage dtype, FP64 of the
@@ -98,7 +123,7 @@ def obstacle_gradients(sim: Simulation, u0: torch.Tensor, dts: Sequence[float], 
         raise ValueError("obstacle_gradients: the simulation has no obstacle")
     if sim.forcing:
         raise ValueError("obstacle_gradients: spectral forcing has no discrete adjoint")
-    K = int(checkpoint_every)
+    K = _auto_interval(sim, len(dts)) if checkpoint_every is None else int(checkpoint_every)
     if K < 1:
         raise ValueError("checkpoint_every must be >= 1")
     dts = [float(d) for d in dts]
@@ -119,14 +144,16 @@ def obstacle_gradients(sim: Simulation, u0: torch.Tensor, dts: Sequence[float], 
     g_vel = torch.zeros(3, dtype=torch.float64, device=dev)
     for seg in reversed(range(len(ckpts))):
         s0, s1 = seg * K, min(n, seg * K + K)
-        _set_clock(sim, clock[0] + s0, clock[1] + sum(dts[:s0]))
-        sim.set_velocity_raw(ckpts[seg])
         states = [ckpts[seg]]
-        for s in range(s0, s1 - 1):
-            sim._advance(dts[s])
-            states.append(sim.velocity_raw())
+        if s1 - s0 > 1:  # recompute the segment's states from its checkpoint
+            _set_clock(sim, clock[0] + s0, clock[1] + sum(dts[:s0]))
+            sim.set_velocity_raw(ckpts[seg])
+            for s in range(s0, s1 - 1):
+                sim._advance(dts[s])
+                states.append(sim.velocity_raw())
         for s in reversed(range(s0, s1)):
             sim.adjoint_step_obstacle(states[s - s0], dts[s], lam, w_force, g_chi, g_vel)
+        ckpts[seg] = None
     _set_clock(sim, *end_clock)
     return lam, g_chi, g_vel, forces
 
@@ -136,9 +163,12 @@ def _set_clock(sim: Simulation, step: int, time: float):
     sim.step, sim.time = int(step), float(time)
 
 
-def rollout(sim: Simulation, u0: torch.Tensor, dts: Sequence[float], checkpoint_every: int = 8) -> torch.Tensor:
+def rollout(sim: Simulation, u0: torch.Tensor, dts: Sequence[float],
+            checkpoint_every: Optional[int] = None) -> torch.Tensor:
     """Differentiable ``len(dts)``-step rollout of ``sim`` from ``u0`` (3, nz, ny, nx).
 
-    The handle's velocity is left at the final state after the forward; after a
-    backward it holds an intermediate state of the recomputation."""
-    return Rollout.apply(u0, sim, list(dts), int(checkpoint_every))
+    ``checkpoint_every``: the checkpoint interval K (None: the smallest that
+    fits half of the free device memory). The handle's velocity is left at the
+    final state after the forward; after a backward with K > 1 it holds an
+    intermediate state of the recomputation."""
+    return Rollout.apply(u0, sim, list(dts), checkpoint_every)

@@ -81,3 +81,14 @@ def test_sphere_arguments_like_bindings():
         cup.Sphere()
     st = s.to_struct()
     assert list(st.bForcedInSimFrame) == [1, 1, 1]
+
+
+def test_rollout_checkpoint_interval():
+    # the smallest checkpoint interval whose checkpoints plus one recomputed
+    # segment fit the memory budget; 1 (keep every state) when all fit
+    from cubismup_3d_b200.adjoint import checkpoint_interval
+    assert checkpoint_interval(64, 25_000_000, 10 ** 12) == 1
+    assert checkpoint_interval(64, 25_000_000, 500_000_000) == 4  # 16 checkpoints + 3 recomputed states
+    assert checkpoint_interval(100, 50_000_000, 10 ** 9) == 8
+    with pytest.raises(MemoryError):
+        checkpoint_interval(100, 50_000_000, 10 ** 6)
