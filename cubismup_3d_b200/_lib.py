@@ -113,6 +113,8 @@ SIGNATURES = {
     "cup_poisson_buffer": (C.c_int, [_H, C.POINTER(C.c_void_p), C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "cup_poisson_reset": (C.c_int, [_H]),
     "cup_set_rhs": (C.c_int, [_H, C.c_void_p, C.c_int]),
+    "cup_set_spectral_window": (C.c_int, [_H, C.c_int, C.c_int]),
+    "cup_poisson_pass": (C.c_int, [_H, C.c_void_p, C.c_int]),
     "cup_pressure_projection": (C.c_int, [_H, C.c_double, C.POINTER(CupSolveStats)]),
     "cup_penalize": (C.c_int, [_H, C.c_double, _dp]),
     "cup_step": (C.c_int, [_H, C.c_double, C.POINTER(CupStepStats)]),

@@ -778,6 +778,9 @@ struct cup_handle {
   float2* tw32[3] = {nullptr, nullptr, nullptr};
   double *cosx = nullptr, *cosy = nullptr, *cosz = nullptr;
   double norm_factor = 0;
+  // spectral window of a y-split pencil of a decomposed grid (cup_set_spectral_window):
+  // the global y length of the cos table and of the null modes, and this handle's first y
+  int spec_ny = 0, spec_y0 = 0;
   // obstacle
   bool has_sphere = false;
   cup_sphere sphere{};  // host mirror; sphere.position follows Obstacle::update
@@ -1116,7 +1119,7 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   const int ntx = H->nx / W;
   const int ntiles = ntx * (AXIS == 1 ? H->nz : H->ny);
   const int grid = std::min(ntiles, bpsm * H->num_sms);
-  SpectralParams sp{H->cosx, H->cosy, H->cosz, H->norm_factor, H->nx, H->ny, H->nz};
+  SpectralParams sp{H->cosx, H->cosy, H->cosz, H->norm_factor, H->nx, H->spec_ny, H->nz, H->spec_y0};
   const bool inv64 = H->fp32 && sizeof(R) == 8;  // FP64 inverse pass of a mixed-precision correction solve
   const char* name = AXIS == 1 ? (inv64 ? "dht_y_f64" : "dht_y")
                                : (sizeof(RIN) < sizeof(R) ? "dht_z_solve_mixed" : "dht_z_solve");
@@ -2410,6 +2413,8 @@ int cup_create(const cup_config* cfg, cup_handle** out) {
     const size_t gsize[3] = {(size_t)N[0], (size_t)N[1], (size_t)N[2]};
     const double h = H->h;
     H->norm_factor = 4 / (gsize[0] * h * gsize[1] * gsize[2]);
+    H->spec_ny = H->ny;
+    H->spec_y0 = 0;
     double** cs[3] = {&H->cosx, &H->cosy, &H->cosz};
     for (int d = 0; d < 3; ++d) {
       const long nK = (long)gsize[d];
@@ -2823,6 +2828,36 @@ int cup_poisson_reset(cup_handle* H) {
   REQUIRE_H(H);
   CK(cudaMemsetAsync(H->rhs, 0, H->n * sizeof(double), H->stream));
   return CUP_OK;
+}
+
+int cup_set_spectral_window(cup_handle* H, int y0, int ny_global) {
+  REQUIRE_H(H);
+  if (ny_global < H->ny || !is_pow2(ny_global) || y0 < 0 || y0 + H->ny > ny_global || y0 % H->ny)
+    return fail(H, CUP_ERR_ARG, "spectral window: need 0 <= y0, y0 + ny <= ny_global (a power of two), y0 a multiple of ny");
+  std::vector<double> c(ny_global);
+  const double wFac = 4 * M_PI / (long)ny_global;
+  for (long i = 0; i < ny_global; ++i) c[i] = std::cos(wFac * i);
+  double* d = nullptr;
+  CK(cudaMalloc(&d, ny_global * sizeof(double)));
+  CK(cudaMemcpy(d, c.data(), ny_global * sizeof(double), cudaMemcpyHostToDevice));
+  cudaFree(H->cosy);
+  H->cosy = d;
+  H->spec_ny = ny_global;
+  H->spec_y0 = y0;
+  H->norm_factor = 4 / ((double)H->nx * H->h * (double)ny_global * (double)H->nz);
+  drop_graph(H);
+  return CUP_OK;
+}
+
+int cup_poisson_pass(cup_handle* H, double* buf, int pass) {
+  REQUIRE_H(H);
+  if (!buf) return fail(H, CUP_ERR_ARG, "null buffer");
+  switch (pass) {
+    case 0: return launch_rows_pipe<double>(H, "dht_x", buf, buf, nullptr);
+    case 1: return launch_cols<double, 1, false>(H, buf, buf, nullptr);
+    case 2: return launch_cols<double, 2, true>(H, buf, buf, nullptr);
+    default: return fail(H, CUP_ERR_ARG, "pass must be 0 (x), 1 (y) or 2 (z with the spectral divide)");
+  }
 }
 
 int cup_poisson_solve(cup_handle* H, cup_solve_stats* stats) {

@@ -759,10 +759,11 @@ __global__ void __launch_bounds__(256, 2) k_dht_rows_pipe(const R* __restrict__ 
 // cos(4 pi k / N) evaluated on the host exactly as the reference does.
 struct SpectralParams {
   const double* cx;
-  const double* cy;
+  const double* cy;  // cos(4 pi ky / ny) for the global ky
   const double* cz;
   double norm_factor;
-  int nx, ny, nz;
+  int nx, ny, nz;  // ny: the global line length in y
+  int y0;          // global y index of the handle's first y (a slab of a decomposed grid; 0 otherwise)
 };
 
 // Scaler of the z pass: the factor of column (kx, ky) at z index k,
@@ -783,10 +784,11 @@ struct ZColumnFactor {
 
 __device__ __forceinline__ ZColumnFactor z_column_factor(const SpectralParams& sp, int kx, int ky) {
   ZColumnFactor f;
-  f.cxy = __ldg(sp.cx + kx) + __ldg(sp.cy + ky);
+  const int gy = sp.y0 + ky;
+  f.cxy = __ldg(sp.cx + kx) + __ldg(sp.cy + gy);
   f.cz = sp.cz;
   f.nf = sp.norm_factor;
-  f.null_col = (kx == 0 || kx == sp.nx / 2) && (ky == 0 || ky == sp.ny / 2);
+  f.null_col = (kx == 0 || kx == sp.nx / 2) && (gy == 0 || gy == sp.ny / 2);
   return f;
 }
 

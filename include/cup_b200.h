@@ -200,6 +200,23 @@ int cup_poisson_solve(struct cup_handle* h, cup_solve_stats* stats);
 int cup_poisson_buffer(struct cup_handle* h, double** data, size_t strides[3], size_t* data_size);
 /* PoissonSolver::reset (source/poisson/PoissonSolver.cpp:132-135): zeroes the buffer. */
 int cup_poisson_reset(struct cup_handle* h);
+/* ---- the Poisson solve of a z-slab decomposed grid (PoissonSolverPeriodic
+ * over MPI ranks, source/poisson/PoissonSolverPeriodic.cpp:94-121: FFTW-MPI
+ * slabs with a transposed spectrum) ----
+ * The solve p = H(f . H(b)) is separable: on a rank's z-slab (a handle of
+ * nx x ny x nz/G cells) the x and y passes are local; after an all-to-all that
+ * makes y-pencils (a handle of nx x ny/G x nz cells) the z pass with the
+ * spectral divide is local too; a second all-to-all and the y and x passes
+ * finish. cubismup_3d_b200/slab.py orchestrates it over torch.distributed. */
+/* Makes the handle's z pass that of the pencil y in [y0, y0 + ny) of a grid
+ * ny_global cells long in y (the global cos table, null modes and 1/N). */
+int cup_set_spectral_window(struct cup_handle* h, int y0, int ny_global);
+/* One FP64 pass of the Poisson solve, in place on the device array buf of the
+ * handle's nx*ny*nz cells ([z][y][x]): pass 0 the Hartley transform of every
+ * x row, 1 of every y column, 2 of every z column with the spectral divide of
+ * PoissonSolverPeriodic::_solve between the forward and the inverse transform.
+ * Stream-ordered on the handle's stream, no host synchronisation. */
+int cup_poisson_pass(struct cup_handle* h, double* buf, int pass);
 /* Writes the Poisson buffer (the mirror of cup_get_rhs); FP64, nx*ny*nz values. */
 int cup_set_rhs(struct cup_handle* h, const double* rhs, int where);
 /* KernelGradP (source/operators/PressureProjection.cpp:38-50) */
