@@ -467,23 +467,35 @@ def test_sphere_adjoint_256x128x128_100_steps():
         grads[name] = (lam.double().cpu().numpy(), g_chi.cpu().numpy(), g_vel.cpu().numpy())
         assert forces[-1][0] > 0  # drag on the sphere
     rng = np.random.default_rng(31)
-    interface = (chi0 > 1e-3) & (chi0 < 1 - 1e-3)
-    worst = {"fp64": 0.0, "fp32": 0.0}
+    # chi directions on the interface cells (0 < chi < 1) whose six neighbours
+    # are all surface cells of the RHS correction (non-zero central chi
+    # differences): the sphere sits on the grid's symmetry planes, where cells
+    # with cancelling differences border the interface, and perturbing their
+    # neighbours would add them to the surface set (a kink the linearisation,
+    # which freezes that set, does not see)
+    grad2 = sum((np.roll(chi0, -1, a) - np.roll(chi0, 1, a)) ** 2 for a in range(3))
+    surf = grad2 > 0
+    nb_surf = np.ones_like(surf)
+    for a in range(3):
+        nb_surf &= np.roll(surf, 1, a) & np.roll(surf, -1, a)
+    interface = (chi0 > 1e-3) & (chi0 < 1 - 1e-3) & nb_surf
+    assert interface.sum() > 1000
+    err = {"fp64": {}, "fp32": {}}
     for k in range(8):
         dc = np.where(interface, rng.standard_normal(chi0.shape), 0.0)
         e = 1e-6
         fd = (J(chi=chi0 + e * dc) - J(chi=chi0 - e * dc)) / (2 * e)
         for name, (_, gc, _) in grads.items():
-            worst[name] = max(worst[name], abs(float(np.sum(gc * dc)) - fd) / abs(fd))
+            err[name][f"chi{k}"] = abs(float(np.sum(gc * dc)) - fd) / abs(fd)
     e = 1e-6
     fd = (J(vel=vel0 + [e, 0, 0]) - J(vel=vel0 - [e, 0, 0])) / (2 * e)
     for name, (_, _, gv) in grads.items():
-        worst[name] = max(worst[name], abs(gv[0] - fd) / abs(fd))
+        err[name]["U"] = abs(gv[0] - fd) / abs(fd)
     du = torch.from_numpy(np.stack(random_solenoidal(s64.shape[::-1], 3, lambda k: np.exp(-(k / 2.0) ** 2),
                                                       rms=1.0))).cuda()
     e = 1e-6
     fd = (J(du=du, eps=e) - J(du=du, eps=-e)) / (2 * e)
     for name, (gu, _, _) in grads.items():
-        worst[name] = max(worst[name], abs(float(np.sum(gu * du.cpu().numpy())) - fd) / abs(fd))
-    assert worst["fp64"] <= 1e-4, worst
-    assert worst["fp32"] <= 1e-3, worst
+        err[name]["u0"] = abs(float(np.sum(gu * du.cpu().numpy())) - fd) / abs(fd)
+    assert max(err["fp64"].values()) <= 1e-4, err
+    assert max(err["fp32"].values()) <= 1e-3, err
