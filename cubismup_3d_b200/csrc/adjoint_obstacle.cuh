@@ -16,7 +16,8 @@
 // returns dJ/du**, adds dJ/dchi and dJ/dU (the penalization target velocity U,
 // the sphere's imposed translation, with uinf held fixed), and applies the
 // transpose of the RHS map M: b0 -> b2. Linearised with the surface set and the
-// sign of corr frozen (they only change where a surface b1 or S crosses zero).
+// sign of corr frozen (they only change where a surface b1 or S crosses zero;
+// a surface cell whose b1 is exactly 0 takes the mean of the two sides).
 // M db0 = m db0 - sigma b1_s dcorr, dcorr = c . db0, so
 //   M^T q = m q - sigma (sum_s b1_s q_s) c,
 //   m = (1 - chi)(1 - sigma corr [s]),  c_j = -chi_j / D - sigma S / D^2 (1 - chi_j) [s_j],
@@ -146,11 +147,19 @@ __global__ void k_adj_rhs_apply(double* q, const double* b0, const T* chi, Box b
     const size_t o = gidx(x, y, z, nx, ny);
     const double X = chi[o], B0 = b0[o], Q = q[o];
     const double b1 = B0 - X * B0;
-    const bool s = rs.sigma != 0 && (rs.sigma > 0 ? b1 > 0 : b1 < 0) && chi_surface(chi, x, y, z, nx, ny, nz);
-    const double fs = s ? 1 - rs.sigma * rs.corr : 1.0;
+    // weight of the cell in the corrected surface set: 1 inside it; 1/2 for
+    // a surface b1 of exactly 0 that a perturbation can move (chi < 1), the
+    // mean of the two sides' slopes, which central differences see (a flow
+    // started from rest has such cells in its first step)
+    double ws = 0.0;
+    if (rs.sigma != 0 && chi_surface(chi, x, y, z, nx, ny, nz)) {
+      if (rs.sigma > 0 ? b1 > 0 : b1 < 0) ws = 1.0;
+      else if (b1 == 0 && X < 1) ws = 0.5;
+    }
+    const double fs = 1 - ws * rs.sigma * rs.corr;
     const double sig = (double)rs.sigma;
-    const double cj = -X * invD - sig * SD2 * (1 - X) * (s ? 1.0 : 0.0);
-    const double ej = -B0 * invD + sig * SD2 * B0 * (s ? 1.0 : 0.0);
+    const double cj = -X * invD - sig * SD2 * (1 - X) * ws;
+    const double ej = -B0 * invD + sig * SD2 * B0 * ws;
     q[o] = (1 - X) * fs * Q - sig * sq * cj;
     g_chi[o] += kappa * (-B0 * Q * fs - sig * sq * ej);
   }

@@ -1110,7 +1110,7 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   constexpr bool WIDEN = sizeof(RIN) < sizeof(R);
   const size_t smem = (size_t)NB * N * W * sizeof(R) + FFTPlan<M>::table_len() * sizeof(typename Cplx<R>::T) +
                       (WIDEN ? FFTPlan<M>::table_len() * sizeof(typename Cplx<RIN>::T) : 0) +
-                      NB * sizeof(uint64_t) + 128;
+                      NB * sizeof(uint64_t) + (DIVIDE ? (M / 2 + 1) * sizeof(double) : 0) + 128;
   auto kern = k_dht_cols_pipe<M, R, AXIS, DIVIDE, W, NB, RIN, T8>;
   const int threads = W * TPL;
   int bpsm = 0;
@@ -1483,7 +1483,7 @@ int launch_finalize_residual(cup_handle* H, const double* partials, int stride, 
   const double inv_class = 8.0 / (double)H->n;
   return launch_named(H, "finalize_residual", [&]() -> int {
     klaunch(H, k_finalize_residual, 1, 256, 0, partials, stride, grid, H->dstate, dc_tol(H), k, dc_min_iter(H),
-                                                  dc_max_iter(H), inv_class);
+            dc_max_iter(H), inv_class);
     CKL();
     return CUP_OK;
   });
@@ -1579,7 +1579,7 @@ int do_poisson_dc(cup_handle* H) {
     {
       int rc_ = launch_named(H, "finalize_residual", [&]() -> int {
         klaunch(H, k_finalize_residual, 1, 256, 0, partial(H, P_RES), 18, grid, H->dstate, tol, k, min_iter, max_iter,
-                                                      inv_class);
+                inv_class);
         CKL();
         return CUP_OK;
       });

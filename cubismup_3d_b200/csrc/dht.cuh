@@ -265,6 +265,7 @@ __device__ __forceinline__ void fft_stage(const In& in, const Out& out, const R2
 
 // No scaling after the forward transform.
 struct NoScale {
+  using type = double;
   static constexpr bool kOn = false;
   __device__ double operator()(int) const { return 1.0; }
 };
@@ -286,12 +287,16 @@ template <int M, typename R, typename R2, class AccO, class Scale>
 __device__ __forceinline__ void split_task(const AccO& ao, int l, int k, R2 A, R2 B, R2 W, const Scale& scale) {
   using RO = typename AccO::elem;
   constexpr int N = 2 * M;
+  using SF = typename Scale::type;  // the factor's type, in which the product is formed
   if (k == 0) {
-    RO h0 = (RO)(A.x + A.y), hM = (RO)(A.x - A.y);
+    RO h0, hM;
     if constexpr (Scale::kOn) {
-      const double f = scale(0);
-      h0 = (RO)((double)h0 * f);
-      hM = (RO)((double)hM * f);
+      const SF f = scale(0);
+      h0 = (RO)((SF)(A.x + A.y) * f);
+      hM = (RO)((SF)(A.x - A.y) * f);
+    } else {
+      h0 = (RO)(A.x + A.y);
+      hM = (RO)(A.x - A.y);
     }
     ao.str(l, 0, h0);
     ao.str(l, M, hM);
@@ -301,13 +306,18 @@ __device__ __forceinline__ void split_task(const AccO& ao, int l, int k, R2 A, R
     const R Or = (A.y + B.y) * half, Oi = (B.x - A.x) * half;
     const R Xr = Er + (W.x * Or - W.y * Oi), Xi = Ei + (W.x * Oi + W.y * Or);
     const R X2r = Er - W.x * Or + W.y * Oi, X2i = -Ei + W.x * Oi + W.y * Or;
-    RO hk = (RO)(Xr - Xi), hNk = (RO)(Xr + Xi), hMk = (RO)(X2r - X2i), hMpk = (RO)(X2r + X2i);
+    RO hk, hNk, hMk, hMpk;
     if constexpr (Scale::kOn) {
-      const double f = scale(k);
-      hk = (RO)((double)hk * f);
-      hNk = (RO)((double)hNk * f);
-      hMk = (RO)((double)hMk * f);
-      hMpk = (RO)((double)hMpk * f);
+      const SF f = scale(k);
+      hk = (RO)((SF)(Xr - Xi) * f);
+      hNk = (RO)((SF)(Xr + Xi) * f);
+      hMk = (RO)((SF)(X2r - X2i) * f);
+      hMpk = (RO)((SF)(X2r + X2i) * f);
+    } else {
+      hk = (RO)(Xr - Xi);
+      hNk = (RO)(Xr + Xi);
+      hMk = (RO)(X2r - X2i);
+      hMpk = (RO)(X2r + X2i);
     }
     ao.str(l, k, hk);
     ao.str(l, N - k, hNk);
@@ -442,7 +452,9 @@ __device__ __forceinline__ void fft_stages(const Acc& a, const P& pad, const typ
 // Meant for column tiles (ColLines), where stage A's 16-strided writes fall in
 // different columns across a warp. `ao` may alias `a` (see dht_post_to).
 // Stage A writes to `pa` and stage B reads from it (column tiles: `a` itself).
-template <typename R, class Acc, class PAcc, class AccO, class Scale>
+// PA_APART: `pa` shares no bytes with `a`, so stage A writes without waiting
+// for every thread's reads (one block barrier less).
+template <typename R, bool PA_APART = false, class Acc, class PAcc, class AccO, class Scale>
 __device__ __forceinline__ void dht128_t8_to(const Acc& a, const PAcc& pa, const AccO& ao,
                                              const typename Cplx<R>::T* tw, int l, int t, bool active,
                                              const Scale& scale) {
@@ -458,7 +470,7 @@ __device__ __forceinline__ void dht128_t8_to(const Acc& a, const PAcc& pa, const
     for (int r = 0; r < 16; ++r) v[r] = a.ld(l, t + 8 * r);
     DFT<16, R2>::run(v);
   }
-  __syncthreads();
+  if constexpr (!PA_APART) __syncthreads();
   if (active) {
 #pragma unroll
     for (int r = 0; r < 16; ++r) pa.st(l, 16 * t + r, v[r]);
@@ -769,24 +781,37 @@ struct SpectralParams {
 // Scaler of the z pass: the factor of column (kx, ky) at z index k,
 // nf / (2 (cos_x + cos_y + cos_z) - 6), zero on the 8 null modes (kx in
 // {0, Nx/2}, ky in {0, Ny/2}, kz in {0, Nz/2}); the z indices 0 and Nz/2 are
-// both handled by task k = 0.
+// both handled by task k = 0. cz: cos_z[0..Nz/4] (the tasks' k range), staged
+// in shared memory by the pass. SF = double divides exactly (the direct FP64
+// solve). SF = float is the correction solve of the defect-correction loop:
+// the denominator is still formed in FP64 (it cancels to 2 (1 - cos(4 pi/N))
+// at the lowest modes), then the FP32 quotient scales the FP32 forward
+// transform's output. A factor with relative error e changes each mode of the
+// correction by the factor 1 + e, which leaves a residual of relative size e:
+// the same order as the FP32 forward transform's own rounding.
+template <typename SF>
 struct ZColumnFactor {
+  using type = SF;
   double cxy;  // cos_x[kx] + cos_y[ky]
   const double* cz;
   double nf;
   bool null_col;
   static constexpr bool kOn = true;
-  __device__ __forceinline__ double operator()(int k) const {
-    if (k == 0 && null_col) return 0.0;
-    return nf / (2 * (cxy + __ldg(cz + k)) - 6);
+  __device__ __forceinline__ SF operator()(int k) const {
+    if (k == 0 && null_col) return (SF)0;
+    const double den = 2 * (cxy + cz[k]) - 6;
+    if constexpr (sizeof(SF) == 4) return __fdividef((float)nf, (float)den);
+    else return nf / den;
   }
 };
 
-__device__ __forceinline__ ZColumnFactor z_column_factor(const SpectralParams& sp, int kx, int ky) {
-  ZColumnFactor f;
+template <typename SF>
+__device__ __forceinline__ ZColumnFactor<SF> z_column_factor(const SpectralParams& sp, const double* cz, int kx,
+                                                             int ky) {
+  ZColumnFactor<SF> f;
   const int gy = sp.y0 + ky;
   f.cxy = __ldg(sp.cx + kx) + __ldg(sp.cy + gy);
-  f.cz = sp.cz;
+  f.cz = cz;
   f.nf = sp.norm_factor;
   f.null_col = (kx == 0 || kx == sp.nx / 2) && (gy == 0 || gy == sp.ny / 2);
   return f;
@@ -827,6 +852,7 @@ __global__ void __launch_bounds__(W * (T8 ? 8 : M / 8)) k_dht_cols_pipe(const __
   R2* tw = reinterpret_cast<R2*>(tiles + (size_t)NB * N * W);
   RI2* tw_in = reinterpret_cast<RI2*>(tw + TL);  // (WIDEN only)
   uint64_t* bar = reinterpret_cast<uint64_t*>(tw_in + (WIDEN ? TL : 0));
+  double* czs = reinterpret_cast<double*>(bar + NB);  // cos_z[0..M/2] (DIVIDE)
   const int tid = threadIdx.x;
   const int my = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   if (tid == 0) {
@@ -854,6 +880,8 @@ __global__ void __launch_bounds__(W * (T8 ? 8 : M / 8)) k_dht_cols_pipe(const __
     for (; issued < min(NB - 1, my); ++issued) issue(issued);
   load_table(tw, tw_g, TL);
   if constexpr (WIDEN) load_table(tw_in, tw_in_g, TL);
+  if constexpr (DIVIDE)
+    for (int i = tid; i <= M / 2; i += blockDim.x) czs[i] = sp.cz[i];
   __syncthreads();
   const int l = tid % W, t = tid / W;
   const bool active = t < TPL;
@@ -878,14 +906,17 @@ __global__ void __launch_bounds__(W * (T8 ? 8 : M / 8)) k_dht_cols_pipe(const __
         ColLines<RIN> An{reinterpret_cast<RIN*>(reinterpret_cast<unsigned char*>(tile) +
                                                 (size_t)N * W * (sizeof(R) - sizeof(RIN))),
                          W};
+        // the lower part of the buffer is free until the widened output:
+        // stage A of the narrow transform writes there
+        ColLines<RIN> Lo{reinterpret_cast<RIN*>(tile), W};
         if constexpr (DIVIDE) {
-          dht128_t8_to<RIN>(An, An, A, tw_in, l, t, active, z_column_factor(sp, x0 + l, other));
+          dht128_t8_to<RIN, true>(An, Lo, A, tw_in, l, t, active, z_column_factor<RIN>(sp, czs, x0 + l, other));
           dht128_t8_to<R>(A, A, A, tw, l, t, active, NoScale());
         } else {
-          dht128_t8_to<RIN>(An, An, A, tw_in, l, t, active, NoScale());
+          dht128_t8_to<RIN, true>(An, Lo, A, tw_in, l, t, active, NoScale());
         }
       } else if constexpr (DIVIDE) {
-        dht128_t8_to<R>(A, A, A, tw, l, t, active, z_column_factor(sp, x0 + l, other));
+        dht128_t8_to<R>(A, A, A, tw, l, t, active, z_column_factor<double>(sp, czs, x0 + l, other));
         dht128_t8_to<R>(A, A, A, tw, l, t, active, NoScale());
       } else {
         dht128_t8_to<R>(A, A, A, tw, l, t, active, NoScale());
@@ -896,14 +927,14 @@ __global__ void __launch_bounds__(W * (T8 ? 8 : M / 8)) k_dht_cols_pipe(const __
                        W};
       fft_stages<M, false, RIN>(An, An, tw_in, l, t, active);
       if constexpr (DIVIDE) {
-        dht_tail_to<M, RIN>(An, A, tw_in, l, t, active, z_column_factor(sp, x0 + l, other));
+        dht_tail_to<M, RIN>(An, A, tw_in, l, t, active, z_column_factor<RIN>(sp, czs, x0 + l, other));
         dht_lines<M, false, R>(A, A, tw, l, t, active);
       } else {
         dht_tail_to<M, RIN>(An, A, tw_in, l, t, active, NoScale());
       }
     } else if constexpr (DIVIDE) {
       // forward, spectral divide fused into the even/odd split, inverse
-      dht_lines<M, false, R>(A, A, tw, l, t, active, z_column_factor(sp, x0 + l, other));
+      dht_lines<M, false, R>(A, A, tw, l, t, active, z_column_factor<double>(sp, czs, x0 + l, other));
       dht_lines<M, false, R>(A, A, tw, l, t, active);
     } else {
       dht_lines<M, false, R>(A, A, tw, l, t, active);

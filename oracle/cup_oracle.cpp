@@ -880,15 +880,20 @@ void stage_tangent(OState& S, double dt, const Real* a, const Real* b, const Rea
       const size_t o = D.idx(bx * BS + ix, by * BS + iy, bz * BS + iz);
       Real* outs[3] = {ou, ov, ow};
       const Real* bgs[3] = {bg_u, bg_v, bg_w};
-      auto deriv = [&](const Lab& L, int d, Real av) -> Real {
+      // mean0: the derivative of a up3(a; f) with respect to a, which at a = 0
+      // (a kink: one-sided derivatives up3(+; f) and up3(-; f)) is taken as
+      // the mean of the two, (f-2 - 8 f-1 + 8 f+1 - f+2) / 2, what central
+      // differences see
+      auto deriv = [&](const Lab& L, int d, Real av, bool mean0) -> Real {
         const int ex = d == 0, ey = d == 1, ez = d == 2;
         const Real fm2 = up ? L(ix - 2 * ex, iy - 2 * ey, iz - 2 * ez) : 0, fp2 = up ? L(ix + 2 * ex, iy + 2 * ey, iz + 2 * ez) : 0;
         const Real fm1 = L(ix - ex, iy - ey, iz - ez), fp1 = L(ix + ex, iy + ey, iz + ez), f0 = L(ix, iy, iz);
+        if (up && mean0 && av == 0) return 0.5 * (fm2 - 8 * fm1 + 8 * fp1 - fp2);
         return up ? up3(av, fm2, fm1, f0, fp1, fp2) : fp1 - fm1;
       };
       for (int q = 0; q < 3; ++q) {
         Real dA = 0;
-        for (int d = 0; d < 3; ++d) dA += dadv[d] * deriv(F[q], d, adv[d]) + adv[d] * deriv(T[q], d, adv[d]);
+        for (int d = 0; d < 3; ++d) dA += dadv[d] * deriv(F[q], d, adv[d], true) + adv[d] * deriv(T[q], d, adv[d], false);
         const Lab& G = T[q];
         const Real lap = G(ix,iy+1,iz) + G(ix,iy-1,iz) + G(ix+1,iy,iz) + G(ix-1,iy,iz) + G(ix,iy,iz-1) + G(ix,iy,iz+1) - G(ix,iy,iz) * 6;
         const Real t = G(ix, iy, iz) + facA * dA + facD * lap;

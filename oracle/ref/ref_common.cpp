@@ -27,6 +27,7 @@
 #include <string>
 
 #include "obstacles/ObstacleVector.h"
+#include "utils/BufferedLogger.h"
 #include "obstacles/Sphere.h"
 #include "operators/AdvectionDiffusion.h"
 #include "operators/FluidSolidForces.h"
@@ -260,5 +261,9 @@ int ref_operator(void* h, const char* name, double dt) {
     return 2;
   }
 }
+
+// Writes the reference logger's buffered lines (the obstacle's force and
+// velocity logs) into the working directory now rather than at exit.
+void ref_flush_logs() { cubismup3d::logger.flush(); }
 
 }  // extern "C"

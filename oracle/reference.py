@@ -13,9 +13,11 @@ else on the path is the reference's code. Only tests import this module.
 """
 from __future__ import annotations
 
+import atexit
 import ctypes as C
 import os
 import subprocess
+import tempfile
 
 import numpy as np
 
@@ -52,6 +54,11 @@ def lib():
         L.ref_obstacle.argtypes = [C.c_void_p, dp]
         L.ref_obstacle.restype = C.c_int
         L.ref_set_clock.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double]
+        L.ref_flush_logs.argtypes = []
+        # the reference's logger writes its files (forceValues_0.dat, ...) once
+        # more when the library unloads, after the interpreter's exit handlers:
+        # into a scratch directory, not wherever the process happens to be
+        atexit.register(os.chdir, tempfile.mkdtemp(prefix="cup_ref_logs_"))
         _lib = L
     return _lib
 
@@ -59,6 +66,11 @@ def lib():
 def _p(a: np.ndarray):
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def flush_logs():
+    """Writes the reference's buffered log files into the working directory."""
+    lib().ref_flush_logs()
 
 
 class ReferenceSim:

@@ -338,6 +338,39 @@ def test_obstacle_adjoint_vs_central_differences():
     assert abs(fd - g_vel[0]) <= 1e-5 * abs(g_vel[0]) + 1e-9, ("U", fd, g_vel[0])
 
 
+def test_obstacle_adjoint_zero_cross_velocity_upwind3():
+    """dJ/du0 (upwind3 + RK2, FP64, sphere in a fixed frame) from an initial
+    velocity with only an x component: a_y = a_z = 0 in every cell of the first
+    step, where a up3(a; f) has a kink in the advecting velocity. The adjoint
+    takes the mean of the one-sided derivatives there, the value central
+    differences see. (The x component varies along x, so the first step's RHS
+    is not zero: at a zero RHS the obstacle correction of the RHS is
+    positively homogeneous but not linear, and no gradient exists.)"""
+    import torch
+    from cubismup_3d_b200.adjoint import obstacle_gradients
+    sim = make_obstacle_sim(scheme="upwind3_rk2")
+    rng = np.random.default_rng(17)
+    nz, ny, nx = sim.shape
+    X, Y, Z = np.meshgrid(np.arange(nx) / nx, np.arange(ny) / ny, np.arange(nz) / nz, indexing="ij")
+    # phases keep every factor (and the RHS, its x difference) away from zero on the grid
+    gx = 0.3 * np.sin(2 * np.pi * X + 0.4) * np.cos(2 * np.pi * Y + 0.3) * (1 + 0.5 * np.sin(2 * np.pi * Z))
+    u0 = torch.zeros((3,) + sim.shape, dtype=torch.float64, device="cuda")
+    u0[0] = torch.from_numpy(np.ascontiguousarray(gx.transpose(2, 1, 0))).cuda()
+    g = to_dev([rng.standard_normal(sim.shape) for _ in range(3)], torch.float64)
+    dts = [0.01] * 4
+    w = np.array([1.0 / len(dts), 0.0, 0.0])
+    chi0 = sim.chi()
+    vel0 = np.array(OBST_SPHERE["enforcedVelocity"])
+    lam, _, _, _ = obstacle_gradients(sim, u0, dts, w, grad_uT=g, checkpoint_every=2)
+    d = rng.standard_normal((3,) + sim.shape)
+    dd = torch.from_numpy(d).cuda()
+    eps = 1e-6
+    fd = (obstacle_loss(sim, u0 + eps * dd, g, dts, w, chi0, vel0) -
+          obstacle_loss(sim, u0 - eps * dd, g, dts, w, chi0, vel0)) / (2 * eps)
+    ad = float(np.sum(lam.double().cpu().numpy() * d))
+    assert abs(fd - ad) <= 1e-6 * abs(ad) + 1e-9, ("u0", fd, ad)
+
+
 def test_obstacle_adjoint_fp32_tracks_fp64():
     """The FP32-storage obstacle adjoint against the FP64 one (same gradients to
     FP32 accuracy)."""
@@ -421,14 +454,16 @@ def test_sphere_adjoint_256x128x128_100_steps():
     the 256x128x128 box of length 2 (U = (1, 0, 0) in a fixed frame, Re = 300,
     implicit penalization lambda = 1e6) from rest, 100 steps; J = the
     time-averaged drag. dJ/dchi on 8 random directions over the interface
-    cells, dJ/dU and dJ/du0 along a smooth solenoidal direction, from the FP64
-    and the FP32-DC forward (checkpoints chosen by the memory budget), against
-    central differences of the FP64 forward."""
+    cells and dJ/dU (the imposed velocity), from the FP64 and the FP32-DC
+    forward (checkpoints chosen by the memory budget), against central
+    differences of the FP64 forward. (From rest the first step's RHS is zero,
+    where the obstacle correction of the RHS is positively homogeneous but not
+    linear: J has no gradient with respect to u0 there. Perturbations of chi
+    and U leave that RHS zero.)"""
     import torch
 
     import cubismup_3d_b200 as cup
     from cubismup_3d_b200.adjoint import obstacle_gradients
-    from cubismup_3d_b200.initial_conditions import random_solenoidal
 
     def sphere_sim(precision):
         sd = cup.SimulationData(CFL=0.1, cells=(256, 128, 128))
@@ -447,12 +482,11 @@ def test_sphere_adjoint_256x128x128_100_steps():
     chi0 = s64.chi()
     vel0 = np.array([1.0, 0.0, 0.0])
 
-    def J(chi=None, vel=None, du=None, eps=0.0):
+    def J(chi=None, vel=None):
         if chi is not None:
             s64.set_chi(chi)
         s64.set_sphere_velocity(vel if vel is not None else vel0)
-        x = u0 if du is None else u0 + eps * du
-        s64.set_velocity_raw(x.contiguous())
+        s64.set_velocity_raw(u0.contiguous())
         tot = 0.0
         for dt in dts:
             tot += float(np.dot(w, s64.timestep(dt).force))
@@ -469,10 +503,8 @@ def test_sphere_adjoint_256x128x128_100_steps():
     rng = np.random.default_rng(31)
     # chi directions on the interface cells (0 < chi < 1) whose six neighbours
     # are all surface cells of the RHS correction (non-zero central chi
-    # differences): the sphere sits on the grid's symmetry planes, where cells
-    # with cancelling differences border the interface, and perturbing their
-    # neighbours would add them to the surface set (a kink the linearisation,
-    # which freezes that set, does not see)
+    # differences), so that a perturbation leaves the set of surface cells,
+    # which the linearisation freezes, as it is
     grad2 = sum((np.roll(chi0, -1, a) - np.roll(chi0, 1, a)) ** 2 for a in range(3))
     surf = grad2 > 0
     nb_surf = np.ones_like(surf)
@@ -491,11 +523,5 @@ def test_sphere_adjoint_256x128x128_100_steps():
     fd = (J(vel=vel0 + [e, 0, 0]) - J(vel=vel0 - [e, 0, 0])) / (2 * e)
     for name, (_, _, gv) in grads.items():
         err[name]["U"] = abs(gv[0] - fd) / abs(fd)
-    du = torch.from_numpy(np.stack(random_solenoidal(s64.shape[::-1], 3, lambda k: np.exp(-(k / 2.0) ** 2),
-                                                      rms=1.0))).cuda()
-    e = 1e-6
-    fd = (J(du=du, eps=e) - J(du=du, eps=-e)) / (2 * e)
-    for name, (gu, _, _) in grads.items():
-        err[name]["u0"] = abs(float(np.sum(gu * du.cpu().numpy())) - fd) / abs(fd)
     assert max(err["fp64"].values()) <= 1e-4, err
-    assert max(err["fp32"].values()) <= 1e-3, err
+    assert max(err["fp32"].values()) <= 1e-4, err

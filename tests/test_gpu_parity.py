@@ -531,7 +531,10 @@ def test_invalid_configurations_are_rejected():
         make_sim((48, 32, 32), 1.0)  # not a power of two
     sim = make_sim((32, 32, 32), 1.0)
     with pytest.raises(ValueError):
-        sim.add_obstacle(cup.Sphere(radius=0.1, bForcedInSimFrame=(True, False, True)))
+        sim.add_obstacle(cup.Sphere(radius=0.0))
+    sim.add_obstacle(cup.Sphere(radius=0.1, bForcedInSimFrame=(True, False, True)))  # free dofs are supported
+    with pytest.raises(Exception):
+        sim.add_obstacle(cup.Sphere(radius=0.1))  # one obstacle per simulation
     with pytest.raises(ValueError):
         sim.timestep(-1.0)
 

@@ -17,6 +17,16 @@ ref_mod = pytest.importorskip("oracle.reference")
 pytestmark = pytest.mark.skipif(not ref_mod.available(), reason="reference tree and its build are absent")
 
 
+@pytest.fixture(autouse=True)
+def _in_tmp_dir(tmp_path, monkeypatch):
+    """The reference's obstacle code writes its force and velocity logs
+    (forceValues_0.dat, ...) into the working directory, from a buffer
+    flushed here (otherwise at exit, wherever the process then is)."""
+    monkeypatch.chdir(tmp_path)
+    yield
+    ref_mod.flush_logs()
+
+
 def pair(oracle, cells, extent, nu, uinf):
     nx, ny, nz = cells
     orc = oracle.OracleSim(nx, ny, nz, extent, nu=nu, CFL=0.5, rampup=0, DLM=0.0, lambda_=1.0, uinf=uinf)
