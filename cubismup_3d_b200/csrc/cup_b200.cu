@@ -1019,22 +1019,19 @@ template <int M, typename R, class Prod, class Cons>
 int launch_rows_M(cup_handle* H, const char* name, const Prod& prod, const Cons& cons, const int* skip) {
   constexpr int N = 2 * M, TPL = M / 8;
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
-  // 256 threads per CTA (16 rows of 256-long lines); the read-modify-write of
-  // p measured 2 % faster on these tiles than on 8-row ones
+  // 256 threads per CTA (16 rows of 256-long lines)
   const int lpc = 256 / TPL;
   const int nrows = H->ny * H->nz;
-  // reduction scratch only for producers that compute rows (and may reduce)
-  const size_t scratch = Prod::kBulk ? 0 : 32 * 20 * sizeof(double);
+  // the producer's reduction scratch
+  const size_t scratch = 32 * 20 * sizeof(double);
   const size_t smem = (size_t)lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
-                      (Cons::kAddBulk ? (size_t)lpc * N * sizeof(double) : 0) +
-                      FFTPlan<M>::rows_table_len() * sizeof(typename Cplx<R>::T) + 16 +
-                      (Cons::kAddBulk ? 8 * sizeof(double) : 0) + scratch + 128;
+                      FFTPlan<M>::rows_table_len() * sizeof(typename Cplx<R>::T) + 16 + scratch + 128;
   auto kern = k_dht_rows<M, R, Prod, Cons>;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, lpc * TPL, &bpsm);
   if (rc) return rc;
   const int grid = (nrows + lpc - 1) / lpc;
-  if (!Prod::kBulk && grid > kPartialCap / 20) return fail(H, CUP_ERR_ARG, "too many row tiles for the partial buffers");
+  if (grid > kPartialCap / 20) return fail(H, CUP_ERR_ARG, "too many row tiles for the partial buffers");
   return launch_named(H, name, [&]() -> int {
     klaunch(H, kern, grid, lpc * TPL, smem, prod, cons, nrows, lpc, table<R>(H, 0), H->derr, skip);
     CKL();
@@ -1089,6 +1086,43 @@ int launch_rows_pipe(cup_handle* H, const char* name, const R* in, R* out, const
     case 64: return launch_rows_pipe_M<64, R>(H, name, in, out, skip);
     case 128: return launch_rows_pipe_M<128, R>(H, name, in, out, skip);
     case 256: return launch_rows_pipe_M<256, R>(H, name, in, out, skip);
+  }
+  return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
+}
+
+// Pipelined last x pass of a correction solve (k_dht_rows_addp_pipe): the
+// FP64 inverse of `in` added into p minus the class means of p.
+template <int M>
+int launch_rows_addp_M(cup_handle* H, const char* name, const double* in, double* p, const int* skip) {
+  constexpr int N = 2 * M, TPL = M / 8, NB = 2;
+  constexpr bool PAD = FFTPlan<M>::nstages > 1;
+  const int lpc = 256 / TPL;
+  const int nrows = H->ny * H->nz;
+  const size_t smem = (size_t)2 * NB * lpc * N * sizeof(double) +
+                      (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(double) : 0) +
+                      FFTPlan<M>::rows_table_len() * sizeof(double2) + NB * sizeof(uint64_t) + 8 * sizeof(double) + 128;
+  auto kern = k_dht_rows_addp_pipe<M, NB>;
+  const int threads = lpc * TPL;
+  int bpsm = 0;
+  int rc = prepare_kernel(H, kern, smem, threads, &bpsm);
+  if (rc) return rc;
+  const int ntiles = (nrows + lpc - 1) / lpc;
+  const int grid = std::min(ntiles, bpsm * H->num_sms);
+  return launch_named(H, name, [&]() -> int {
+    klaunch(H, kern, grid, threads, smem, in, p, (const double*)H->dstate->cmean, ilog2(H->ny), nrows, lpc,
+            table<double>(H, 0), H->derr, skip);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+int launch_rows_addp(cup_handle* H, const char* name, const double* in, double* p, const int* skip) {
+  switch (H->nx / 2) {
+    case 8: return launch_rows_addp_M<8>(H, name, in, p, skip);
+    case 16: return launch_rows_addp_M<16>(H, name, in, p, skip);
+    case 32: return launch_rows_addp_M<32>(H, name, in, p, skip);
+    case 64: return launch_rows_addp_M<64>(H, name, in, p, skip);
+    case 128: return launch_rows_addp_M<128>(H, name, in, p, skip);
   }
   return fail(H, CUP_ERR_ARG, "unsupported nx %d", H->nx);
 }
@@ -1170,8 +1204,7 @@ int dc_correction_solve(cup_handle* H, double* p, const int* skip) {
   if ((rc = launch_cols<float, 1, false>(H, H->work32, H->work32, skip))) return rc;
   if ((rc = launch_cols<double, 2, true, float>(H, H->work32, H->work64, skip))) return rc;
   if ((rc = launch_cols<double, 1, false>(H, H->work64, H->work64, skip))) return rc;
-  return launch_rows<double>(H, "dht_x_update_p", RowsFromArray<double>{H->work64},
-                             RowsAddToP{p, H->dstate->cmean, ilog2(H->ny)}, skip);
+  return launch_rows_addp(H, "dht_x_update_p", H->work64, p, skip);
 }
 
 // p = H(f . H(work)) over the three axes, in place on `work`; the last x

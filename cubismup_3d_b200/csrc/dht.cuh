@@ -544,45 +544,20 @@ __device__ __forceinline__ void load_table(R2* dst, const R2* src, int n) {
 // ---------------------------------------------------------------------------
 // x pass: LPC consecutive rows of length N = 2M per CTA (rows are contiguous
 // in the [z][y][x] layout: row r is (y, z) = (r % ny, r / ny)). A producer
-// fills the rows in shared memory (a 1-D bulk copy, or rows computed from
-// other fields), the rows are transformed, and a consumer drains them (a bulk
-// store, or an update of another field).
-
-// Producer: rows copied from an array (one bulk copy).
-template <typename R>
-struct RowsFromArray {
-  static constexpr bool kBulk = true;
-  const R* in;
-  __device__ const R* src(int row0, int N) const { return in + (size_t)row0 * N; }
-  __device__ void fill(R*, int, int, int, double*) const {}
-  __device__ void finish(double*, double*) const {}
-};
+// computes the rows in shared memory from other fields (and may reduce over
+// them), the rows are transformed, and a consumer stores them (one bulk store).
 
 // Consumer: rows stored to an array (one bulk store).
 template <typename R>
 struct RowsToArray {
-  static constexpr bool kBulk = true;
-  static constexpr bool kAddBulk = false;
   R* out;
   __device__ R* dst(int row0, int N) const { return out + (size_t)row0 * N; }
-  __device__ void drain(const R*, int, int, int) const {}
 };
 
-// Consumer of the last x pass of a correction solve: p += rows - (parity-class
-// means of p measured by the preceding residual pass), in FP64. The p rows
-// arrive by bulk copy with the input rows and leave by one bulk store; the
-// transform's last step adds into them directly (AddToPRows).
-struct RowsAddToP {
-  static constexpr bool kBulk = false;
-  static constexpr bool kAddBulk = true;
-  double* p;
-  const double* cmean;
-  int log2ny;  // ny is a power of two: row r is (y, z) = (r & (ny-1), r >> log2ny)
-  __device__ double* rows_of(int row0, int N) const { return p + (size_t)row0 * N; }
-};
-
-// Output accessor of the transform's last step for RowsAddToP: element n of
-// line l is added to the shared-memory p row, minus the class mean of p.
+// Output accessor of the last step of a correction solve's last x pass
+// (k_dht_rows_addp_pipe): element n of line l is added to the shared-memory p
+// row, minus the parity-class mean of p measured by the preceding residual
+// pass (row r is (y, z) = (r & (ny-1), r >> log2ny); ny is a power of two).
 struct AddToPRows {
   using elem = double;
   double* prow;
@@ -606,79 +581,35 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
   constexpr int TL = FFTPlan<M>::rows_table_len();
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
   constexpr int PPITCH = 2 * (M + M / 8);
-  constexpr bool ADD = Cons::kAddBulk;
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
-  R* rows = reinterpret_cast<R*>(smem_raw);                        // lpc * N
-  R* padb = rows + (size_t)lpc * N;                                // lpc * PPITCH
-  double* prow = reinterpret_cast<double*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));  // lpc * N (ADD)
-  R2* tw = reinterpret_cast<R2*>(prow + (ADD ? (size_t)lpc * N : 0));
-  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
-  double* cms = reinterpret_cast<double*>(bar + 1);                // 8 class means (ADD)
-  double* scratch = cms + (ADD ? 8 : 0);                           // 32 * 20 doubles (computing producers)
+  R* rows = reinterpret_cast<R*>(smem_raw);  // lpc * N
+  R* padb = rows + (size_t)lpc * N;          // lpc * PPITCH
+  R2* tw = reinterpret_cast<R2*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));
+  double* scratch = reinterpret_cast<double*>(tw + TL + 1);  // 32 * 20 doubles (the producer's reductions)
   const int row0 = blockIdx.x * lpc;
   const int nr = min(lpc, nrows - row0);
   if (nr <= 0) return;
   const uint32_t bytes = (uint32_t)((size_t)nr * N * sizeof(R));
-  const uint32_t pbytes = ADD ? (uint32_t)((size_t)nr * N * sizeof(double)) : 0u;
   double acc[20];
 #pragma unroll
   for (int i = 0; i < 20; ++i) acc[i] = 0.0;
-  if constexpr (Prod::kBulk) {
-    // the barrier must be initialised before any thread waits on it
-    if (threadIdx.x == 0) {
-      mbar_init(bar, 1);
-      mbar_fence_init();
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      mbar_arrive_expect_tx(bar, bytes + pbytes);
-      bulk_load(rows, prod.src(row0, N), bytes, bar);
-      if constexpr (ADD) bulk_load(prow, cons.rows_of(row0, N), pbytes, bar);
-    }
-    if constexpr (ADD)
-      if (threadIdx.x < 8) cms[threadIdx.x] = cons.cmean[threadIdx.x];
-    load_table(tw, tw_g, TL);
-    const bool ok = __syncthreads_and(mbar_wait(bar, 0, err));
-    if (!ok) return;
-  } else {
-    static_assert(!ADD, "the bulk read-modify-write consumer needs a bulk producer");
-    load_table(tw, tw_g, TL);
-    prod.fill(rows, row0, nr, N, acc);
-    __syncthreads();
-  }
+  load_table(tw, tw_g, TL);
+  prod.fill(rows, row0, nr, N, acc);
+  __syncthreads();
   const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
   const bool active = l < nr;
   RowLines<R> A{rows, N};
   RowLinesPad<R> P{padb, PPITCH};
-  if constexpr (ADD) {
-    fft_stages<M, PAD, R>(A, P, tw, l, t, active);
-    dht_tail_to<M, R>(A, AddToPRows{prow, cms, N, row0, cons.log2ny}, tw, l, t, active, NoScale());
-  } else {
-    dht_lines<M, PAD, R>(A, P, tw, l, t, active);
+  dht_lines<M, PAD, R>(A, P, tw, l, t, active);
+  fence_proxy_async_smem();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bulk_store(cons.dst(row0, N), rows, bytes);
+    bulk_commit();
+    bulk_wait_all();
   }
-  if constexpr (Cons::kBulk || ADD) {
-    if constexpr (ADD) {
-      fence_proxy_async_smem();
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        bulk_store(cons.rows_of(row0, N), prow, pbytes);
-        bulk_commit();
-        bulk_wait_all();
-      }
-    } else {
-      fence_proxy_async_smem();
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        bulk_store(cons.dst(row0, N), rows, bytes);
-        bulk_commit();
-        bulk_wait_all();
-      }
-    }
-  } else {
-    cons.drain(rows, row0, nr, N);
-  }
-  if constexpr (!Prod::kBulk) prod.finish(acc, scratch);
+  prod.finish(acc, scratch);
 }
 
 // Pipelined x pass: persistent CTAs walk tiles of lpc consecutive rows
@@ -754,6 +685,97 @@ __global__ void __launch_bounds__(256, 2) k_dht_rows_pipe(const R* __restrict__ 
     __syncthreads();
     if (tid == 0) {
       bulk_store(out + (size_t)row0 * N, rows, (uint32_t)((size_t)nr * N * sizeof(R)));
+      bulk_commit();
+    }
+    done = i + 1;
+  }
+  if (tid == 0) {
+    bulk_wait_all();
+    // after a timed-out wait: bounded drain of the loads still in flight
+    if (!ok)
+      for (int r = done; r < issued; ++r) mbar_wait(&bar[r % NB], (r / NB) & 1, nullptr);
+  }
+}
+
+// Pipelined last x pass of a correction solve (FP64): persistent CTAs walk
+// tiles of lpc rows through NB buffer pairs, each pair holding the tile's
+// transform rows and its p rows, both filled by 1-D bulk copies on one
+// barrier. The inverse transform's last step adds into the p rows (AddToPRows:
+// p += rows - class means of p) and one bulk store writes them back. The loads
+// of the next NB-1 tiles and the store of the previous one overlap the
+// transform of the current tile; the twiddle table and the class means are
+// loaded once per CTA.
+template <int M, int NB>
+__global__ void __launch_bounds__(256, 1) k_dht_rows_addp_pipe(const double* __restrict__ in, double* p,
+                                                               const double* cmean, int log2ny, int nrows, int lpc,
+                                                               const double2* tw_g, int* err, const int* skip) {
+  pdl_entry();
+  static_assert(NB >= 2, "need at least two buffer pairs");
+  if (skip && *skip) return;
+  constexpr int N = 2 * M, TPL = M / 8;
+  constexpr int TL = FFTPlan<M>::rows_table_len();
+  constexpr bool PAD = FFTPlan<M>::nstages > 1;
+  constexpr int PPITCH = 2 * (M + M / 8);
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw = smem_align128(smem_dyn);
+  double* bufs = reinterpret_cast<double*>(smem_raw);  // NB * lpc * N transform rows
+  double* pbufs = bufs + (size_t)NB * lpc * N;         // NB * lpc * N p rows
+  double* padb = pbufs + (size_t)NB * lpc * N;         // lpc * PPITCH
+  double2* tw = reinterpret_cast<double2*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tw + TL);
+  double* cms = reinterpret_cast<double*>(bar + NB);   // the 8 class means
+  const int tid = threadIdx.x;
+  const int ntiles = (nrows + lpc - 1) / lpc;
+  const int my = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  if (tid == 0) {
+    for (int b = 0; b < NB; ++b) mbar_init(&bar[b], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto rows_of = [&](int i, int& row0, int& nr) {
+    row0 = (blockIdx.x + i * gridDim.x) * lpc;
+    nr = min(lpc, nrows - row0);
+  };
+  auto issue = [&](int i) {
+    int row0, nr;
+    rows_of(i, row0, nr);
+    const int b = i % NB;
+    const uint32_t bytes = (uint32_t)((size_t)nr * N * sizeof(double));
+    mbar_arrive_expect_tx(&bar[b], 2 * bytes);
+    bulk_load(bufs + (size_t)b * lpc * N, in + (size_t)row0 * N, bytes, &bar[b]);
+    bulk_load(pbufs + (size_t)b * lpc * N, p + (size_t)row0 * N, bytes, &bar[b]);
+  };
+  int issued = 0;
+  if (tid == 0)
+    for (; issued < min(NB - 1, my); ++issued) issue(issued);
+  load_table(tw, tw_g, TL);
+  if (tid < 8) cms[tid] = cmean[tid];
+  __syncthreads();
+  const int l = tid / TPL, t = tid % TPL;
+  RowLinesPad<double> P{padb, PPITCH};
+  bool ok = true;
+  int done = 0;
+  for (int i = 0; i < my; ++i) {
+    // refill: tile i + NB - 1 goes into the buffer pair of tile i - 1, once
+    // the store of its p rows has read them
+    if (tid == 0 && ok && issued < my) {
+      bulk_wait_read<0>();
+      issue(issued++);
+    }
+    int row0, nr;
+    rows_of(i, row0, nr);
+    const int b = i % NB;
+    ok = __syncthreads_and(ok && mbar_wait(&bar[b], (i / NB) & 1, err));
+    if (!ok) break;
+    RowLines<double> A{bufs + (size_t)b * lpc * N, N};
+    double* prow = pbufs + (size_t)b * lpc * N;
+    const bool active = l < nr;
+    fft_stages<M, PAD, double>(A, P, tw, l, t, active);
+    dht_tail_to<M, double>(A, AddToPRows{prow, cms, N, row0, log2ny}, tw, l, t, active, NoScale());
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      bulk_store(p + (size_t)row0 * N, prow, (uint32_t)((size_t)nr * N * sizeof(double)));
       bulk_commit();
     }
     done = i + 1;

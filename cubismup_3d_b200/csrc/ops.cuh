@@ -193,7 +193,6 @@ struct OpResidual {
 // RHS never goes to HBM.
 template <typename T>
 struct RowsRhs {
-  static constexpr bool kBulk = false;
   const T *u, *v, *w;
   DtArg dt;
   double h;
