@@ -20,6 +20,7 @@
 #include <vector>
 
 #include "adjoint.cuh"
+#include "adjoint_f2.cuh"
 #include "adjoint_obstacle.cuh"
 #include "advect.cuh"
 #include "advect_f2.cuh"
@@ -2087,6 +2088,69 @@ int do_project_fields(cup_handle* H, void* const* in, void* const* out, double* 
 //   upwind3 + RK2:  lam* = P lam,  u1 = S(un),
 //                   mu = 1/2 S'(u1)^T lam*,  lam = 1/2 lam* + S'(un)^T mu
 //   central + Euler: lam = S'(un)^T (P lam)
+// FP32 upwind3 stage transposes on x-pairs (k_adjoint_zq_f2); grids of nx 64,
+// 128 or 256 with nz >= ZC take the compile-time-size kernels.
+template <bool LAM, int TY, int NS, int PPT, int NXC = 0, int ZCC = 0>
+int launch_adjoint_f2(cup_handle* H, const char* name, const void* const* f, const void* const* g,
+                      const void* const* lam, void* const* out, double alpha, double beta, DtArg dt, int zmax) {
+  constexpr int G = 2;
+  const int pairs = TY * H->nx / 2;
+  if (pairs % PPT || pairs / PPT > 512 || H->ny % TY)
+    return fail(H, CUP_ERR_ARG, "adjoint tile does not fit the grid");
+  AdjointMaps maps;
+  for (int q = 0; q < 3; ++q) {
+    int rc = make_map(H, &maps.main[q], f[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float), H->nx, TY, 1);
+    if (!rc) rc = make_map(H, &maps.halo[q], f[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float), H->nx, G, 1);
+    if (!rc) rc = make_map(H, &maps.main[3 + q], g[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float), H->nx, TY, 1);
+    if (!rc) rc = make_map(H, &maps.halo[3 + q], g[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float), H->nx, G, 1);
+    if (!rc)
+      rc = make_map(H, &maps.lam[q], LAM ? lam[q] : g[q], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, sizeof(float), H->nx, TY, 1);
+    if (rc) return rc;
+  }
+  const int zc = std::min(zmax, H->nz);
+  if ((NXC && NXC != H->nx) || (ZCC && ZCC != zc)) return fail(H, CUP_ERR_ARG, "adjoint specialisation mismatch");
+  StreamGeom geo{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
+  const size_t smem = adjoint_f2_smem_bytes<LAM, TY, NS, PPT>(H->nx) + 128;
+  auto kern = k_adjoint_zq_f2<LAM, TY, NS, PPT, NXC, ZCC>;
+  const int threads = pairs / PPT;
+  int bpsm = 0;
+  int rc = prepare_kernel(H, kern, smem, threads, &bpsm);
+  if (rc) return rc;
+  const int grid = std::min(geo.n_items, bpsm * H->num_sms);
+  return launch_named(H, name, [&]() -> int {
+    klaunch(H, kern, grid, threads, smem, maps, geo, (float*)out[0], (float*)out[1], (float*)out[2], (float)alpha,
+            (float)beta, dt, H->h, H->cfg.nu, H->uinf[0], H->uinf[1], H->uinf[2], H->derr);
+    CKL();
+    return CUP_OK;
+  });
+}
+
+template <bool LAM, int TY, int NS, int PPT, int ZC>
+int launch_adjoint_f2_sized(cup_handle* H, const char* name, const void* const* f, const void* const* g,
+                            const void* const* lam, void* const* out, double alpha, double beta, DtArg dt) {
+  if (H->nz >= ZC) {
+    switch (H->nx) {
+      case 64: return launch_adjoint_f2<LAM, TY, NS, PPT, 64, ZC>(H, name, f, g, lam, out, alpha, beta, dt, ZC);
+      case 128: return launch_adjoint_f2<LAM, TY, NS, PPT, 128, ZC>(H, name, f, g, lam, out, alpha, beta, dt, ZC);
+      case 256: return launch_adjoint_f2<LAM, TY, NS, PPT, 256, ZC>(H, name, f, g, lam, out, alpha, beta, dt, ZC);
+      default: break;
+    }
+  }
+  return launch_adjoint_f2<LAM, TY, NS, PPT>(H, name, f, g, lam, out, alpha, beta, dt, ZC);
+}
+
+// The two transposed upwind3 stages of an FP32 adjoint step: mu = 1/2 S'(u1)^T
+// lam*, then lam = 1/2 lam* + S'(u^n)^T mu (lam* = the projected adjoint, in
+// lam on entry). 4-row tiles, a 3-deep ring and one pair per thread measured
+// best at 256^3: 1.235 ms per adjoint step against 1.52 ms with 2-row tiles
+// and a 4-deep ring, and 2.17 ms for the scalar kernels (k_adjoint_zq).
+int adjoint_upwind_f32(cup_handle* H, void* const* un, void* const* st1, void* const* lam, void* const* mu, DtArg dt) {
+  int rc;
+  if ((rc = launch_adjoint_f2_sized<false, 4, 3, 1, 8>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt)))
+    return rc;
+  return launch_adjoint_f2_sized<true, 4, 3, 1, 8>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
+}
+
 template <typename T>
 int do_adjoint_step(cup_handle* H, void* const* un, void* const* lam, DtArg dt) {
   constexpr bool F32 = std::is_same<T, float>::value;
@@ -2101,8 +2165,7 @@ int do_adjoint_step(cup_handle* H, void* const* un, void* const* lam, DtArg dt) 
   if ((rc = do_project_fields<T>(H, lam, lam, H->p_adj, dt))) return rc;
   if constexpr (F32) {
     if ((rc = upwind_stage1_f32(H, "adjoint_recompute_stage1", un, st1, dt))) return rc;
-    if ((rc = launch_adjoint<T, 1, false, 2, 3, 1>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt))) return rc;
-    return launch_adjoint<T, 1, true, 2, 3, 1>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
+    return adjoint_upwind_f32(H, un, st1, lam, mu, dt);
   } else {
     if ((rc = launch_advect<T, 1, 4, 3, 2>(H, "adjoint_recompute_stage1", un, un, st1, dt))) return rc;
     if ((rc = launch_adjoint<T, 1, false, 2, 2, 1>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt))) return rc;
@@ -2186,8 +2249,7 @@ int do_adjoint_step_obstacle(cup_handle* H, void* const* un, void* const* lam, D
   }
   if ((rc = do_grad_fields<T>(H, "adjoint_grad_p", lam, lam, H->p_adj, dt))) return rc;
   if constexpr (F32) {
-    if ((rc = launch_adjoint<T, 1, false, 2, 3, 1>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt))) return rc;
-    return launch_adjoint<T, 1, true, 2, 3, 1>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
+    return adjoint_upwind_f32(H, un, st1, lam, mu, dt);
   } else {
     if ((rc = launch_adjoint<T, 1, false, 2, 2, 1>(H, "adjoint_stage2", st1, lam, nullptr, mu, 0.0, 0.5, dt))) return rc;
     return launch_adjoint<T, 1, true, 2, 2, 1>(H, "adjoint_stage1", un, mu, lam, lam, 0.5, 1.0, dt);
