@@ -233,8 +233,10 @@ def run_reference(args, rank: int):
         "config": workload_config(args),
         "cpu_baseline": {"value": rate, "unit": "cell-steps/s", "cores": thr, "kind": "port",
                          "sample": f"{args.steps} full {n}^3 FP64 steps after {args.warmup} warm-up steps "
-                                   "(oracle: C++/OpenMP restatement; the reference itself needs MPI, FFTW-MPI, HDF5, "
-                                   "GSL and Cubism, absent on this image)"},
+                                   "(oracle: C++/OpenMP restatement of the reference's operators; the reference's "
+                                   "own operator sources build here only against stand-ins for Cubism, MPI and "
+                                   "FFTW-MPI (a direct-DFT Poisson solve), which pin parity but do not measure its "
+                                   "speed)"},
         "e2e": {"value": rate, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)

@@ -792,6 +792,12 @@ struct cup_handle {
   double sphere_quat[4] = {1, 0, 0, 0};      // Obstacle::quaternion
   SphereParams* sp_dev = nullptr;
   Box box{};
+  // FP32_DC with the sphere: the RHS's obstacle terms on the box (b2 - b0,
+  // box order) that the z-queue passes add to the b they recompute from u*,
+  // and the box array the obstacle kernels work on; box_cap: their length
+  double* box_delta = nullptr;
+  double* box_b = nullptr;
+  long long box_cap = 0;
   // host mirrors
   int step = 0;
   double time = 0, dt = 0, lambda = 0;
@@ -1429,7 +1435,7 @@ int do_pressure_rhs(cup_handle* H, DtArg dt, void* const* fields = nullptr, doub
     {
       int rc_ = launch_named(H, "rhs_obstacle_correct", [&]() -> int {
         klaunch(H, k_rhs_obstacle_correct<T>, gb, kBoxThreads, 0, H->rhs, (const T*)H->chi, H->box, H->nx, H->ny,
-                                                                 H->nz, &H->dstate->corr);
+                                                                 H->nz, &H->dstate->corr, (double*)nullptr);
         CKL();
         return CUP_OK;
       });
@@ -1439,6 +1445,35 @@ int do_pressure_rhs(cup_handle* H, DtArg dt, void* const* fields = nullptr, doub
   return CUP_OK;
 }
 
+// The sphere's RHS terms on its box for the FP32 defect correction: b0 of u*
+// on the box, the obstacle terms (bulk source, surface sums, correction) on
+// that box array, and H->box_delta = b2 - b0.
+template <typename T>
+int do_box_rhs_terms(cup_handle* H, DtArg dt) {
+  if (H->box.count() > H->box_cap) return fail(H, CUP_ERR_STATE, "obstacle box larger than its buffers");
+  const int gb = box_grid(H->box);
+  int rc = launch_named(H, "box_rhs_obstacle", [&]() -> int {
+    klaunch(H, k_box_rhs_obstacle<T>, gb, kBoxThreads, 0, (const T*)H->u, (const T*)H->v, (const T*)H->w,
+            (const T*)H->chi, H->box, H->nx, H->ny, H->nz, dt, H->h, H->box_b, H->box_delta, partial(H, P_RHSOB));
+    CKL();
+    return CUP_OK;
+  });
+  if (!rc)
+    rc = launch_named(H, "finalize_rhs_obstacle", [&]() -> int {
+      klaunch(H, k_finalize_rhs_obstacle, 1, 256, 0, partial(H, P_RHSOB), gb, H->dstate);
+      CKL();
+      return CUP_OK;
+    });
+  if (!rc)
+    rc = launch_named(H, "rhs_obstacle_correct", [&]() -> int {
+      klaunch(H, k_rhs_obstacle_correct<T, true>, gb, kBoxThreads, 0, H->box_b, (const T*)H->chi, H->box, H->nx,
+              H->ny, H->nz, &H->dstate->corr, H->box_delta);
+      CKL();
+      return CUP_OK;
+    });
+  return rc;
+}
+
 double dc_tol(const cup_handle* H) { return H->cfg.dc_tol > 0 ? H->cfg.dc_tol : 1e-10; }
 int dc_max_iter(const cup_handle* H) { return H->cfg.dc_max_iter > 0 ? H->cfg.dc_max_iter : 2; }
 int dc_min_iter(const cup_handle* H) {
@@ -1446,7 +1481,7 @@ int dc_min_iter(const cup_handle* H) {
 }
 
 // Launches one k_pres_zq pass; returns the grid size (number of partials).
-template <typename T, int MODE, int TY, int NS, int CPT, int NXC, int ZCC, bool BU>
+template <typename T, int MODE, int TY, int NS, int CPT, int NXC, int ZCC, bool BD>
 int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
                      int* grid_out, const int* skip, int pred_order, double* pred_out, void* const* out) {
   const int cells = TY * H->nx;
@@ -1457,7 +1492,6 @@ int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partia
   if (!rc) rc = make_map(H, &maps.p_halo, pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), H->nx, 2, 1);
   if (!rc) rc = make_map(H, &maps.h_main, pred_order >= 1 ? H->p : pw, CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                          sizeof(double), H->nx, TY, 1);
-  if (!rc) rc = make_map(H, &maps.b_main, H->rhs, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, sizeof(double), H->nx, TY, 1);
   const void* f[3] = {H->u, H->v, H->w};
   for (int q = 0; q < 3 && !rc; ++q) rc = make_map(H, &maps.f_main[q], f[q], tma_dtype<T>(), sizeof(T), H->nx, TY, 1);
   if (!rc) rc = make_map(H, &maps.v_halo, H->v, tma_dtype<T>(), sizeof(T), H->nx, 1, 1);
@@ -1465,20 +1499,21 @@ int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partia
   const int zc = ZCC ? ZCC : std::min(16, H->nz);
   if ((NXC && NXC != H->nx) || (ZCC && ZCC != zc)) return fail(H, CUP_ERR_ARG, "pressure specialisation mismatch");
   StreamGeom geo{H->nx, H->ny, H->nz, ilog2(H->nx), zc, H->ny / TY, (H->ny / TY) * (H->nz / zc)};
-  const size_t smem = pzq_smem_bytes_host<T, MODE, TY, NS, BU>(H->nx) + 128;
-  auto kern = k_pres_zq<T, MODE, TY, NS, CPT, NXC, ZCC, BU>;
+  const size_t smem = pzq_smem_bytes_host<T, MODE, TY, NS>(H->nx) + 128;
+  auto kern = k_pres_zq<T, MODE, TY, NS, CPT, NXC, ZCC, BD>;
   const int threads = cells / CPT;
   int bpsm = 0;
   if ((rc = prepare_kernel(H, kern, smem, threads, &bpsm))) return rc;
   const int grid = std::min(geo.n_items, bpsm * H->num_sms);
   if (grid > kPartialCap / pzq_partials_per_cta<MODE>())
     return fail(H, CUP_ERR_ARG, "too many CTAs for the partial buffers");
-  PzqParams prm{dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, pred_order, pred_out, H->box};
+  if (BD && !H->box_delta) return fail(H, CUP_ERR_STATE, "no obstacle RHS terms on the box");
+  PzqParams prm{dt, H->h, {H->uinf[0], H->uinf[1], H->uinf[2]}, pred_order, pred_out, H->box, H->box_delta};
   T* o[3] = {nullptr, nullptr, nullptr};
   if (out)
     for (int q = 0; q < 3; ++q) o[q] = (T*)out[q];
   rc = launch_named(H, name, [&]() -> int {
-    klaunch(H, kern, grid, threads, smem, maps, geo, o[0], o[1], o[2], H->rhs, H->work32, partials, rmean, prm,
+    klaunch(H, kern, grid, threads, smem, maps, geo, o[0], o[1], o[2], H->work32, partials, rmean, prm,
                                              H->derr, skip);
     CKL();
     return CUP_OK;
@@ -1488,28 +1523,28 @@ int launch_pzq_sized(cup_handle* H, const char* name, double* pw, double* partia
   return CUP_OK;
 }
 
-// Grids of nx 64, 128 or 256 with nz >= 16 take the compile-time-size
-// kernels; other shapes the same kernel with runtime sizes. BU: b from u*
-// (not stored).
-template <typename T, int MODE, int TY, int NS, int CPT, bool BU = false, int ZC = 16>
+// Grids of nx 64, 128 or 256 with nz >= ZC take the compile-time-size
+// kernels; other shapes the same kernel with runtime sizes. BD: b carries the
+// obstacle terms on the box (H->box_delta).
+template <typename T, int MODE, int TY, int NS, int CPT, int ZC = 16, bool BD = false>
 int launch_pzq(cup_handle* H, const char* name, double* pw, double* partials, const double* rmean, DtArg dt,
                int* grid_out, const int* skip, int pred_order = -1, double* pred_out = nullptr,
                void* const* out = nullptr) {
   if (H->nz >= ZC) {
     switch (H->nx) {
       case 64:
-        return launch_pzq_sized<T, MODE, TY, NS, CPT, 64, ZC, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 64, ZC, BD>(H, name, pw, partials, rmean, dt, grid_out, skip,
                                                               pred_order, pred_out, out);
       case 128:
-        return launch_pzq_sized<T, MODE, TY, NS, CPT, 128, ZC, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 128, ZC, BD>(H, name, pw, partials, rmean, dt, grid_out, skip,
                                                                pred_order, pred_out, out);
       case 256:
-        return launch_pzq_sized<T, MODE, TY, NS, CPT, 256, ZC, BU>(H, name, pw, partials, rmean, dt, grid_out, skip,
+        return launch_pzq_sized<T, MODE, TY, NS, CPT, 256, ZC, BD>(H, name, pw, partials, rmean, dt, grid_out, skip,
                                                                pred_order, pred_out, out);
       default: break;
     }
   }
-  return launch_pzq_sized<T, MODE, TY, NS, CPT, 0, 0, BU>(H, name, pw, partials, rmean, dt, grid_out, skip, pred_order,
+  return launch_pzq_sized<T, MODE, TY, NS, CPT, 0, 0, BD>(H, name, pw, partials, rmean, dt, grid_out, skip, pred_order,
                                                       pred_out, out);
 }
 
@@ -1535,18 +1570,21 @@ int launch_finalize_residual(cup_handle* H, const double* partials, int stride, 
 // solves) turns every later kernel of the loop into an exit at entry, so the
 // loop needs no host round trip. Only the first gradient pass writes the next
 // step's warm start.
-// rhs_given: b (with the obstacle terms) is already in H->rhs; check 0 reads it.
+// b is recomputed from u* in every pass (not stored); with the sphere the
+// passes add its RHS terms on the box (H->box_delta, from do_box_rhs_terms).
 template <typename T>
-int do_pressure_dc_zq(cup_handle* H, DtArg dt, bool rhs_given = false) {
+int do_pressure_dc_zq(cup_handle* H, DtArg dt) {
   const int max_iter = dc_max_iter(H);
   const int* conv = &H->dstate->converged;
+  const bool box = H->has_sphere;
   double* W = H->p_pred;  // this step's pressure, starting from the warm start
   if (!H->pred_ready) CK(cudaMemcpyAsync(W, H->p, H->n * sizeof(double), cudaMemcpyDeviceToDevice, H->stream));
   int rc, grid = 0;
-  // without a given RHS, b = div u* is recomputed in every pass (not stored)
-  if (rhs_given) rc = launch_pzq<T, PZQ_RES0, 4, 4, 2>(H, "dc_residual0", W, partial(H, P_RES), nullptr, dt, &grid, nullptr);
+  if (box)
+    rc = launch_pzq<T, PZQ_RHS_RES, 4, 4, 2, 16, true>(H, "rhs_residual", W, partial(H, P_RES), nullptr, dt,
+                                                             &grid, nullptr);
   else
-    rc = launch_pzq<T, PZQ_RHS_RES, 4, 4, 2, true>(H, "rhs_residual", W, partial(H, P_RES), nullptr, dt, &grid,
+    rc = launch_pzq<T, PZQ_RHS_RES, 4, 4, 2>(H, "rhs_residual", W, partial(H, P_RES), nullptr, dt, &grid,
                                                    nullptr);
   if (rc) return rc;
   if ((rc = launch_finalize_residual(H, partial(H, P_RES), 18, grid, 0))) return rc;
@@ -1555,24 +1593,23 @@ int do_pressure_dc_zq(cup_handle* H, DtArg dt, bool rhs_given = false) {
   constexpr int kGradStride = pzq_partials_per_cta<PZQ_GRAD_CHECK>();
   for (int k = 1; k <= max_iter; ++k) {
     if (k > 1) {
-      if (rhs_given)
-        rc = launch_pzq<T, PZQ_RES, 4, 4, 2>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid, conv);
+      if (box)
+        rc = launch_pzq<T, PZQ_RES, 4, 4, 2, 16, true>(H, "dc_residual", W, partial(H, P_RES),
+                                                             H->dstate->rmean, dt, &grid, conv);
       else
-        rc = launch_pzq<T, PZQ_RES, 4, 4, 2, true>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid,
+        rc = launch_pzq<T, PZQ_RES, 4, 4, 2>(H, "dc_residual", W, partial(H, P_RES), H->dstate->rmean, dt, &grid,
                                                    conv);
       if (rc) return rc;
     }
     if ((rc = dc_correction_solve(H, W, conv))) return rc;
     const int* skip = k > 1 ? conv : nullptr;
     const int pred = k == 1 ? order : -1;
-    if (H->has_sphere)
-      rc = launch_pzq<T, PZQ_GRAD_CHECK_BOX, 4, 4, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
-                                                      &H->n_grad_partials, skip, pred, H->p_old, unew);
-    else if (rhs_given)
-      rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
-                                                  &H->n_grad_partials, skip, pred, H->p_old, unew);
+    if (box)
+      rc = launch_pzq<T, PZQ_GRAD_CHECK_BOX, 4, 4, 2, 8, true>(H, "grad_p_check", W, partial(H, P_GRAD),
+                                                                     H->dstate->rmean, dt, &H->n_grad_partials, skip,
+                                                                     pred, H->p_old, unew);
     else
-      rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2, true, 8>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
+      rc = launch_pzq<T, PZQ_GRAD_CHECK, 4, 4, 2, 8>(H, "grad_p_check", W, partial(H, P_GRAD), H->dstate->rmean, dt,
                                                         &H->n_grad_partials, skip, pred, H->p_old, unew);
     if (rc) return rc;
     if ((rc = launch_finalize_residual(H, partial(H, P_GRAD), kGradStride, H->n_grad_partials, k))) return rc;
@@ -1984,10 +2021,11 @@ int do_step(cup_handle* H, DtArg dt, const double* lambda_dev, int advance, int 
     if ((rc = do_spectral_forcing<T>(H, dt.host))) return rc;
   }
   if (H->has_sphere && H->fp32) {
-    // the obstacle terms need global sums over the RHS first: RHS pass, then
-    // the z-queue defect correction on the given RHS
-    if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
-    if ((rc = do_pressure_dc_zq<T>(H, dt, true))) return rc;
+    // the obstacle terms need global sums over the RHS first: they are formed
+    // on the sphere's box and added back by the z-queue defect correction's
+    // passes, which recompute the rest of b from u*
+    if ((rc = do_box_rhs_terms<T>(H, dt))) return rc;
+    if ((rc = do_pressure_dc_zq<T>(H, dt))) return rc;
   } else if (H->has_sphere) {
     if ((rc = do_pressure_rhs<T>(H, dt))) return rc;
     if ((rc = do_poisson(H))) return rc;
@@ -2544,7 +2582,7 @@ int cup_destroy(cup_handle* H) {
   for (void* f : {H->u, H->v, H->w, H->tu, H->tv, H->tw, H->u1, H->v1, H->w1, H->au, H->av, H->aw, (void*)H->p_adj,
                   H->chi, (void*)H->p, (void*)H->p_old, (void*)H->p_pred, (void*)H->rhs,
                   (void*)H->work32, (void*)H->work64, (void*)H->partials, (void*)H->dstate, (void*)H->cosx,
-                  (void*)H->cosy, (void*)H->cosz, (void*)H->sp_dev})
+                  (void*)H->cosy, (void*)H->cosz, (void*)H->sp_dev, (void*)H->box_b, (void*)H->box_delta})
     if (f) cudaFree(f);
   for (int d = 0; d < 3; ++d) {
     if (H->tw64[d]) cudaFree(H->tw64[d]);
@@ -2710,6 +2748,16 @@ int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
   }
   sp.lambda_factor = 1.0;
   sphere_box(H);
+  if (H->fp32) {
+    // the box spans at most 2 (R + 3h) / h + 5 cells per axis wherever the sphere moves
+    const int N[3] = {H->nx, H->ny, H->nz};
+    long long cap = 1;
+    for (int d = 0; d < 3; ++d)
+      cap *= std::min<long long>(N[d], (long long)std::ceil(2 * (s->radius + 3 * H->h) / H->h) + 6);
+    H->box_cap = cap;
+    CK(cudaMalloc(&H->box_b, cap * sizeof(double)));
+    CK(cudaMalloc(&H->box_delta, cap * sizeof(double)));
+  }
   CK(cudaMemcpyAsync(H->sp_dev, &sp, sizeof(sp), cudaMemcpyHostToDevice, H->stream));
   int rc = build_sphere_chi(H);
   if (rc) return rc;

@@ -221,7 +221,14 @@ struct Box {
     int dz = z - lo[2]; dz += dz < 0 ? nz : 0;
     return dx < n[0] && dy < n[1] && dz < n[2];
   }
-  __device__ __forceinline__ long long count() const { return (long long)n[0] * n[1] * n[2]; }
+  __host__ __device__ __forceinline__ long long count() const { return (long long)n[0] * n[1] * n[2]; }
+  // index of cell (x, y, z) in the box's [z][y][x] order, -1 outside
+  __device__ __forceinline__ int index(int x, int y, int z, int nx, int ny, int nz) const {
+    int dx = x - lo[0]; dx += dx < 0 ? nx : 0;
+    int dy = y - lo[1]; dy += dy < 0 ? ny : 0;
+    int dz = z - lo[2]; dz += dz < 0 ? nz : 0;
+    return (dx < n[0] && dy < n[1] && dz < n[2]) ? dx + n[0] * (dy + n[1] * dz) : -1;
+  }
 };
 
 // KernelGradP (source/operators/PressureProjection.cpp:38-50):
@@ -390,10 +397,13 @@ __global__ void k_rhs_obstacle(double* rhs, const T* chi, Box box, int nx, int n
 }
 
 // KernelFinalizePerimeters (source/operators/PressureRHS.cpp:215-256) with the
-// correction factor computed on the device (:331-334).
-template <typename T>
+// correction factor computed on the device (:331-334). BOXARR: rhs is an array
+// over the box, and delta (holding b0, the RHS before its obstacle terms) is
+// replaced by b2 - b0, the obstacle terms a pass that recomputes b0 from u*
+// adds back on the box.
+template <typename T, bool BOXARR = false>
 __global__ void k_rhs_obstacle_correct(double* rhs, const T* chi, Box box, int nx, int ny, int nz,
-                                       const double* corr_dev) {
+                                       const double* corr_dev, double* delta = nullptr) {
   pdl_entry();
   const double corr = *corr_dev;
   const long long n = box.count();
@@ -404,13 +414,56 @@ __global__ void k_rhs_obstacle_correct(double* rhs, const T* chi, Box box, int n
     const double dXx = (double)chi[gidx(wrapi(x + 1, nx), y, z, nx, ny)] - (double)chi[gidx(wrapi(x - 1, nx), y, z, nx, ny)];
     const double dXy = (double)chi[gidx(x, wrapi(y + 1, ny), z, nx, ny)] - (double)chi[gidx(x, wrapi(y - 1, ny), z, nx, ny)];
     const double dXz = (double)chi[gidx(x, y, wrapi(z + 1, nz), nx, ny)] - (double)chi[gidx(x, y, wrapi(z - 1, nz), nx, ny)];
-    if (!(dXx * dXx + dXy * dXy + dXz * dXz > 0)) continue;
-    const size_t o = gidx(x, y, z, nx, ny);
-    double r = rhs[o];
-    if (r > 0 && corr > 0) r -= corr * r;
-    else if (r < 0 && corr < 0) r += corr * r;
-    rhs[o] = r;
+    const size_t ro = BOXARR ? (size_t)i : gidx(x, y, z, nx, ny);
+    double r = rhs[ro];
+    if (dXx * dXx + dXy * dXy + dXz * dXz > 0) {
+      if (r > 0 && corr > 0) r -= corr * r;
+      else if (r < 0 && corr < 0) r += corr * r;
+      if (!BOXARR) rhs[ro] = r;
+    }
+    if constexpr (BOXARR) delta[i] = r - delta[i];
   }
+}
+
+// The first half of the RHS obstacle terms on the box, for passes that
+// recompute b0 = KernelPressureRHS(u*) (source/operators/PressureRHS.cpp:51-76)
+// themselves: b0 at each box cell (in the operation order of the z-queue
+// passes' b from u*) into d, b1 = b0 - chi b0 into b (box [z][y][x] order), and
+// the partial sums of k_rhs_obstacle (bulk source, positive / negative surface
+// b1). k_rhs_obstacle_correct<T, true> then turns d into b2 - b0.
+template <typename T>
+__global__ void k_box_rhs_obstacle(const T* u, const T* v, const T* w, const T* chi, Box box, int nx, int ny, int nz,
+                                   DtArg dt, double h, double* b, double* d, double* partials /* [gridDim.x][3] */) {
+  pdl_entry();
+  __shared__ double scratch[3 * 32];
+  const double facB = 0.5 * h * h / dt.get();
+  double acc[3] = {0, 0, 0};
+  const long long n = box.count();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int x = wrapi(box.lo[0] + (int)(i % box.n[0]), nx);
+    const int y = wrapi(box.lo[1] + (int)((i / box.n[0]) % box.n[1]), ny);
+    const int z = wrapi(box.lo[2] + (int)(i / ((long long)box.n[0] * box.n[1])), nz);
+    const size_t oxp = gidx(wrapi(x + 1, nx), y, z, nx, ny), oxm = gidx(wrapi(x - 1, nx), y, z, nx, ny);
+    const size_t oyp = gidx(x, wrapi(y + 1, ny), z, nx, ny), oym = gidx(x, wrapi(y - 1, ny), z, nx, ny);
+    const size_t ozp = gidx(x, y, wrapi(z + 1, nz), nx, ny), ozm = gidx(x, y, wrapi(z - 1, nz), nx, ny);
+    const double partD = facB * (((double)u[oxp] - (double)u[oxm]) + ((double)v[oyp] - (double)v[oym]));
+    const double b0 = partD + facB * ((double)w[ozp] - (double)w[ozm]);
+    const double X = chi[gidx(x, y, z, nx, ny)];
+    const double dXx = (double)chi[oxp] - (double)chi[oxm];
+    const double dXy = (double)chi[oyp] - (double)chi[oym];
+    const double dXz = (double)chi[ozp] - (double)chi[ozm];
+    const bool bSurface = dXx * dXx + dXy * dXy + dXz * dXz > 0;
+    const double srcBulk = -X * b0;
+    acc[0] += srcBulk;
+    const double r = b0 + srcBulk;
+    acc[1] += bSurface * r * (r > 0);
+    acc[2] -= bSurface * r * (r < 0);
+    b[i] = r;
+    d[i] = b0;
+  }
+  block_reduce<3, false>(acc, scratch);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) partials[3 * blockIdx.x + k] = acc[k];
 }
 
 // Surface forces of the sphere: the surface points of KernelCharacteristicFunction

@@ -1,12 +1,10 @@
-// Pressure-stage kernels of the FP32 defect-correction step (no obstacle),
-// register z-queue form:
-//   RHS_RES    b = KernelPressureRHS(u*) (source/operators/PressureRHS.cpp:51-76)
-//              and the first FP64 residual r = b - h/4 L_2h p of the warm start,
-//              in one pass: b to HBM in FP64, r in FP32 for the FFT solve.
+// Pressure-stage kernels of the FP32 defect-correction step, register z-queue
+// form; every pass recomputes b = KernelPressureRHS(u*)
+// (source/operators/PressureRHS.cpp:51-76) from u* (bit-identical in each):
+//   RHS_RES    the first FP64 residual r = b - h/4 L_2h p of the warm start,
+//              r in FP32 for the FFT solve.
 //   RES        r = b - h/4 L_2h p before a further correction solve, minus the
 //              class means of b (its null-mode part), in FP32.
-//   RES0       check 0 on a given b (the RHS with its obstacle terms, which need
-//              global sums first): RES's loads, RHS_RES's outputs.
 //   GRAD_CHECK KernelGradP (source/operators/PressureProjection.cpp:38-50) on
 //              u* with the current p, written to a separate buffer so that it
 //              can be redone, fused with the residual check of that p (the
@@ -16,17 +14,20 @@
 //              unpredictable part of b is the white FP32 rounding noise of the
 //              stored velocity; a quadratic extrapolation amplifies it more
 //              than it gains on the smooth part.)
+//   GRAD_CHECK_BOX  GRAD_CHECK with an obstacle: the max |u + uinf| leaves
+//              out the obstacle's box (the penalization pass covers it).
+// BD: with the obstacle, b also carries the RHS obstacle terms
+// (PressureRHS.cpp:78-112, 215-256), formed on the obstacle's box by one small
+// pass and added back here on the box.
 // L_2h is the wide-stencil Laplacian (neighbours at +-2) the spectral solve
-// inverts; p is FP64 throughout. (Storing b costs 16 B/cell against
-// recomputing it from u* in every pass, but the gradient pass is
-// instruction-bound and measured faster reading b.)
+// inverts; p is FP64 throughout.
 //
 // Structure as k_advect_zq: each thread owns CPT (x, y) columns of a TY x nx
 // row tile and marches down z; planes of p (TY + 4 rows: the +-2 halo in y)
 // arrive by TMA into a ring of NS slots, the centre values of the last 5
 // planes sit in a register queue (the z stencil), the x/y part of each plane
 // is computed on arrival and completed two planes later. The point-wise fields
-// of an output plane (b, u*, the previous p) ride in the slot of the load that
+// of an output plane (u*, the previous p) ride in the slot of the load that
 // completes it.
 // Partial sums per CTA: the 18-value residual layout (sum r^2 with the null
 // parts removed after check 0, sum b^2 and the class sums of r at check 0,
@@ -40,9 +41,7 @@
 
 namespace cup {
 
-// GRAD_CHECK_BOX: GRAD_CHECK with an obstacle (the max |u + uinf| leaves out
-// the obstacle's box, which the penalization pass covers)
-enum { PZQ_RHS_RES = 0, PZQ_RES = 1, PZQ_GRAD_CHECK = 2, PZQ_RES0 = 3, PZQ_GRAD_CHECK_BOX = 4 };
+enum { PZQ_RHS_RES = 0, PZQ_RES = 1, PZQ_GRAD_CHECK = 2, PZQ_GRAD_CHECK_BOX = 3 };
 
 template <int MODE>
 constexpr bool pzq_grad() {
@@ -52,8 +51,7 @@ constexpr bool pzq_grad() {
 struct PzqMaps {
   CUtensorMap p_main, p_halo;  // FP64 p: box {nx, TY, 1} and {nx, 2, 1}
   CUtensorMap f_main[3];       // u*, v*, w* (storage type): box {nx, TY, 1}
-  CUtensorMap v_halo;          // v*: box {nx, 1, 1} (RHS_RES)
-  CUtensorMap b_main;          // FP64 b: box {nx, TY, 1} (RES, GRAD_CHECK)
+  CUtensorMap v_halo;          // v*: box {nx, 1, 1}
   CUtensorMap h_main;          // FP64 pressure of the previous step p_n: box {nx, TY, 1} (GRAD_CHECK)
 };
 
@@ -73,60 +71,45 @@ struct PzqParams {
   int pred_order;
   double* pred_out;
   Box box;  // GRAD_CHECK_BOX: the obstacle's box
+  // BD: the obstacle terms of the RHS on the box (b2 - b0, box [z][y][x]
+  // order), added to the b the pass recomputes from u*
+  const double* bdelta;
 };
 
-// Whether a pass computes b from u* (RHS_RES always; RES and GRAD_CHECK when
-// BU: b is not stored) or reads the stored b (RES0, GRAD_CHECK_BOX: the RHS
-// with its obstacle terms; RES and GRAD_CHECK without BU).
-template <int MODE, bool BU>
-constexpr bool pzq_div() {
-  return MODE == PZQ_RHS_RES || BU;
-}
-
 // Byte layout of one ring slot (all parts multiples of 64 B for nx >= 16).
-template <typename T, int MODE, int TY, bool BU>
+template <typename T, int MODE, int TY>
 struct PzqSlot {
   static constexpr int G = 2;
-  static constexpr bool DIV = pzq_div<MODE, BU>();
-  static constexpr bool READ_B = !DIV;
   __host__ __device__ static size_t p_bytes(int nx) { return (size_t)(TY + 2 * G) * nx * sizeof(double); }
   // b from u*: u [TY], v [TY + 2], w [TY] rows of T
   __host__ __device__ static size_t u_off(int nx) { return p_bytes(nx); }
   __host__ __device__ static size_t v_off(int nx) { return u_off(nx) + (size_t)TY * nx * sizeof(T); }
   __host__ __device__ static size_t w_off(int nx) { return v_off(nx) + (size_t)(TY + 2) * nx * sizeof(T); }
-  __host__ __device__ static size_t div_end(int nx) {
-    return DIV ? w_off(nx) + (size_t)TY * nx * sizeof(T) : p_bytes(nx);
-  }
-  // stored b: b [TY] rows of double
-  __host__ __device__ static size_t b_off(int nx) { return div_end(nx); }
-  __host__ __device__ static size_t b_end(int nx) {
-    return b_off(nx) + (READ_B ? (size_t)TY * nx * sizeof(double) : 0);
-  }
+  __host__ __device__ static size_t div_end(int nx) { return w_off(nx) + (size_t)TY * nx * sizeof(T); }
   // GRAD_CHECK: u*, v*, w* [TY] rows of T of the output plane
-  __host__ __device__ static size_t f_off(int nx, int f) { return b_end(nx) + (size_t)f * TY * nx * sizeof(T); }
+  __host__ __device__ static size_t f_off(int nx, int f) { return div_end(nx) + (size_t)f * TY * nx * sizeof(T); }
   // GRAD_CHECK: then the rows of the previous step's p [TY] of double
   __host__ __device__ static size_t h_off(int nx) { return f_off(nx, 3); }
   __host__ __device__ static size_t bytes(int nx) {
-    size_t s = pzq_grad<MODE>() ? h_off(nx) + (size_t)TY * nx * sizeof(double) : b_end(nx);
+    size_t s = pzq_grad<MODE>() ? h_off(nx) + (size_t)TY * nx * sizeof(double) : div_end(nx);
     return (s + 127) / 128 * 128;
   }
 };
 
-template <typename T, int MODE, int TY, int NS, bool BU = false>
+template <typename T, int MODE, int TY, int NS>
 constexpr size_t pzq_smem_bytes_host(int nx) {
-  return (size_t)NS * PzqSlot<T, MODE, TY, BU>::bytes(nx) + NS * sizeof(uint64_t) + 18 * 32 * sizeof(double);
+  return (size_t)NS * PzqSlot<T, MODE, TY>::bytes(nx) + NS * sizeof(uint64_t) + 18 * 32 * sizeof(double);
 }
 
 // blockDim.x * CPT == TY * nx (<= 512 threads), TY even.
 // NXC, ZCC: nx and the planes per work item fixed at compile time (0: read
 // from g); fixed, the stencil's shared-memory offsets are immediates and the
 // ring slot of each plane is known.
-// BU: b recomputed from u* in every pass instead of stored by RHS_RES (no
-// obstacle: the RHS is the divergence alone).
-template <typename T, int MODE, int TY, int NS, int CPT, int NXC = 0, int ZCC = 0, bool BU = false>
+// BD: the obstacle terms of b added back on the box (prm.bdelta).
+template <typename T, int MODE, int TY, int NS, int CPT, int NXC = 0, int ZCC = 0, bool BD = false>
 __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps maps, const StreamGeom g,
                                                 T* __restrict__ ou, T* __restrict__ ov, T* __restrict__ ow,
-                                                double* __restrict__ bout, float* __restrict__ rout,
+                                                float* __restrict__ rout,
                                                 double* __restrict__ partials, const double* __restrict__ rmean,
                                                 const PzqParams prm, int* err, const int* skip) {
   pdl_entry();
@@ -136,10 +119,8 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
   constexpr bool SLOT_CT = ZCC != 0 && (ZCC + 2 * G) % NS == 0;  // ring slot of plane j is j % NS
   static_assert(TY >= G && TY % 2 == 0, "tile height must cover the halo depth and keep the row parity");
   static_assert(ZCC % 2 == 0, "paired barriers and the z parity need an even plane count");
-  using Slot = PzqSlot<T, MODE, TY, BU>;
-  constexpr bool DIV = Slot::DIV;
-  static_assert(!BU || MODE == PZQ_RHS_RES || MODE == PZQ_RES || MODE == PZQ_GRAD_CHECK,
-                "obstacle passes read the stored RHS");
+  using Slot = PzqSlot<T, MODE, TY>;
+  static_assert(BD || MODE != PZQ_GRAD_CHECK_BOX, "with the obstacle, b needs its terms");
   if (skip && *skip) return;  // converged defect correction: nothing to check
   extern __shared__ __align__(128) unsigned char smem_dyn[];
   unsigned char* smem_raw = smem_align128(smem_dyn);
@@ -179,13 +160,8 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     const bool xy_plane = j >= G && j < G + zc;    // planes whose x/y part is computed
     const bool w_plane = j >= 1 && j < PL - 1;        // planes at z0-1 .. z0+zc (w at z +- 1)
     const bool out_plane = j >= 2 * G;                // completes output plane j - 2G
-    if constexpr (DIV) {
-      if (xy_plane) bytes += rowsT + (uint32_t)((TY + 2) * nx * sizeof(T));
-      if (w_plane) bytes += rowsT;
-    }
-    if constexpr (Slot::READ_B) {
-      if (out_plane) bytes += rowsD;
-    }
+    if (xy_plane) bytes += rowsT + (uint32_t)((TY + 2) * nx * sizeof(T));
+    if (w_plane) bytes += rowsT;
     if constexpr (pzq_grad<MODE>()) {
       if (out_plane) bytes += 3 * rowsT + (prm.pred_order >= 1 ? rowsD : 0u);
     }
@@ -194,19 +170,16 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     tma_load_3d(P, &maps.p_halo, 0, ylo, z, &full[s]);
     tma_load_3d(P + G * nx, &maps.p_main, 0, y0, z, &full[s]);
     tma_load_3d(P + (G + TY) * nx, &maps.p_halo, 0, yhi, z, &full[s]);
-    if constexpr (DIV) {
-      if (xy_plane) {
-        tma_load_3d(dst + Slot::u_off(nx), &maps.f_main[0], 0, y0, z, &full[s]);
-        T* V = reinterpret_cast<T*>(dst + Slot::v_off(nx));
-        tma_load_3d(V, &maps.v_halo, 0, y0 == 0 ? ny - 1 : y0 - 1, z, &full[s]);
-        tma_load_3d(V + nx, &maps.f_main[1], 0, y0, z, &full[s]);
-        tma_load_3d(V + (TY + 1) * nx, &maps.v_halo, 0, yhi, z, &full[s]);
-      }
-      if (w_plane) tma_load_3d(dst + Slot::w_off(nx), &maps.f_main[2], 0, y0, z, &full[s]);
+    if (xy_plane) {
+      tma_load_3d(dst + Slot::u_off(nx), &maps.f_main[0], 0, y0, z, &full[s]);
+      T* V = reinterpret_cast<T*>(dst + Slot::v_off(nx));
+      tma_load_3d(V, &maps.v_halo, 0, y0 == 0 ? ny - 1 : y0 - 1, z, &full[s]);
+      tma_load_3d(V + nx, &maps.f_main[1], 0, y0, z, &full[s]);
+      tma_load_3d(V + (TY + 1) * nx, &maps.v_halo, 0, yhi, z, &full[s]);
     }
+    if (w_plane) tma_load_3d(dst + Slot::w_off(nx), &maps.f_main[2], 0, y0, z, &full[s]);
     if (out_plane) {
       const int zk = z0 + (j - 2 * G);  // output plane completed by this load (< nz)
-      if constexpr (Slot::READ_B) tma_load_3d(dst + Slot::b_off(nx), &maps.b_main, 0, y0, zk, &full[s]);
       if constexpr (pzq_grad<MODE>()) {
 #pragma unroll
         for (int f = 0; f < 3; ++f) tma_load_3d(dst + Slot::f_off(nx, f), &maps.f_main[f], 0, y0, zk, &full[s]);
@@ -236,8 +209,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
     xp2[i] = (cx[i] + 2) & mask;
 #pragma unroll
     for (int zp = 0; zp < 2; ++zp)
-      rm[i][zp] = (MODE == PZQ_RHS_RES || MODE == PZQ_RES0) ? 0.0
-                                                            : rmean[(cx[i] & 1) | ((cy[i] & 1) << 1) | (zp << 2)];
+      rm[i][zp] = MODE == PZQ_RHS_RES ? 0.0 : rmean[(cx[i] & 1) | ((cy[i] & 1) << 1) | (zp << 2)];
   }
   const size_t plane = (size_t)nx * ny;
   const double dtv = prm.dt.get();
@@ -304,12 +276,10 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
           const int QN = jj % Q;
 #pragma unroll
           for (int i = 0; i < CPT; ++i) pq[QN][i] = P[(G + cy[i]) * nx + cx[i]];
-          if constexpr (DIV) {
-            if (j >= 1 && j < PL - 1) {
-              const T* W = reinterpret_cast<const T*>(sl + Slot::w_off(nx));
+          if (j >= 1 && j < PL - 1) {
+            const T* W = reinterpret_cast<const T*>(sl + Slot::w_off(nx));
 #pragma unroll
-              for (int i = 0; i < CPT; ++i) wq[QN][i] = W[cy[i] * nx + cx[i]];
-            }
+            for (int i = 0; i < CPT; ++i) wq[QN][i] = W[cy[i] * nx + cx[i]];
           }
           // output plane k = j - 2G (z parity of k = jj parity: z0 and j0 are even)
           if (j >= 2 * G) {
@@ -326,15 +296,13 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
               const double p0 = pq[QC][i];
               const double lap = partL[PS][i] + (pq[QP2][i] + pq[QM2][i] - 2 * p0);
               pc[i][zp] += p0;
-              // b: from u* (x/y part on arrival, z part here) or the stored RHS
-              double b;
-              if constexpr (DIV) {
-                b = partD[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
-              } else {
-                b = reinterpret_cast<const double*>(sl + Slot::b_off(nx))[c];
+              // b from u* (x/y part on arrival, z part here), plus the obstacle terms on the box
+              double b = partD[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
+              if constexpr (BD) {
+                const int bi = prm.box.index(cx[i], y0 + cy[i], z0 + k, nx, ny, nz);
+                if (bi >= 0) b += prm.bdelta[bi];
               }
-              if constexpr (MODE == PZQ_RHS_RES || MODE == PZQ_RES0) {
-                if constexpr (MODE == PZQ_RHS_RES && !BU) bout[o] = b;
+              if constexpr (MODE == PZQ_RHS_RES) {
                 const double r = b - cL * lap;
                 rc[i][zp] += r;  // the class means of b (only check 0 needs them)
                 rout[o] = (float)r;
@@ -383,7 +351,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
               const double p0 = pq[QN][i];
               const double* Pc = P + (G + cy[i]) * nx;  // this column's row of p
               partL[PS][i] = (Pc[xp2[i]] + Pc[xm2[i]] - 2 * p0) + (Pc[2 * nx + x] + Pc[x - 2 * nx] - 2 * p0);
-              if constexpr (DIV) {
+              {
                 const T* Urow = reinterpret_cast<const T*>(sl + Slot::u_off(nx)) + cy[i] * nx;
                 const T* Vc = reinterpret_cast<const T*>(sl + Slot::v_off(nx)) + (cy[i] + 1) * nx;  // row of v*
                 partD[PS][i] = facB * (((double)Urow[xp1[i]] - (double)Urow[xm1[i]]) +
