@@ -224,6 +224,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
   // (GRAD_CHECK) the gradient of p and the u*, v* centre values
   double partL[G][CPT];
   double partD[G][CPT];          // x/y part of the divergence (b from u*)
+  double partB[BD ? G : 1][CPT];  // BD: the obstacle terms of the output cell, loaded two planes ahead
   double gA[G][CPT], gB[G][CPT];  // x- and y-gradient of p (GRAD_CHECK)
   double pc[CPT][2], rc[CPT][2];  // parity-class sums of p and r by z parity
   double acc0 = 0, acc1 = 0;
@@ -248,6 +249,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
 #pragma unroll
     for (int i = 0; i < CPT; ++i) {
       partL[d][i] = partD[d][i] = gA[d][i] = gB[d][i] = 0.0;
+      if constexpr (BD) partB[d][i] = 0.0;
     }
 #pragma unroll
   for (int i = 0; i < CPT; ++i) pc[i][0] = pc[i][1] = rc[i][0] = rc[i][1] = 0.0;
@@ -298,10 +300,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
               pc[i][zp] += p0;
               // b from u* (x/y part on arrival, z part here), plus the obstacle terms on the box
               double b = partD[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
-              if constexpr (BD) {
-                const int bi = prm.box.index(cx[i], y0 + cy[i], z0 + k, nx, ny, nz);
-                if (bi >= 0) b += prm.bdelta[bi];
-              }
+              if constexpr (BD) b += partB[PS][i];
               if constexpr (MODE == PZQ_RHS_RES) {
                 const double r = b - cL * lap;
                 rc[i][zp] += r;  // the class means of b (only check 0 needs them)
@@ -356,6 +355,11 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
                 const T* Vc = reinterpret_cast<const T*>(sl + Slot::v_off(nx)) + (cy[i] + 1) * nx;  // row of v*
                 partD[PS][i] = facB * (((double)Urow[xp1[i]] - (double)Urow[xm1[i]]) +
                                        ((double)Vc[nx + x] - (double)Vc[x - nx]));
+              }
+              if constexpr (BD) {
+                // the box's b2 - b0 of output cell (x, y, z0 + j - G), used two planes later
+                const int bi = prm.box.index(x, y0 + cy[i], z0 + j - G, nx, ny, nz);
+                partB[PS][i] = bi >= 0 ? __ldg(prm.bdelta + bi) : 0.0;
               }
               if constexpr (pzq_grad<MODE>()) {
                 gA[PS][i] = Pc[xp1[i]] - Pc[xm1[i]];
