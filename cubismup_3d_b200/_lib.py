@@ -25,6 +25,7 @@ CUP_SCHEME_REF = 0
 CUP_SCHEME_UPWIND3_RK2 = 1
 CUP_WHERE_HOST = 0
 CUP_WHERE_DEVICE = 1
+CUP_FIELD_U, CUP_FIELD_V, CUP_FIELD_W, CUP_FIELD_P, CUP_FIELD_RHS = 0, 1, 2, 3, 4
 
 ERROR_NAMES = {
     CUP_ERR_ARG: "CUP_ERR_ARG", CUP_ERR_CUDA: "CUP_ERR_CUDA", CUP_ERR_NONFINITE: "CUP_ERR_NONFINITE",
@@ -47,6 +48,7 @@ class CupConfig(C.Structure):
         ("dc_max_iter", C.c_int),
         ("dc_min_iter", C.c_int),
         ("device", C.c_int),
+        ("z_halo", C.c_int),
     ]
 
 
@@ -90,6 +92,7 @@ SIGNATURES = {
     "cup_get_pressure": (C.c_int, [_H, C.c_void_p, C.c_int]),
     "cup_get_chi": (C.c_int, [_H, C.c_void_p, C.c_int]),
     "cup_get_rhs": (C.c_int, [_H, C.c_void_p, C.c_int]),
+    "cup_field_ptr": (C.c_int, [_H, C.c_int, C.POINTER(C.c_void_p)]),
     "cup_blocks_to_global": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "cup_global_to_blocks": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
     "cup_add_sphere": (C.c_int, [_H, C.POINTER(CupSphere)]),

@@ -1143,6 +1143,8 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   constexpr bool T8 = M == 128;
   constexpr int N = 2 * M, TPL = T8 ? 8 : M / 8, NB = T8 ? 2 : 3;
   constexpr int W = sizeof(R) == 4 ? 32 : 16;
+  if (AXIS == 2 && H->cfg.z_halo)
+    return fail(H, CUP_ERR_STATE, "a z-slab handle has no z transform (the Poisson solve runs over the ranks)");
   if (H->nx % W) return fail(H, CUP_ERR_ARG, "nx must be a multiple of %d for this precision", W);
   CUtensorMap map_in, map_out;
   int rc = make_map(H, &map_in, in, tma_dtype<RIN>(), sizeof(RIN), W, AXIS == 1 ? N : 1, AXIS == 2 ? N : 1);
@@ -2471,11 +2473,26 @@ int cup_create(const cup_config* cfg, cup_handle** out) {
     delete H;
     return code;
   };
-  for (int d = 0; d < 3; ++d)
+  const bool slab = cfg->z_halo != 0;
+  for (int d = 0; d < 3; ++d) {
+    if (slab && d == 2) {
+      // a z-slab with ghost planes: no z transform on this handle
+      if (cfg->z_halo < 4 || N[2] < 2 * cfg->z_halo + 16 || N[2] > 512) {
+        fail(H, CUP_ERR_ARG, "a z-slab handle needs z_halo >= 4 and 16 to %d interior planes (got z_halo %d, nz %d)",
+             512 - 2 * cfg->z_halo, cfg->z_halo, N[2]);
+        return reject(CUP_ERR_ARG);
+      }
+      continue;
+    }
     if (N[d] < 16 || N[d] > 256 || !is_pow2(N[d])) {
       fail(H, CUP_ERR_ARG, "cells per dimension must be a power of two in [16, 256] (got %d)", N[d]);
       return reject(CUP_ERR_ARG);
     }
+  }
+  if (slab && cfg->precision != CUP_PREC_FP64) {
+    fail(H, CUP_ERR_ARG, "a z-slab handle is FP64 (its defect correction would need sums over the ranks)");
+    return reject(CUP_ERR_ARG);
+  }
   if (!(cfg->maxextent > 0)) {
     fail(H, CUP_ERR_ARG, "maxextent must be > 0");
     return reject(CUP_ERR_ARG);
@@ -2535,6 +2552,7 @@ int cup_create(const cup_config* cfg, cup_handle** out) {
     // FFT tables per axis, spectral cosines exactly as PoissonSolverPeriodic::_solve
     // computes them (source/poisson/PoissonSolverPeriodic.cpp:23-33).
     for (int d = 0; d < 3; ++d) {
+      if (slab && d == 2) continue;  // no z transform on a z-slab handle
       std::vector<double2> t64;
       std::vector<float2> t32;
       build_table(N[d], t64, t32);
@@ -2550,6 +2568,7 @@ int cup_create(const cup_config* cfg, cup_handle** out) {
     H->spec_y0 = 0;
     double** cs[3] = {&H->cosx, &H->cosy, &H->cosz};
     for (int d = 0; d < 3; ++d) {
+      if (slab && d == 2) continue;
       const long nK = (long)gsize[d];
       const double wFac = 4 * M_PI / nK;
       std::vector<double> c(nK);
@@ -2667,6 +2686,20 @@ int cup_get_rhs(cup_handle* H, double* r, int where) {
                      where == CUP_WHERE_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, H->stream));
   CK(cudaStreamSynchronize(H->stream));
   return check_dev_error(H);
+}
+
+int cup_field_ptr(cup_handle* H, int field, void** ptr) {
+  REQUIRE_H(H);
+  if (!ptr) return fail(H, CUP_ERR_ARG, "cup_field_ptr: null output");
+  switch (field) {
+    case CUP_FIELD_U: *ptr = H->u; break;
+    case CUP_FIELD_V: *ptr = H->v; break;
+    case CUP_FIELD_W: *ptr = H->w; break;
+    case CUP_FIELD_P: *ptr = H->p; break;
+    case CUP_FIELD_RHS: *ptr = H->rhs; break;
+    default: return fail(H, CUP_ERR_ARG, "cup_field_ptr: unknown field %d", field);
+  }
+  return CUP_OK;
 }
 
 int cup_get_chi(cup_handle* H, double* chi, int where) {

@@ -53,6 +53,7 @@ class SimulationData:
     dc_max_iter: int = 2
     dc_min_iter: int = 1
     device: int = 0
+    z_halo: int = 0           # > 0: one rank's z-slab with this many ghost planes a side (slab.SlabSimulation)
     verbose: bool = False
     freqDiagnostics: int = 0  # ComputeDissipation every this many steps (0: off), to diagnostics.dat
     turbKinEn_target: float = 0.0   # SpectralForcing: hold the kinetic energy at this value ...
@@ -95,6 +96,7 @@ class SimulationData:
         cfg.dc_max_iter = int(self.dc_max_iter)
         cfg.dc_min_iter = int(self.dc_min_iter)
         cfg.device = int(self.device)
+        cfg.z_halo = int(self.z_halo)
         return cfg
 
 

@@ -22,6 +22,16 @@ send/recv where the backend has no all-to-all) and ``LocalExchange`` (G ranks
 emulated in one process, for tests). The transforms are pluggable too: the
 CUDA passes of the library (``CudaPasses``) or any object with the same two
 methods.
+
+``SlabSimulation`` runs the whole FP64 step on such a slab, the reference's
+Cartesian decomposition (source/SimulationData.cpp:211-230) restricted to z:
+the rank's handle holds its slab plus HALO ghost planes on each side
+(cup_config.z_halo), the stencil operators run on all of it (the ghost planes
+absorb the periodic wrap of the kernels, so the interior outputs are exact
+while the stencils reach at most HALO planes out), and ghost planes are
+refreshed from the neighbouring ranks by a halo exchange of whole planes
+(contiguous in the [z][y][x] layout) before they are read: the velocity after
+every step, the pressure after the solve. The Poisson solve is ``solve`` above.
 """
 from __future__ import annotations
 
@@ -60,14 +70,53 @@ class TorchExchange:
         return recv
 
 
+    def halo(self, send_down, send_up):
+        """Ghost planes from the neighbours: ``send_down`` (this rank's first
+        interior planes) goes to rank - 1, ``send_up`` (its last ones) to rank +
+        1 (periodic); returns (from the rank above, from the rank below), i.e.
+        the upper and the lower ghost planes. Messages between two ranks pair up
+        in posting order, which also holds when both neighbours are the same rank."""
+        import torch
+        dist = self.dist
+        up, down = (self.rank + 1) % self.world, (self.rank - 1) % self.world
+        from_up, from_down = torch.empty_like(send_down), torch.empty_like(send_up)
+        if self.world == 1:
+            from_up.copy_(send_down)
+            from_down.copy_(send_up)
+            return from_up, from_down
+        ops = [dist.P2POp(dist.isend, send_down.contiguous(), down, self.group),
+               dist.P2POp(dist.isend, send_up.contiguous(), up, self.group),
+               dist.P2POp(dist.irecv, from_up, up, self.group),
+               dist.P2POp(dist.irecv, from_down, down, self.group)]
+        for r in dist.batch_isend_irecv(ops):
+            r.wait()
+        return from_up, from_down
+
+    def max(self, value: float) -> float:
+        """Maximum of a scalar over the ranks."""
+        import torch
+        t = torch.tensor([float(value)], dtype=torch.float64,
+                         device="cuda" if self.dist.get_backend(self.group) == "nccl" else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX, group=self.group)
+        return float(t.item())
+
+
 class LocalExchange:
     """G ranks emulated in one process: ``exchange_all(sends)`` takes every
-    rank's send list and returns every rank's receive list."""
+    rank's send list and returns every rank's receive list; ``halo_all`` does
+    the same for the ghost-plane exchange."""
 
     @staticmethod
     def exchange_all(sends: Sequence[Sequence]) -> List[List]:
         G = len(sends)
         return [[sends[r][s] for r in range(G)] for s in range(G)]
+
+    @staticmethod
+    def halo_all(sends: Sequence) -> List:
+        """sends[r] = (send_down, send_up) of rank r; returns, per rank, (from
+        the rank above, from the rank below)."""
+        G = len(sends)
+        return [(sends[(r + 1) % G][0], sends[(r - 1) % G][1]) for r in range(G)]
 
 
 class CudaPasses:
@@ -164,3 +213,155 @@ def solve_emulated(rhs_slabs: Sequence, passes: Sequence):
     for b, ps in zip(bufs, passes):
         ps.yx(b)
     return bufs
+
+
+class SlabSimulation:
+    """One rank's z-slab (nz/G planes) of a periodic FP64 simulation split over
+    G ranks along z, with HALO ghost planes on each side. ``sd`` describes the
+    whole grid (cells, extent, nu, CFL, scheme, ...); ``device`` the rank's GPU.
+
+    A step (``step`` with a TorchExchange, or ``step_emulated`` for G slabs in
+    one process): AdvectionDiffusion and PressureRHS on the slab with its ghost
+    planes (upwind3 + RK2 reaches 4 planes out, the RHS one more: the interior
+    RHS is exact), the decomposed Poisson solve of the interior RHS, the
+    pressure's ghost planes from the neighbours, the gradient correction, and
+    the velocity's ghost planes from the neighbours for the next step and its
+    CFL maximum (over the ranks: Simulation::calcMaxTimestep,
+    source/Simulation.cpp:403-424). No obstacle."""
+
+    HALO = 8  # a multiple of 8 keeps the slab's planes a multiple of 16; the stencils need 5
+
+    def __init__(self, sd, rank: int, world: int, device=None):
+        import dataclasses
+        from .simulation import Simulation
+        nx, ny, nz = sd.cells
+        if nz % world or ny % world:
+            raise ValueError("ny and nz must be divisible by the number of ranks")
+        self.nzl = nz // world
+        if self.nzl < 16 or self.nzl % 16:
+            raise ValueError("each rank's slab must be a multiple of 16 planes")
+        if sd.precision != "fp64":
+            raise ValueError("the z-slab step is FP64")
+        self.sd, self.rank, self.world = sd, rank, world
+        self.device = sd.device if device is None else device
+        self.h = sd.extent / max(sd.cells)
+        H = self.HALO
+        ext = (nx, ny, self.nzl + 2 * H)
+        local = dataclasses.replace(sd, cells=ext, extent=self.h * max(ext), z_halo=H, device=self.device,
+                                    freqDiagnostics=0, saveFreq=0, saveTime=0.0)
+        self.sim = Simulation(local)
+        self.passes = CudaPasses(sd.cells, self.h, rank, world, device=self.device)
+        self.step_count, self.time = 0, 0.0
+
+    # -- fields -------------------------------------------------------------------
+    def _field(self, which: int):
+        import torch
+        from .simulation import _DeviceArray
+        ptr = C.c_void_p()
+        L.check(L.lib().cup_field_ptr(self.sim._h, which, C.byref(ptr)), self.sim._h, "field pointer")
+        return torch.as_tensor(_DeviceArray(ptr.value, self.sim.shape, self.device), device=f"cuda:{self.device}")
+
+    def _velocity(self):
+        return [self._field(f) for f in (L.CUP_FIELD_U, L.CUP_FIELD_V, L.CUP_FIELD_W)]
+
+    @property
+    def interior(self):
+        return slice(self.HALO, self.HALO + self.nzl)
+
+    def set_velocity(self, u, v, w):
+        """From the whole grid's velocity (host arrays of shape (nz, ny, nx)): this
+        rank's slab and its ghost planes (the periodic neighbours' planes)."""
+        import numpy as np
+        nz = self.sd.cells[2]
+        z = (np.arange(-self.HALO, self.nzl + self.HALO) + self.rank * self.nzl) % nz
+        self.sim.set_velocity(*(np.ascontiguousarray(np.asarray(a)[z]) for a in (u, v, w)))
+
+    def velocity(self):
+        """This rank's slab of the velocity (host arrays, nz/G planes)."""
+        return [a[self.interior] for a in self.sim.velocity()]
+
+    # -- the step's phases ----------------------------------------------------------
+    def _halo_sends(self, fields):
+        H, n = self.HALO, self.nzl
+        return [(f[H:2 * H].clone(), f[n:n + H].clone()) for f in fields]
+
+    def _halo_recv(self, fields, recvs):
+        H, n = self.HALO, self.nzl
+        for f, (from_up, from_down) in zip(fields, recvs):
+            f[n + H:].copy_(from_up)
+            f[:H].copy_(from_down)
+
+    def _advect_rhs(self, dt: float):
+        self.sim.bind_torch_stream()
+        L.check(L.lib().cup_advect_diffuse(self.sim._h, float(dt)), self.sim._h, "AdvectionDiffusion")
+        L.check(L.lib().cup_pressure_rhs(self.sim._h, float(dt)), self.sim._h, "PressureRHS")
+        return self._field(L.CUP_FIELD_RHS)[self.interior].contiguous()
+
+    def _set_pressure(self, p):
+        self._field(L.CUP_FIELD_P)[self.interior].copy_(p)
+
+    def _grad(self, dt: float):
+        self.sim.bind_torch_stream()
+        L.check(L.lib().cup_grad_correct(self.sim._h, float(dt)), self.sim._h, "PressureProjection")
+        self.step_count += 1
+        self.time += dt
+
+    def local_umax(self) -> float:
+        """max |u + uinf| over the slab and its ghost planes (neighbours' cells)."""
+        return self.sim.max_velocity()
+
+    def dt_from_umax(self, umax: float) -> float:
+        """Simulation::calcMaxTimestep (source/Simulation.cpp:403-424) on the
+        maximum over the ranks."""
+        import math
+        sd = self.sd
+        dt_dif = self.h * self.h / sd.nu if sd.nu > 0 else math.inf
+        dt_adv = self.h / (umax + 1e-8)
+        cfl = sd.CFL
+        if self.step_count < sd.rampup:
+            x = (self.step_count + 1.0) / sd.rampup
+            cfl = math.exp(math.log(1e-3) * (1 - x) + math.log(sd.CFL) * x)
+        return cfl * min(dt_dif, dt_adv)
+
+    # -- one rank per process -------------------------------------------------------
+    def calc_max_timestep(self, exchange) -> float:
+        return self.dt_from_umax(exchange.max(self.local_umax()))
+
+    def step(self, dt: float, exchange):
+        rhs = self._advect_rhs(dt)
+        p = solve(rhs, self.passes, exchange, self.world)
+        self._set_pressure(p)
+        pf = [self._field(L.CUP_FIELD_P)]
+        self._halo_recv(pf, [exchange.halo(*snd) for snd in self._halo_sends(pf)])
+        self._grad(dt)
+        vel = self._velocity()
+        self._halo_recv(vel, [exchange.halo(*snd) for snd in self._halo_sends(vel)])
+
+    def close(self):
+        self.sim.close()
+        self.passes.close()
+
+
+def calc_max_timestep_emulated(slabs: Sequence[SlabSimulation]) -> float:
+    return slabs[0].dt_from_umax(max(s.local_umax() for s in slabs))
+
+
+def _halo_emulated(slabs: Sequence[SlabSimulation], fields: Sequence[Sequence]):
+    """Ghost planes of fields[r] (lists of the same fields on every slab r) from the neighbouring slabs."""
+    G = len(slabs)
+    sends = [s._halo_sends(f) for s, f in zip(slabs, fields)]
+    for k in range(len(fields[0])):
+        recvs = LocalExchange.halo_all([sends[r][k] for r in range(G)])
+        for r in range(G):
+            slabs[r]._halo_recv([fields[r][k]], [recvs[r]])
+
+
+def step_emulated(slabs: Sequence[SlabSimulation], dt: float):
+    """One step of G slabs held in one process (LocalExchange), phase by phase."""
+    rhs = [s._advect_rhs(dt) for s in slabs]
+    for s, p in zip(slabs, solve_emulated(rhs, [s.passes for s in slabs])):
+        s._set_pressure(p)
+    _halo_emulated(slabs, [[s._field(L.CUP_FIELD_P)] for s in slabs])
+    for s in slabs:
+        s._grad(dt)
+    _halo_emulated(slabs, [s._velocity() for s in slabs])

@@ -72,6 +72,13 @@ typedef struct cup_config {
                              one check per step, still verified against dc_tol */
   int dc_min_iter;        /* FP32_DC: solves always done per step (default 1 if <= 0) */
   int device;             /* CUDA device ordinal */
+  int z_halo;             /* 0: a whole periodic grid. > 0 (4 or more, FP64): the handle holds one rank's
+                             z-slab of a grid split over ranks along z, with z_halo ghost planes on each
+                             side included in bpdz; nz = 16*bpdz then needs only be a multiple of 16 (32..512)
+                             and the handle has no z Fourier transform: the stencil operators
+                             (cup_advect_diffuse, cup_pressure_rhs, cup_grad_correct, cup_max_velocity,
+                             cup_calc_max_timestep) run on it, with the ghost planes filled by the caller and
+                             the Poisson solve done over the ranks (the z-slab decomposed solve) */
 } cup_config;
 
 /* One sphere obstacle (source/obstacles/Sphere.cpp, ObstacleArguments in
@@ -121,6 +128,16 @@ int cup_get_pressure(struct cup_handle* h, double* p, int where);
 int cup_get_chi(struct cup_handle* h, double* chi, int where);
 /* Pressure-RHS buffer (h^3 div u* / dt after PressureRHS), FP64 */
 int cup_get_rhs(struct cup_handle* h, double* rhs, int where);
+
+/* Device address of one of the handle's fields (no counterpart in the reference,
+ * whose fields are the blocks' FluidElement members): CUP_FIELD_U/V/W (storage
+ * type: FP64, or FP32 with CUP_PREC_FP32_DC), CUP_FIELD_P and CUP_FIELD_RHS
+ * (FP64), each nz*ny*nx values in the field layout. The address holds until the
+ * next call that advances the handle (a step or operator swaps the velocity
+ * buffers); writes through it must be ordered with the handle's stream. Used to
+ * exchange the ghost planes of a z-slab handle (cup_config.z_halo) in place. */
+enum { CUP_FIELD_U = 0, CUP_FIELD_V = 1, CUP_FIELD_W = 2, CUP_FIELD_P = 3, CUP_FIELD_RHS = 4 };
+int cup_field_ptr(struct cup_handle* h, int field, void** ptr);
 
 /* Block-structured <-> global layout (Cubism FluidBlock data[z][y][x] per block,
  * blocks ordered x fastest): n = nx*ny*nz values. */

@@ -832,3 +832,66 @@ def test_slab_decomposed_poisson_solve(oracle, world):
     assert rel_l2(p, oracle.poisson_solve(rhs, h)) < 1e-12
     for x in passes:
         x.close()
+
+
+def make_sd(cells, extent, **kw):
+    import cubismup_3d_b200 as cup
+    sd = cup.SimulationData(CFL=kw.pop("CFL", 0.5), cells=cells)
+    sd.extent = extent
+    for k, v in kw.items():
+        setattr(sd, k, v)
+    return sd
+
+
+@pytest.mark.parametrize("world,scheme", [(1, "upwind3_rk2"), (2, "upwind3_rk2"), (4, "upwind3_rk2"), (2, "ref")])
+def test_slab_step_matches_whole_grid(oracle, world, scheme):
+    # The whole FP64 step on z-slabs with ghost planes (advection, RHS and
+    # gradient on each slab handle, the decomposed Poisson solve, halo
+    # exchanges of pressure and velocity), the ranks emulated in one process,
+    # against the one-handle step of the whole grid and against the oracle;
+    # the CFL dt from the maximum over the slabs
+    from cubismup_3d_b200 import slab
+    cells = (64, 64, 64)
+    sd = make_sd(cells, 2 * np.pi, nu=1e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0, scheme=scheme)
+    import cubismup_3d_b200 as cup
+    u, v, w = random_velocity(cells, 5, 0.5)
+    whole = cup.Simulation(sd)
+    whole.set_velocity(u, v, w)
+    slabs = [slab.SlabSimulation(sd, r, world) for r in range(world)]
+    for s in slabs:
+        s.set_velocity(u, v, w)
+    orc = oracle.OracleSim(*cells, 2 * np.pi, nu=1e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0, scheme=scheme)
+    orc.set_velocity(u, v, w)
+    for _ in range(3):
+        dt = whole.calcMaxTimestep()
+        assert slab.calc_max_timestep_emulated(slabs) == pytest.approx(dt, rel=1e-14)
+        whole.timestep(dt)
+        slab.step_emulated(slabs, dt)
+        orc.timestep(dt)
+    got = [np.concatenate([s.velocity()[q] for s in slabs], axis=0) for q in range(3)]
+    ref = whole.velocity()
+    ref_o = orc.velocity()
+    for q in range(3):
+        assert rel_l2(got[q], ref[q]) < 1e-12, q
+        assert rel_l2(got[q], ref_o[q]) < 1e-10, q
+    for s in slabs:
+        s.close()
+
+
+def test_slab_handle_has_no_z_transform():
+    # a z-slab handle (ghost planes, non-power-of-two nz) runs the stencil
+    # operators but refuses the Poisson solve, and needs FP64 and 4+ ghost planes
+    import cubismup_3d_b200 as cup
+    sd = make_sd((32, 32, 48), 1.0)
+    sd.z_halo = 8
+    sim = cup.Simulation(sd)
+    with pytest.raises(Exception):
+        sim.pressureSolver.solve()
+    sd2 = make_sd((32, 32, 48), 1.0, precision="fp32_dc")
+    sd2.z_halo = 8
+    with pytest.raises(ValueError):
+        cup.Simulation(sd2)
+    sd3 = make_sd((32, 32, 48), 1.0)
+    sd3.z_halo = 2
+    with pytest.raises(ValueError):
+        cup.Simulation(sd3)

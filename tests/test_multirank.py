@@ -216,3 +216,53 @@ def test_slab_blocks_round_trip():
     recv = slab.LocalExchange.exchange_all([slab.to_slab_blocks(pc, G) for pc in pencils])
     for r, rv in enumerate(recv):
         assert torch.equal(slab.from_slab_blocks(rv), slabs[r])
+
+
+def _halo_worker(rank, world, port, outdir):
+    import datetime
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    sys.path.insert(0, REPO)
+    from cubismup_3d_b200 import slab
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        ex = slab.TorchExchange()
+        H, n = 2, 5  # ghost planes, interior planes per rank; plane value = its global z
+        mine = torch.arange(rank * n, (rank + 1) * n, dtype=torch.float64).reshape(n, 1, 1).expand(n, 3, 4)
+        from_up, from_down = ex.halo(mine[:H].clone(), mine[n - H:].clone())
+        umax = ex.max(float(rank) + 0.5)
+        np.savez(os.path.join(outdir, f"halo{rank}.npz"), up=from_up.numpy(), down=from_down.numpy(), umax=umax)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_slab_halo_exchange_gloo(tmp_path, world):
+    # ghost planes of a z-slab from the periodic neighbours (with two ranks both
+    # neighbours are the same rank), and the maximum over the ranks
+    import numpy as np
+    pytest.importorskip("torch")
+    import torch.multiprocessing as mp
+    mp.spawn(_halo_worker, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    H, n, nz = 2, 5, 5 * world
+    for r in range(world):
+        d = np.load(tmp_path / f"halo{r}.npz")
+        up = [(r * n + n + k) % nz for k in range(H)]      # the first planes of the rank above
+        down = [(r * n - H + k) % nz for k in range(H)]    # the last planes of the rank below
+        assert np.array_equal(d["up"][:, 0, 0], up) and np.array_equal(d["down"][:, 0, 0], down)
+        assert float(d["umax"]) == world - 0.5
+
+
+def test_slab_halo_exchange_emulated():
+    import torch
+    sys.path.insert(0, REPO)
+    from cubismup_3d_b200 import slab
+    for G in (1, 2, 3):
+        sends = [(torch.full((1,), 10.0 * r), torch.full((1,), 10.0 * r + 1)) for r in range(G)]
+        recvs = slab.LocalExchange.halo_all(sends)
+        for r, (from_up, from_down) in enumerate(recvs):
+            assert float(from_up) == 10.0 * ((r + 1) % G)        # the send_down of the rank above
+            assert float(from_down) == 10.0 * ((r - 1) % G) + 1  # the send_up of the rank below
