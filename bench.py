@@ -566,7 +566,7 @@ def run_ours(args, rank: int, world: int, local_rank: int):
         if not args.no_oracle_parity and u_final is not None:
             par = {"oracle_steps": nsteps, "oracle_time": t_o, "gpu_time": st.time,
                    "rel_l2_velocity_vs_oracle": rel_l2_fields(u_final, vel_o),
-                   "bar": "north_star: <= 1e-6 relative L2 velocity (FP32-DC against the FP64 oracle)"}
+                   "bar": "<= 1e-6 relative L2 velocity (FP32-DC against the FP64 oracle)"}
             if fp64 is not None:
                 par["rel_l2_velocity_fp64_vs_oracle"] = rel_l2_fields(r64, vel_o)
             line["rel_l2_vs_oracle"] = par["rel_l2_velocity_vs_oracle"]
