@@ -2460,6 +2460,14 @@ int run_graph(cup_handle* H, int nsteps, int next_dt, bool* ran) {
     if (e0_ != cudaSuccess) return fail(H, CUP_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e0_)); \
   } while (0)
 
+// Entry points that need the whole grid (its z transform, obstacle or global
+// sums) refuse a z-slab handle (cup_config.z_halo) before they change anything.
+#define REQUIRE_WHOLE_GRID(H)                                                                          \
+  do {                                                                                                 \
+    if ((H)->cfg.z_halo)                                                                               \
+      return fail(H, CUP_ERR_STATE, "%s needs a whole grid (this handle holds a z-slab)", __func__); \
+  } while (0)
+
 extern "C" {
 
 int cup_create(const cup_config* cfg, cup_handle** out) {
@@ -2750,6 +2758,7 @@ int cup_global_to_blocks(const double* global, double* blocks, int nx, int ny, i
 
 int cup_add_sphere(cup_handle* H, const cup_sphere* s) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   reset_pressure_history(H);
   if (!s || !(s->radius > 0)) return fail(H, CUP_ERR_ARG, "sphere radius must be > 0");
   if (H->has_sphere) return fail(H, CUP_ERR_STATE, "only one obstacle is supported");
@@ -2843,6 +2852,7 @@ int cup_set_graphs(cup_handle* H, int on) {
 
 int cup_prepare_run(cup_handle* H, int nsteps, int* captured) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   if (captured) *captured = 0;
   if (nsteps < 0) return fail(H, CUP_ERR_ARG, "nsteps must be >= 0");
   if (!graph_ok(H)) return CUP_OK;
@@ -3042,6 +3052,7 @@ int cup_poisson_pass(cup_handle* H, double* buf, int pass) {
 
 int cup_poisson_solve(cup_handle* H, cup_solve_stats* stats) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   reset_pressure_history(H);
   int rc = do_poisson(H);
   if (rc) return rc;
@@ -3135,6 +3146,7 @@ static int fill_stats(cup_handle* H, cup_step_stats* st) {
 
 int cup_step(cup_handle* H, double dt, cup_step_stats* stats) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
   H->dt = dt;
   if (H->cfg.DLM > 0) H->lambda = H->cfg.DLM / dt;
@@ -3186,6 +3198,7 @@ static int check_adjoint_fields(cup_handle* H, const void* un, const void* vn, c
 int cup_adjoint_step(cup_handle* H, const void* un, const void* vn, const void* wn, double dt, void* lu, void* lv,
                      void* lw) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
   if (H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_adjoint_step: the handle has an obstacle (use cup_adjoint_step_obstacle)");
   if (H->forcing)
@@ -3201,6 +3214,7 @@ int cup_adjoint_step(cup_handle* H, const void* un, const void* vn, const void* 
 int cup_adjoint_step_obstacle(cup_handle* H, const void* un, const void* vn, const void* wn, double dt, void* lu,
                               void* lv, void* lw, const double w_force[3], double* g_chi, double* g_vel) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
   if (!H->has_sphere) return fail(H, CUP_ERR_ARG, "cup_adjoint_step_obstacle: the handle has no obstacle");
   if (H->sphere_moves)
@@ -3265,6 +3279,7 @@ int cup_set_velocity_raw(cup_handle* H, const void* u, const void* v, const void
 
 int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   if (nsteps < 0) return fail(H, CUP_ERR_ARG, "nsteps must be >= 0");
   int rc;
   if (!H->umax_fresh) {
@@ -3330,6 +3345,7 @@ int cup_run(cup_handle* H, int nsteps, cup_step_stats* stats) {
 
 int cup_poisson_solve_field(cup_handle* H, const double* rhs, double* p, int where) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   reset_pressure_history(H);
   if (!rhs || !p || !valid_where(where)) return fail(H, CUP_ERR_ARG, "bad poisson arguments");
   const cudaMemcpyKind in = where == CUP_WHERE_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
@@ -3345,6 +3361,7 @@ int cup_poisson_solve_field(cup_handle* H, const double* rhs, double* p, int whe
 
 int cup_diagnostics(cup_handle* H, double out[3]) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   if (!out) return fail(H, CUP_ERR_ARG, "null output");
   const int grid = std::min<size_t>(H->num_sms * 4, (H->n + 255) / 256);
   double* part = partial(H, P_DIAG);
@@ -3379,6 +3396,7 @@ int cup_diagnostics(cup_handle* H, double out[3]) {
 
 int cup_spectral_analysis(cup_handle* H, double stats[7], double* spectrum, int nbin) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   if (!stats) return fail(H, CUP_ERR_ARG, "null stats");
   const int N = std::max(H->nx, std::max(H->ny, H->nz));
   if (spectrum && nbin != N / 2 - 1) return fail(H, CUP_ERR_ARG, "spectrum needs max(N)/2 - 1 = %d bins", N / 2 - 1);
@@ -3415,6 +3433,7 @@ int cup_set_spectral_forcing(cup_handle* H, double turbKinEn_target, double enIn
 
 int cup_spectral_forcing(cup_handle* H, double dt, double stats[6]) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   if (!(dt > 0)) return fail(H, CUP_ERR_ARG, "dt must be > 0");
   reset_pressure_history(H);
   H->umax_fresh = false;
@@ -3465,6 +3484,7 @@ int cup_compute_forces(cup_handle* H, double out[27]) {
 
 int cup_compute_dissipation(cup_handle* H, double out[20]) {
   REQUIRE_H(H);
+  REQUIRE_WHOLE_GRID(H);
   if (!out) return fail(H, CUP_ERR_ARG, "null output");
   const int grid = std::min<size_t>(H->num_sms * 4, (H->n + 255) / 256);
   double* part = partial(H, P_DIAG);

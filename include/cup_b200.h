@@ -78,7 +78,9 @@ typedef struct cup_config {
                              and the handle has no z Fourier transform: the stencil operators
                              (cup_advect_diffuse, cup_pressure_rhs, cup_grad_correct, cup_max_velocity,
                              cup_calc_max_timestep) run on it, with the ghost planes filled by the caller and
-                             the Poisson solve done over the ranks (the z-slab decomposed solve) */
+                             the Poisson solve done over the ranks (the z-slab decomposed solve); the entry
+                             points that need the whole grid (steps and runs, Poisson solves, adjoint steps,
+                             obstacles, diagnostics and spectral sums) return CUP_ERR_STATE */
 } cup_config;
 
 /* One sphere obstacle (source/obstacles/Sphere.cpp, ObstacleArguments in

@@ -885,8 +885,13 @@ def test_slab_handle_has_no_z_transform():
     sd = make_sd((32, 32, 48), 1.0)
     sd.z_halo = 8
     sim = cup.Simulation(sd)
-    with pytest.raises(Exception):
-        sim.pressureSolver.solve()
+    u, v, w = random_velocity((32, 32, 48), 3, 0.5)
+    sim.set_velocity(u, v, w)
+    before = sim.velocity()
+    for call in (sim.pressureSolver.solve, lambda: sim.timestep(1e-3), lambda: sim.run_steps(2)):
+        with pytest.raises(Exception, match="whole grid"):
+            call()
+    assert all(np.array_equal(a, b) for a, b in zip(sim.velocity(), before))  # refused before any change
     sd2 = make_sd((32, 32, 48), 1.0, precision="fp32_dc")
     sd2.z_halo = 8
     with pytest.raises(ValueError):
