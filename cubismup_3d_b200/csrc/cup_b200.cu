@@ -1026,19 +1026,16 @@ template <int M, typename R, class Prod, class Cons>
 int launch_rows_M(cup_handle* H, const char* name, const Prod& prod, const Cons& cons, const int* skip) {
   constexpr int N = 2 * M, TPL = M / 8;
   constexpr bool PAD = FFTPlan<M>::nstages > 1;
-  // 256 threads per CTA (16 rows of 256-long lines)
+  // 256 threads per CTA (16 rows of 256-long lines; 8- and 4-row tiles measured no faster)
   const int lpc = 256 / TPL;
   const int nrows = H->ny * H->nz;
-  // the producer's reduction scratch
-  const size_t scratch = 32 * 20 * sizeof(double);
   const size_t smem = (size_t)lpc * N * sizeof(R) + (PAD ? (size_t)lpc * 2 * (M + M / 8) * sizeof(R) : 0) +
-                      FFTPlan<M>::rows_table_len() * sizeof(typename Cplx<R>::T) + 16 + scratch + 128;
+                      FFTPlan<M>::rows_table_len() * sizeof(typename Cplx<R>::T) + 128;
   auto kern = k_dht_rows<M, R, Prod, Cons>;
   int bpsm = 0;
   int rc = prepare_kernel(H, kern, smem, lpc * TPL, &bpsm);
   if (rc) return rc;
   const int grid = (nrows + lpc - 1) / lpc;
-  if (grid > kPartialCap / 20) return fail(H, CUP_ERR_ARG, "too many row tiles for the partial buffers");
   return launch_named(H, name, [&]() -> int {
     klaunch(H, kern, grid, lpc * TPL, smem, prod, cons, nrows, lpc, table<R>(H, 0), H->derr, skip);
     CKL();

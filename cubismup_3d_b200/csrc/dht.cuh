@@ -544,8 +544,8 @@ __device__ __forceinline__ void load_table(R2* dst, const R2* src, int n) {
 // ---------------------------------------------------------------------------
 // x pass: LPC consecutive rows of length N = 2M per CTA (rows are contiguous
 // in the [z][y][x] layout: row r is (y, z) = (r % ny, r / ny)). A producer
-// computes the rows in shared memory from other fields (and may reduce over
-// them), the rows are transformed, and a consumer stores them (one bulk store).
+// computes the rows in shared memory from other fields, the rows are
+// transformed, and a consumer stores them (one bulk store).
 
 // Consumer: rows stored to an array (one bulk store).
 template <typename R>
@@ -586,16 +586,12 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
   R* rows = reinterpret_cast<R*>(smem_raw);  // lpc * N
   R* padb = rows + (size_t)lpc * N;          // lpc * PPITCH
   R2* tw = reinterpret_cast<R2*>(padb + (PAD ? (size_t)lpc * PPITCH : 0));
-  double* scratch = reinterpret_cast<double*>(tw + TL + 1);  // 32 * 20 doubles (the producer's reductions)
   const int row0 = blockIdx.x * lpc;
   const int nr = min(lpc, nrows - row0);
   if (nr <= 0) return;
   const uint32_t bytes = (uint32_t)((size_t)nr * N * sizeof(R));
-  double acc[20];
-#pragma unroll
-  for (int i = 0; i < 20; ++i) acc[i] = 0.0;
   load_table(tw, tw_g, TL);
-  prod.fill(rows, row0, nr, N, acc);
+  prod.fill(rows, row0, nr, N);
   __syncthreads();
   const int l = threadIdx.x / TPL, t = threadIdx.x % TPL;
   const bool active = l < nr;
@@ -609,7 +605,6 @@ __global__ void __launch_bounds__(256) k_dht_rows(const Prod prod, const Cons co
     bulk_commit();
     bulk_wait_all();
   }
-  prod.finish(acc, scratch);
 }
 
 // Pipelined x pass: persistent CTAs walk tiles of lpc consecutive rows

@@ -197,7 +197,7 @@ struct RowsRhs {
   DtArg dt;
   double h;
   int nx, ny, nz;
-  __device__ void fill(double* rows, int row0, int nr, int N, double*) const {
+  __device__ void fill(double* rows, int row0, int nr, int N) const {
     const double fac = 0.5 * h * h / dt.get();
     for (int i = threadIdx.x; i < nr * N; i += blockDim.x) {
       const int l = i / N, x = i - l * N;
@@ -208,7 +208,6 @@ struct RowsRhs {
       rows[i] = fac * (uE - uW + vN - vS + wB - wF);
     }
   }
-  __device__ void finish(double*, double*) const {}
 };
 
 // Active box of the obstacle: cells [lo, lo+n) per dimension (global indices,
