@@ -950,8 +950,8 @@ int prepare_kernel(cup_handle* H, K kern, size_t smem, int threads, int* blocks_
   return CUP_OK;
 }
 
-// Launches a kernel on the handle's stream; with H->pdl (the default) as a
-// programmatic dependent launch: its CTAs may be scheduled while the previous
+// Launches a kernel on the handle's stream; with H->pdl (off unless CUP_PDL=1) as
+// a programmatic dependent launch: its CTAs may be scheduled while the previous
 // kernel of the stream finishes, and wait in pdl_entry() for that kernel's
 // completion before touching its data. A failure is left for CKL() to report.
 template <typename... KArgs, typename... Args>
@@ -1188,6 +1188,44 @@ int launch_cols(cup_handle* H, RIN* in, R* out, const int* skip) {
   return fail(H, CUP_ERR_ARG, "unsupported line length %d", N);
 }
 
+// Mixed-precision z pass of 256-long lines with a narrow input ring
+// (k_dht_z_mixed): W columns per tile, NBN FP32 input buffers and one FP64
+// buffer per CTA. Measured at 256^3: 58.2 us with W = 32, NBN = 1 (two CTAs
+// per SM), 64.2 with W = 16, NBN = 1 (four), 69.2 with W = 16, NBN = 2
+// (three), against 70.4 for the two-FP64-buffer ring of k_dht_cols_pipe.
+template <int W, int NBN>
+int launch_z_mixed(cup_handle* H, float* in, double* out, const int* skip) {
+  constexpr int M = 128, N = 2 * M;
+  using Pl = FFTPlan<M>;
+  if (H->cfg.z_halo)
+    return fail(H, CUP_ERR_STATE, "a z-slab handle has no z transform (the Poisson solve runs over the ranks)");
+  if (H->nz != N) return fail(H, CUP_ERR_ARG, "the narrow-ring z pass needs 256-long z lines");
+  if (H->nx % W) return fail(H, CUP_ERR_ARG, "nx must be a multiple of %d for this precision", W);
+  CUtensorMap map_in, map_out;
+  int rc = make_map(H, &map_in, in, tma_dtype<float>(), sizeof(float), W, 1, N);
+  if (!rc) rc = make_map(H, &map_out, out, tma_dtype<double>(), sizeof(double), W, 1, N);
+  if (rc) return rc;
+  constexpr int TN = Pl::table_len() - Pl::post_off();
+  const size_t smem = (size_t)N * W * sizeof(double) + (size_t)NBN * N * W * sizeof(float) +
+                      (size_t)TN * (sizeof(double2) + sizeof(float2)) + NBN * sizeof(uint64_t) +
+                      (M / 2 + 1) * sizeof(double) + 128;
+  auto kern = k_dht_z_mixed<W, NBN>;
+  const int threads = W * 8;
+  int bpsm = 0;
+  rc = prepare_kernel(H, kern, smem, threads, &bpsm);
+  if (rc) return rc;
+  const int ntx = H->nx / W;
+  const int ntiles = ntx * H->ny;
+  const int grid = std::min(ntiles, bpsm * H->num_sms);
+  SpectralParams sp{H->cosx, H->cosy, H->cosz, H->norm_factor, H->nx, H->spec_ny, H->nz, H->spec_y0};
+  return launch_named(H, "dht_z_solve_mixed", [&]() -> int {
+    klaunch(H, kern, grid, threads, smem, map_in, map_out, ntx, ntiles, table<double>(H, 2), table<float>(H, 2), sp,
+            H->derr, skip);
+    CKL();
+    return CUP_OK;
+  });
+}
+
 // p = H(f . H(work)) over the three axes, in place on `work`; the last x
 // pass writes to `out` (may equal work).
 // The y, z (+ divide + inverse) and y passes, in place on `work`.
@@ -1212,7 +1250,11 @@ int dc_correction_solve(cup_handle* H, double* p, const int* skip) {
   int rc;
   if ((rc = launch_rows_pipe<float>(H, "dht_x", H->work32, H->work32, skip))) return rc;
   if ((rc = launch_cols<float, 1, false>(H, H->work32, H->work32, skip))) return rc;
-  if ((rc = launch_cols<double, 2, true, float>(H, H->work32, H->work64, skip))) return rc;
+  if (H->nz == 256) {
+    if ((rc = launch_z_mixed<32, 1>(H, H->work32, H->work64, skip))) return rc;
+  } else if ((rc = launch_cols<double, 2, true, float>(H, H->work32, H->work64, skip))) {
+    return rc;
+  }
   if ((rc = launch_cols<double, 1, false>(H, H->work64, H->work64, skip))) return rc;
   return launch_rows_addp(H, "dht_x_update_p", H->work64, p, skip);
 }

@@ -972,4 +972,99 @@ __global__ void __launch_bounds__(W * (T8 ? 8 : M / 8)) k_dht_cols_pipe(const __
   }
 }
 
+// Mixed-precision z pass of the correction solve (256-long lines, the 8-thread
+// plan) with a narrow input ring: the FP32 input tiles (W columns by the whole
+// z line) arrive by TMA in NBN narrow buffers and each tile is transformed in
+// one FP64 buffer. Stage A of the FP32 forward transform reads the narrow tile
+// and writes into the lower half of the FP64 buffer, so once the forward
+// transform is done the narrow buffer takes the load of tile i + NBN while the
+// FP64 inverse runs; the FP64 buffer is reused once the store of the previous
+// tile has read it. Only the post-split and radix-16 twiddles of the 8-thread
+// plan are staged. At W = 32, NBN = 1 a CTA needs 101 KB of shared memory
+// (two CTAs per SM) and its tile rows are 128 B in FP32 and 256 B in FP64;
+// the ring of two FP64 buffers at W = 16 needed 70 KB (three CTAs per SM) for
+// 64-B and 128-B rows. Same arithmetic, in the same order, as
+// k_dht_cols_pipe<128, double, 2, true, W, NB, float, true>.
+template <int W, int NBN>
+__global__ void __launch_bounds__(W * 8) k_dht_z_mixed(const __grid_constant__ CUtensorMap map_in,
+                                                      const __grid_constant__ CUtensorMap map_out, int ntiles_x,
+                                                      int ntiles, const double2* tw_g, const float2* tw_in_g,
+                                                      SpectralParams sp, int* err, const int* skip) {
+  pdl_entry();
+  if (skip && *skip) return;
+  using Pl = FFTPlan<128>;
+  constexpr int M = 128, N = 2 * M;
+  constexpr int T0 = Pl::post_off(), TN = Pl::table_len() - Pl::post_off();  // staged part of the tables
+  constexpr uint32_t IN_BYTES = (uint32_t)(N * W * sizeof(float));
+  extern __shared__ __align__(128) unsigned char smem_dyn[];
+  unsigned char* smem_raw = smem_align128(smem_dyn);
+  double* wide = reinterpret_cast<double*>(smem_raw);         // [N][W]
+  float* narrow = reinterpret_cast<float*>(wide + N * W);      // [NBN][N][W]
+  double2* tws = reinterpret_cast<double2*>(narrow + NBN * N * W);
+  float2* tws_in = reinterpret_cast<float2*>(tws + TN);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(tws_in + TN);
+  double* czs = reinterpret_cast<double*>(bar + NBN);  // cos_z[0..M/2]
+  // the transforms index the tables from their start; entries below T0 are never read
+  const double2* tw = tws - T0;
+  const float2* tw_in = tws_in - T0;
+  const int tid = threadIdx.x;
+  const int my = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  if (tid == 0) {
+    for (int b = 0; b < NBN; ++b) mbar_init(&bar[b], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto coords = [&](int i, int& x0, int& y) {
+    const int t = blockIdx.x + i * gridDim.x;
+    x0 = (t % ntiles_x) * W;
+    y = t / ntiles_x;
+  };
+  auto issue = [&](int i) {
+    int x0, y;
+    coords(i, x0, y);
+    const int b = i % NBN;
+    mbar_arrive_expect_tx(&bar[b], IN_BYTES);
+    tma_load_3d(narrow + (size_t)b * N * W, &map_in, x0, y, 0, &bar[b]);
+  };
+  int issued = 0;
+  if (tid == 0)
+    for (; issued < min(NBN, my); ++issued) issue(issued);
+  load_table(tws, tw_g + T0, TN);
+  load_table(tws_in, tw_in_g + T0, TN);
+  for (int i = tid; i <= M / 2; i += blockDim.x) czs[i] = sp.cz[i];
+  __syncthreads();
+  const int l = tid % W, t = tid / W;
+  bool ok = true;
+  int done = 0;
+  for (int i = 0; i < my; ++i) {
+    // the store of tile i - 1 must have read the FP64 buffer before stage A writes it
+    if (tid == 0 && i > 0) bulk_wait_read<0>();
+    const int b = i % NBN;
+    ok = __syncthreads_and(ok && mbar_wait(&bar[b], (i / NBN) & 1, err));
+    if (!ok) break;
+    int x0, y;
+    coords(i, x0, y);
+    ColLines<float> An{narrow + (size_t)b * N * W, W};
+    ColLines<float> Lo{reinterpret_cast<float*>(wide), W};
+    ColLines<double> A{wide, W};
+    dht128_t8_to<float, true>(An, Lo, A, tw_in, l, t, true, z_column_factor<float>(sp, czs, x0 + l, y));
+    // every read of the narrow tile came before the barriers of the forward transform
+    if (tid == 0 && issued < my) issue(issued++);
+    dht128_t8_to<double>(A, A, A, tw, l, t, true, NoScale());
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      tma_store_3d(&map_out, x0, y, 0, wide);
+      bulk_commit();
+    }
+    done = i + 1;
+  }
+  if (tid == 0) {
+    bulk_wait_all();
+    // after a timed-out wait: bounded drain of the loads still in flight
+    if (!ok)
+      for (int r = done; r < issued; ++r) mbar_wait(&bar[r % NBN], (r / NBN) & 1, nullptr);
+  }
+}
+
 }  // namespace cup

@@ -651,6 +651,28 @@ def test_wide_grid_steps_vs_oracle(oracle, scheme, precision):
             assert rel_l2(a, b) < tol
 
 
+def test_fp32_dc_256_z_lines_vs_oracle(oracle):
+    # 256-long z lines take the mixed z pass with the narrow input ring
+    # (k_dht_z_mixed); 2 steps against the FP64 oracle at the FP32-DC bar
+    cells = (64, 32, 256)
+    nx, ny, nz = cells
+    sim = make_sim(cells, 2 * np.pi, nu=1e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0, scheme="upwind3_rk2",
+                   precision="fp32_dc")
+    orc = oracle.OracleSim(nx, ny, nz, 2 * np.pi, nu=1e-3, CFL=0.3, rampup=0, DLM=0.0, lambda_=1.0,
+                           scheme="upwind3_rk2")
+    from cubismup_3d_b200 import initial_conditions as ic
+    u, v, w = ic.random_solenoidal(cells, 7, lambda k: k ** 4 * np.exp(-2 * (k / 4) ** 2), rms=1.0)
+    sim.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    for s in range(2):
+        dt = orc.calc_max_timestep()
+        st = sim.timestep(dt)
+        orc.timestep(dt)
+        assert st.n_unconverged == 0
+        for a, b in zip(sim.velocity(), orc.velocity()):
+            assert rel_l2(a, b) < 1e-6
+
+
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32_dc", 1e-9)])
 def test_poisson_buffer_contract_vs_oracle(oracle, precision, tol):
     # PoissonSolver's public buffer (source/poisson/PoissonSolver.h:51-122): the
