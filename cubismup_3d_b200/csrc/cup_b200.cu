@@ -2404,7 +2404,7 @@ void set_step_state(cup_handle* H, const cup_handle::StepState& s) {
 }
 
 bool same_state(const cup_handle::StepState& a, const cup_handle::StepState& b) {
-  for (int i = 0; i < 9; ++i)
+  for (size_t i = 0; i < sizeof(a.f) / sizeof(a.f[0]); ++i)
     if (a.f[i] != b.f[i]) return false;
   return a.p_valid == b.p_valid && a.n_grad_partials == b.n_grad_partials && a.grad_stride == b.grad_stride &&
          a.grad_max_off == b.grad_max_off && a.grad_ke_off == b.grad_ke_off && a.pred_ready == b.pred_ready;

@@ -424,6 +424,22 @@ __global__ void k_rhs_obstacle_correct(double* rhs, const T* chi, Box box, int n
   }
 }
 
+// b = KernelPressureRHS(u*) (source/operators/PressureRHS.cpp:51-76) as the
+// FP32 defect-correction passes recompute it: the differences of the stored
+// velocities and their sum in the storage type T, then one conversion to FP64
+// and the scaling (one conversion per cell instead of six; T rounding of the
+// differences is far below the storage rounding of u* itself). Every pass that
+// recomputes b and the obstacle's box pass use these two functions, so b is
+// the same bits wherever it is formed.
+template <typename T>
+__device__ __forceinline__ T div_xy(T uxp, T uxm, T vyp, T vym) {
+  return (uxp - uxm) + (vyp - vym);
+}
+template <typename T>
+__device__ __forceinline__ double div_b(double facB, T dxy, T wzp, T wzm) {
+  return facB * (double)(dxy + (wzp - wzm));
+}
+
 // The first half of the RHS obstacle terms on the box, for passes that
 // recompute b0 = KernelPressureRHS(u*) (source/operators/PressureRHS.cpp:51-76)
 // themselves: b0 at each box cell (in the operation order of the z-queue
@@ -445,8 +461,7 @@ __global__ void k_box_rhs_obstacle(const T* u, const T* v, const T* w, const T* 
     const size_t oxp = gidx(wrapi(x + 1, nx), y, z, nx, ny), oxm = gidx(wrapi(x - 1, nx), y, z, nx, ny);
     const size_t oyp = gidx(x, wrapi(y + 1, ny), z, nx, ny), oym = gidx(x, wrapi(y - 1, ny), z, nx, ny);
     const size_t ozp = gidx(x, y, wrapi(z + 1, nz), nx, ny), ozm = gidx(x, y, wrapi(z - 1, nz), nx, ny);
-    const double partD = facB * (((double)u[oxp] - (double)u[oxm]) + ((double)v[oyp] - (double)v[oym]));
-    const double b0 = partD + facB * ((double)w[ozp] - (double)w[ozm]);
+    const double b0 = div_b<T>(facB, div_xy<T>(u[oxp], u[oxm], v[oyp], v[oym]), w[ozp], w[ozm]);
     const double X = chi[gidx(x, y, z, nx, ny)];
     const double dXx = (double)chi[oxp] - (double)chi[oxm];
     const double dXy = (double)chi[oyp] - (double)chi[oym];

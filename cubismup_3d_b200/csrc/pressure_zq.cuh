@@ -1,6 +1,7 @@
 // Pressure-stage kernels of the FP32 defect-correction step, register z-queue
 // form; every pass recomputes b = KernelPressureRHS(u*)
-// (source/operators/PressureRHS.cpp:51-76) from u* (bit-identical in each):
+// (source/operators/PressureRHS.cpp:51-76) from u* (div_xy / div_b:
+// bit-identical in each):
 //   RHS_RES    the first FP64 residual r = b - h/4 L_2h p of the warm start,
 //              r in FP32 for the FFT solve.
 //   RES        r = b - h/4 L_2h p before a further correction solve, minus the
@@ -223,7 +224,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
   // x/y parts of the planes in flight (G of them): Laplacian, divergence and
   // (GRAD_CHECK) the gradient of p and the u*, v* centre values
   double partL[G][CPT];
-  double partD[G][CPT];          // x/y part of the divergence (b from u*)
+  T partD[G][CPT];               // x/y part of the divergence (b from u*: div_xy, div_b)
   double partB[BD ? G : 1][CPT];  // BD: the obstacle terms of the output cell, loaded two planes ahead
   double gA[G][CPT], gB[G][CPT];  // x- and y-gradient of p (GRAD_CHECK)
   double pc[CPT][2], rc[CPT][2];  // parity-class sums of p and r by z parity
@@ -248,7 +249,8 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
   for (int d = 0; d < G; ++d)
 #pragma unroll
     for (int i = 0; i < CPT; ++i) {
-      partL[d][i] = partD[d][i] = gA[d][i] = gB[d][i] = 0.0;
+      partL[d][i] = gA[d][i] = gB[d][i] = 0.0;
+      partD[d][i] = (T)0;
       if constexpr (BD) partB[d][i] = 0.0;
     }
 #pragma unroll
@@ -299,7 +301,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
               const double lap = partL[PS][i] + (pq[QP2][i] + pq[QM2][i] - 2 * p0);
               pc[i][zp] += p0;
               // b from u* (x/y part on arrival, z part here), plus the obstacle terms on the box
-              double b = partD[PS][i] + facB * ((double)wq[QP1][i] - (double)wq[QM1][i]);
+              double b = div_b<T>(facB, partD[PS][i], wq[QP1][i], wq[QM1][i]);
               if constexpr (BD) b += partB[PS][i];
               if constexpr (MODE == PZQ_RHS_RES) {
                 const double r = b - cL * lap;
@@ -353,8 +355,7 @@ __global__ void __launch_bounds__(512) k_pres_zq(const __grid_constant__ PzqMaps
               {
                 const T* Urow = reinterpret_cast<const T*>(sl + Slot::u_off(nx)) + cy[i] * nx;
                 const T* Vc = reinterpret_cast<const T*>(sl + Slot::v_off(nx)) + (cy[i] + 1) * nx;  // row of v*
-                partD[PS][i] = facB * (((double)Urow[xp1[i]] - (double)Urow[xm1[i]]) +
-                                       ((double)Vc[nx + x] - (double)Vc[x - nx]));
+                partD[PS][i] = div_xy<T>(Urow[xp1[i]], Urow[xm1[i]], Vc[nx + x], Vc[x - nx]);
               }
               if constexpr (BD) {
                 // the box's b2 - b0 of output cell (x, y, z0 + j - G), used two planes later
