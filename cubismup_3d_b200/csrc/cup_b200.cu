@@ -1138,7 +1138,8 @@ int launch_cols_M(cup_handle* H, RIN* in, R* out, const int* skip) {
   // W x-columns per tile (FP32: 128-B rows of a tile, FP64: 128 B), NB = 3 tile buffers
   // 256-long lines: the 8-thread plan (radix 16, then radix 8 fused with the
   // split), also for the mixed-precision z pass (the 16-thread plan measured
-  // 89 against 75 us there at 256^3)
+  // 89 against 75 us there at 256^3; that pass now runs k_dht_z_mixed for
+  // 256-long lines, this kernel for shorter ones)
   constexpr bool T8 = M == 128;
   // (a 3-deep ring for the mixed z pass, 2 CTAs per SM: 85 against 70 us)
   constexpr int N = 2 * M, TPL = T8 ? 8 : M / 8, NB = T8 ? 2 : 3;
@@ -1392,8 +1393,9 @@ int launch_advect_f2(cup_handle* H, const char* name, void* const* in, void* con
 
 // FP32 upwind3 stages: packed FP32x2 kernels (shared by the forward step and
 // the adjoint's stage recompute, so both see the same u1). Tile height, ring
-// depth and pairs per thread measured best at 256^3: stage 1 126 us
-// (TY 8, NS 3, 2 pairs), stage 2 152 us (TY 4, NS 3, 1 pair).
+// depth and pairs per thread as measured best at 256^3: stage 1 (TY 8, NS 4,
+// 2 pairs, 8-plane items) about 100 us, stage 2 (TY 4, NS 4, 1 pair, 16-plane
+// items) about 129 us; rings of 6 and 5 slots measured the same.
 // Grids of nx 64, 128 or 256 with nz >= ZC take the compile-time-size
 // kernels; other shapes the same kernel with runtime sizes.
 template <bool STAGE2, int TY, int NS, int PPT, int ZC>
@@ -1424,8 +1426,9 @@ int do_advect_diffuse(cup_handle* H, DtArg dt) {
   int rc;
   void* uvw[3] = {H->u, H->v, H->w};
   void* tmp[3] = {H->tu, H->tv, H->tw};
-  // tile height TY, ring depth NS, cells per thread CPT: measured best at 256^3
-  // (FP64: 143 / 231 / 299 us; FP32: 113 / 176 / 206 us for ref / stage 1 / stage 2)
+  // tile height TY, ring depth NS, cells per thread CPT: the shapes measured
+  // best at 256^3 for each scheme and precision (the FP32 upwind3 stages run
+  // the packed FP32x2 kernels)
   if (H->cfg.scheme == CUP_SCHEME_REF) {
     if constexpr (F32) rc = launch_advect<T, 0, 8, 5, 4>(H, "advect_diffuse_ref", uvw, uvw, tmp, dt);
     else rc = launch_advect<T, 0, 4, 5, 2>(H, "advect_diffuse_ref", uvw, uvw, tmp, dt);
