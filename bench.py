@@ -469,7 +469,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
     e2e = world * n ** 3 * sim_e2e_steps / (ems * 1e-3)
     field_bytes = 3 * n ** 3 * 8
     h2d = (field_bytes + sim_e2e_steps * 8) / sim_e2e_steps
-    d2h = (field_bytes + sim_e2e_steps * (8 + 256)) / sim_e2e_steps
+    # per step one read of the device state (464 B) by timestep: its stats and the
+    # next step's dt, which calcMaxTimestep then returns without another read
+    d2h = (field_bytes + sim_e2e_steps * 464) / sim_e2e_steps
 
     # ---- discrete adjoint against forward (same handle, fixed dt) ----
     adj = adjoint_cost(torch, sim, stream) if not args.no_adjoint else None
@@ -534,8 +536,9 @@ def run_ours(args, rank: int, world: int, local_rank: int):
                            "GBps": k[3]} for k in kern},
         "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": sim_e2e_steps,
-                "note": "one FP64 velocity upload and download per run (3 x %d MB each way) and per step the dt "
-                        "and the step stats read back; the transfers weigh less in longer runs"
+                "note": "one FP64 velocity upload and download per run (3 x %d MB each way) and per step the "
+                        "step's device state read back (its stats and the next dt); the transfers weigh less "
+                        "in longer runs"
                         % (n ** 3 * 8 // 2 ** 20)},
         "graphs_captured_before_timing": graph_ready,
         "gpu_launches": launches,

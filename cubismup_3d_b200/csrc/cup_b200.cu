@@ -826,6 +826,12 @@ struct cup_handle {
   // step, the three FP32-DC pressure levels every step); the graph is tied to
   // the pointer tuple it was captured with
   bool use_graphs = true;
+  // calcMaxTimestep right after timestep: cup_step's stats read-back brings
+  // the next step's CFL dt (computed on the device at the end of the step) to
+  // the host; dt_next_call is the API call count at that read, and the cached
+  // dt is used only by the next API call (api_calls counts every entry point)
+  unsigned long long api_calls = 0, dt_next_call = 0;
+  double dt_next = 0, lambda_next = 0;
   // kernels launched as programmatic dependent launches: off by default (the
   // captured 6-step graphs measured 34 us per step slower at 256^3 with it);
   // CUP_PDL=1 in the environment at cup_create turns it on
@@ -2498,6 +2504,7 @@ int run_graph(cup_handle* H, int nsteps, int next_dt, bool* ran) {
 #define REQUIRE_H(H)                        \
   do {                                      \
     if (!(H)) return CUP_ERR_ARG;           \
+    ++(H)->api_calls;                       \
     cudaError_t e0_ = cudaSetDevice((H)->dev); \
     if (e0_ != cudaSuccess) return fail(H, CUP_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e0_)); \
   } while (0)
@@ -3003,6 +3010,14 @@ int cup_max_velocity(cup_handle* H, double* umax) {
 int cup_calc_max_timestep(cup_handle* H, double* dt) {
   REQUIRE_H(H);
   int rc;
+  if (H->dt_next_call && H->api_calls == H->dt_next_call + 1 && H->umax_fresh) {
+    // nothing happened since timestep read back the dt its step computed
+    // (the same calc_dt_device on the same max |u| and step counter)
+    H->dt = H->dt_next;
+    if (H->cfg.DLM > 0) H->lambda = H->lambda_next;
+    if (dt) *dt = H->dt;
+    return CUP_OK;
+  }
   if (!H->umax_fresh) {
     if ((rc = DISPATCH_T(H, do_max_u))) return rc;
     H->umax_fresh = true;
@@ -3202,18 +3217,28 @@ int cup_step(cup_handle* H, double dt, cup_step_stats* stats) {
     if (rc_) return rc_;
   }
   // one step from a captured graph in the steady state (it reads dt from the
-  // device state set above), else launched
+  // device state set above), else launched; either way the step ends by
+  // computing the next step's CFL dt on the device, which the stats read-back
+  // brings to the host for a following calcMaxTimestep
   bool ran = false;
-  int rc = graph_ok(H) ? run_graph(H, 1, 0, &ran) : CUP_OK;
+  int rc = graph_ok(H) ? run_graph(H, 1, 1, &ran) : CUP_OK;
   if (rc) return rc;
-  if (!ran) rc = DISPATCH_T(H, do_step, DtArg{dt, nullptr}, (const double*)&H->dstate->lambda, 1);
+  if (!ran) rc = DISPATCH_T(H, do_step, DtArg{dt, nullptr}, (const double*)&H->dstate->lambda, 1, 1);
   if (rc) return rc;
   if (H->has_sphere && H->sphere_free && (rc = read_sphere_motion(H))) return rc;
   H->step += 1;
   H->time += dt;
   H->umax_fresh = true;
-  if (stats) return fill_stats(H, stats);
-  return CUP_OK;
+  H->dt_next_call = 0;
+  if (!stats) return CUP_OK;
+  rc = fill_stats(H, stats);
+  stats->dt = dt;  // this step's dt (the device state now holds the next one)
+  if (rc == CUP_OK && H->hstate->step == H->step) {
+    H->dt_next = H->hstate->dt;
+    H->lambda_next = H->hstate->lambda;
+    H->dt_next_call = H->api_calls;
+  }
+  return rc;
 }
 
 static int alloc_adjoint(cup_handle* H) {

@@ -196,7 +196,11 @@ int cup_get_obstacle_state(struct cup_handle* h, double force[3], double torque[
 int cup_set_clock(struct cup_handle* h, int step, double time);
 /* findMaxU (source/operators/ProcessHelpers.h:74-99) */
 int cup_max_velocity(struct cup_handle* h, double* umax);
-/* Simulation::calcMaxTimestep (source/Simulation.cpp:403-424) */
+/* Simulation::calcMaxTimestep (source/Simulation.cpp:403-424). Called right
+ * after cup_step with stats (no other call between), it returns the dt that
+ * step computed on the device from the same max |u| and step counter, which
+ * the stats read-back already brought to the host: no device work and no
+ * synchronisation. */
 int cup_calc_max_timestep(struct cup_handle* h, double* dt);
 /* AdvectionDiffusion::operator() (source/operators/AdvectionDiffusion.cpp:402-428) */
 int cup_advect_diffuse(struct cup_handle* h, double dt);
@@ -245,7 +249,9 @@ int cup_pressure_projection(struct cup_handle* h, double dt, cup_solve_stats* st
 /* Penalization::operator() (source/operators/Penalization.cpp:129-156) */
 int cup_penalize(struct cup_handle* h, double dt, double force_torque[6]);
 /* Simulation::timestep (source/Simulation.cpp:593-623): the hot-path pipeline with
- * fused kernels. stats may be NULL (then no host synchronisation happens). */
+ * fused kernels. stats may be NULL (then no host synchronisation happens);
+ * stats->dt is this step's dt. The step ends by computing the next step's CFL
+ * dt on the device (read back with the stats for cup_calc_max_timestep). */
 int cup_step(struct cup_handle* h, double dt, cup_step_stats* stats);
 /* Simulation::run (source/Simulation.cpp:582-591) for nsteps: calcMaxTimestep + timestep,
  * with dt computed on the device (no host round trip per step). */

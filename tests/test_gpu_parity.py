@@ -525,6 +525,32 @@ def test_calc_max_timestep_rampup_and_dlm(oracle):
     assert sim.calcMaxTimestep() == pytest.approx(orc.calc_max_timestep(), rel=1e-14)
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp32_dc"])
+def test_calc_max_timestep_after_timestep_matches_recomputed(oracle, precision):
+    # calcMaxTimestep right after timestep returns the dt the step computed on
+    # the device; with any call in between it recomputes it (k_calc_dt). Both
+    # must give the same bits through the CFL ramp-up, with DLM on, and match
+    # the oracle's calcMaxTimestep along the trajectory.
+    n = 32
+    kw = dict(nu=0.01, CFL=0.5, rampup=4, DLM=1.0, lambda_=1.0)
+    fast = make_sim((n, n, n), 1.0, precision=precision, **kw)
+    slow = make_sim((n, n, n), 1.0, precision=precision, **kw)
+    orc = oracle.OracleSim(n, n, n, 1.0, **kw)
+    u, v, w = random_velocity((n, n, n), 3)
+    for s in (fast, slow):
+        s.set_velocity(u, v, w)
+    orc.set_velocity(u, v, w)
+    for step in range(7):
+        dt_f = fast.calcMaxTimestep()
+        slow.sync()  # any API call in between: the recomputing path
+        dt_s = slow.calcMaxTimestep()
+        assert dt_f == dt_s, (step, dt_f, dt_s)
+        assert dt_f == pytest.approx(orc.calc_max_timestep(), rel=1e-5 if precision == "fp32_dc" else 1e-13)
+        st_f, st_s = fast.timestep(dt_f), slow.timestep(dt_s)
+        assert st_f.dt == dt_f and st_s.dt == dt_s
+        orc.timestep(dt_f)
+
+
 def test_invalid_configurations_are_rejected():
     import cubismup_3d_b200 as cup
     with pytest.raises(Exception):
